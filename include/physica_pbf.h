@@ -1,0 +1,270 @@
+/*
+ * physica_pbf.h -- C ABI of the B200 Position Based Fluids solver.
+ *
+ * Drop-in boundary for the PBF substep of Xayah-Graphics/physica's
+ * fluids/liquid/particle module.  Every entry point mirrors one member of the
+ * reference's C++23 solver interface (pbf/pbf.ixx:14-141, domain/domain.ixx:12-165);
+ * the reference file:line it replaces is given beside each declaration.
+ *
+ * Conventions
+ *  - All field pointers are DEVICE pointers, structure-of-arrays x/y/z, `particle_count`
+ *    elements each, owned by the caller (the reference's State/Parameters/adjoint structs
+ *    own them as cuda::device_buffer, domain/domain.cpp:35-57).  The solver never frees them.
+ *  - Every call is asynchronous on the solver's stream, like the reference
+ *    (domain/domain.ixx:313); the only synchronising calls are pbf_create,
+ *    pbf_synchronize and the *_host entry points.
+ *  - Every call returns a pbf_status and never throws or aborts.  The reference's
+ *    launchers return void and check nothing (pbf/kernels.h:12-46); its constructors
+ *    throw from CCCL.  Here the failing call returns a non-zero status and
+ *    pbf_last_error() gives a message for the calling thread.
+ *  - A solver, its caches and its batches are not thread-safe; use one host thread each
+ *    (the reference solver is non-copyable, non-movable, pbf/pbf.ixx:74-77).
+ *  - vjp_step ACCUMULATES into previous_state_adjoint, control_adjoint and
+ *    parameter_adjoint; zero them first (pbf/pbf.cpp:143-160 zero-fills at allocation).
+ */
+#ifndef PHYSICA_PBF_H
+#define PHYSICA_PBF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define PHYSICA_PBF_ABI_VERSION 1
+
+typedef enum {
+    PBF_SUCCESS = 0,
+    PBF_ERROR_INVALID_ARGUMENT = 1,
+    PBF_ERROR_OUT_OF_MEMORY = 2,
+    PBF_ERROR_CUDA = 3,
+    PBF_ERROR_NOT_DIFFERENTIABLE = 4,   /* adjoint/tangent call on a forward-mode solver */
+    PBF_ERROR_UNSUPPORTED = 5,
+    PBF_ERROR_DEVICE_TIMEOUT = 6,       /* a bounded device-side wait gave up */
+    PBF_ERROR_CAPACITY = 7              /* a size exceeds a documented maximum */
+} pbf_status;
+
+/* domain/domain.ixx:231-234 ExecutionMode */
+typedef enum { PBF_EXECUTION_FORWARD = 0, PBF_EXECUTION_DIFFERENTIABLE = 1 } pbf_execution_mode;
+
+/* domain/domain.ixx:202-206 Vector3 */
+typedef struct { float x, y, z; } pbf_vector3;
+
+/* domain/domain.ixx:208-213 BoxBoundary */
+typedef struct {
+    pbf_vector3 minimum;
+    pbf_vector3 maximum;
+    pbf_vector3 velocity;
+    uint32_t no_slip;                    /* accepted and stored; the PBF kernels do not read it */
+} pbf_box_boundary;
+
+/* domain/domain.ixx:215-219 BoundaryParticle */
+typedef struct {
+    pbf_vector3 position;
+    pbf_vector3 velocity;
+    float volume;
+} pbf_boundary_particle;
+
+/* domain/domain.ixx:221-229 DomainConfiguration */
+typedef struct {
+    uint32_t particle_count;
+    float time_step;
+    float support_radius;
+    float particle_radius;
+    pbf_vector3 gravity;
+    pbf_box_boundary boundary;
+    const pbf_boundary_particle* boundary_particles;   /* host array, copied at creation */
+    uint32_t boundary_particle_count;
+} pbf_domain_configuration;
+
+/* pbf/pbf.ixx:15-18 PBF::Configuration */
+typedef struct {
+    uint32_t pressure_iterations;        /* reference default 5 */
+    uint32_t checkpoint_interval;        /* reference default 2 */
+} pbf_configuration;
+
+/* domain/domain.ixx:244-254 VectorField / VectorAdjointField (device SoA) */
+typedef struct { float* x; float* y; float* z; } pbf_vector_field;
+typedef struct { double* x; double* y; double* z; } pbf_vector_adjoint_field;
+
+/* domain/domain.ixx:256-260 ParticleState (PBF::State, pbf/pbf.ixx:20) */
+typedef struct {
+    pbf_vector_field positions;
+    pbf_vector_field velocities;
+    uint64_t step_index;
+} pbf_particle_state;
+
+/* domain/domain.ixx:262-273 Control / ControlTangent */
+typedef struct { pbf_vector_field external_accelerations; } pbf_control;
+
+/* domain/domain.ixx:266-269 ParticleStateTangent (PBF::StateTangent, pbf/pbf.ixx:21) */
+typedef struct { pbf_vector_field positions; pbf_vector_field velocities; } pbf_particle_state_tangent;
+
+/* domain/domain.ixx:275-282 ParticleStateAdjoint / ControlAdjoint */
+typedef struct { pbf_vector_adjoint_field positions; pbf_vector_adjoint_field velocities; } pbf_particle_state_adjoint;
+typedef struct { pbf_vector_adjoint_field external_accelerations; } pbf_control_adjoint;
+
+/* pbf/pbf.ixx:24-32 PBF::Parameters (particles = domain/domain.ixx:284-289) */
+typedef struct {
+    const float* masses;
+    const float* rest_densities;
+    const float* viscosities;            /* unused by PBF, as in the reference */
+    const float* surface_tensions;       /* unused by PBF, as in the reference */
+    const float* relaxation;
+    const float* artificial_pressure_strength;
+    const float* artificial_pressure_exponent;
+    const float* artificial_pressure_radius;
+    const float* xsph_viscosity;
+    const float* vorticity_confinement;
+} pbf_parameters;
+
+/* pbf/pbf.ixx:34-42 PBF::ParameterTangent (same layout, tangents) */
+typedef pbf_parameters pbf_parameter_tangent;
+
+/* pbf/pbf.ixx:44-52 PBF::ParameterAdjoint (FP64, accumulated) */
+typedef struct {
+    double* masses;
+    double* rest_densities;
+    double* viscosities;
+    double* surface_tensions;
+    double* relaxation;
+    double* artificial_pressure_strength;
+    double* artificial_pressure_exponent;
+    double* artificial_pressure_radius;
+    double* xsph_viscosity;
+    double* vorticity_confinement;
+} pbf_parameter_adjoint;
+
+/* Host-memory state for the *_host entry points (pinned or pageable). */
+typedef struct {
+    float* positions[3];
+    float* velocities[3];
+    uint64_t step_index;
+} pbf_host_state;
+
+typedef struct pbf_solver pbf_solver;          /* PBF (pbf/pbf.ixx:14-141) */
+typedef struct pbf_step_cache pbf_step_cache;  /* PBF::StepCache (pbf/pbf.ixx:54-70) */
+typedef struct pbf_batch pbf_batch;            /* many independent scenes in one launch sequence (no reference counterpart) */
+
+/* Fields of a step cache that pbf_step_cache_read copies out, in ORIGINAL particle order
+ * unless stated otherwise.  Each maps to a StepCache / Neighborhood member. */
+typedef enum {
+    PBF_CACHE_SORTED_PARTICLE_INDICES = 0, /* uint32[N]   neighborhood/neighborhood.ixx:323 */
+    PBF_CACHE_CELL_OFFSETS = 1,            /* uint32[C+1] neighborhood/neighborhood.ixx:324 */
+    PBF_CACHE_SORTED_KEYS = 2,             /* uint64[N]   neighborhood/neighborhood.ixx:322 */
+    PBF_CACHE_PREDICTED_POSITIONS = 3,     /* float[3N]   pbf/pbf.ixx:61 (x block, y block, z block) */
+    PBF_CACHE_CORRECTED_POSITIONS = 4,     /* float[3N]   pbf/pbf.ixx:62 */
+    PBF_CACHE_RECONSTRUCTED_VELOCITIES = 5,/* float[3N]   pbf/pbf.ixx:64 */
+    PBF_CACHE_VORTICITIES = 6,             /* float[3N]   pbf/pbf.ixx:65 */
+    PBF_CACHE_VORTICITY_MAGNITUDES = 7,    /* float[N]    pbf/pbf.ixx:66 */
+    PBF_CACHE_VORTICITY_NORMALS = 8,       /* float[3N]   pbf/pbf.ixx:67 */
+    PBF_CACHE_VORTICITY_NORMALIZERS = 9,   /* float[N]    pbf/pbf.ixx:68 */
+    PBF_CACHE_CONFINED_VELOCITIES = 10,    /* float[3N]   pbf/pbf.ixx:69 */
+    PBF_CACHE_FIRST_DENSITIES = 11,        /* float[N]    densities of Jacobi iteration 0 (pbf.cpp:175) */
+    PBF_CACHE_FIRST_LAMBDAS = 12,          /* float[N]    lambdas of Jacobi iteration 0 (pbf.cpp:176) */
+    PBF_CACHE_NEIGHBOR_COUNTS = 13,        /* uint32[N]   poly6 in-radius neighbours (self excluded) at iteration 0 */
+    PBF_CACHE_GRID_RESOLUTION = 14         /* uint32[3]   neighborhood/neighborhood.ixx:328 (host memory) */
+} pbf_cache_field;
+
+/* Per-iteration fields of a step cache (the reference's StepCache::IterationCheckpoint positions and
+ * the IterationPrimal members, pbf/pbf.ixx:55-58, 98-105), ORIGINAL particle order.  Positions exist for
+ * iterations 0..K in every mode (0 = predicted, K = corrected); the others for 0..K-1 and only in
+ * PBF_EXECUTION_DIFFERENTIABLE mode, where every iteration is recorded. */
+typedef enum {
+    PBF_ITERATION_POSITIONS = 0,        /* float[3N] */
+    PBF_ITERATION_DENSITIES = 1,        /* float[N]  */
+    PBF_ITERATION_LAMBDAS = 2,          /* float[N]  */
+    PBF_ITERATION_GRADIENT_SUMS = 3,    /* float[3N] */
+    PBF_ITERATION_DENOMINATORS = 4,     /* float[N]  */
+    PBF_ITERATION_COLLISION_MASKS = 5   /* uint32[N] */
+} pbf_iteration_field;
+
+/* ---- solver lifetime: PBF::PBF (pbf/pbf.cpp:39-72) and the implicit destructor ---- */
+int pbf_create(const pbf_domain_configuration* domain, const pbf_configuration* configuration,
+               pbf_execution_mode mode, void* cuda_stream, pbf_solver** solver);
+int pbf_destroy(pbf_solver* solver);
+
+/* ---- PBF::allocate_step_cache (pbf/pbf.cpp:108-125) ---- */
+int pbf_allocate_step_cache(pbf_solver* solver, pbf_step_cache** cache);
+int pbf_free_step_cache(pbf_step_cache* cache);
+
+/* ---- PBF::forward_step (pbf/pbf.cpp:167-191) ---- */
+int pbf_forward_step(pbf_solver* solver, const pbf_particle_state* state, const pbf_control* control,
+                     const pbf_parameters* parameters, pbf_particle_state* next_state, pbf_step_cache* cache);
+
+/* ---- PBF::jvp_step (pbf/pbf.cpp:193-215) ---- */
+int pbf_jvp_step(pbf_solver* solver, const pbf_particle_state* state, const pbf_control* control,
+                 const pbf_parameters* parameters, const pbf_particle_state* next_state, const pbf_step_cache* cache,
+                 const pbf_particle_state_tangent* state_tangent, const pbf_control* control_tangent,
+                 const pbf_parameter_tangent* parameter_tangent, pbf_particle_state_tangent* next_state_tangent);
+
+/* ---- PBF::vjp_step (pbf/pbf.cpp:217-258) ---- */
+int pbf_vjp_step(pbf_solver* solver, const pbf_particle_state* state, const pbf_control* control,
+                 const pbf_parameters* parameters, const pbf_particle_state* next_state, const pbf_step_cache* cache,
+                 const pbf_particle_state_adjoint* next_state_adjoint, pbf_particle_state_adjoint* previous_state_adjoint,
+                 pbf_control_adjoint* control_adjoint, pbf_parameter_adjoint* parameter_adjoint);
+
+/* ---- PBF::copy_state / copy_state_adjoint / accumulate_state_adjoint (pbf/pbf.cpp:162-165,
+ *      domain/domain.cpp:129-199) ---- */
+int pbf_copy_state(pbf_solver* solver, const pbf_particle_state* source, pbf_particle_state* destination);
+int pbf_copy_state_adjoint(pbf_solver* solver, const pbf_particle_state_adjoint* source,
+                           pbf_particle_state_adjoint* destination);
+int pbf_accumulate_state_adjoint(pbf_solver* solver, const pbf_particle_state_adjoint* source,
+                                 pbf_particle_state_adjoint* destination);
+
+/* ---- forward_step over host buffers: copies in, steps, copies out and waits.  No reference
+ *      counterpart; it is the call a C caller without device memory makes (the reference example
+ *      uploads with cuda::copy_bytes, examples/fluids/liquid/pbf-dam-break/simulation.ixx:97-105). ---- */
+int pbf_forward_step_host(pbf_solver* solver, const pbf_host_state* state, const pbf_control* control,
+                          const pbf_parameters* parameters, pbf_host_state* next_state, pbf_step_cache* cache);
+
+/* ---- inspection of a step cache (copies to device memory, or host memory for the grid
+ *      resolution).  `bytes` is the capacity of `destination`. ---- */
+int pbf_step_cache_read(pbf_solver* solver, const pbf_step_cache* cache, pbf_cache_field field,
+                        void* destination, size_t bytes);
+int pbf_step_cache_read_iteration(pbf_solver* solver, const pbf_step_cache* cache, pbf_iteration_field field,
+                                  uint32_t iteration, void* destination, size_t bytes);
+int pbf_grid_cell_count(const pbf_solver* solver, uint64_t* cells);
+
+/* ---- batched scenes: many independent dam breaks advance in one launch sequence per substep,
+ *      replayed as one CUDA graph.  No counterpart in the reference (it runs one solver per
+ *      scene); each scene behaves exactly as pbf_forward_step / pbf_vjp_step on its own.
+ *      Particle arrays are the scenes' arrays concatenated in scene order. ---- */
+int pbf_batch_create(const pbf_domain_configuration* scenes, uint32_t scene_count,
+                     const pbf_configuration* configuration, pbf_execution_mode mode, void* cuda_stream,
+                     pbf_batch** batch);
+int pbf_batch_destroy(pbf_batch* batch);
+int pbf_batch_particle_offset(const pbf_batch* batch, uint32_t scene, uint32_t* offset, uint32_t* count);
+int pbf_batch_forward_step(pbf_batch* batch, const pbf_particle_state* state, const pbf_control* control,
+                           const pbf_parameters* parameters, pbf_particle_state* next_state, uint32_t cache_slot);
+int pbf_batch_vjp_step(pbf_batch* batch, const pbf_particle_state* state, const pbf_control* control,
+                       const pbf_parameters* parameters, const pbf_particle_state* next_state, uint32_t cache_slot,
+                       const pbf_particle_state_adjoint* next_state_adjoint,
+                       pbf_particle_state_adjoint* previous_state_adjoint, pbf_control_adjoint* control_adjoint,
+                       pbf_parameter_adjoint* parameter_adjoint);
+int pbf_batch_reserve_caches(pbf_batch* batch, uint32_t cache_slots);
+int pbf_batch_set_launch_shape(pbf_batch* batch, uint32_t bucket, uint32_t block_size);
+
+/* ---- misc ---- */
+int pbf_synchronize(pbf_solver* solver);
+int pbf_batch_synchronize(pbf_batch* batch);
+const char* pbf_status_string(int status);
+const char* pbf_last_error(void);
+int pbf_abi_version(void);
+/* Number of kernels this library launched since load (all threads). */
+uint64_t pbf_launch_count(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHYSICA_PBF_H */

@@ -1,0 +1,480 @@
+// Replay harness of the reference PBF -- TEST INFRASTRUCTURE ONLY.
+//
+// Linked with the reference's own kernel translation units (pbf/pbf.cu, density/density.cu,
+// neighborhood/neighborhood.cu, domain/domain.cu of fluids/liquid/particle, compiled from the
+// reference sources by oracle/build.py into oracle/_ref/libpbf_ref.so).  The reference's host
+// layer is a set of C++23 module units (import std) that this toolchain cannot build, so this
+// file replays PBF::forward_step (pbf/pbf.cpp:167-191) and PBF::vjp_step (pbf/pbf.cpp:217-258)
+// call for call over the reference's launch_* functions, with plain cudaMalloc buffers in place
+// of cuda::device_buffer.  It exists to produce golden outputs of the reference on a GPU and to
+// time the reference as the baseline arm of bench.py; the product never links it.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+#include <cuda/stream>
+
+#include "density/kernels.h"
+#include "domain/kernels.h"
+#include "neighborhood/device.cuh"
+#include "neighborhood/kernels.h"
+#include "pbf/kernels.h"
+
+namespace cd = physica::fluids::liquid::particle::cuda_detail;
+
+namespace {
+
+struct Vec { float* x = nullptr; float* y = nullptr; float* z = nullptr; };
+struct DVec { double* x = nullptr; double* y = nullptr; double* z = nullptr; };
+
+struct Iteration {
+    float* densities;
+    Vec gradient_sums;
+    float* denominators;
+    float* lambdas;
+    Vec corrections;
+    uint32_t* masks;
+};
+
+}  // namespace
+
+extern "C" {
+
+typedef struct {
+    uint32_t particle_count;
+    float time_step, support_radius, particle_radius;
+    float gravity[3];
+    float box_min[3], box_max[3], box_velocity[3];
+    uint32_t no_slip;
+    uint32_t pressure_iterations, checkpoint_interval;
+    int differentiable;
+} ref_config;
+
+typedef struct {
+    const float* px; const float* py; const float* pz;
+    const float* vx; const float* vy; const float* vz;
+} ref_state_in;
+
+typedef struct {
+    float* px; float* py; float* pz;
+    float* vx; float* vy; float* vz;
+} ref_state_out;
+
+typedef struct {
+    const float* masses; const float* rest_densities; const float* relaxation;
+    const float* strength; const float* exponent; const float* radius;
+    const float* xsph; const float* vorticity;
+} ref_params;
+
+typedef struct {
+    double* px; double* py; double* pz;
+    double* vx; double* vy; double* vz;
+} ref_adjoint_state;
+
+typedef struct {
+    double* masses; double* rest_densities; double* relaxation;
+    double* strength; double* exponent; double* radius;
+    double* xsph; double* vorticity;
+} ref_param_adjoint;
+
+}  // extern "C"
+
+namespace {
+
+struct Harness {
+    ref_config cfg{};
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocations;
+    uint32_t cells_x = 0, cells_y = 0, cells_z = 0, cells = 0;
+    // neighbourhood (neighborhood/neighborhood.ixx:321-332, neighborhood.cpp:14-42)
+    uint64_t *unsorted_keys, *sorted_keys, *sorted_boundary_keys, *unsorted_boundary_keys;
+    uint32_t *unsorted_indices, *sorted_indices, *cell_offsets, *sorted_boundary_indices, *unsorted_boundary_indices,
+        *boundary_cell_offsets;
+    void* sort_scratch = nullptr;
+    size_t sort_scratch_bytes = 0;
+    void* boundary_scratch = nullptr;
+    size_t boundary_scratch_bytes = 0;
+    float origin[3] = {0, 0, 0};
+    float boundary_time = 0.0F;
+    // step cache (pbf/pbf.ixx:54-70)
+    Vec predicted, corrected, reconstructed, vorticities, normals, confined;
+    float *magnitudes, *normalizers;
+    std::vector<std::pair<uint32_t, Vec>> checkpoints;
+    Iteration forward_iteration{};
+    float* first_densities;
+    float* first_lambdas;
+    uint64_t step_index = 0;
+    // differentiation workspace (pbf/pbf.ixx:107-132)
+    std::vector<Vec> segment_positions;
+    std::vector<Iteration> segment_iterations;
+    DVec current_position_adjoint, next_position_adjoint, correction_adjoint, reconstructed_velocity_adjoint,
+        vorticity_adjoint, vorticity_normal_adjoint, confined_velocity_adjoint;
+    double *lambda_adjoint, *density_adjoint;
+    // empty boundary set
+    float* empty_f = nullptr;
+
+    template <class T>
+    T* alloc(size_t n) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        allocations.push_back(p);
+        return static_cast<T*>(p);
+    }
+    Vec vec() { const size_t n = cfg.particle_count; return {alloc<float>(n), alloc<float>(n), alloc<float>(n)}; }
+    DVec dvec() { const size_t n = cfg.particle_count; return {alloc<double>(n), alloc<double>(n), alloc<double>(n)}; }
+    Iteration iteration() {
+        const size_t n = cfg.particle_count;
+        return {alloc<float>(n), vec(), alloc<float>(n), alloc<float>(n), vec(), alloc<uint32_t>(n)};
+    }
+    ~Harness() {
+        cudaStreamSynchronize(stream);
+        for (void* p : allocations) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    cd::ConstVectorView<float> cv(const Vec& v) const { return {v.x, v.y, v.z}; }
+    cd::VectorView<float> mv(const Vec& v) const { return {v.x, v.y, v.z}; }
+    cd::ConstVectorView<double> cdv(const DVec& v) const { return {v.x, v.y, v.z}; }
+    cd::VectorView<double> mdv(const DVec& v) const { return {v.x, v.y, v.z}; }
+
+    cd::NeighborhoodView neighborhood() const {
+        return {sorted_keys, sorted_indices, cell_offsets, sorted_boundary_keys, sorted_boundary_indices, boundary_cell_offsets,
+                cfg.particle_count, 0u, cells_x, cells_y, cells_z, origin[0], origin[1], origin[2], cfg.support_radius};
+    }
+    cd::BoundaryView boundary() const { return {empty_f, empty_f, empty_f, empty_f, empty_f, empty_f, empty_f, 0u, boundary_time}; }
+
+    // pbf/pbf.cpp:17-31
+    cd::Box collision_box(const uint64_t step) const {
+        const float time = static_cast<float>(step) * cfg.time_step;
+        return {cfg.box_min[0] + time * cfg.box_velocity[0] + cfg.particle_radius,
+                cfg.box_min[1] + time * cfg.box_velocity[1] + cfg.particle_radius,
+                cfg.box_min[2] + time * cfg.box_velocity[2] + cfg.particle_radius,
+                cfg.box_max[0] + time * cfg.box_velocity[0] - cfg.particle_radius,
+                cfg.box_max[1] + time * cfg.box_velocity[1] - cfg.particle_radius,
+                cfg.box_max[2] + time * cfg.box_velocity[2] - cfg.particle_radius,
+                cfg.box_velocity[0], cfg.box_velocity[1], cfg.box_velocity[2], cfg.no_slip};
+    }
+
+    void copy(const Vec& src, const Vec& dst) const {
+        const size_t b = cfg.particle_count * sizeof(float);
+        cudaMemcpyAsync(dst.x, src.x, b, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(dst.y, src.y, b, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(dst.z, src.z, b, cudaMemcpyDeviceToDevice, stream);
+    }
+    void clear(const DVec& v) const {
+        const size_t b = cfg.particle_count * sizeof(double);
+        cudaMemsetAsync(v.x, 0, b, stream);
+        cudaMemsetAsync(v.y, 0, b, stream);
+        cudaMemsetAsync(v.z, 0, b, stream);
+    }
+    void clear(double* v) const { cudaMemsetAsync(v, 0, cfg.particle_count * sizeof(double), stream); }
+    void copy(const DVec& src, const DVec& dst) const {
+        const size_t b = cfg.particle_count * sizeof(double);
+        cudaMemcpyAsync(dst.x, src.x, b, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(dst.y, src.y, b, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(dst.z, src.z, b, cudaMemcpyDeviceToDevice, stream);
+    }
+
+    // NeighborhoodSearch::build (neighborhood/neighborhood.cpp:44-89)
+    void build(const uint64_t step, const Vec& positions) {
+        const cd::Box box{cfg.box_min[0], cfg.box_min[1], cfg.box_min[2], cfg.box_max[0], cfg.box_max[1], cfg.box_max[2],
+                          cfg.box_velocity[0], cfg.box_velocity[1], cfg.box_velocity[2], cfg.no_slip};
+        cd::build_neighborhood(::cuda::stream_ref{stream}, cfg.particle_count, 0u, cfg.support_radius, cfg.time_step, step, box,
+                               cv(positions), cd::ConstVectorView<float>{empty_f, empty_f, empty_f},
+                               cd::ConstVectorView<float>{empty_f, empty_f, empty_f}, unsorted_keys, unsorted_indices,
+                               unsorted_boundary_keys, unsorted_boundary_indices, sort_scratch, sort_scratch_bytes,
+                               boundary_scratch, boundary_scratch_bytes, sorted_keys, sorted_indices, cell_offsets,
+                               sorted_boundary_keys, sorted_boundary_indices, boundary_cell_offsets);
+        boundary_time = static_cast<float>(step) * cfg.time_step;
+        for (int a = 0; a < 3; ++a) origin[a] = cfg.box_min[a] + boundary_time * cfg.box_velocity[a];
+    }
+
+    void iterate(const ref_params& p, const cd::ParticleParameterView& pv, const Vec& positions, Iteration& it,
+                 const Vec& output, const uint64_t step) {
+        const ::cuda::stream_ref s{stream};
+        const uint32_t n = cfg.particle_count;
+        cd::density_forward(s, n, cfg.support_radius, true, cv(predicted), cv(positions), pv, neighborhood(), boundary(),
+                            it.densities);
+        cd::pbf::launch_lambda_forward(s, n, cfg.support_radius, cv(predicted), cv(positions), pv, neighborhood(), boundary(),
+                                       it.densities, p.relaxation, mv(it.gradient_sums), it.denominators, it.lambdas);
+        cd::pbf::launch_correction_forward(s, n, cfg.support_radius, cv(predicted), cv(positions), pv, neighborhood(), boundary(),
+                                           it.lambdas, p.strength, p.exponent, p.radius, mv(it.corrections));
+        cd::pbf::launch_project_forward(s, n, collision_box(step), cv(positions), cv(it.corrections), it.masks, mv(output));
+    }
+};
+
+cd::ParticleParameterView param_view(const ref_params& p) {
+    return {p.masses, p.rest_densities, nullptr, nullptr};
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_create(const ref_config* cfg, void** handle) {
+    if (!cfg || !handle) return 1;
+    auto* h = new Harness();
+    h->cfg = *cfg;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return 3; }
+    const uint32_t n = cfg->particle_count;
+    h->cells_x = static_cast<uint32_t>(std::ceil((cfg->box_max[0] - cfg->box_min[0]) / cfg->support_radius));
+    h->cells_y = static_cast<uint32_t>(std::ceil((cfg->box_max[1] - cfg->box_min[1]) / cfg->support_radius));
+    h->cells_z = static_cast<uint32_t>(std::ceil((cfg->box_max[2] - cfg->box_min[2]) / cfg->support_radius));
+    h->cells = h->cells_x * h->cells_y * h->cells_z;
+    h->unsorted_keys = h->alloc<uint64_t>(n);
+    h->sorted_keys = h->alloc<uint64_t>(n);
+    h->unsorted_indices = h->alloc<uint32_t>(n);
+    h->sorted_indices = h->alloc<uint32_t>(n);
+    h->cell_offsets = h->alloc<uint32_t>(h->cells + 1);
+    h->unsorted_boundary_keys = h->alloc<uint64_t>(0);
+    h->sorted_boundary_keys = h->alloc<uint64_t>(0);
+    h->unsorted_boundary_indices = h->alloc<uint32_t>(0);
+    h->sorted_boundary_indices = h->alloc<uint32_t>(0);
+    h->boundary_cell_offsets = h->alloc<uint32_t>(h->cells + 1);
+    h->sort_scratch_bytes = cd::radix_sort_storage_size(n);
+    h->sort_scratch = h->alloc<uint8_t>(h->sort_scratch_bytes);
+    h->boundary_scratch_bytes = cd::radix_sort_storage_size(0u);
+    h->boundary_scratch = h->alloc<uint8_t>(h->boundary_scratch_bytes);
+    h->empty_f = h->alloc<float>(1);
+    h->predicted = h->vec();
+    h->corrected = h->vec();
+    h->reconstructed = h->vec();
+    h->vorticities = h->vec();
+    h->normals = h->vec();
+    h->confined = h->vec();
+    h->magnitudes = h->alloc<float>(n);
+    h->normalizers = h->alloc<float>(n);
+    h->first_densities = h->alloc<float>(n);
+    h->first_lambdas = h->alloc<float>(n);
+    h->forward_iteration = h->iteration();
+    // PBF::allocate_step_cache (pbf/pbf.cpp:108-125): checkpoints at 0, ci, 2ci, ... and K.
+    const uint32_t K = cfg->pressure_iterations, ci = cfg->checkpoint_interval ? cfg->checkpoint_interval : 1u;
+    h->checkpoints.push_back({0u, h->vec()});
+    for (uint32_t it = ci; it < K; it += ci) h->checkpoints.push_back({it, h->vec()});
+    if (K != 0u) h->checkpoints.push_back({K, h->vec()});
+    if (cfg->differentiable) {
+        for (uint32_t k = 0; k <= ci; ++k) h->segment_positions.push_back(h->vec());
+        for (uint32_t k = 0; k < ci; ++k) h->segment_iterations.push_back(h->iteration());
+        h->current_position_adjoint = h->dvec();
+        h->next_position_adjoint = h->dvec();
+        h->correction_adjoint = h->dvec();
+        h->reconstructed_velocity_adjoint = h->dvec();
+        h->vorticity_adjoint = h->dvec();
+        h->vorticity_normal_adjoint = h->dvec();
+        h->confined_velocity_adjoint = h->dvec();
+        h->lambda_adjoint = h->alloc<double>(n);
+        h->density_adjoint = h->alloc<double>(n);
+    }
+    for (void* p : h->allocations)
+        if (!p) { delete h; return 2; }
+    cudaMemsetAsync(h->magnitudes, 0, n * sizeof(float), h->stream);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) { delete h; return 3; }
+    *handle = h;
+    return 0;
+}
+
+int ref_destroy(void* handle) {
+    delete static_cast<Harness*>(handle);
+    return 0;
+}
+
+// PBF::forward_step (pbf/pbf.cpp:167-191).
+int ref_forward_step(void* handle, const ref_state_in* state, const float* const* controls, const ref_params* p,
+                     const ref_state_out* next, const uint64_t step_index) {
+    auto* h = static_cast<Harness*>(handle);
+    const ::cuda::stream_ref s{h->stream};
+    const uint32_t n = h->cfg.particle_count;
+    const float h_radius = h->cfg.support_radius;
+    const cd::ConstVectorView<float> x{state->px, state->py, state->pz}, v{state->vx, state->vy, state->vz},
+        a{controls[0], controls[1], controls[2]};
+    const cd::ParticleParameterView pv = param_view(*p);
+    cd::pbf::launch_predict_forward(s, n, h->cfg.time_step, h->cfg.gravity[0], h->cfg.gravity[1], h->cfg.gravity[2], x, v, a,
+                                    h->mv(h->predicted));
+    h->build(step_index + 1u, h->predicted);
+    h->copy(h->predicted, h->corrected);
+    h->copy(h->corrected, h->checkpoints[0].second);
+    size_t checkpoint = 1;
+    for (uint32_t it = 0; it < h->cfg.pressure_iterations; ++it) {
+        h->iterate(*p, pv, h->corrected, h->forward_iteration, h->corrected, step_index + 1u);
+        if (it == 0) {
+            cudaMemcpyAsync(h->first_densities, h->forward_iteration.densities, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
+            cudaMemcpyAsync(h->first_lambdas, h->forward_iteration.lambdas, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
+        }
+        if (checkpoint < h->checkpoints.size() && h->checkpoints[checkpoint].first == it + 1u) {
+            h->copy(h->corrected, h->checkpoints[checkpoint].second);
+            ++checkpoint;
+        }
+    }
+    cd::pbf::launch_reconstruct_forward(s, n, 1.0F / h->cfg.time_step, x, h->cv(h->corrected), h->mv(h->reconstructed));
+    cd::pbf::launch_vorticity_forward(s, n, h_radius, h->cv(h->predicted), h->cv(h->corrected), h->cv(h->reconstructed),
+                                      h->neighborhood(), h->mv(h->vorticities));
+    cd::pbf::launch_normal_forward(s, n, h_radius, h->cv(h->predicted), h->cv(h->corrected), h->cv(h->vorticities),
+                                   h->neighborhood(), h->magnitudes, h->mv(h->normals), h->normalizers);
+    cd::pbf::launch_confinement_forward(s, n, h->cfg.time_step, h->cv(h->reconstructed), h->cv(h->vorticities),
+                                        h->cv(h->normals), p->vorticity, h->mv(h->confined));
+    cd::pbf::launch_xsph_forward(s, n, h_radius, h->cv(h->predicted), h->cv(h->corrected), h->cv(h->confined),
+                                 h->neighborhood(), p->xsph, cd::VectorView<float>{next->vx, next->vy, next->vz});
+    h->copy(h->corrected, Vec{next->px, next->py, next->pz});
+    h->step_index = step_index;
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+// PBF::vjp_step (pbf/pbf.cpp:217-258).  Adjoint outputs are accumulated.
+int ref_vjp_step(void* handle, const ref_state_in* state, const ref_params* p, const ref_adjoint_state* next_adjoint,
+                 const ref_adjoint_state* previous_adjoint, double* const* control_adjoint, const ref_param_adjoint* pa) {
+    auto* h = static_cast<Harness*>(handle);
+    if (!h->cfg.differentiable) return 4;
+    const ::cuda::stream_ref s{h->stream};
+    const uint32_t n = h->cfg.particle_count;
+    const float hr = h->cfg.support_radius;
+    const cd::ParticleParameterView pv = param_view(*p);
+    const cd::ParticleParameterAdjointView pav{pa->masses, pa->rest_densities, nullptr, nullptr};
+    const cd::VectorView<double> prev_x{previous_adjoint->px, previous_adjoint->py, previous_adjoint->pz};
+    const cd::VectorView<double> prev_v{previous_adjoint->vx, previous_adjoint->vy, previous_adjoint->vz};
+    const cd::ConstVectorView<double> next_x{next_adjoint->px, next_adjoint->py, next_adjoint->pz};
+    const cd::ConstVectorView<double> next_v{next_adjoint->vx, next_adjoint->vy, next_adjoint->vz};
+    const cd::ConstVectorView<float> x{state->px, state->py, state->pz};
+    (void)x;
+    const size_t db = n * sizeof(double);
+    cudaMemcpyAsync(h->current_position_adjoint.x, next_x.x, db, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->current_position_adjoint.y, next_x.y, db, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->current_position_adjoint.z, next_x.z, db, cudaMemcpyDeviceToDevice, h->stream);
+    h->clear(h->confined_velocity_adjoint);
+    cd::pbf::launch_xsph_vjp(s, n, hr, h->cv(h->predicted), h->cv(h->corrected), h->cv(h->confined), h->neighborhood(), p->xsph,
+                             next_v, h->mdv(h->current_position_adjoint), h->mdv(h->confined_velocity_adjoint), pa->xsph);
+    h->clear(h->reconstructed_velocity_adjoint);
+    h->clear(h->vorticity_adjoint);
+    h->clear(h->vorticity_normal_adjoint);
+    cd::pbf::launch_confinement_vjp(s, n, h->cfg.time_step, h->cv(h->vorticities), h->cv(h->normals), p->vorticity,
+                                    h->cdv(h->confined_velocity_adjoint), h->mdv(h->reconstructed_velocity_adjoint),
+                                    h->mdv(h->vorticity_adjoint), h->mdv(h->vorticity_normal_adjoint), pa->vorticity);
+    cd::pbf::launch_normal_vjp(s, n, hr, h->cv(h->predicted), h->cv(h->corrected), h->cv(h->vorticities), h->neighborhood(),
+                               h->magnitudes, h->cv(h->normals), h->normalizers, h->cdv(h->vorticity_normal_adjoint),
+                               h->mdv(h->current_position_adjoint), h->mdv(h->vorticity_adjoint));
+    cd::pbf::launch_vorticity_vjp(s, n, hr, h->cv(h->predicted), h->cv(h->corrected), h->cv(h->reconstructed), h->neighborhood(),
+                                  h->cdv(h->vorticity_adjoint), h->mdv(h->current_position_adjoint),
+                                  h->mdv(h->reconstructed_velocity_adjoint));
+    cd::pbf::launch_reconstruct_vjp(s, n, 1.0F / h->cfg.time_step, h->cdv(h->reconstructed_velocity_adjoint), prev_x,
+                                    h->mdv(h->current_position_adjoint));
+    for (size_t segment = h->checkpoints.size(); segment-- > 1;) {
+        const auto& start = h->checkpoints[segment - 1];
+        const auto& end = h->checkpoints[segment];
+        const uint32_t length = end.first - start.first;
+        h->copy(start.second, h->segment_positions[0]);
+        for (uint32_t k = 0; k < length; ++k)
+            h->iterate(*p, pv, h->segment_positions[k], h->segment_iterations[k], h->segment_positions[k + 1], h->step_index + 1u);
+        for (uint32_t k = length; k-- > 0;) {
+            Iteration& it = h->segment_iterations[k];
+            h->clear(h->next_position_adjoint);
+            h->clear(h->correction_adjoint);
+            h->clear(h->lambda_adjoint);
+            h->clear(h->density_adjoint);
+            cd::pbf::launch_project_vjp(s, n, it.masks, h->cdv(h->current_position_adjoint), h->mdv(h->next_position_adjoint),
+                                        h->mdv(h->correction_adjoint));
+            cd::pbf::launch_correction_vjp(s, n, hr, h->cv(h->predicted), h->cv(h->segment_positions[k]), pv, h->neighborhood(),
+                                           h->boundary(), it.lambdas, p->strength, p->exponent, p->radius,
+                                           h->cdv(h->correction_adjoint), h->mdv(h->next_position_adjoint), h->lambda_adjoint,
+                                           pav, pa->strength, pa->exponent, pa->radius);
+            cd::pbf::launch_lambda_vjp(s, n, hr, h->cv(h->predicted), h->cv(h->segment_positions[k]), pv, h->neighborhood(),
+                                       h->boundary(), it.densities, h->cv(it.gradient_sums), it.denominators, h->lambda_adjoint,
+                                       h->mdv(h->next_position_adjoint), h->density_adjoint, pav, pa->relaxation);
+            cd::density_vjp(s, n, hr, true, h->cv(h->predicted), h->cv(h->segment_positions[k]), pv, h->neighborhood(),
+                            h->boundary(), h->density_adjoint, h->mdv(h->next_position_adjoint), pav);
+            std::swap(h->current_position_adjoint, h->next_position_adjoint);
+        }
+    }
+    cd::pbf::launch_predict_vjp(s, n, h->cfg.time_step, h->cdv(h->current_position_adjoint), prev_x, prev_v,
+                                cd::VectorView<double>{control_adjoint[0], control_adjoint[1], control_adjoint[2]});
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+// Copy a step-cache field of the last forward step to device memory `dst`.
+//   0 sorted_keys (u64 N)  1 sorted indices (u32 N)  2 cell offsets (u32 C+1)  3 predicted (3N)
+//   4 corrected (3N)  5 reconstructed (3N)  6 vorticities (3N)  7 magnitudes (N)  8 normals (3N)
+//   9 normalizers (N)  10 confined (3N)  11 first densities (N)  12 first lambdas (N)
+int ref_read(void* handle, const int field, void* dst) {
+    auto* h = static_cast<Harness*>(handle);
+    const size_t n = h->cfg.particle_count;
+    auto vec3 = [&](const Vec& v) {
+        float* d = static_cast<float*>(dst);
+        cudaMemcpyAsync(d, v.x, n * 4, cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(d + n, v.y, n * 4, cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(d + 2 * n, v.z, n * 4, cudaMemcpyDeviceToDevice, h->stream);
+    };
+    switch (field) {
+        case 0: cudaMemcpyAsync(dst, h->sorted_keys, n * 8, cudaMemcpyDeviceToDevice, h->stream); break;
+        case 1: cudaMemcpyAsync(dst, h->sorted_indices, n * 4, cudaMemcpyDeviceToDevice, h->stream); break;
+        case 2: cudaMemcpyAsync(dst, h->cell_offsets, (h->cells + 1ull) * 4, cudaMemcpyDeviceToDevice, h->stream); break;
+        case 3: vec3(h->predicted); break;
+        case 4: vec3(h->corrected); break;
+        case 5: vec3(h->reconstructed); break;
+        case 6: vec3(h->vorticities); break;
+        case 7: cudaMemcpyAsync(dst, h->magnitudes, n * 4, cudaMemcpyDeviceToDevice, h->stream); break;
+        case 8: vec3(h->normals); break;
+        case 9: cudaMemcpyAsync(dst, h->normalizers, n * 4, cudaMemcpyDeviceToDevice, h->stream); break;
+        case 10: vec3(h->confined); break;
+        case 11: cudaMemcpyAsync(dst, h->first_densities, n * 4, cudaMemcpyDeviceToDevice, h->stream); break;
+        case 12: cudaMemcpyAsync(dst, h->first_lambdas, n * 4, cudaMemcpyDeviceToDevice, h->stream); break;
+        default: return 1;
+    }
+    return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : 3;
+}
+
+// ---- single passes of the reference on caller-chosen inputs (all pointers: device SoA) ----
+// Build the neighbourhood from topology positions `x*` for the step `step` (= state step + 1).
+int ref_pass_topology(void* handle, const float* const* topology, const uint64_t step) {
+    auto* h = static_cast<Harness*>(handle);
+    const size_t b = h->cfg.particle_count * sizeof(float);
+    cudaMemcpyAsync(h->predicted.x, topology[0], b, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->predicted.y, topology[1], b, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->predicted.z, topology[2], b, cudaMemcpyDeviceToDevice, h->stream);
+    h->build(step, h->predicted);
+    return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : 3;
+}
+
+// pass: 0 density, 1 lambda, 2 correction, 3 project, 4 vorticity, 5 normal (+magnitude), 6 confinement, 7 xsph
+//   in3[0..2] : vector inputs (positions, velocities/vorticities/..., normals) as SoA triples
+//   sin[0..1] : scalar inputs (densities, lambdas / magnitudes)
+//   out3[0..1]: vector outputs; sout[0..1]: scalar outputs; mask: uint32 masks
+int ref_pass(void* handle, const int pass, const float* const* in3, const float* const* sin, const ref_params* p,
+             float* const* out3, float* const* sout, uint32_t* mask, const uint64_t step) {
+    auto* h = static_cast<Harness*>(handle);
+    const ::cuda::stream_ref s{h->stream};
+    const uint32_t n = h->cfg.particle_count;
+    const float hr = h->cfg.support_radius;
+    const cd::ParticleParameterView pv = param_view(*p);
+    auto cin = [&](int k) { return cd::ConstVectorView<float>{in3[3 * k], in3[3 * k + 1], in3[3 * k + 2]}; };
+    auto vout = [&](int k) { return cd::VectorView<float>{out3[3 * k], out3[3 * k + 1], out3[3 * k + 2]}; };
+    switch (pass) {
+        case 0: cd::density_forward(s, n, hr, true, h->cv(h->predicted), cin(0), pv, h->neighborhood(), h->boundary(), sout[0]); break;
+        case 1: cd::pbf::launch_lambda_forward(s, n, hr, h->cv(h->predicted), cin(0), pv, h->neighborhood(), h->boundary(), sin[0],
+                                               p->relaxation, vout(0), sout[0], sout[1]); break;
+        case 2: cd::pbf::launch_correction_forward(s, n, hr, h->cv(h->predicted), cin(0), pv, h->neighborhood(), h->boundary(), sin[0],
+                                                   p->strength, p->exponent, p->radius, vout(0)); break;
+        case 3: cd::pbf::launch_project_forward(s, n, h->collision_box(step), cin(0), cin(1), mask, vout(0)); break;
+        case 4: cd::pbf::launch_vorticity_forward(s, n, hr, h->cv(h->predicted), cin(0), cin(1), h->neighborhood(), vout(0)); break;
+        case 5: cd::pbf::launch_normal_forward(s, n, hr, h->cv(h->predicted), cin(0), cin(1), h->neighborhood(), sout[0], vout(0), sout[1]); break;
+        case 6: cd::pbf::launch_confinement_forward(s, n, h->cfg.time_step, cin(0), cin(1), cin(2), p->vorticity, vout(0)); break;
+        case 7: cd::pbf::launch_xsph_forward(s, n, hr, h->cv(h->predicted), cin(0), cin(1), h->neighborhood(), p->xsph, vout(0)); break;
+        case 8: cd::pbf::launch_reconstruct_forward(s, n, 1.0F / h->cfg.time_step, cin(0), cin(1), vout(0)); break;
+        default: return 1;
+    }
+    return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : 3;
+}
+
+int ref_cells(void* handle, uint32_t* dims) {
+    auto* h = static_cast<Harness*>(handle);
+    dims[0] = h->cells_x; dims[1] = h->cells_y; dims[2] = h->cells_z;
+    return 0;
+}
+
+int ref_synchronize(void* handle) {
+    return cudaStreamSynchronize(static_cast<Harness*>(handle)->stream) == cudaSuccess ? 0 : 3;
+}
+
+// Stream of the harness (to time it with events on that stream).
+void* ref_stream(void* handle) { return static_cast<Harness*>(handle)->stream; }
+
+}  // extern "C"

@@ -1,0 +1,185 @@
+"""ctypes front end of the reference's own CUDA PBF (oracle/_ref/libpbf_ref.so) -- TEST INFRASTRUCTURE ONLY.
+
+The library is compiled from the reference sources by oracle/build.py and driven by
+oracle/ref_harness.cu.  Tests use it to pin parity against the reference itself; bench.py
+uses it as the reference arm.  Nothing in physica_b200 imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+import torch
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "_ref" / "libpbf_ref.so"
+
+
+class RefConfig(ctypes.Structure):
+    _fields_ = [
+        ("particle_count", ctypes.c_uint32),
+        ("time_step", ctypes.c_float), ("support_radius", ctypes.c_float), ("particle_radius", ctypes.c_float),
+        ("gravity", ctypes.c_float * 3), ("box_min", ctypes.c_float * 3), ("box_max", ctypes.c_float * 3),
+        ("box_velocity", ctypes.c_float * 3), ("no_slip", ctypes.c_uint32),
+        ("pressure_iterations", ctypes.c_uint32), ("checkpoint_interval", ctypes.c_uint32),
+        ("differentiable", ctypes.c_int),
+    ]
+
+
+class RefStateIn(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("px", "py", "pz", "vx", "vy", "vz")]
+
+
+RefStateOut = RefStateIn
+RefAdjointState = RefStateIn
+
+
+class RefParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("masses", "rest_densities", "relaxation", "strength", "exponent",
+                                               "radius", "xsph", "vorticity")]
+
+
+RefParamAdjoint = RefParams
+
+FIELDS = {"sorted_keys": 0, "sorted_indices": 1, "cell_offsets": 2, "predicted": 3, "corrected": 4,
+          "reconstructed": 5, "vorticities": 6, "magnitudes": 7, "normals": 8, "normalizers": 9, "confined": 10,
+          "first_densities": 11, "first_lambdas": 12}
+
+_lib = None
+
+
+def available() -> bool:
+    return LIB_PATH.exists()
+
+
+def load():
+    global _lib
+    if _lib is None:
+        lib = ctypes.CDLL(str(LIB_PATH))
+        vp = ctypes.c_void_p
+        P = ctypes.POINTER
+        lib.ref_create.argtypes = [P(RefConfig), P(vp)]
+        lib.ref_destroy.argtypes = [vp]
+        lib.ref_forward_step.argtypes = [vp, P(RefStateIn), P(vp), P(RefParams), P(RefStateOut), ctypes.c_uint64]
+        lib.ref_vjp_step.argtypes = [vp, P(RefStateIn), P(RefParams), P(RefAdjointState), P(RefAdjointState), P(vp),
+                                     P(RefParamAdjoint)]
+        lib.ref_read.argtypes = [vp, ctypes.c_int, vp]
+        lib.ref_cells.argtypes = [vp, P(ctypes.c_uint32)]
+        lib.ref_synchronize.argtypes = [vp]
+        lib.ref_stream.argtypes = [vp]
+        lib.ref_stream.restype = vp
+        _lib = lib
+    return _lib
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class ReferencePBF:
+    """The reference PBF kernels replayed by the harness, on device tensors."""
+
+    def __init__(self, scene, checkpoint_interval=2, differentiable=False, device="cuda"):
+        lib = load()
+        self.scene = scene
+        self.device = torch.device(device)
+        c = RefConfig()
+        c.particle_count = scene.count
+        c.time_step = scene.time_step
+        c.support_radius = scene.support_radius
+        c.particle_radius = scene.particle_radius
+        c.gravity = (ctypes.c_float * 3)(*scene.gravity)
+        c.box_min = (ctypes.c_float * 3)(*scene.box_min)
+        c.box_max = (ctypes.c_float * 3)(*scene.box_max)
+        c.box_velocity = (ctypes.c_float * 3)(*scene.box_velocity)
+        c.no_slip = 1
+        c.pressure_iterations = scene.pressure_iterations
+        c.checkpoint_interval = checkpoint_interval
+        c.differentiable = 1 if differentiable else 0
+        h = ctypes.c_void_p()
+        torch.cuda.synchronize(self.device)
+        rc = lib.ref_create(ctypes.byref(c), ctypes.byref(h))
+        if rc:
+            raise RuntimeError(f"ref_create failed: {rc}")
+        self.handle = h
+        dims = (ctypes.c_uint32 * 3)()
+        lib.ref_cells(h, dims)
+        self.dims = tuple(dims)
+        self.cells = dims[0] * dims[1] * dims[2]
+        n = scene.count
+        f = lambda *s: torch.zeros(*s, dtype=torch.float32, device=self.device)
+        self.params = {k: torch.from_numpy(v).to(self.device) for k, v in scene.parameter_arrays().items()}
+        self.controls = torch.from_numpy(scene.controls).to(self.device).contiguous()
+        self.n = n
+
+    @property
+    def stream(self):
+        return load().ref_stream(self.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().ref_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _pstruct(self):
+        p = self.params
+        return RefParams(_p(p["masses"]), _p(p["rest_densities"]), _p(p["relaxation"]),
+                         _p(p["artificial_pressure_strength"]), _p(p["artificial_pressure_exponent"]),
+                         _p(p["artificial_pressure_radius"]), _p(p["xsph_viscosity"]), _p(p["vorticity_confinement"]))
+
+    def forward_step(self, x, v, x_out, v_out, step_index, synchronize=True):
+        """x, v, x_out, v_out: (3, N) float32 CUDA tensors."""
+        lib = load()
+        sin = RefStateIn(_p(x[0]), _p(x[1]), _p(x[2]), _p(v[0]), _p(v[1]), _p(v[2]))
+        sout = RefStateOut(_p(x_out[0]), _p(x_out[1]), _p(x_out[2]), _p(v_out[0]), _p(v_out[1]), _p(v_out[2]))
+        ctrl = (ctypes.c_void_p * 3)(self.controls[0].data_ptr(), self.controls[1].data_ptr(), self.controls[2].data_ptr())
+        self._keep = (sin, sout, ctrl)
+        rc = lib.ref_forward_step(self.handle, ctypes.byref(sin), ctrl, ctypes.byref(self._pstruct()), ctypes.byref(sout),
+                                  step_index)
+        if rc:
+            raise RuntimeError(f"ref_forward_step failed: {rc}")
+        if synchronize:
+            lib.ref_synchronize(self.handle)
+
+    def vjp_step(self, x, v, next_adjoint, previous_adjoint, control_adjoint, param_adjoint):
+        """Adjoints are dicts of float64 CUDA tensors; outputs are accumulated."""
+        lib = load()
+        sin = RefStateIn(_p(x[0]), _p(x[1]), _p(x[2]), _p(v[0]), _p(v[1]), _p(v[2]))
+        na = RefAdjointState(*[_p(next_adjoint[k][a]) for k in ("positions", "velocities") for a in range(3)])
+        pa = RefAdjointState(*[_p(previous_adjoint[k][a]) for k in ("positions", "velocities") for a in range(3)])
+        ca = (ctypes.c_void_p * 3)(*[control_adjoint[a].data_ptr() for a in range(3)])
+        g = param_adjoint
+        pp = RefParamAdjoint(_p(g["masses"]), _p(g["rest_densities"]), _p(g["relaxation"]),
+                             _p(g["artificial_pressure_strength"]), _p(g["artificial_pressure_exponent"]),
+                             _p(g["artificial_pressure_radius"]), _p(g["xsph_viscosity"]), _p(g["vorticity_confinement"]))
+        torch.cuda.synchronize(self.device)
+        rc = lib.ref_vjp_step(self.handle, ctypes.byref(sin), ctypes.byref(self._pstruct()), ctypes.byref(na),
+                              ctypes.byref(pa), ca, ctypes.byref(pp))
+        if rc:
+            raise RuntimeError(f"ref_vjp_step failed: {rc}")
+        lib.ref_synchronize(self.handle)
+
+    def read(self, field: str) -> torch.Tensor:
+        n = self.n
+        code = FIELDS[field]
+        if code == 0:
+            out = torch.empty(n, dtype=torch.int64, device=self.device)
+        elif code == 1:
+            out = torch.empty(n, dtype=torch.int32, device=self.device)
+        elif code == 2:
+            out = torch.empty(self.cells + 1, dtype=torch.int32, device=self.device)
+        elif code in (7, 9, 11, 12):
+            out = torch.empty(n, dtype=torch.float32, device=self.device)
+        else:
+            out = torch.empty((3, n), dtype=torch.float32, device=self.device)
+        torch.cuda.synchronize(self.device)
+        rc = load().ref_read(self.handle, code, ctypes.c_void_p(out.data_ptr()))
+        if rc:
+            raise RuntimeError(f"ref_read failed: {rc}")
+        return out

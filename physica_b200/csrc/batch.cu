@@ -1,0 +1,98 @@
+// Batched scenes (pbf_batch_*): many independent dam breaks in one launch sequence.
+#include <memory>
+#include <vector>
+
+#include "engine.h"
+
+struct pbf_batch {
+    pbf::Engine engine;
+    std::vector<std::unique_ptr<pbf::StepRecord>> caches;
+};
+
+extern "C" {
+
+int pbf_batch_create(const pbf_domain_configuration* scenes, const uint32_t scene_count, const pbf_configuration* configuration,
+                     const pbf_execution_mode mode, void* cuda_stream, pbf_batch** batch) {
+    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
+    *batch = nullptr;
+    try {
+        auto b = std::make_unique<pbf_batch>();
+        const int rc = b->engine.init(scenes, scene_count, configuration, mode, static_cast<cudaStream_t>(cuda_stream));
+        if (rc) return rc;
+        *batch = b.release();
+        return PBF_SUCCESS;
+    } catch (...) {
+        pbf::set_error("batch creation failed");
+        return PBF_ERROR_OUT_OF_MEMORY;
+    }
+}
+
+int pbf_batch_destroy(pbf_batch* batch) {
+    if (!batch) return PBF_SUCCESS;
+    cudaStreamSynchronize(batch->engine.stream());
+    delete batch;
+    return PBF_SUCCESS;
+}
+
+int pbf_batch_particle_offset(const pbf_batch* batch, const uint32_t scene, uint32_t* offset, uint32_t* count) {
+    if (!batch || !offset || !count) return PBF_ERROR_INVALID_ARGUMENT;
+    const auto& sc = batch->engine.scenes();
+    if (scene >= sc.size()) {
+        pbf::set_error("scene index out of range");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    *offset = sc[scene].first;
+    *count = sc[scene].config.particle_count;
+    return PBF_SUCCESS;
+}
+
+int pbf_batch_reserve_caches(pbf_batch* batch, const uint32_t cache_slots) {
+    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
+    try {
+        while (batch->caches.size() < cache_slots) {
+            auto r = std::make_unique<pbf::StepRecord>();
+            if (int rc = batch->engine.allocate_record(*r)) return rc;
+            batch->caches.push_back(std::move(r));
+        }
+        return PBF_SUCCESS;
+    } catch (...) {
+        pbf::set_error("cache reservation failed");
+        return PBF_ERROR_OUT_OF_MEMORY;
+    }
+}
+
+int pbf_batch_forward_step(pbf_batch* batch, const pbf_particle_state* state, const pbf_control* control,
+                           const pbf_parameters* parameters, pbf_particle_state* next_state, const uint32_t cache_slot) {
+    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
+    if (int rc = pbf_batch_reserve_caches(batch, cache_slot + 1)) return rc;
+    return batch->engine.forward(state, control, parameters, next_state, *batch->caches[cache_slot]);
+}
+
+int pbf_batch_vjp_step(pbf_batch* batch, const pbf_particle_state* state, const pbf_control* control,
+                       const pbf_parameters* parameters, const pbf_particle_state* next_state, const uint32_t cache_slot,
+                       const pbf_particle_state_adjoint* next_state_adjoint, pbf_particle_state_adjoint* previous_state_adjoint,
+                       pbf_control_adjoint* control_adjoint, pbf_parameter_adjoint* parameter_adjoint) {
+    (void)next_state;
+    if (!batch || cache_slot >= batch->caches.size()) return PBF_ERROR_INVALID_ARGUMENT;
+    if (!batch->engine.differentiable()) return PBF_ERROR_NOT_DIFFERENTIABLE;
+    return batch->engine.reverse(state, control, parameters, *batch->caches[cache_slot], next_state_adjoint,
+                                 previous_state_adjoint, control_adjoint, parameter_adjoint);
+}
+
+int pbf_batch_set_launch_shape(pbf_batch* batch, const uint32_t bucket, const uint32_t block_size) {
+    (void)bucket;
+    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
+    if (block_size != 128) {
+        pbf::set_error("only 128-thread blocks are built");
+        return PBF_ERROR_UNSUPPORTED;
+    }
+    batch->engine.set_block(block_size);
+    return PBF_SUCCESS;
+}
+
+int pbf_batch_synchronize(pbf_batch* batch) {
+    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
+    return batch->engine.check(cudaStreamSynchronize(batch->engine.stream()), "synchronize");
+}
+
+}  // extern "C"

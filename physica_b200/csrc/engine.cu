@@ -1,0 +1,433 @@
+// Engine: scene table, buffers and the forward launch sequence of one substep.
+//
+// Forward substep (reference orchestration pbf/pbf.cpp:167-191):
+//   grid build (predict + key + stable counting sort + reorder)      5 kernels + memset
+//   K x [density+lambda, correction+project(+reconstruct on the last)]  2K kernels
+//   vorticity(+magnitude), normal(+confinement), XSPH(+write-back)      3 kernels
+// All launches are asynchronous on the engine's stream; nothing synchronises.
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "engine.h"
+
+namespace pbf {
+
+namespace {
+thread_local std::string g_last_error;
+std::atomic<uint64_t> g_launches{0};
+}  // namespace
+
+void set_error(const std::string& message) { g_last_error = message; }
+const char* last_error_cstr() { return g_last_error.c_str(); }
+void count_launch(const unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+int Engine::check(const cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return PBF_SUCCESS;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? PBF_ERROR_OUT_OF_MEMORY : PBF_ERROR_CUDA;
+}
+
+void destroy_adjoint_workspace(void* workspace);
+
+Engine::~Engine() {
+    destroy_adjoint_workspace(adjoint_);
+    adjoint_ = nullptr;
+    arena_.release();
+}
+
+static bool finite_positive(const float v) { return std::isfinite(v) && v > 0.0F; }
+
+int Engine::init(const pbf_domain_configuration* scenes, const uint32_t scene_count, const pbf_configuration* configuration,
+                 const pbf_execution_mode mode, cudaStream_t stream) {
+    if (!scenes || scene_count == 0 || !configuration) {
+        set_error("null configuration or zero scenes");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (mode != PBF_EXECUTION_FORWARD && mode != PBF_EXECUTION_DIFFERENTIABLE) {
+        set_error("unknown execution mode");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (configuration->pressure_iterations > kMaxIterations) {
+        set_error("pressure_iterations exceeds " + std::to_string(kMaxIterations));
+        return PBF_ERROR_CAPACITY;
+    }
+    if (configuration->checkpoint_interval == 0) {
+        set_error("checkpoint_interval must be at least 1");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    iterations_ = configuration->pressure_iterations;
+    checkpoint_interval_ = configuration->checkpoint_interval;
+    mode_ = mode;
+    stream_ = stream;
+    arena_.set_stream(stream);
+    uint64_t total_cells = 0, total_particles = 0;
+    scenes_.resize(scene_count);
+    for (uint32_t s = 0; s < scene_count; ++s) {
+        const pbf_domain_configuration& c = scenes[s];
+        SceneHost& h = scenes_[s];
+        h.config = c;
+        h.config.boundary_particles = nullptr;
+        if (!finite_positive(c.time_step) || !finite_positive(c.support_radius) || !std::isfinite(c.particle_radius)) {
+            set_error("scene " + std::to_string(s) + ": time_step and support_radius must be finite and positive");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        if (c.boundary_particle_count > 0) {
+            if (!c.boundary_particles) {
+                set_error("boundary_particles is null but boundary_particle_count > 0");
+                return PBF_ERROR_INVALID_ARGUMENT;
+            }
+            set_error("boundary particles are not supported by this build");
+            return PBF_ERROR_UNSUPPORTED;
+        }
+        const float mins[3] = {c.boundary.minimum.x, c.boundary.minimum.y, c.boundary.minimum.z};
+        const float maxs[3] = {c.boundary.maximum.x, c.boundary.maximum.y, c.boundary.maximum.z};
+        uint64_t cells = 1;
+        for (int a = 0; a < 3; ++a) {
+            // neighborhood/neighborhood.cpp:28-32: ceil((max - min) / h) in float
+            const float extent = maxs[a] - mins[a];
+            const float n = std::ceil(extent / c.support_radius);
+            if (!(n >= 1.0F) || n > 1048576.0F) {
+                set_error("scene " + std::to_string(s) + ": box extent / support_radius must be in [1, 2^20] per axis");
+                return PBF_ERROR_INVALID_ARGUMENT;
+            }
+            h.dims[a] = static_cast<uint32_t>(n);
+            cells *= h.dims[a];
+        }
+        h.cells = cells;
+        h.cell_base = static_cast<uint32_t>(total_cells);
+        h.first = static_cast<uint32_t>(total_particles);
+        total_cells += cells;
+        total_particles += c.particle_count;
+        if (total_cells >= (1ull << 31) || total_particles >= (1ull << 31)) {
+            set_error("total cells and particles must each stay below 2^31");
+            return PBF_ERROR_CAPACITY;
+        }
+    }
+    count_ = static_cast<uint32_t>(total_particles);
+    cells_ = total_cells;
+    cudaError_t e = cudaSuccess;
+    scene_table_.resize(scene_count);
+    d_scenes_ = arena_.alloc<SceneDesc>(scene_count, e);
+    d_constants_ = arena_.alloc<KernelConstants>(scene_count, e);
+    float* d_radii = arena_.alloc<float>(scene_count, e);
+    predicted_ = arena_.alloc<float4>(count_, e);
+    arrival_ = arena_.alloc<uint32_t>(count_, e);
+    unordered_ = arena_.alloc<uint32_t>(count_, e);
+    tile_sums_ = arena_.alloc<uint32_t>(scan_tile_count(cells_ + 1), e);
+    if (scene_count > 1) d_scene_of_ = arena_.alloc<uint32_t>(count_, e);
+    if (int rc = check(e, "device allocation")) return rc;
+    std::vector<float> radii(scene_count);
+    for (uint32_t s = 0; s < scene_count; ++s) radii[s] = scenes_[s].config.support_radius;
+    e = cudaMemcpyAsync(d_radii, radii.data(), radii.size() * sizeof(float), cudaMemcpyHostToDevice, stream_);
+    if (int rc = check(e, "upload support radii")) return rc;
+    if (int rc = check(launch_constants(stream_, d_radii, scene_count, d_constants_), "kernel constants")) return rc;
+    if (scene_count > 1) {
+        std::vector<uint32_t> scene_of(count_);
+        for (uint32_t s = 0; s < scene_count; ++s)
+            for (uint32_t i = 0; i < scenes_[s].config.particle_count; ++i) scene_of[scenes_[s].first + i] = s;
+        e = cudaMemcpyAsync(d_scene_of_, scene_of.data(), scene_of.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_);
+        if (int rc = check(e, "upload scene table")) return rc;
+        e = cudaStreamSynchronize(stream_);
+        if (int rc = check(e, "synchronise")) return rc;
+    }
+    table_step_ = ~0ull;
+    return check(cudaStreamSynchronize(stream_), "engine initialisation");
+}
+
+int Engine::update_scene_table(const uint64_t step_index) {
+    if (table_step_ == step_index) return PBF_SUCCESS;
+    for (size_t s = 0; s < scenes_.size(); ++s) {
+        const SceneHost& h = scenes_[s];
+        const pbf_domain_configuration& c = h.config;
+        SceneDesc& d = scene_table_[s];
+        // The step computes state step_index + 1 (pbf/pbf.cpp:170, 178): time = float(step + 1) * dt.
+        const float time = static_cast<float>(step_index + 1u) * c.time_step;
+        d.grid.cells_x = h.dims[0];
+        d.grid.cells_y = h.dims[1];
+        d.grid.cells_z = h.dims[2];
+        d.grid.cell_base = h.cell_base;
+        d.grid.key_min_x = c.boundary.minimum.x;
+        d.grid.key_min_y = c.boundary.minimum.y;
+        d.grid.key_min_z = c.boundary.minimum.z;
+        d.grid.key_vel_x = c.boundary.velocity.x;
+        d.grid.key_vel_y = c.boundary.velocity.y;
+        d.grid.key_vel_z = c.boundary.velocity.z;
+        d.grid.time = time;
+        d.grid.cell_size = c.support_radius;
+        // gather-side origin (neighborhood/neighborhood.cpp:83-88)
+        d.grid.origin_x = c.boundary.minimum.x + time * c.boundary.velocity.x;
+        d.grid.origin_y = c.boundary.minimum.y + time * c.boundary.velocity.y;
+        d.grid.origin_z = c.boundary.minimum.z + time * c.boundary.velocity.z;
+        // collision box (pbf/pbf.cpp:17-31)
+        d.box.min_x = c.boundary.minimum.x + time * c.boundary.velocity.x + c.particle_radius;
+        d.box.min_y = c.boundary.minimum.y + time * c.boundary.velocity.y + c.particle_radius;
+        d.box.min_z = c.boundary.minimum.z + time * c.boundary.velocity.z + c.particle_radius;
+        d.box.max_x = c.boundary.maximum.x + time * c.boundary.velocity.x - c.particle_radius;
+        d.box.max_y = c.boundary.maximum.y + time * c.boundary.velocity.y - c.particle_radius;
+        d.box.max_z = c.boundary.maximum.z + time * c.boundary.velocity.z - c.particle_radius;
+        d.first = h.first;
+        d.count = c.particle_count;
+        d.time_step = c.time_step;
+        d.inverse_time_step = 1.0F / c.time_step;
+        d.gravity_x = c.gravity.x;
+        d.gravity_y = c.gravity.y;
+        d.gravity_z = c.gravity.z;
+        d.constants = static_cast<uint32_t>(s);
+    }
+    const cudaError_t e = cudaMemcpyAsync(d_scenes_, scene_table_.data(), scene_table_.size() * sizeof(SceneDesc),
+                                          cudaMemcpyHostToDevice, stream_);
+    if (e == cudaSuccess) table_step_ = step_index;
+    return check(e, "upload scene table");
+}
+
+int Engine::allocate_record(StepRecord& r) {
+    r.arena.set_stream(stream_);
+    cudaError_t e = cudaSuccess;
+    const uint32_t n = count_, K = iterations_;
+    const bool diff = differentiable();
+    r.cell_offsets = r.arena.alloc<uint32_t>(cells_ + 1, e);
+    r.sorted_index = r.arena.alloc<uint32_t>(n, e);
+    r.slot_of = r.arena.alloc<uint32_t>(n, e);
+    r.keys = r.arena.alloc<uint32_t>(n, e);
+    r.cell = r.arena.alloc<int4>(n, e);
+    r.topology = r.arena.alloc<float4>(n, e);
+    r.params_a = r.arena.alloc<float4>(n, e);
+    r.params_b = r.arena.alloc<float4>(n, e);
+    const uint32_t npos = diff ? K : (K < 2 ? K : 2);
+    r.positions.assign(npos, nullptr);
+    for (auto& p : r.positions) p = r.arena.alloc<float4>(n, e);
+    r.lambda.assign(diff ? K : (K ? 1 : 0), nullptr);
+    for (auto& p : r.lambda) p = r.arena.alloc<float>(n, e);
+    if (diff) {
+        r.density.assign(K, nullptr);
+        r.gsum.assign(K, nullptr);
+        r.mask.assign(K, nullptr);
+        for (uint32_t k = 0; k < K; ++k) {
+            r.density[k] = r.arena.alloc<float>(n, e);
+            r.gsum[k] = r.arena.alloc<float4>(n, e);
+            r.mask[k] = r.arena.alloc<uint8_t>(n, e);
+        }
+    }
+    r.first_density = r.arena.alloc<float>(n, e);
+    r.first_lambda = r.arena.alloc<float>(n, e);
+    r.neighbor_count = r.arena.alloc<uint32_t>(n, e);
+    r.velocity = r.arena.alloc<float4>(n, e);
+    r.vorticity = r.arena.alloc<float4>(n, e);
+    r.normal = r.arena.alloc<float4>(n, e);
+    r.confined = r.arena.alloc<float4>(n, e);
+    r.valid = false;
+    if (int rc = check(e, "step cache allocation")) return rc;
+    return check(cudaStreamSynchronize(stream_), "step cache allocation");
+}
+
+static bool has3(const pbf_vector_field& f) { return f.x && f.y && f.z; }
+
+int Engine::forward(const pbf_particle_state* state, const pbf_control* control, const pbf_parameters* parameters,
+                    pbf_particle_state* next_state, StepRecord& r) {
+    if (!state || !control || !parameters || !next_state) {
+        set_error("null argument");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (count_ > 0) {
+        if (!has3(state->positions) || !has3(state->velocities) || !has3(control->external_accelerations) ||
+            !has3(next_state->positions) || !has3(next_state->velocities)) {
+            set_error("null field pointer");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        const pbf_parameters& p = *parameters;
+        if (!p.masses || !p.rest_densities || !p.relaxation || !p.artificial_pressure_strength ||
+            !p.artificial_pressure_exponent || !p.artificial_pressure_radius || !p.xsph_viscosity || !p.vorticity_confinement) {
+            set_error("null parameter pointer");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+    }
+    if (int rc = update_scene_table(state->step_index)) return rc;
+    const bool diff = differentiable();
+    const uint32_t K = iterations_;
+    GridBuildArgs g{};
+    g.count = count_;
+    g.cells = cells_;
+    g.scenes = d_scenes_;
+    g.scene_of = d_scene_of_;
+    g.positions = {state->positions.x, state->positions.y, state->positions.z};
+    g.velocities = {state->velocities.x, state->velocities.y, state->velocities.z};
+    g.controls = {control->external_accelerations.x, control->external_accelerations.y, control->external_accelerations.z};
+    g.params = {parameters->masses, parameters->rest_densities, parameters->relaxation,
+                parameters->artificial_pressure_strength, parameters->artificial_pressure_exponent,
+                parameters->artificial_pressure_radius, parameters->xsph_viscosity, parameters->vorticity_confinement};
+    g.predicted = predicted_;
+    g.keys = r.keys;
+    g.arrival = arrival_;
+    g.cell_offsets = r.cell_offsets;
+    g.tile_sums = tile_sums_;
+    g.unordered = unordered_;
+    g.sorted_index = r.sorted_index;
+    g.slot_of = r.slot_of;
+    g.cell = r.cell;
+    g.topology = r.topology;
+    g.params_a = r.params_a;
+    g.params_b = r.params_b;
+    if (int rc = check(launch_grid_build(stream_, g), "grid build")) return rc;
+
+    const GatherCommon gc{count_, d_scenes_, d_constants_, r.cell_offsets, r.cell, r.params_a, r.params_b};
+    const Field3 previous{state->positions.x, state->positions.y, state->positions.z};
+    const MutField3 out_positions{next_state->positions.x, next_state->positions.y, next_state->positions.z};
+    for (uint32_t k = 0; k < K; ++k) {
+        const float4* xk = r.iterate(k, K, diff);
+        float4* xk1 = const_cast<float4*>(r.iterate(k + 1, K, diff));
+        float* lam = diff ? r.lambda[k] : (k == 0 ? r.first_lambda : r.lambda[0]);
+        DensityLambdaArgs d{gc, xk, lam, diff ? r.density[k] : (k == 0 ? r.first_density : nullptr),
+                            diff ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr};
+        if (int rc = check(launch_density_lambda(stream_, d, block_), "density/lambda")) return rc;
+        CorrectionArgs c{gc, xk, lam, xk1, diff ? r.mask[k] : nullptr, k + 1 == K ? 1 : 0, previous, r.sorted_index,
+                         out_positions, r.velocity};
+        if (int rc = check(launch_correction(stream_, c, block_), "correction/project")) return rc;
+    }
+    const float4* xK = r.iterate(K, K, diff);
+    if (K == 0) {
+        if (int rc = check(launch_reconstruct(stream_, count_, d_scenes_, r.cell, r.topology, previous, r.sorted_index,
+                                              out_positions, r.velocity),
+                           "reconstruct"))
+            return rc;
+    }
+    VorticityArgs v{gc, xK, r.velocity, r.vorticity};
+    if (int rc = check(launch_vorticity(stream_, v, block_), "vorticity")) return rc;
+    NormalArgs nm{gc, xK, r.velocity, r.vorticity, r.normal, r.confined};
+    if (int rc = check(launch_normal(stream_, nm, block_), "normal/confinement")) return rc;
+    XsphArgs x{gc, xK, r.confined, r.sorted_index, {next_state->velocities.x, next_state->velocities.y, next_state->velocities.z}};
+    if (int rc = check(launch_xsph(stream_, x, block_), "xsph")) return rc;
+    next_state->step_index = state->step_index + 1u;
+    r.valid = true;
+    r.step_index = state->step_index;
+    return PBF_SUCCESS;
+}
+
+int Engine::read(const StepRecord& r, const pbf_cache_field field, void* destination, const size_t bytes) {
+    const uint32_t n = count_;
+    const bool diff = differentiable();
+    if (field == PBF_CACHE_GRID_RESOLUTION) {
+        if (!destination || bytes < 3 * sizeof(uint32_t)) {
+            set_error("destination too small");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        std::memcpy(destination, scenes_[0].dims, 3 * sizeof(uint32_t));
+        return PBF_SUCCESS;
+    }
+    if (!r.valid) {
+        set_error("step cache holds no step yet");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    size_t need = 0;
+    switch (field) {
+        case PBF_CACHE_SORTED_PARTICLE_INDICES: need = n * sizeof(uint32_t); break;
+        case PBF_CACHE_CELL_OFFSETS: need = (cells_ + 1) * sizeof(uint32_t); break;
+        case PBF_CACHE_SORTED_KEYS: need = n * sizeof(uint64_t); break;
+        case PBF_CACHE_VORTICITY_MAGNITUDES:
+        case PBF_CACHE_VORTICITY_NORMALIZERS:
+        case PBF_CACHE_FIRST_DENSITIES:
+        case PBF_CACHE_FIRST_LAMBDAS:
+        case PBF_CACHE_NEIGHBOR_COUNTS: need = n * sizeof(float); break;
+        case PBF_CACHE_PREDICTED_POSITIONS:
+        case PBF_CACHE_CORRECTED_POSITIONS:
+        case PBF_CACHE_RECONSTRUCTED_VELOCITIES:
+        case PBF_CACHE_VORTICITIES:
+        case PBF_CACHE_VORTICITY_NORMALS:
+        case PBF_CACHE_CONFINED_VELOCITIES: need = 3ull * n * sizeof(float); break;
+        default: set_error("unknown cache field"); return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (!destination || bytes < need) {
+        set_error("destination too small for the requested field");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (n == 0 && field != PBF_CACHE_CELL_OFFSETS) return PBF_SUCCESS;
+    float* f = static_cast<float*>(destination);
+    auto vec = [&](const float4* src) {
+        return launch_unsort_float4(stream_, n, r.sorted_index, src, 3, f, f + n, f + 2ull * n, nullptr);
+    };
+    auto w = [&](const float4* src) { return launch_unsort_float4(stream_, n, r.sorted_index, src, 0, nullptr, nullptr, nullptr, f); };
+    cudaError_t e = cudaSuccess;
+    switch (field) {
+        case PBF_CACHE_SORTED_PARTICLE_INDICES:
+            e = cudaMemcpyAsync(destination, r.sorted_index, need, cudaMemcpyDeviceToDevice, stream_);
+            break;
+        case PBF_CACHE_CELL_OFFSETS:
+            e = cudaMemcpyAsync(destination, r.cell_offsets, need, cudaMemcpyDeviceToDevice, stream_);
+            break;
+        case PBF_CACHE_SORTED_KEYS:
+            e = launch_sorted_keys(stream_, n, r.sorted_index, r.keys, static_cast<unsigned long long*>(destination));
+            break;
+        case PBF_CACHE_PREDICTED_POSITIONS: e = vec(r.topology); break;
+        case PBF_CACHE_CORRECTED_POSITIONS: e = vec(r.iterate(iterations_, iterations_, diff)); break;
+        case PBF_CACHE_RECONSTRUCTED_VELOCITIES: e = vec(r.velocity); break;
+        case PBF_CACHE_VORTICITIES: e = vec(r.vorticity); break;
+        case PBF_CACHE_VORTICITY_MAGNITUDES: e = w(r.vorticity); break;
+        case PBF_CACHE_VORTICITY_NORMALS: e = vec(r.normal); break;
+        case PBF_CACHE_VORTICITY_NORMALIZERS: e = w(r.normal); break;
+        case PBF_CACHE_CONFINED_VELOCITIES: e = vec(r.confined); break;
+        case PBF_CACHE_FIRST_DENSITIES:
+            if (iterations_ == 0) { set_error("no Jacobi iteration ran"); return PBF_ERROR_INVALID_ARGUMENT; }
+            e = launch_unsort_scalar(stream_, n, r.sorted_index, diff ? r.density[0] : r.first_density, 4, destination);
+            break;
+        case PBF_CACHE_FIRST_LAMBDAS:
+            if (iterations_ == 0) { set_error("no Jacobi iteration ran"); return PBF_ERROR_INVALID_ARGUMENT; }
+            e = launch_unsort_scalar(stream_, n, r.sorted_index, diff ? r.lambda[0] : r.first_lambda, 4, destination);
+            break;
+        case PBF_CACHE_NEIGHBOR_COUNTS:
+            if (iterations_ == 0) { set_error("no Jacobi iteration ran"); return PBF_ERROR_INVALID_ARGUMENT; }
+            e = launch_unsort_scalar(stream_, n, r.sorted_index, r.neighbor_count, 4, destination);
+            break;
+        default: break;
+    }
+    return check(e, "read step cache");
+}
+
+int Engine::read_iteration(const StepRecord& r, const pbf_iteration_field field, const uint32_t k, void* destination,
+                           const size_t bytes) {
+    const uint32_t n = count_, K = iterations_;
+    const bool diff = differentiable();
+    if (!r.valid) {
+        set_error("step cache holds no step yet");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    const bool vec = field == PBF_ITERATION_POSITIONS || field == PBF_ITERATION_GRADIENT_SUMS;
+    const size_t need = (vec ? 3ull : 1ull) * n * 4ull;
+    if (!destination || bytes < need) {
+        set_error("destination too small for the requested field");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (field == PBF_ITERATION_POSITIONS) {
+        if (k > K || (!diff && k != 0 && k != K)) {
+            set_error("iteration positions exist for 0..K (every k only in differentiable mode)");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+    } else if (!diff || k >= K) {
+        set_error("per-iteration fields need differentiable mode and iteration < K");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (n == 0) return PBF_SUCCESS;
+    float* f = static_cast<float*>(destination);
+    cudaError_t e = cudaSuccess;
+    switch (field) {
+        case PBF_ITERATION_POSITIONS:
+            e = launch_unsort_float4(stream_, n, r.sorted_index, r.iterate(k, K, diff), 3, f, f + n, f + 2ull * n, nullptr);
+            break;
+        case PBF_ITERATION_DENSITIES: e = launch_unsort_scalar(stream_, n, r.sorted_index, r.density[k], 4, destination); break;
+        case PBF_ITERATION_LAMBDAS: e = launch_unsort_scalar(stream_, n, r.sorted_index, r.lambda[k], 4, destination); break;
+        case PBF_ITERATION_GRADIENT_SUMS:
+            e = launch_unsort_float4(stream_, n, r.sorted_index, r.gsum[k], 3, f, f + n, f + 2ull * n, nullptr);
+            break;
+        case PBF_ITERATION_DENOMINATORS:
+            e = launch_unsort_float4(stream_, n, r.sorted_index, r.gsum[k], 0, nullptr, nullptr, nullptr, f);
+            break;
+        case PBF_ITERATION_COLLISION_MASKS:
+            e = launch_unsort_mask(stream_, n, r.sorted_index, r.mask[k], static_cast<uint32_t*>(destination));
+            break;
+        default: set_error("unknown iteration field"); return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    return check(e, "read iteration field");
+}
+
+}  // namespace pbf

@@ -1,0 +1,147 @@
+// Host-side engine of the PBF substep: device buffers, the scene table and the launch
+// sequence of one forward / reverse substep.  One scene is a pbf_solver; many scenes
+// advancing together are a pbf_batch.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/physica_pbf.h"
+#include "pbf_internal.h"
+#include "pbf_launch.h"
+
+namespace pbf {
+
+void set_error(const std::string& message);
+
+// Stream-ordered device allocations released together.
+class DeviceArena {
+public:
+    explicit DeviceArena(cudaStream_t stream = nullptr) : stream_(stream) {}
+    DeviceArena(const DeviceArena&) = delete;
+    DeviceArena& operator=(const DeviceArena&) = delete;
+    ~DeviceArena() { release(); }
+    void set_stream(cudaStream_t s) { stream_ = s; }
+    template <class T>
+    T* alloc(size_t count, cudaError_t& err) {
+        void* p = nullptr;
+        if (err != cudaSuccess) return nullptr;
+        const size_t bytes = count ? count * sizeof(T) : sizeof(T);
+        err = cudaMallocAsync(&p, bytes, stream_);
+        if (err == cudaSuccess) ptrs_.push_back(p);
+        return static_cast<T*>(p);
+    }
+    void release() {
+        for (void* p : ptrs_) cudaFreeAsync(p, stream_);
+        ptrs_.clear();
+    }
+    size_t size() const { return ptrs_.size(); }
+
+private:
+    cudaStream_t stream_;
+    std::vector<void*> ptrs_;
+};
+
+struct SceneHost {
+    pbf_domain_configuration config;     // boundary pointer cleared
+    std::vector<pbf_boundary_particle> boundary;
+    uint32_t dims[3];
+    uint64_t cells;
+    uint32_t cell_base;
+    uint32_t first;
+};
+
+// Everything one forward substep leaves behind for export and for the reverse pass.
+struct StepRecord {
+    DeviceArena arena;
+    bool valid = false;
+    uint64_t step_index = 0;         // index of the input state
+    uint32_t* cell_offsets = nullptr;
+    uint32_t* sorted_index = nullptr;
+    uint32_t* slot_of = nullptr;
+    uint32_t* keys = nullptr;        // original order
+    int4* cell = nullptr;
+    float4* topology = nullptr;      // x* and mass (iterate 0)
+    float4* params_a = nullptr;
+    float4* params_b = nullptr;
+    std::vector<float4*> positions;  // iterates 1..K (forward mode: 2 ping-pong buffers)
+    std::vector<float*> lambda;      // per iteration (forward mode: 1)
+    std::vector<float*> density;     // per iteration (differentiable mode)
+    std::vector<float4*> gsum;       // per iteration (differentiable mode)
+    std::vector<uint8_t*> mask;      // per iteration (differentiable mode)
+    float* first_density = nullptr;
+    float* first_lambda = nullptr;
+    uint32_t* neighbor_count = nullptr;
+    float4* velocity = nullptr;
+    float4* vorticity = nullptr;
+    float4* normal = nullptr;
+    float4* confined = nullptr;
+
+    const float4* iterate(uint32_t k, uint32_t K, bool differentiable) const {
+        if (k == 0) return topology;
+        if (differentiable) return positions[k - 1];
+        (void)K;
+        return positions[(k - 1) & 1u];
+    }
+};
+
+class Engine {
+public:
+    Engine() = default;
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+    ~Engine();
+
+    int init(const pbf_domain_configuration* scenes, uint32_t scene_count, const pbf_configuration* configuration,
+             pbf_execution_mode mode, cudaStream_t stream);
+    int allocate_record(StepRecord& r);
+    int forward(const pbf_particle_state* state, const pbf_control* control, const pbf_parameters* parameters,
+                pbf_particle_state* next_state, StepRecord& record);
+    int reverse(const pbf_particle_state* state, const pbf_control* control, const pbf_parameters* parameters,
+                const StepRecord& record, const pbf_particle_state_adjoint* next_adjoint,
+                pbf_particle_state_adjoint* previous_adjoint, pbf_control_adjoint* control_adjoint,
+                pbf_parameter_adjoint* parameter_adjoint);
+    int read(const StepRecord& record, pbf_cache_field field, void* destination, size_t bytes);
+    int read_iteration(const StepRecord& record, pbf_iteration_field field, uint32_t iteration, void* destination,
+                       size_t bytes);
+
+    uint32_t count() const { return count_; }
+    uint64_t cells() const { return cells_; }
+    uint32_t iterations() const { return iterations_; }
+    bool differentiable() const { return mode_ == PBF_EXECUTION_DIFFERENTIABLE; }
+    cudaStream_t stream() const { return stream_; }
+    const std::vector<SceneHost>& scenes() const { return scenes_; }
+    void set_block(unsigned block) { block_ = block; }
+
+    int check(cudaError_t e, const char* what);
+
+private:
+    int update_scene_table(uint64_t step_index);
+
+    uint32_t count_ = 0;
+    uint64_t cells_ = 0;
+    uint32_t iterations_ = 0;
+    uint32_t checkpoint_interval_ = 1;
+    pbf_execution_mode mode_ = PBF_EXECUTION_FORWARD;
+    cudaStream_t stream_ = nullptr;
+    unsigned block_ = 128;
+    std::vector<SceneHost> scenes_;
+    std::vector<SceneDesc> scene_table_;
+    DeviceArena arena_;
+    SceneDesc* d_scenes_ = nullptr;
+    KernelConstants* d_constants_ = nullptr;
+    uint32_t* d_scene_of_ = nullptr;
+    // grid-build scratch
+    float4* predicted_ = nullptr;
+    uint32_t* arrival_ = nullptr;
+    uint32_t* unordered_ = nullptr;
+    uint32_t* tile_sums_ = nullptr;
+    uint64_t table_step_ = ~0ull;
+    friend struct AdjointWorkspace;
+    void* adjoint_ = nullptr;  // AdjointWorkspace*, differentiable mode
+};
+
+}  // namespace pbf

@@ -1,0 +1,524 @@
+// Forward neighbour-gather passes of the PBF substep over cell-sorted particles.
+//
+// Reference passes and the fused kernels that replace them:
+//   density (density/density.cu:18-40) + lambda (pbf/pbf.cu:95-127)    -> density_lambda_kernel
+//   correction (pbf/pbf.cu:254-288) + project (pbf/pbf.cu:417-431)
+//     [+ reconstruct (pbf/pbf.cu:456-460) on the last iteration]        -> correction_kernel
+//   vorticity (pbf/pbf.cu:476-497) + magnitude (pbf/pbf.cu:565-569)    -> vorticity_kernel
+//   normal (pbf/pbf.cu:571-593) + confinement (pbf/pbf.cu:674-678)     -> normal_kernel
+//   XSPH (pbf/pbf.cu:700-721) + write-back of next_state               -> xsph_kernel
+//
+// One thread owns one cell-sorted particle.  It walks the 27 stencil cells in the
+// reference order (x offset outer, z inner; particles of a cell in ascending original
+// index, which is their sorted order) and, in a first phase, keeps only candidates whose
+// squared distance is below the pass's exact support threshold, appending their sorted
+// slots to a per-thread list in shared memory.  The list is drained in order with the
+// reference's per-pair expressions, so every per-particle sum is accumulated in the
+// reference's order and equals it bit for bit; skipped candidates contribute an exact
+// zero in the reference.  The list keeps the costly per-pair math (sqrt, divisions)
+// convergent across the warp instead of running under a 15%-taken branch.
+#include "pbf_internal.h"
+#include "pbf_launch.h"
+
+namespace pbf {
+
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kListCap = 16;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Walks the candidates of one particle's 27-cell stencil in reference order.
+struct Walker {
+    const uint32_t* offsets;
+    uint32_t nx, ny, nz, base;
+    int cx, cy, cz;
+    int next_cell;
+    uint32_t cur, end;
+
+    __device__ __forceinline__ void init(const uint32_t* cell_offsets, const Grid& g, const int4 c, const bool active) {
+        offsets = cell_offsets;
+        nx = g.cells_x; ny = g.cells_y; nz = g.cells_z; base = g.cell_base;
+        cx = c.x; cy = c.y; cz = c.z;
+        next_cell = active ? 0 : 27;
+        cur = end = 0;
+    }
+
+    __device__ __forceinline__ bool next(uint32_t& t) {
+        while (cur == end) {
+            if (next_cell >= 27) return false;
+            const int o = next_cell++;
+            const int x = cx + o / 9 - 1, y = cy + (o / 3) % 3 - 1, z = cz + o % 3 - 1;
+            if (x < 0 || y < 0 || z < 0 || x >= static_cast<int>(nx) || y >= static_cast<int>(ny) || z >= static_cast<int>(nz)) continue;
+            const uint32_t c = base + (static_cast<uint32_t>(z) * ny + static_cast<uint32_t>(y)) * nx + static_cast<uint32_t>(x);
+            cur = offsets[c];
+            end = offsets[c + 1];
+        }
+        t = cur++;
+        return true;
+    }
+};
+
+// Two-phase gather: accept() filters candidates in stencil order into the per-thread
+// list; process() consumes them in the same order.  All lanes stay in the loop until
+// every lane is exhausted so the warp votes are well defined.
+template <class Op>
+__device__ __forceinline__ void gather(Op& op, Walker& w, const bool active) {
+    __shared__ uint32_t lists[kListCap * kBlock];
+    uint32_t* list = lists + threadIdx.x;
+    int n = 0;
+    bool more = active;
+    while (__any_sync(kFull, more)) {
+        if (more) {
+            uint32_t t;
+            more = w.next(t);
+            if (more && op.accept(t)) {
+                list[n * kBlock] = t;
+                ++n;
+            }
+        }
+        if (__any_sync(kFull, n == kListCap)) {
+            for (int k = 0; k < n; ++k) op.process(list[k * kBlock]);
+            n = 0;
+        }
+    }
+    for (int k = 0; k < n; ++k) op.process(list[k * kBlock]);
+}
+
+struct Particle {
+    uint32_t s;
+    bool active;
+    int4 c;
+    const SceneDesc* scene;
+    KernelConstants k;
+};
+
+__device__ __forceinline__ Particle locate(const GatherCommon& g) {
+    Particle p;
+    p.s = blockIdx.x * blockDim.x + threadIdx.x;
+    p.active = p.s < g.count;
+    p.c = p.active ? g.cell[p.s] : make_int4(0, 0, 0, 0);
+    p.scene = g.scenes + p.c.w;
+    p.k = g.constants[p.scene->constants];
+    return p;
+}
+
+// ------------------------------------------------------------------ density + lambda
+struct DensityLambdaOp {
+    const float4* __restrict__ pos;
+    f3 x;
+    uint32_t self;
+    float rest_density;
+    KernelConstants k;
+    float density;
+    f3 gradient_sum;
+    float denominator;
+    uint32_t neighbors;
+
+    __device__ __forceinline__ bool accept(const uint32_t t) const {
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        return dot(d, d) < k.union_threshold;
+    }
+    __device__ __forceinline__ void process(const uint32_t t) {
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        const float r2 = dot(d, d);
+        if (r2 < k.h2) density += q.w * poly6_inside(r2, k);
+        if (t == self) return;
+        if (r2 < k.h2) ++neighbors;
+        const float distance = sqrtf(r2);
+        if (distance == 0.0F || distance >= k.h) return;
+        const f3 gradient = spiky_gradient_at(d, distance, k);
+        const float coefficient = q.w / rest_density;
+        gradient_sum = gradient_sum + times(gradient, coefficient);
+        denominator += coefficient * coefficient * dot(gradient, gradient);
+    }
+};
+
+__global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLambdaArgs a) {
+    const Particle p = locate(a.g);
+    DensityLambdaOp op;
+    op.pos = a.pos;
+    op.self = p.s;
+    op.k = p.k;
+    const float4 xi = p.active ? a.pos[p.s] : make_float4(0, 0, 0, 0);
+    const float4 pa = p.active ? a.g.params_a[p.s] : make_float4(1, 0, 0, 0);
+    op.x = xyz(xi);
+    op.rest_density = pa.x;
+    op.density = 0.0F;
+    op.gradient_sum = mk(0.0F, 0.0F, 0.0F);
+    op.denominator = pa.y;  // relaxation
+    op.neighbors = 0;
+    Walker w;
+    w.init(a.g.cell_offsets, p.scene->grid, p.c, p.active);
+    gather(op, w, p.active);
+    if (!p.active) return;
+    const float denominator = op.denominator + dot(op.gradient_sum, op.gradient_sum);
+    a.lambda[p.s] = -(op.density / op.rest_density - 1.0F) / denominator;
+    if (a.density) a.density[p.s] = op.density;
+    if (a.gsum_denom) a.gsum_denom[p.s] = make_float4(op.gradient_sum.x, op.gradient_sum.y, op.gradient_sum.z, denominator);
+    if (a.neighbor_count) a.neighbor_count[p.s] = op.neighbors;
+}
+
+// ------------------------------------------------------- correction + project
+struct CorrectionOp {
+    const float4* __restrict__ pos;
+    const float* __restrict__ lambda;
+    f3 x;
+    uint32_t self;
+    float rest_density;
+    float lambda_i;
+    float strength, exponent, reference_weight;
+    bool artificial_full;
+    KernelConstants k;
+    f3 correction;
+
+    __device__ __forceinline__ bool accept(const uint32_t t) const {
+        if (t == self) return false;
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        const float r2 = dot(d, d);
+        return r2 > 0.0F && r2 < k.spiky_threshold;
+    }
+    __device__ __forceinline__ void process(const uint32_t t) {
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        const float r2 = dot(d, d);
+        const float distance = sqrtf(r2);
+        if (distance == 0.0F || distance >= k.h) return;
+        // s_corr of pbf/pbf.cu:56-71; with zero strength it is -strength * ratio^n = -0 inside
+        // the poly6 support and 0 outside, which is what the fast branch yields.
+        float artificial;
+        if (artificial_full) {
+            const float weight = r2 >= k.h2 ? 0.0F : poly6_inside(r2, k);
+            artificial = weight == 0.0F ? 0.0F : -strength * powf(weight / reference_weight, exponent);
+        } else {
+            artificial = r2 < k.h2 ? -strength : 0.0F;
+        }
+        const float coefficient = q.w / rest_density;
+        correction = correction + times(spiky_gradient_at(d, distance, k), coefficient * (lambda_i + lambda[t] + artificial));
+    }
+};
+
+__global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs a) {
+    const Particle p = locate(a.g);
+    CorrectionOp op;
+    op.pos = a.pos;
+    op.lambda = a.lambda;
+    op.self = p.s;
+    op.k = p.k;
+    const float4 xi = p.active ? a.pos[p.s] : make_float4(0, 0, 0, 0);
+    const float4 pa = p.active ? a.g.params_a[p.s] : make_float4(1, 0, 0, 0);
+    const float4 pb = p.active ? a.g.params_b[p.s] : make_float4(0, 0, 0, 0);
+    op.x = xyz(xi);
+    op.rest_density = pa.x;
+    op.lambda_i = p.active ? a.lambda[p.s] : 0.0F;
+    op.strength = pb.x;
+    op.exponent = pb.y;
+    op.artificial_full = pb.x != 0.0F;
+    op.reference_weight = op.artificial_full ? poly6(mk(pb.z, 0.0F, 0.0F), p.k) : 1.0F;
+    op.correction = mk(0.0F, 0.0F, 0.0F);
+    Walker w;
+    w.init(a.g.cell_offsets, p.scene->grid, p.c, p.active);
+    gather(op, w, p.active);
+    if (!p.active) return;
+    const Box& box = p.scene->box;
+    const f3 candidate = op.x + op.correction;
+    uint32_t mask = 0u;
+    if (candidate.x < box.min_x || candidate.x > box.max_x) mask |= 1u;
+    if (candidate.y < box.min_y || candidate.y > box.max_y) mask |= 2u;
+    if (candidate.z < box.min_z || candidate.z > box.max_z) mask |= 4u;
+    const f3 projected = mk(fminf(box.max_x, fmaxf(box.min_x, candidate.x)), fminf(box.max_y, fmaxf(box.min_y, candidate.y)),
+                            fminf(box.max_z, fmaxf(box.min_z, candidate.z)));
+    a.pos_next[p.s] = make_float4(projected.x, projected.y, projected.z, xi.w);
+    if (a.mask) a.mask[p.s] = static_cast<uint8_t>(mask);
+    if (a.last) {
+        const uint32_t i = a.sorted_index[p.s];
+        const f3 previous = mk(a.previous_positions.x[i], a.previous_positions.y[i], a.previous_positions.z[i]);
+        const f3 velocity = times(projected - previous, p.scene->inverse_time_step);
+        a.velocity[p.s] = make_float4(velocity.x, velocity.y, velocity.z, 0.0F);
+        a.out_positions.x[i] = projected.x;
+        a.out_positions.y[i] = projected.y;
+        a.out_positions.z[i] = projected.z;
+    }
+}
+
+// ---------------------------------------------------------------- vorticity
+struct SpikyAccept {
+    const float4* __restrict__ pos;
+    f3 x;
+    uint32_t self;
+    KernelConstants k;
+    __device__ __forceinline__ bool accept(const uint32_t t) const {
+        if (t == self) return false;
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        const float r2 = dot(d, d);
+        return r2 > 0.0F && r2 < k.spiky_threshold;
+    }
+};
+
+struct VorticityOp : SpikyAccept {
+    const float4* __restrict__ velocity;
+    f3 v;
+    f3 vorticity;
+    __device__ __forceinline__ void process(const uint32_t t) {
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        const float distance = sqrtf(dot(d, d));
+        if (distance == 0.0F || distance >= k.h) return;
+        vorticity = vorticity + cross(xyz(velocity[t]) - v, spiky_gradient_at(d, distance, k));
+    }
+};
+
+__global__ void __launch_bounds__(kBlock) vorticity_kernel(const VorticityArgs a) {
+    const Particle p = locate(a.g);
+    VorticityOp op;
+    op.pos = a.pos;
+    op.velocity = a.velocity;
+    op.self = p.s;
+    op.k = p.k;
+    op.x = p.active ? xyz(a.pos[p.s]) : mk(0, 0, 0);
+    op.v = p.active ? xyz(a.velocity[p.s]) : mk(0, 0, 0);
+    op.vorticity = mk(0.0F, 0.0F, 0.0F);
+    Walker w;
+    w.init(a.g.cell_offsets, p.scene->grid, p.c, p.active);
+    gather(op, w, p.active);
+    if (!p.active) return;
+    a.vorticity[p.s] = make_float4(op.vorticity.x, op.vorticity.y, op.vorticity.z, norm(op.vorticity));
+}
+
+// ------------------------------------------------------- normal + confinement
+struct NormalOp : SpikyAccept {
+    const float4* __restrict__ vorticity;
+    float magnitude;
+    f3 gradient;
+    __device__ __forceinline__ void process(const uint32_t t) {
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        const float distance = sqrtf(dot(d, d));
+        if (distance == 0.0F || distance >= k.h) return;
+        gradient = gradient + times(spiky_gradient_at(d, distance, k), vorticity[t].w - magnitude);
+    }
+};
+
+__global__ void __launch_bounds__(kBlock) normal_kernel(const NormalArgs a) {
+    const Particle p = locate(a.g);
+    NormalOp op;
+    op.pos = a.pos;
+    op.vorticity = a.vorticity;
+    op.self = p.s;
+    op.k = p.k;
+    const float4 wi = p.active ? a.vorticity[p.s] : make_float4(0, 0, 0, 0);
+    op.x = p.active ? xyz(a.pos[p.s]) : mk(0, 0, 0);
+    op.magnitude = wi.w;
+    op.gradient = mk(0.0F, 0.0F, 0.0F);
+    Walker w;
+    w.init(a.g.cell_offsets, p.scene->grid, p.c, p.active);
+    gather(op, w, p.active);
+    if (!p.active) return;
+    const float normalizer = norm(op.gradient);
+    const f3 normal = normalizer > 0.0F ? times(op.gradient, 1.0F / normalizer) : mk(0.0F, 0.0F, 0.0F);
+    a.normal[p.s] = make_float4(normal.x, normal.y, normal.z, normalizer);
+    const float4 pa = a.g.params_a[p.s];
+    const f3 v = xyz(a.velocity[p.s]);
+    const f3 confined = v + times(cross(normal, xyz(wi)), p.scene->time_step * pa.w);
+    a.confined[p.s] = make_float4(confined.x, confined.y, confined.z, 0.0F);
+}
+
+// ---------------------------------------------------------------------- XSPH
+struct XsphOp {
+    const float4* __restrict__ pos;
+    const float4* __restrict__ confined;
+    f3 x, v;
+    uint32_t self;
+    KernelConstants k;
+    f3 smoothing;
+    __device__ __forceinline__ bool accept(const uint32_t t) const {
+        if (t == self) return false;
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        return dot(d, d) < k.h2;
+    }
+    __device__ __forceinline__ void process(const uint32_t t) {
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        const float r2 = dot(d, d);
+        if (r2 >= k.h2) return;
+        smoothing = smoothing + times(xyz(confined[t]) - v, poly6_inside(r2, k));
+    }
+};
+
+__global__ void __launch_bounds__(kBlock) xsph_kernel(const XsphArgs a) {
+    const Particle p = locate(a.g);
+    XsphOp op;
+    op.pos = a.pos;
+    op.confined = a.confined;
+    op.self = p.s;
+    op.k = p.k;
+    op.x = p.active ? xyz(a.pos[p.s]) : mk(0, 0, 0);
+    op.v = p.active ? xyz(a.confined[p.s]) : mk(0, 0, 0);
+    op.smoothing = mk(0.0F, 0.0F, 0.0F);
+    Walker w;
+    w.init(a.g.cell_offsets, p.scene->grid, p.c, p.active);
+    gather(op, w, p.active);
+    if (!p.active) return;
+    const float viscosity = a.g.params_a[p.s].z;
+    const f3 out = op.v + times(op.smoothing, viscosity);
+    const uint32_t i = a.sorted_index[p.s];
+    a.out_velocities.x[i] = out.x;
+    a.out_velocities.y[i] = out.y;
+    a.out_velocities.z[i] = out.z;
+}
+
+// ------------------------------------------------------------------ constants
+__global__ void constants_kernel(const float* __restrict__ radii, const uint32_t n, KernelConstants* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float h = radii[i];
+    const float squared_radius = h * h;
+    KernelConstants k;
+    k.h = h;
+    k.h2 = squared_radius;
+    k.poly6_denominator = 64.0F * kPi * squared_radius * squared_radius * squared_radius * h * h * h;
+    k.poly6_grad_denominator = 32.0F * kPi * squared_radius * squared_radius * squared_radius * h * h * h;
+    k.spiky_coefficient = -45.0F / (kPi * powf(h, 6.0F));
+    // Smallest float r2 with sqrtf(r2) >= h; sqrtf is monotone, so bisect on the bit pattern.
+    uint32_t lo = 0u, hi = 0x7f800000u;
+    while (hi - lo > 1u) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        if (sqrtf(__uint_as_float(mid)) >= h) hi = mid;
+        else lo = mid;
+    }
+    k.spiky_threshold = __uint_as_float(hi);
+    k.union_threshold = fmaxf(k.h2, k.spiky_threshold);
+    k.poly6_radial_coefficient = 315.0F / (64.0F * kPi * powf(h, 9.0F));
+    k.spiky_coefficient_d = -45.0 / (static_cast<double>(kPi) * pow(static_cast<double>(h), 6.0));
+    out[i] = k;
+}
+
+__global__ void unsort_float4_kernel(const uint32_t count, const uint32_t* __restrict__ sorted_index,
+                                     const float4* __restrict__ in, const int components, float* out_x, float* out_y,
+                                     float* out_z, float* out_w) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    const uint32_t i = sorted_index[s];
+    const float4 v = in[s];
+    if (out_x) out_x[i] = v.x;
+    if (components > 1 && out_y) out_y[i] = v.y;
+    if (components > 2 && out_z) out_z[i] = v.z;
+    if (out_w) out_w[i] = v.w;
+}
+
+__global__ void unsort_mask_kernel(const uint32_t count, const uint32_t* __restrict__ sorted_index,
+                                   const uint8_t* __restrict__ in, uint32_t* __restrict__ out) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    out[sorted_index[s]] = in[s];
+}
+
+__global__ void unsort_scalar_kernel(const uint32_t count, const uint32_t* __restrict__ sorted_index, const uint8_t* in,
+                                     const uint32_t bytes, uint8_t* out) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    const uint32_t i = sorted_index[s];
+    for (uint32_t b = 0; b < bytes; ++b) out[static_cast<size_t>(i) * bytes + b] = in[static_cast<size_t>(s) * bytes + b];
+}
+
+__global__ void reconstruct_kernel(const uint32_t count, const SceneDesc* __restrict__ scenes, const int4* __restrict__ cell,
+                                   const float4* __restrict__ positions, const Field3 previous,
+                                   const uint32_t* __restrict__ sorted_index, const MutField3 out, float4* __restrict__ velocity) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    const SceneDesc& sc = scenes[cell[s].w];
+    const uint32_t i = sorted_index[s];
+    const f3 x = xyz(positions[s]);
+    const f3 v = times(x - mk(previous.x[i], previous.y[i], previous.z[i]), sc.inverse_time_step);
+    velocity[s] = make_float4(v.x, v.y, v.z, 0.0F);
+    out.x[i] = x.x;
+    out.y[i] = x.y;
+    out.z[i] = x.z;
+}
+
+inline unsigned grid_of(const uint32_t n, const unsigned block) { return (n + block - 1) / block; }
+
+}  // namespace
+
+cudaError_t launch_constants(cudaStream_t stream, const float* radii, const uint32_t n, KernelConstants* out) {
+    constants_kernel<<<grid_of(n, 64), 64, 0, stream>>>(radii, n, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_density_lambda(cudaStream_t stream, const DensityLambdaArgs& a, unsigned) {
+    if (a.g.count == 0) return cudaSuccess;
+    density_lambda_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_correction(cudaStream_t stream, const CorrectionArgs& a, unsigned) {
+    if (a.g.count == 0) return cudaSuccess;
+    correction_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vorticity(cudaStream_t stream, const VorticityArgs& a, unsigned) {
+    if (a.g.count == 0) return cudaSuccess;
+    vorticity_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normal(cudaStream_t stream, const NormalArgs& a, unsigned) {
+    if (a.g.count == 0) return cudaSuccess;
+    normal_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_xsph(cudaStream_t stream, const XsphArgs& a, unsigned) {
+    if (a.g.count == 0) return cudaSuccess;
+    xsph_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reconstruct(cudaStream_t stream, const uint32_t count, const SceneDesc* scenes, const int4* cell,
+                               const float4* positions, const Field3 previous_positions, const uint32_t* sorted_index,
+                               const MutField3 out_positions, float4* velocity) {
+    if (count == 0) return cudaSuccess;
+    reconstruct_kernel<<<grid_of(count, 256), 256, 0, stream>>>(count, scenes, cell, positions, previous_positions, sorted_index,
+                                                               out_positions, velocity);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unsort_float4(cudaStream_t stream, const uint32_t count, const uint32_t* sorted_index, const float4* in,
+                                 const int components, float* out_x, float* out_y, float* out_z, float* out_w) {
+    if (count == 0) return cudaSuccess;
+    unsort_float4_kernel<<<grid_of(count, 256), 256, 0, stream>>>(count, sorted_index, in, components, out_x, out_y, out_z, out_w);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unsort_mask(cudaStream_t stream, const uint32_t count, const uint32_t* sorted_index, const uint8_t* in,
+                               uint32_t* out) {
+    if (count == 0) return cudaSuccess;
+    unsort_mask_kernel<<<grid_of(count, 256), 256, 0, stream>>>(count, sorted_index, in, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unsort_scalar(cudaStream_t stream, const uint32_t count, const uint32_t* sorted_index, const void* in,
+                                 const uint32_t bytes, void* out) {
+    if (count == 0) return cudaSuccess;
+    unsort_scalar_kernel<<<grid_of(count, 256), 256, 0, stream>>>(count, sorted_index, static_cast<const uint8_t*>(in), bytes,
+                                                                 static_cast<uint8_t*>(out));
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace pbf

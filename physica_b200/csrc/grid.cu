@@ -1,0 +1,227 @@
+// Uniform-grid build of one substep: predict + cell key, a stable counting sort by cell,
+// and the reorder of every per-particle input into cell-sorted float4 arrays.
+//
+// Reference behaviour (neighborhood/neighborhood.cu:20-70, pbf/pbf.cu:73-78):
+//   key  = (z * cells_y + y) * cells_x + x of the clamped cell of x*,
+//   order = stable sort of (key, original index)  [CUB radix sort in the reference],
+//   cell_offsets[c] = first sorted slot with key >= c, c in [0, C].
+// Here the same order comes from a counting sort: an atomic histogram, an exclusive
+// scan over cells, a scatter, and a per-cell ranking by original index that restores
+// the stable order, so sorted_index / cell_offsets equal the reference's bit for bit.
+// Keys are global across the scenes of a batch (scene cell ranges are disjoint and
+// ordered), so one sort serves one scene or many.
+#include "pbf_internal.h"
+#include "pbf_launch.h"
+
+namespace pbf {
+
+namespace {
+
+__device__ __forceinline__ int clamp_cell(const float q, const uint32_t cells) {
+    return min(static_cast<int>(cells) - 1, max(0, __float2int_rd(q)));
+}
+
+// x* = x + dt (v + dt (g + a)) and the cell key of x*; histogram of keys.
+__global__ void predict_key_kernel(const uint32_t count, const SceneDesc* __restrict__ scenes,
+                                   const uint32_t* __restrict__ scene_of, const Field3 positions,
+                                   const Field3 velocities, const Field3 controls,
+                                   const float* __restrict__ masses, float4* __restrict__ predicted,
+                                   uint32_t* __restrict__ keys, uint32_t* __restrict__ arrival,
+                                   uint32_t* __restrict__ histogram) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const SceneDesc& sc = scenes[scene_of ? scene_of[i] : 0u];
+    const f3 gravity = mk(sc.gravity_x, sc.gravity_y, sc.gravity_z);
+    const f3 v = mk(velocities.x[i], velocities.y[i], velocities.z[i]);
+    const f3 a = mk(controls.x[i], controls.y[i], controls.z[i]);
+    const f3 x = mk(positions.x[i], positions.y[i], positions.z[i]);
+    const float dt = sc.time_step;
+    const f3 predicted_velocity = v + times(gravity + a, dt);
+    const f3 xs = x + times(predicted_velocity, dt);
+    predicted[i] = make_float4(xs.x, xs.y, xs.z, masses[i]);
+    const Grid& g = sc.grid;
+    const int cx = clamp_cell((xs.x - g.key_min_x - g.time * g.key_vel_x) / g.cell_size, g.cells_x);
+    const int cy = clamp_cell((xs.y - g.key_min_y - g.time * g.key_vel_y) / g.cell_size, g.cells_y);
+    const int cz = clamp_cell((xs.z - g.key_min_z - g.time * g.key_vel_z) / g.cell_size, g.cells_z);
+    const uint32_t key = g.cell_base + (static_cast<uint32_t>(cz) * g.cells_y + static_cast<uint32_t>(cy)) * g.cells_x +
+                         static_cast<uint32_t>(cx);
+    keys[i] = key;
+    arrival[i] = atomicAdd(histogram + key, 1u);
+}
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t warp_inclusive(uint32_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += n;
+    }
+    return v;
+}
+
+__global__ void scan_reduce_kernel(const uint32_t* __restrict__ data, const uint64_t n, uint32_t* __restrict__ tile_sums) {
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile;
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint64_t idx = base + static_cast<uint64_t>(k) * kScanThreads + threadIdx.x;
+        if (idx < n) s += data[idx];
+    }
+    // warp + block reduction
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __shared__ uint32_t partial[kScanThreads / 32];
+    if ((threadIdx.x & 31) == 0) partial[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint32_t t = threadIdx.x < kScanThreads / 32 ? partial[threadIdx.x] : 0u;
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (threadIdx.x == 0) tile_sums[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of the tile sums by one block, in chunks.
+__global__ void scan_tiles_kernel(uint32_t* __restrict__ tile_sums, const uint32_t tiles) {
+    __shared__ uint32_t carry_s;
+    __shared__ uint32_t warp_tot[kScanThreads / 32];
+    if (threadIdx.x == 0) carry_s = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < tiles; base += kScanThreads) {
+        const uint32_t idx = base + threadIdx.x;
+        const uint32_t v = idx < tiles ? tile_sums[idx] : 0u;
+        const uint32_t inc = warp_inclusive(v);
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 31) warp_tot[warp] = inc;
+        __syncthreads();
+        uint32_t warp_prefix = 0, chunk_total = 0;
+        for (int w = 0; w < kScanThreads / 32; ++w) {
+            if (w < warp) warp_prefix += warp_tot[w];
+            chunk_total += warp_tot[w];
+        }
+        const uint32_t carry = carry_s;
+        if (idx < tiles) tile_sums[idx] = carry + warp_prefix + inc - v;
+        __syncthreads();
+        if (threadIdx.x == 0) carry_s = carry + chunk_total;
+        __syncthreads();
+    }
+}
+
+// In-place exclusive scan of each tile plus its tile prefix: histogram -> cell offsets.
+__global__ void scan_apply_kernel(uint32_t* __restrict__ data, const uint64_t n, const uint32_t* __restrict__ tile_sums) {
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile;
+    // each thread owns kScanItems consecutive elements
+    uint32_t vals[kScanItems];
+    uint32_t local = 0;
+    const uint64_t first = base + static_cast<uint64_t>(threadIdx.x) * kScanItems;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint64_t idx = first + k;
+        vals[k] = idx < n ? data[idx] : 0u;
+        local += vals[k];
+    }
+    __shared__ uint32_t warp_tot[kScanThreads / 32];
+    const uint32_t inc = warp_inclusive(local);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    uint32_t warp_prefix = 0;
+    for (int w = 0; w < warp; ++w) warp_prefix += warp_tot[w];
+    uint32_t running = tile_sums[blockIdx.x] + warp_prefix + inc - local;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint64_t idx = first + k;
+        if (idx < n) data[idx] = running;
+        running += vals[k];
+    }
+}
+
+__global__ void scatter_kernel(const uint32_t count, const uint32_t* __restrict__ keys, const uint32_t* __restrict__ arrival,
+                               const uint32_t* __restrict__ cell_offsets, uint32_t* __restrict__ unordered) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    unordered[cell_offsets[keys[i]] + arrival[i]] = i;
+}
+
+// Restore ascending original index inside each cell and gather the sorted arrays.
+__global__ void reorder_kernel(const uint32_t count, const SceneDesc* __restrict__ scenes,
+                               const uint32_t* __restrict__ scene_of, const uint32_t* __restrict__ keys,
+                               const uint32_t* __restrict__ cell_offsets, const uint32_t* __restrict__ unordered,
+                               const float4* __restrict__ predicted, const ParamPointers params,
+                               uint32_t* __restrict__ sorted_index, uint32_t* __restrict__ slot_of,
+                               int4* __restrict__ cell, float4* __restrict__ topology, float4* __restrict__ params_a,
+                               float4* __restrict__ params_b) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint32_t i = unordered[t];
+    const uint32_t key = keys[i];
+    const uint32_t first = cell_offsets[key], last = cell_offsets[key + 1u];
+    uint32_t rank = 0;
+    for (uint32_t u = first; u < last; ++u) rank += unordered[u] < i ? 1u : 0u;
+    const uint32_t s = first + rank;
+    sorted_index[s] = i;
+    slot_of[i] = s;
+    const float4 xs = predicted[i];
+    topology[s] = xs;
+    const uint32_t scene = scene_of ? scene_of[i] : 0u;
+    const Grid& g = scenes[scene].grid;
+    // gather-side cell of x* (neighborhood/device.cuh:44-48)
+    const int cx = clamp_cell((xs.x - g.origin_x) / g.cell_size, g.cells_x);
+    const int cy = clamp_cell((xs.y - g.origin_y) / g.cell_size, g.cells_y);
+    const int cz = clamp_cell((xs.z - g.origin_z) / g.cell_size, g.cells_z);
+    cell[s] = make_int4(cx, cy, cz, static_cast<int>(scene));
+    params_a[s] = make_float4(params.rest_densities[i], params.relaxation[i], params.xsph[i], params.vorticity[i]);
+    params_b[s] = make_float4(params.strength[i], params.exponent[i], params.radius[i], 0.0F);
+}
+
+// Sorted keys as the reference stores them (uint64), for inspection.
+__global__ void sorted_keys_kernel(const uint32_t count, const uint32_t* __restrict__ sorted_index,
+                                   const uint32_t* __restrict__ keys, unsigned long long* __restrict__ out) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    out[s] = keys[sorted_index[s]];
+}
+
+inline unsigned blocks_for(const uint64_t n, const unsigned threads) { return static_cast<unsigned>((n + threads - 1) / threads); }
+
+}  // namespace
+
+size_t scan_tile_count(const uint64_t n) { return static_cast<size_t>((n + kScanTile - 1) / kScanTile); }
+
+cudaError_t launch_grid_build(cudaStream_t stream, const GridBuildArgs& a) {
+    const unsigned tpb = 256;
+    cudaError_t e = cudaMemsetAsync(a.cell_offsets, 0, (a.cells + 1) * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    if (a.count > 0) {
+        predict_key_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.scenes, a.scene_of, a.positions,
+                                                                         a.velocities, a.controls, a.params.masses,
+                                                                         a.predicted, a.keys, a.arrival, a.cell_offsets);
+        count_launch();
+    }
+    const uint64_t n = a.cells + 1;
+    const unsigned tiles = static_cast<unsigned>(scan_tile_count(n));
+    scan_reduce_kernel<<<tiles, kScanThreads, 0, stream>>>(a.cell_offsets, n, a.tile_sums);
+    scan_tiles_kernel<<<1, kScanThreads, 0, stream>>>(a.tile_sums, tiles);
+    scan_apply_kernel<<<tiles, kScanThreads, 0, stream>>>(a.cell_offsets, n, a.tile_sums);
+    count_launch(3);
+    if (a.count > 0) {
+        scatter_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.keys, a.arrival, a.cell_offsets, a.unordered);
+        reorder_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(
+            a.count, a.scenes, a.scene_of, a.keys, a.cell_offsets, a.unordered, a.predicted, a.params, a.sorted_index,
+            a.slot_of, a.cell, a.topology, a.params_a, a.params_b);
+        count_launch(2);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sorted_keys(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const uint32_t* keys,
+                               unsigned long long* out) {
+    if (count == 0) return cudaSuccess;
+    sorted_keys_kernel<<<blocks_for(count, 256), 256, 0, stream>>>(count, sorted_index, keys, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace pbf

@@ -1,0 +1,119 @@
+// Launcher declarations and argument blocks of the PBF kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pbf_internal.h"
+
+namespace pbf {
+
+void count_launch(unsigned n = 1);
+uint64_t launch_count();
+
+struct GridBuildArgs {
+    uint32_t count;
+    uint64_t cells;
+    const SceneDesc* scenes;
+    const uint32_t* scene_of;      // original particle -> scene (null: one scene)
+    Field3 positions, velocities, controls;
+    ParamPointers params;
+    float4* predicted;             // original order, x* and mass
+    uint32_t* keys;                // original order
+    uint32_t* arrival;             // original order
+    uint32_t* cell_offsets;        // cells + 1
+    uint32_t* tile_sums;
+    uint32_t* unordered;
+    uint32_t* sorted_index;
+    uint32_t* slot_of;
+    int4* cell;
+    float4* topology;
+    float4* params_a;
+    float4* params_b;
+};
+
+size_t scan_tile_count(uint64_t n);
+cudaError_t launch_grid_build(cudaStream_t stream, const GridBuildArgs& args);
+cudaError_t launch_sorted_keys(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const uint32_t* keys,
+                               unsigned long long* out);
+
+// Common inputs of every neighbour-gather pass.
+struct GatherCommon {
+    uint32_t count;
+    const SceneDesc* scenes;
+    const KernelConstants* constants;
+    const uint32_t* cell_offsets;
+    const int4* cell;
+    const float4* params_a;
+    const float4* params_b;
+};
+
+struct DensityLambdaArgs {
+    GatherCommon g;
+    const float4* pos;         // current iterate x_k (and mass)
+    float* lambda;
+    float* density;            // optional record
+    float4* gsum_denom;        // optional record: gradient sum S and denominator D
+    uint32_t* neighbor_count;  // optional: poly6 in-radius neighbours, self excluded
+};
+
+struct CorrectionArgs {
+    GatherCommon g;
+    const float4* pos;
+    const float* lambda;
+    float4* pos_next;
+    uint8_t* mask;             // optional record of the collision mask
+    int last;                  // last iteration: reconstruct velocities and write positions out
+    Field3 previous_positions; // original order (state.positions)
+    const uint32_t* sorted_index;
+    MutField3 out_positions;   // original order (next_state.positions)
+    float4* velocity;          // reconstructed velocity (sorted)
+};
+
+struct VorticityArgs {
+    GatherCommon g;
+    const float4* pos;
+    const float4* velocity;
+    float4* vorticity;         // (omega, |omega|)
+};
+
+struct NormalArgs {
+    GatherCommon g;
+    const float4* pos;
+    const float4* velocity;
+    const float4* vorticity;
+    float4* normal;            // (N, normalizer)
+    float4* confined;          // confined velocity
+};
+
+struct XsphArgs {
+    GatherCommon g;
+    const float4* pos;
+    const float4* confined;
+    const uint32_t* sorted_index;
+    MutField3 out_velocities;  // original order (next_state.velocities)
+};
+
+cudaError_t launch_constants(cudaStream_t stream, const float* support_radii, uint32_t n, KernelConstants* out);
+cudaError_t launch_density_lambda(cudaStream_t stream, const DensityLambdaArgs& a, unsigned block);
+cudaError_t launch_correction(cudaStream_t stream, const CorrectionArgs& a, unsigned block);
+cudaError_t launch_vorticity(cudaStream_t stream, const VorticityArgs& a, unsigned block);
+cudaError_t launch_normal(cudaStream_t stream, const NormalArgs& a, unsigned block);
+cudaError_t launch_xsph(cudaStream_t stream, const XsphArgs& a, unsigned block);
+// Reconstruct velocities and write positions when no Jacobi iteration runs (K = 0).
+cudaError_t launch_reconstruct(cudaStream_t stream, uint32_t count, const SceneDesc* scenes, const int4* cell,
+                               const float4* positions, Field3 previous_positions, const uint32_t* sorted_index,
+                               MutField3 out_positions, float4* velocity);
+
+// FP64 dst[f][i] += src[f][i] for up to six fields.
+cudaError_t launch_accumulate(cudaStream_t stream, size_t count, const double* const* src, double* const* dst, int fields);
+
+// Inspection helpers: scatter sorted arrays back to original order.
+cudaError_t launch_unsort_float4(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const float4* in,
+                                 int components, float* out_x, float* out_y, float* out_z, float* out_w);
+cudaError_t launch_unsort_mask(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const uint8_t* in,
+                               uint32_t* out);
+cudaError_t launch_unsort_scalar(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const void* in,
+                                 uint32_t element_bytes, void* out);
+
+}  // namespace pbf

@@ -1,0 +1,220 @@
+"""Seeded synthetic dam-break scenes for the PBF substep.
+
+Every scene is generated on the host from one counter-based SplitMix64 stream,
+so the same seed gives byte-identical float32 inputs to the CUDA solver, the
+reference kernels and the FP64 host oracle.
+
+The workloads follow the particle module's dam-break example
+(examples/fluids/liquid/pbf-dam-break/simulation.ixx:16-21,62-79,83-112):
+mass = rest_density * spacing^3, relaxation 1000, artificial pressure
+strength 0 / exponent 4 / radius 0.3 h, a static box with no boundary
+particles.  Lattice point (i, j, k) sits at box_min + (i+1, j+1, k+1) * spacing
+plus a uniform jitter of +-0.01 h per axis.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(seed: int, count: int, stream: int = 0) -> np.ndarray:
+    """Counter-based SplitMix64: element i is the mix of seed + (stream, i)."""
+    with np.errstate(over="ignore"):
+        base = np.uint64(seed & 0xFFFFFFFFFFFFFFFF) + np.uint64(stream) * np.uint64(0xD1B54A32D192ED03)
+        z = base + (np.arange(1, count + 1, dtype=np.uint64) * _GOLDEN)
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform01(seed: int, count: int, stream: int = 0) -> np.ndarray:
+    """Float64 uniforms in [0, 1) with 53 random bits."""
+    return (splitmix64(seed, count, stream) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def normal(seed: int, count: int, stream: int = 0) -> np.ndarray:
+    """Standard normals by Box-Muller from two uniform streams."""
+    u1 = uniform01(seed, count, 2 * stream + 1)
+    u2 = uniform01(seed, count, 2 * stream + 2)
+    u1 = np.maximum(u1, 1e-300)
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * math.pi * u2)
+
+
+@dataclasses.dataclass
+class Scene:
+    """One dam-break scene: float32 SoA state plus the domain description."""
+
+    positions: np.ndarray          # (3, N) float32
+    velocities: np.ndarray         # (3, N) float32
+    controls: np.ndarray           # (3, N) float32 external accelerations
+    masses: np.ndarray             # (N,) float32
+    rest_densities: np.ndarray
+    relaxation: np.ndarray
+    artificial_pressure_strength: np.ndarray
+    artificial_pressure_exponent: np.ndarray
+    artificial_pressure_radius: np.ndarray
+    xsph_viscosity: np.ndarray
+    vorticity_confinement: np.ndarray
+    time_step: float
+    support_radius: float
+    particle_radius: float
+    gravity: tuple
+    box_min: tuple
+    box_max: tuple
+    box_velocity: tuple
+    pressure_iterations: int
+    name: str = ""
+    targets: np.ndarray | None = None  # (3, N) float32 target cloud for the loss
+
+    @property
+    def count(self) -> int:
+        return int(self.positions.shape[1])
+
+    def grid_dims(self) -> tuple:
+        h = np.float32(self.support_radius)
+        return tuple(int(np.ceil(np.float32(np.float32(self.box_max[a]) - np.float32(self.box_min[a])) / h)) for a in range(3))
+
+    def parameter_arrays(self) -> dict:
+        return {
+            "masses": self.masses,
+            "rest_densities": self.rest_densities,
+            "relaxation": self.relaxation,
+            "artificial_pressure_strength": self.artificial_pressure_strength,
+            "artificial_pressure_exponent": self.artificial_pressure_exponent,
+            "artificial_pressure_radius": self.artificial_pressure_radius,
+            "xsph_viscosity": self.xsph_viscosity,
+            "vorticity_confinement": self.vorticity_confinement,
+        }
+
+
+H = 0.025
+SPACING = 0.5 * H
+
+
+def dam_break(lattice, box_min, box_max, seed, iterations, *, h=H, dt=1.0 / 120.0,
+              velocity_sigma=0.0, xsph=0.01, vorticity=1e-4, gravity=(0.0, -9.8, 0.0),
+              fill_order="zyx", count=None, name="") -> Scene:
+    """Jittered lattice in the low corner of a box.
+
+    fill_order "zyx" fills x fastest, then y, then z (the example's order);
+    "yzx" fills x fastest, then z, then y (used by the batched scenes, which
+    truncate the lattice at an exact particle count).
+    """
+    nx, ny, nz = lattice
+    spacing = np.float64(0.5 * h)
+    if fill_order == "zyx":
+        k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    else:
+        j, k, i = np.meshgrid(np.arange(ny), np.arange(nz), np.arange(nx), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    if count is not None:
+        i, j, k = i[:count], j[:count], k[:count]
+    n = i.size
+    jitter = (uniform01(seed, 3 * n, 0).reshape(3, n) * 2.0 - 1.0) * (0.01 * h)
+    pos = np.empty((3, n), dtype=np.float32)
+    pos[0] = (box_min[0] + (i + 1) * spacing + jitter[0]).astype(np.float32)
+    pos[1] = (box_min[1] + (j + 1) * spacing + jitter[1]).astype(np.float32)
+    pos[2] = (box_min[2] + (k + 1) * spacing + jitter[2]).astype(np.float32)
+    if velocity_sigma > 0.0:
+        vel = (normal(seed, 3 * n, 1).reshape(3, n) * velocity_sigma).astype(np.float32)
+    else:
+        vel = np.zeros((3, n), dtype=np.float32)
+    f32 = np.float32
+    full = lambda value: np.full(n, value, dtype=np.float32)
+    return Scene(
+        positions=pos,
+        velocities=vel,
+        controls=np.zeros((3, n), dtype=np.float32),
+        masses=full(f32(1000.0) * f32(spacing) * f32(spacing) * f32(spacing)),
+        rest_densities=full(1000.0),
+        relaxation=full(1000.0),
+        artificial_pressure_strength=full(0.0),
+        artificial_pressure_exponent=full(4.0),
+        artificial_pressure_radius=full(f32(0.3) * f32(h)),
+        # The reference's XSPH and confinement sums (pbf/pbf.cu:476-497, 674-678, 700-721)
+        # carry no particle volume m_j/rho_j, so the physical coefficients c and eps are
+        # stored premultiplied by the particle volume V = m/rho0 = spacing^3.
+        xsph_viscosity=full(f32(xsph) * f32(spacing) ** 3),
+        vorticity_confinement=full(f32(vorticity) * f32(spacing) ** 3),
+        time_step=float(f32(dt)),
+        support_radius=float(f32(h)),
+        particle_radius=float(f32(0.2) * f32(h)),
+        gravity=tuple(float(f32(g)) for g in gravity),
+        box_min=tuple(float(f32(b)) for b in box_min),
+        box_max=tuple(float(f32(b)) for b in box_max),
+        box_velocity=(0.0, 0.0, 0.0),
+        pressure_iterations=iterations,
+        name=name,
+    )
+
+
+def target_cloud(seed: int, n: int, lo=(0.25, 0.0, 0.25), hi=(0.75, 0.5, 0.75)) -> np.ndarray:
+    u = uniform01(seed ^ 0x7A7A7A7A, 3 * n, 7).reshape(3, n)
+    out = np.empty((3, n), dtype=np.float32)
+    for a in range(3):
+        out[a] = (lo[a] + (hi[a] - lo[a]) * u[a]).astype(np.float32)
+    return out
+
+
+def plain_small(seed=1, lattice=(32, 32, 32), iterations=4) -> Scene:
+    """32,768-particle dam break in a [0,1]x[0,2]x[0,1] box (4 iterations, 100 steps)."""
+    return dam_break(lattice, (0.0, 0.0, 0.0), (1.0, 2.0, 1.0), seed, iterations, name="dam_break_32k")
+
+
+def plain_large(seed=2, lattice=(128, 64, 128), iterations=8) -> Scene:
+    """1,048,576-particle dam break (128x64x128 lattice) in a [0,4]^3 box, 8 iterations."""
+    return dam_break(lattice, (0.0, 0.0, 0.0), (4.0, 4.0, 4.0), seed, iterations, name="dam_break_1m")
+
+
+def differentiable(seed=3, lattice=(32, 64, 32), iterations=4) -> Scene:
+    """65,536 particles with v0 ~ N(0, 0.1) and a uniform target cloud in a 0.5^3 box."""
+    scene = dam_break(lattice, (0.0, 0.0, 0.0), (1.0, 2.0, 1.0), seed, iterations,
+                      velocity_sigma=0.1, name="differentiable_64k")
+    scene.targets = target_cloud(seed, scene.count)
+    return scene
+
+
+def batched_counts(seed: int, scenes: int, lo: int, hi: int, log_uniform: bool) -> list:
+    u = uniform01(seed, scenes, 11)
+    if log_uniform:
+        counts = np.round(np.exp(np.log(lo) + u * (np.log(hi) - np.log(lo))))
+    else:
+        counts = np.floor(lo + u * (hi - lo + 1))
+    return [int(min(max(c, lo), hi)) for c in counts]
+
+
+def batched_scene(count: int, seed: int, iterations: int, velocity_sigma=0.0, name="") -> Scene:
+    """A dam break of exactly `count` particles in a box whose side scales with the count.
+
+    Lattice nx = nz = ceil((count/2)^(1/3)), filled x fastest, then z, then y,
+    truncated at `count`; box [0,L]x[0,2L]x[0,L] with L = 2.5 nx spacing.
+    """
+    nx = int(math.ceil((count / 2.0) ** (1.0 / 3.0)))
+    ny = int(math.ceil(count / float(nx * nx)))
+    side = 2.5 * nx * SPACING
+    return dam_break((nx, ny, nx), (0.0, 0.0, 0.0), (side, 2.0 * side, side), seed, iterations,
+                     velocity_sigma=velocity_sigma, fill_order="yzx", count=count, name=name)
+
+
+def batched_forward(seed=4, scenes=256, iterations=4) -> list:
+    """256 scenes with counts log-uniform in [2048, 65536]."""
+    counts = batched_counts(seed, scenes, 2048, 65536, True)
+    return [batched_scene(c, seed * 1000003 + s, iterations, name=f"scene{s}") for s, c in enumerate(counts)]
+
+
+def batched_adjoint(seed=5, scenes=32, iterations=4) -> list:
+    """32 scenes with counts uniform in [16384, 131072], each with its own target cloud."""
+    counts = batched_counts(seed, scenes, 16384, 131072, False)
+    out = []
+    for s, c in enumerate(counts):
+        sc = batched_scene(c, seed * 1000003 + s, iterations, name=f"scene{s}")
+        side = sc.box_max[0]
+        sc.targets = target_cloud(seed * 7919 + s, c, (0.25 * side, 0.0, 0.25 * side), (0.75 * side, 0.5 * side, 0.75 * side))
+        out.append(sc)
+    return out
