@@ -1,0 +1,442 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 PBF solver on the reference's headline workload.
+
+Metric: PBF particle-substeps/s of the 1,048,576-particle dam break (128x64x128 lattice, h = 0.025,
+box [0,4]^3, 8 Jacobi iterations, dt = 1/120), and, as a second figure, differentiable grad-steps/s
+of the 65,536-particle rollout (4 iterations, trajectory checkpoint every 10 steps).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One process per GPU (torchrun for N > 1).  The single-scene substep does not shard, so N GPUs run
+N independent replicas (weak scaling); rank 0 prints one JSON line.  Timing: W untimed steps,
+then K steps between a barrier + synchronize on both sides; every step is timed with CUDA events
+on the solver's stream, with a 256 MiB write between steps to flush the 126 MB L2; the reported
+time is the maximum over ranks.  `--impl reference` times the reference's own CUDA PBF (compiled
+from its sources into oracle/_ref) on the same workload and GPU; the reference has no CPU path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import torch  # noqa: E402
+import torch.distributed as dist  # noqa: E402
+
+METRIC = "PBF particle-substeps/s at 1M (fwd) & grad-steps/s at 64k, vs plain, same GPU"
+UNIT = "particle-substeps/s"
+FLUSH_BYTES = 256 << 20
+
+
+def peaks():
+    try:
+        p = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback (6.65 TB/s)"
+
+
+# Nominal FP32 FMA peak of a B200: 148 SMs x 128 lanes x 2 FLOP x 1.965 GHz (not measured here).
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = pathlib.Path(f"/tmp/pbf_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.strip()]
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if len(r) > 2 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 2 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(name)
+        load = sorted(sm)[len(sm) // 4:] if sm else []
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def setup_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def timed(step, steps, warmup, world, stream, flush):
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    events = []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.add_(1.0)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        step()
+        b.record(stream)
+        events.append((a, b))
+    torch.cuda.synchronize()
+    barrier(world)
+    wall = time.perf_counter() - t0
+    ms = sum(a.elapsed_time(b) for a, b in events)
+    return ms, wall
+
+
+# ------------------------------------------------------------------------------ B200 arm
+def bench_b200(args, world, rank):
+    from physica_b200 import pbf, scenes, trajectory
+    from physica_b200.pbf import CacheField
+
+    sc = scenes.plain_large(seed=2 + rank)
+    n = sc.count
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    cur, nxt = state, solver.allocate_state()
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = solver.stream
+    holder = {"cur": cur, "nxt": nxt}
+
+    def step():
+        solver.forward_step(holder["cur"], control, params, holder["nxt"], cache)
+        holder["cur"], holder["nxt"] = holder["nxt"], holder["cur"]
+
+    launches0 = pbf.launch_count()
+    with Clocks(torch.cuda.current_device()) as clk:
+        ms, wall = timed(step, args.steps, args.warmup, world, stream, flush)
+    launches = pbf.launch_count() - launches0
+    per_step_launches = launches / (args.steps + args.warmup)
+    ms_max = max_over_ranks(ms, world)
+    ms_per_step = ms_max / args.steps
+    value = world * n / (ms_per_step * 1e-3)
+
+    # per-pass timing (profiled rerun, events around each kernel group on the same stream)
+    lib = pbf.library()
+    lib.pbf_profile_enable(solver.handle, 1)
+    for _ in range(3):
+        flush.add_(1.0)
+        step()
+    passes = read_profile(lib, solver.handle)
+    lib.pbf_profile_enable(solver.handle, 0)
+    neighbors = float(cache.read(CacheField.NEIGHBOR_COUNTS).double().mean())
+    K = sc.pressure_iterations
+    cells = solver.cells
+    bytes_per_particle = {"density_lambda": 16, "correction_project": 28, "vorticity": 36, "normal_confinement": 48,
+                          "xsph": 48}
+    flops_per_pair = {"density_lambda": 14 + 30, "correction_project": 25, "vorticity": 34, "normal_confinement": 26,
+                      "xsph": 21}
+    hbm, hbm_src = peaks()
+    top = max((p for p in passes if p["name"] in bytes_per_particle), key=lambda p: p["ms"], default=None)
+    roofline = None
+    per_pass = {}
+    for p in passes:
+        avg = p["ms"] / max(p["launches"], 1)
+        entry = {"launches_per_step": p["launches"] / 3, "avg_ms": round(avg, 5)}
+        if p["name"] in bytes_per_particle:
+            entry["algorithmic_GBps"] = round(bytes_per_particle[p["name"]] * n / (avg * 1e-3) / 1e9, 2)
+            entry["fp32_TFLOPs"] = round(neighbors * flops_per_pair[p["name"]] * n / (avg * 1e-3) / 1e12, 3)
+        per_pass[p["name"]] = entry
+    if top is not None:
+        avg = top["ms"] / top["launches"]
+        achieved = bytes_per_particle[top["name"]] * n / (avg * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
+                    "frac": round(achieved / hbm, 5), "traffic": traffic_from_profiles(top["name"]),
+                    "kernel": top["name"], "peak_source": hbm_src,
+                    "note": "gather passes are FP32/issue bound; fp32 fraction in per_pass and step_roofline"}
+    b_alg = (192 + 44 * K) * n + 12 * cells
+    f_alg = neighbors * (69 * K + 81) * n
+    step_s = ms_per_step * 1e-3
+    step_roofline = {"algorithmic_bytes": b_alg, "algorithmic_flops": round(f_alg),
+                     "hbm_fraction": round(b_alg / step_s / (hbm * 1e9), 5),
+                     "fp32_fraction_nominal": round(f_alg / step_s / (FP32_NOMINAL_TFLOPS * 1e12), 5),
+                     "mean_neighbors": round(neighbors, 3)}
+
+    # end to end through the host-buffer C ABI entry: H2D of the state, the step, D2H of the result
+    e2e = None
+    if not args.no_e2e:
+        hx = torch.from_numpy(sc.positions.copy()).pin_memory()
+        hv = torch.from_numpy(sc.velocities.copy()).pin_memory()
+        ox, ov = torch.empty_like(hx).pin_memory(), torch.empty_like(hv).pin_memory()
+        host = {"x": hx, "v": hv, "ox": ox, "ov": ov, "step": 0}
+
+        def host_step():
+            host["step"] = solver.forward_step_host(host["x"], host["v"], control, params, host["ox"], host["ov"], cache,
+                                                    host["step"])
+            host["x"], host["ox"] = host["ox"], host["x"]
+            host["v"], host["ov"] = host["ov"], host["v"]
+
+        for _ in range(2):
+            host_step()
+        barrier(world)
+        ke = max(3, min(args.steps, 10))
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            host_step()
+        dt = max_over_ranks((time.perf_counter() - t0) / ke, world)
+        e2e = {"value": world * n / dt, "unit": UNIT, "h2d_bytes_per_step": 6 * 4 * n, "d2h_bytes_per_step": 6 * 4 * n}
+
+    # differentiable rollout: grad-steps/s at 64k
+    grad = None
+    if not args.no_grad:
+        grad = bench_grad(args, world, rank)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(sc)
+    return {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered-lattice dam break)",
+        "config": {"workload": "dam_break_1m: 1,048,576 particles (128x64x128 lattice, spacing 0.5h, h=0.025), "
+                               "box [0,4]^3, 8 Jacobi iterations, dt=1/120, XSPH c=0.01, vorticity eps=1e-4",
+                   "particles_per_gpu": n, "pressure_iterations": K, "cells": cells, "replicas": world,
+                   "l2": "flushed between timed steps (256 MiB write)", "wall_s": round(wall, 3)},
+        "roofline": roofline, "step_roofline": step_roofline, "per_pass": per_pass,
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(round(per_step_launches * args.steps)),
+        "clocks": clk.summary(), "grad_steps_per_s": grad,
+    }
+
+
+def read_profile(lib, handle):
+    import ctypes
+    from physica_b200 import pbf
+
+    class PassTime(ctypes.Structure):
+        _fields_ = [("name", ctypes.c_char_p), ("launches", ctypes.c_uint64), ("milliseconds", ctypes.c_double)]
+
+    arr = (PassTime * 32)()
+    cnt = ctypes.c_uint32()
+    lib.pbf_profile_read.argtypes = [ctypes.c_void_p, ctypes.POINTER(PassTime), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+    pbf.check(lib.pbf_profile_read(handle, arr, 32, ctypes.byref(cnt)))
+    return [{"name": arr[k].name.decode(), "launches": int(arr[k].launches), "ms": float(arr[k].milliseconds)}
+            for k in range(cnt.value)]
+
+
+def traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` recorded from an ncu capture under profiles/ (or None)."""
+    for p in sorted((ROOT / "profiles").glob("*.md")):
+        for line in p.read_text().splitlines():
+            if line.startswith("traffic_bytes_per_launch") and f"[{kernel}]" in line:
+                try:
+                    return int(line.split("=")[-1].strip())
+                except ValueError:
+                    pass
+    return None
+
+
+def bench_grad(args, world, rank):
+    from physica_b200 import pbf, scenes, trajectory
+    sc = scenes.differentiable(seed=3 + rank)
+    solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
+    targets = torch.from_numpy(sc.targets).cuda()
+    steps = 20
+    trajectory.loss_and_gradients(solver, state, control, params, targets, 10, 10)   # warm-up
+    torch.cuda.synchronize()
+    barrier(world)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(solver.stream)
+    g = trajectory.loss_and_gradients(solver, state, control, params, targets, steps, 10)
+    b.record(solver.stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(a.elapsed_time(b), world)
+    return {"value": round(world * steps / (ms * 1e-3), 3), "unit": "grad-steps/s",
+            "config": {"workload": "differentiable_64k: 65,536 particles (32x64x32 lattice), v0 ~ N(0, 0.1), "
+                                   "4 iterations, target-cloud loss", "rollout_steps": steps,
+                       "trajectory_checkpoint_every": 10}, "loss": g.loss}
+
+
+def cpu_baseline(sc):
+    """FP64 host oracle, one substep of the same 1M workload on all host cores."""
+    from oracle import oracle
+    t0 = time.perf_counter()
+    oracle.forward_step(sc, sc.positions, sc.velocities)
+    dt = time.perf_counter() - t0
+    return {"value": round(sc.count / dt, 1), "unit": UNIT, "cores": oracle.thread_count(), "kind": "port",
+            "sample": f"one substep of the 1,048,576-particle workload (FP64 OpenMP oracle, {dt:.2f} s)"}
+
+
+# --------------------------------------------------------------------------- reference arm
+def bench_reference(args, world, rank):
+    from oracle import reference
+    from physica_b200 import scenes
+    if not reference.available():
+        return {"impl": "reference", "unavailable": "reference kernels not built (oracle/_ref/libpbf_ref.so missing)"}
+    sc = scenes.plain_large(seed=2 + rank)
+    n = sc.count
+    ref = reference.ReferencePBF(sc)
+    x = torch.from_numpy(sc.positions).cuda().contiguous()
+    v = torch.from_numpy(sc.velocities).cuda().contiguous()
+    xo, vo = torch.zeros_like(x), torch.zeros_like(v)
+    stream = torch.cuda.ExternalStream(ref.stream)
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    holder = {"x": x, "v": v, "xo": xo, "vo": vo, "k": 0}
+    torch.cuda.synchronize()
+
+    def step():
+        ref.forward_step(holder["x"], holder["v"], holder["xo"], holder["vo"], holder["k"], synchronize=False)
+        holder["x"], holder["xo"] = holder["xo"], holder["x"]
+        holder["v"], holder["vo"] = holder["vo"], holder["v"]
+        holder["k"] += 1
+
+    with Clocks(torch.cuda.current_device()) as clk:
+        ms, wall = timed(step, args.steps, args.warmup, world, stream, flush)
+    ms_max = max_over_ranks(ms, world)
+    ms_per_step = ms_max / args.steps
+    value = world * n / (ms_per_step * 1e-3)
+    grad = None if args.no_grad else bench_reference_grad(world, rank)
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered-lattice dam break)",
+        "config": {"workload": "dam_break_1m: 1,048,576 particles (128x64x128 lattice, spacing 0.5h, h=0.025), "
+                               "box [0,4]^3, 8 Jacobi iterations, dt=1/120, XSPH c=0.01, vorticity eps=1e-4",
+                   "particles_per_gpu": n, "replicas": world, "l2": "flushed between timed steps (256 MiB write)",
+                   "wall_s": round(wall, 3)},
+        "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": 0, "kind": "reference",
+                         "sample": "the reference's own CUDA PBF kernels (pbf.cu, density.cu, neighborhood.cu, domain.cu "
+                                   "compiled from its sources) replaying PBF::forward_step on the same B200; the reference "
+                                   "has no CPU implementation of this path"},
+        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(), "grad_steps_per_s": grad,
+    }
+
+
+def bench_reference_grad(world, rank):
+    """The same 64k rollout through the reference's vjp_step: one harness (solver + cache) per step of a segment."""
+    from oracle import reference
+    from physica_b200 import scenes
+    sc = scenes.differentiable(seed=3 + rank)
+    steps, every = 20, 10
+    refs = [reference.ReferencePBF(sc, checkpoint_interval=2, differentiable=True) for _ in range(every)]
+    dev = "cuda"
+    n = sc.count
+    names = ("masses", "rest_densities", "relaxation", "artificial_pressure_strength", "artificial_pressure_exponent",
+             "artificial_pressure_radius", "xsph_viscosity", "vorticity_confinement")
+    targets = torch.from_numpy(sc.targets).cuda()
+
+    def run():
+        x = torch.from_numpy(sc.positions).to(dev).contiguous()
+        v = torch.from_numpy(sc.velocities).to(dev).contiguous()
+        checkpoints = []
+        for k in range(steps):
+            if k % every == 0:
+                checkpoints.append((x.clone(), v.clone()))
+            xo, vo = torch.empty_like(x), torch.empty_like(v)
+            refs[k % every].forward_step(x, v, xo, vo, k)
+            x, v = xo, vo
+        adj = {"positions": (x.double() - targets.double()) * (2.0 / n),
+               "velocities": torch.zeros((3, n), dtype=torch.float64, device=dev)}
+        pa = {k: torch.zeros(n, dtype=torch.float64, device=dev) for k in names}
+        ctrl = torch.zeros((3, n), dtype=torch.float64, device=dev)
+        for seg in reversed(range(len(checkpoints))):
+            xs, vs = [checkpoints[seg][0]], [checkpoints[seg][1]]
+            begin = seg * every
+            for k in range(begin, min(begin + every, steps)):
+                xo, vo = torch.empty_like(xs[-1]), torch.empty_like(vs[-1])
+                refs[k - begin].forward_step(xs[-1], vs[-1], xo, vo, k)
+                xs.append(xo)
+                vs.append(vo)
+            for k in reversed(range(begin, min(begin + every, steps))):
+                j = k - begin
+                prev = {"positions": torch.zeros((3, n), dtype=torch.float64, device=dev),
+                        "velocities": torch.zeros((3, n), dtype=torch.float64, device=dev)}
+                refs[j].vjp_step(xs[j], vs[j], adj, prev, ctrl, pa)
+                adj = prev
+        torch.cuda.synchronize()
+
+    run()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run()
+    dt = max_over_ranks(time.perf_counter() - t0, world)
+    return {"value": round(world * steps / dt, 3), "unit": "grad-steps/s",
+            "config": {"workload": "differentiable_64k", "rollout_steps": steps, "trajectory_checkpoint_every": every,
+                       "in_step_checkpoint_interval": 2}}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-grad", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = setup_dist()
+    if args.impl == "reference":
+        out = bench_reference(args, world, rank)
+    else:
+        out = bench_b200(args, world, rank)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

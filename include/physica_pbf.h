@@ -250,6 +250,28 @@ int pbf_batch_vjp_step(pbf_batch* batch, const pbf_particle_state* state, const 
 int pbf_batch_reserve_caches(pbf_batch* batch, uint32_t cache_slots);
 int pbf_batch_set_launch_shape(pbf_batch* batch, uint32_t bucket, uint32_t block_size);
 
+/* ---- compensated FP64 sum of a per-particle adjoint (Neumaier summation in a fixed, deterministic
+ *      order), e.g. dL/dc for a scalar parameter shared by all particles: dL/dc = sum_i dL/dc_i.
+ *      `values` and `result` are device pointers; `result` receives one double.  No reference
+ *      counterpart: the reference keeps only the per-particle parameter adjoints (pbf/pbf.ixx:44-52). ---- */
+int pbf_sum_compensated(pbf_solver* solver, const double* values, uint32_t count, double* result);
+/* Per-scene compensated sums over a batch's concatenated per-particle values: result[scene_count]. */
+int pbf_batch_scene_sums(pbf_batch* batch, const double* values, double* result);
+
+/* ---- per-pass timing: CUDA events recorded on the solver's stream around every kernel group
+ *      while enabled (pbf_profile_enable resets the totals); pbf_profile_read synchronises and
+ *      returns one entry per pass that ran.  No reference counterpart (the reference has no
+ *      timing); bench.py reports per-kernel GB/s from it. ---- */
+typedef struct {
+    const char* name;          /* static string, e.g. "density_lambda" */
+    uint64_t launches;
+    double milliseconds;       /* summed over launches */
+} pbf_pass_time;
+int pbf_profile_enable(pbf_solver* solver, int enable);
+int pbf_profile_read(pbf_solver* solver, pbf_pass_time* passes, uint32_t capacity, uint32_t* count);
+int pbf_batch_profile_enable(pbf_batch* batch, int enable);
+int pbf_batch_profile_read(pbf_batch* batch, pbf_pass_time* passes, uint32_t capacity, uint32_t* count);
+
 /* ---- misc ---- */
 int pbf_synchronize(pbf_solver* solver);
 int pbf_batch_synchronize(pbf_batch* batch);

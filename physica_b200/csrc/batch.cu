@@ -7,6 +7,9 @@
 struct pbf_batch {
     pbf::Engine engine;
     std::vector<std::unique_ptr<pbf::StepRecord>> caches;
+    pbf::DeviceArena arena;
+    uint32_t* scene_first = nullptr;
+    uint32_t* scene_count = nullptr;
 };
 
 extern "C" {
@@ -88,6 +91,43 @@ int pbf_batch_set_launch_shape(pbf_batch* batch, const uint32_t bucket, const ui
     }
     batch->engine.set_block(block_size);
     return PBF_SUCCESS;
+}
+
+int pbf_batch_scene_sums(pbf_batch* batch, const double* values, double* result) {
+    if (!batch || !values || !result) return PBF_ERROR_INVALID_ARGUMENT;
+    const auto& sc = batch->engine.scenes();
+    const uint32_t n = static_cast<uint32_t>(sc.size());
+    if (!batch->scene_first) {
+        cudaError_t e = cudaSuccess;
+        batch->arena.set_stream(batch->engine.stream());
+        batch->scene_first = batch->arena.alloc<uint32_t>(n, e);
+        batch->scene_count = batch->arena.alloc<uint32_t>(n, e);
+        if (int rc = batch->engine.check(e, "scene table")) return rc;
+        std::vector<uint32_t> f(n), c(n);
+        for (uint32_t s = 0; s < n; ++s) {
+            f[s] = sc[s].first;
+            c[s] = sc[s].config.particle_count;
+        }
+        e = cudaMemcpyAsync(batch->scene_first, f.data(), n * 4, cudaMemcpyHostToDevice, batch->engine.stream());
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(batch->scene_count, c.data(), n * 4, cudaMemcpyHostToDevice, batch->engine.stream());
+        if (e == cudaSuccess) e = cudaStreamSynchronize(batch->engine.stream());
+        if (int rc = batch->engine.check(e, "scene table upload")) return rc;
+    }
+    return batch->engine.check(pbf::launch_segment_sums(batch->engine.stream(), values, batch->scene_first, batch->scene_count, n, 0,
+                                                        result),
+                               "batch scene sums");
+}
+
+int pbf_batch_profile_enable(pbf_batch* batch, const int enable) {
+    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
+    batch->engine.timer().enable(enable != 0);
+    return PBF_SUCCESS;
+}
+
+int pbf_batch_profile_read(pbf_batch* batch, pbf_pass_time* passes, const uint32_t capacity, uint32_t* count) {
+    if (!batch || !count) return PBF_ERROR_INVALID_ARGUMENT;
+    return pbf::read_profile(batch->engine, passes, capacity, count);
 }
 
 int pbf_batch_synchronize(pbf_batch* batch) {

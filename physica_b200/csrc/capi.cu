@@ -284,6 +284,23 @@ int pbf_grid_cell_count(const pbf_solver* solver, uint64_t* cells) {
     return PBF_SUCCESS;
 }
 
+int pbf_sum_compensated(pbf_solver* solver, const double* values, const uint32_t count, double* result) {
+    if (!solver || !result || (count && !values)) return null_arg("solver/values/result");
+    return solver->engine.check(pbf::launch_segment_sums(solver->engine.stream(), values, nullptr, nullptr, 1, count, result),
+                                "sum_compensated");
+}
+
+int pbf_profile_enable(pbf_solver* solver, const int enable) {
+    if (!solver) return null_arg("solver");
+    solver->engine.timer().enable(enable != 0);
+    return PBF_SUCCESS;
+}
+
+int pbf_profile_read(pbf_solver* solver, pbf_pass_time* passes, const uint32_t capacity, uint32_t* count) {
+    if (!solver || !count) return null_arg("solver/count");
+    return pbf::read_profile(solver->engine, passes, capacity, count);
+}
+
 int pbf_synchronize(pbf_solver* solver) {
     if (!solver) return null_arg("solver");
     return solver->engine.check(cudaStreamSynchronize(solver->engine.stream()), "synchronize");

@@ -24,6 +24,85 @@ const char* last_error_cstr() { return g_last_error.c_str(); }
 void count_launch(const unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
+const char* pass_name(const int pass) {
+    static const char* names[kPassCount] = {"grid_build", "density_lambda", "correction_project", "vorticity",
+                                            "normal_confinement", "xsph", "adjoint_seed", "xsph_vjp", "normal_vjp",
+                                            "vorticity_vjp", "correction_vjp", "lambda_vjp", "density_vjp"};
+    return pass >= 0 && pass < kPassCount ? names[pass] : "unknown";
+}
+
+PassTimer::~PassTimer() {
+    for (auto& m : pending_) {
+        cudaEventDestroy(m.start);
+        cudaEventDestroy(m.end);
+    }
+    for (cudaEvent_t ev : pool_) cudaEventDestroy(ev);
+    if (open_) cudaEventDestroy(open_);
+}
+
+void PassTimer::enable(const bool on) {
+    enabled_ = on;
+    for (int p = 0; p < kPassCount; ++p) {
+        ms_[p] = 0.0;
+        launches_[p] = 0;
+    }
+}
+
+cudaEvent_t PassTimer::take() {
+    if (!pool_.empty()) {
+        cudaEvent_t ev = pool_.back();
+        pool_.pop_back();
+        return ev;
+    }
+    cudaEvent_t ev = nullptr;
+    cudaEventCreate(&ev);
+    return ev;
+}
+
+void PassTimer::begin(cudaStream_t stream, int) {
+    if (!enabled_) return;
+    open_ = take();
+    cudaEventRecord(open_, stream);
+}
+
+void PassTimer::end(cudaStream_t stream, const int pass) {
+    if (!enabled_ || !open_) return;
+    cudaEvent_t stop = take();
+    cudaEventRecord(stop, stream);
+    pending_.push_back({pass, open_, stop});
+    open_ = nullptr;
+}
+
+int PassTimer::collect(cudaStream_t stream) {
+    const cudaError_t e = cudaStreamSynchronize(stream);
+    for (auto& m : pending_) {
+        float ms = 0.0F;
+        if (cudaEventElapsedTime(&ms, m.start, m.end) == cudaSuccess) {
+            ms_[m.pass] += ms;
+            launches_[m.pass] += 1;
+        }
+        pool_.push_back(m.start);
+        pool_.push_back(m.end);
+    }
+    pending_.clear();
+    return e == cudaSuccess ? PBF_SUCCESS : PBF_ERROR_CUDA;
+}
+
+int read_profile(Engine& engine, pbf_pass_time* passes, const uint32_t capacity, uint32_t* count) {
+    if (int rc = engine.timer().collect(engine.stream())) {
+        set_error("synchronise for profile");
+        return rc;
+    }
+    uint32_t k = 0;
+    for (int p = 0; p < kPassCount; ++p) {
+        if (engine.timer().launches(p) == 0) continue;
+        if (passes && k < capacity) passes[k] = {pass_name(p), engine.timer().launches(p), engine.timer().milliseconds(p)};
+        ++k;
+    }
+    *count = k;
+    return PBF_SUCCESS;
+}
+
 int Engine::check(const cudaError_t e, const char* what) {
     if (e == cudaSuccess) return PBF_SUCCESS;
     set_error(std::string(what) + ": " + cudaGetErrorString(e));
@@ -218,6 +297,16 @@ int Engine::allocate_record(StepRecord& r) {
     r.vorticity = r.arena.alloc<float4>(n, e);
     r.normal = r.arena.alloc<float4>(n, e);
     r.confined = r.arena.alloc<float4>(n, e);
+    // Neighbour lists: kListCapacity entries per particle, warp-interleaved.
+    r.list_capacity = kListCapacity;
+    const size_t padded = (static_cast<size_t>(n) + 31u) / 32u * 32u;
+    const uint32_t lists = diff ? K + 1 : 1;
+    r.list_entries.assign(lists, nullptr);
+    r.list_counts.assign(lists, nullptr);
+    for (uint32_t l = 0; l < lists; ++l) {
+        r.list_entries[l] = r.arena.alloc<uint32_t>(padded * r.list_capacity, e);
+        r.list_counts[l] = r.arena.alloc<uint32_t>(n, e);
+    }
     r.valid = false;
     if (int rc = check(e, "step cache allocation")) return rc;
     return check(cudaStreamSynchronize(stream_), "step cache allocation");
@@ -270,7 +359,9 @@ int Engine::forward(const pbf_particle_state* state, const pbf_control* control,
     g.topology = r.topology;
     g.params_a = r.params_a;
     g.params_b = r.params_b;
+    timer_.begin(stream_, kPassGrid);
     if (int rc = check(launch_grid_build(stream_, g), "grid build")) return rc;
+    timer_.end(stream_, kPassGrid);
 
     const GatherCommon gc{count_, d_scenes_, d_constants_, r.cell_offsets, r.cell, r.params_a, r.params_b};
     const Field3 previous{state->positions.x, state->positions.y, state->positions.z};
@@ -279,12 +370,18 @@ int Engine::forward(const pbf_particle_state* state, const pbf_control* control,
         const float4* xk = r.iterate(k, K, diff);
         float4* xk1 = const_cast<float4*>(r.iterate(k + 1, K, diff));
         float* lam = diff ? r.lambda[k] : (k == 0 ? r.first_lambda : r.lambda[0]);
+        const uint32_t l = diff ? k : 0u;
         DensityLambdaArgs d{gc, xk, lam, diff ? r.density[k] : (k == 0 ? r.first_density : nullptr),
-                            diff ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr};
+                            diff ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr,
+                            r.list_entries[l], r.list_counts[l], r.list_capacity};
+        timer_.begin(stream_, kPassDensityLambda);
         if (int rc = check(launch_density_lambda(stream_, d, block_), "density/lambda")) return rc;
+        timer_.end(stream_, kPassDensityLambda);
         CorrectionArgs c{gc, xk, lam, xk1, diff ? r.mask[k] : nullptr, k + 1 == K ? 1 : 0, previous, r.sorted_index,
-                         out_positions, r.velocity};
+                         out_positions, r.velocity, r.list_entries[l], r.list_counts[l], r.list_capacity};
+        timer_.begin(stream_, kPassCorrection);
         if (int rc = check(launch_correction(stream_, c, block_), "correction/project")) return rc;
+        timer_.end(stream_, kPassCorrection);
     }
     const float4* xK = r.iterate(K, K, diff);
     if (K == 0) {
@@ -293,12 +390,21 @@ int Engine::forward(const pbf_particle_state* state, const pbf_control* control,
                            "reconstruct"))
             return rc;
     }
-    VorticityArgs v{gc, xK, r.velocity, r.vorticity};
+    const uint32_t lp = diff ? K : 0u;
+    VorticityArgs v{gc, xK, r.velocity, r.vorticity, r.list_entries[lp], r.list_counts[lp], r.list_capacity};
+    timer_.begin(stream_, kPassVorticity);
     if (int rc = check(launch_vorticity(stream_, v, block_), "vorticity")) return rc;
-    NormalArgs nm{gc, xK, r.velocity, r.vorticity, r.normal, r.confined};
+    timer_.end(stream_, kPassVorticity);
+    NormalArgs nm{gc, xK, r.velocity, r.vorticity, r.normal, r.confined, r.list_entries[lp], r.list_counts[lp],
+                  r.list_capacity};
+    timer_.begin(stream_, kPassNormal);
     if (int rc = check(launch_normal(stream_, nm, block_), "normal/confinement")) return rc;
-    XsphArgs x{gc, xK, r.confined, r.sorted_index, {next_state->velocities.x, next_state->velocities.y, next_state->velocities.z}};
+    timer_.end(stream_, kPassNormal);
+    XsphArgs x{gc, xK, r.confined, r.sorted_index, {next_state->velocities.x, next_state->velocities.y, next_state->velocities.z},
+               r.list_entries[lp], r.list_counts[lp], r.list_capacity};
+    timer_.begin(stream_, kPassXsph);
     if (int rc = check(launch_xsph(stream_, x, block_), "xsph")) return rc;
+    timer_.end(stream_, kPassXsph);
     next_state->step_index = state->step_index + 1u;
     r.valid = true;
     r.step_index = state->step_index;

@@ -79,6 +79,10 @@ struct StepRecord {
     float4* vorticity = nullptr;
     float4* normal = nullptr;
     float4* confined = nullptr;
+    // Stored neighbour lists: one per iterate in differentiable mode (0..K), else one reused.
+    std::vector<uint32_t*> list_entries;
+    std::vector<uint32_t*> list_counts;
+    uint32_t list_capacity = 0;
 
     const float4* iterate(uint32_t k, uint32_t K, bool differentiable) const {
         if (k == 0) return topology;
@@ -86,6 +90,48 @@ struct StepRecord {
         (void)K;
         return positions[(k - 1) & 1u];
     }
+};
+
+enum PassId : int {
+    kPassGrid = 0,
+    kPassDensityLambda,
+    kPassCorrection,
+    kPassVorticity,
+    kPassNormal,
+    kPassXsph,
+    kPassSeed,
+    kPassXsphVjp,
+    kPassNormalVjp,
+    kPassVorticityVjp,
+    kPassCorrectionVjp,
+    kPassLambdaVjp,
+    kPassDensityVjp,
+    kPassCount
+};
+
+const char* pass_name(int pass);
+
+// CUDA-event timing of kernel groups on the engine's stream.
+class PassTimer {
+public:
+    ~PassTimer();
+    void enable(bool on);
+    bool enabled() const { return enabled_; }
+    void begin(cudaStream_t stream, int pass);
+    void end(cudaStream_t stream, int pass);
+    int collect(cudaStream_t stream);   // synchronises; folds pending intervals into the totals
+    double milliseconds(int pass) const { return ms_[pass]; }
+    uint64_t launches(int pass) const { return launches_[pass]; }
+
+private:
+    cudaEvent_t take();
+    struct Mark { int pass; cudaEvent_t start, end; };
+    bool enabled_ = false;
+    std::vector<Mark> pending_;
+    std::vector<cudaEvent_t> pool_;
+    cudaEvent_t open_ = nullptr;
+    double ms_[kPassCount] = {};
+    uint64_t launches_[kPassCount] = {};
 };
 
 class Engine {
@@ -117,8 +163,10 @@ public:
     void set_block(unsigned block) { block_ = block; }
 
     int check(cudaError_t e, const char* what);
+    PassTimer& timer() { return timer_; }
 
 private:
+    PassTimer timer_;
     int update_scene_table(uint64_t step_index);
 
     uint32_t count_ = 0;
@@ -143,5 +191,7 @@ private:
     friend struct AdjointWorkspace;
     void* adjoint_ = nullptr;  // AdjointWorkspace*, differentiable mode
 };
+
+int read_profile(Engine& engine, pbf_pass_time* passes, uint32_t capacity, uint32_t* count);
 
 }  // namespace pbf

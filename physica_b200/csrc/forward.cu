@@ -17,93 +17,16 @@
 // reference's order and equals it bit for bit; skipped candidates contribute an exact
 // zero in the reference.  The list keeps the costly per-pair math (sqrt, divisions)
 // convergent across the warp instead of running under a 15%-taken branch.
-#include "pbf_internal.h"
-#include "pbf_launch.h"
+#include "gather.cuh"
 
 namespace pbf {
 
 namespace {
 
-constexpr int kBlock = 128;
-constexpr int kListCap = 16;
-constexpr unsigned kFull = 0xffffffffu;
-
-// Walks the candidates of one particle's 27-cell stencil in reference order.
-struct Walker {
-    const uint32_t* offsets;
-    uint32_t nx, ny, nz, base;
-    int cx, cy, cz;
-    int next_cell;
-    uint32_t cur, end;
-
-    __device__ __forceinline__ void init(const uint32_t* cell_offsets, const Grid& g, const int4 c, const bool active) {
-        offsets = cell_offsets;
-        nx = g.cells_x; ny = g.cells_y; nz = g.cells_z; base = g.cell_base;
-        cx = c.x; cy = c.y; cz = c.z;
-        next_cell = active ? 0 : 27;
-        cur = end = 0;
-    }
-
-    __device__ __forceinline__ bool next(uint32_t& t) {
-        while (cur == end) {
-            if (next_cell >= 27) return false;
-            const int o = next_cell++;
-            const int x = cx + o / 9 - 1, y = cy + (o / 3) % 3 - 1, z = cz + o % 3 - 1;
-            if (x < 0 || y < 0 || z < 0 || x >= static_cast<int>(nx) || y >= static_cast<int>(ny) || z >= static_cast<int>(nz)) continue;
-            const uint32_t c = base + (static_cast<uint32_t>(z) * ny + static_cast<uint32_t>(y)) * nx + static_cast<uint32_t>(x);
-            cur = offsets[c];
-            end = offsets[c + 1];
-        }
-        t = cur++;
-        return true;
-    }
-};
-
-// Two-phase gather: accept() filters candidates in stencil order into the per-thread
-// list; process() consumes them in the same order.  All lanes stay in the loop until
-// every lane is exhausted so the warp votes are well defined.
-template <class Op>
-__device__ __forceinline__ void gather(Op& op, Walker& w, const bool active) {
-    __shared__ uint32_t lists[kListCap * kBlock];
-    uint32_t* list = lists + threadIdx.x;
-    int n = 0;
-    bool more = active;
-    while (__any_sync(kFull, more)) {
-        if (more) {
-            uint32_t t;
-            more = w.next(t);
-            if (more && op.accept(t)) {
-                list[n * kBlock] = t;
-                ++n;
-            }
-        }
-        if (__any_sync(kFull, n == kListCap)) {
-            for (int k = 0; k < n; ++k) op.process(list[k * kBlock]);
-            n = 0;
-        }
-    }
-    for (int k = 0; k < n; ++k) op.process(list[k * kBlock]);
-}
-
-struct Particle {
-    uint32_t s;
-    bool active;
-    int4 c;
-    const SceneDesc* scene;
-    KernelConstants k;
-};
-
-__device__ __forceinline__ Particle locate(const GatherCommon& g) {
-    Particle p;
-    p.s = blockIdx.x * blockDim.x + threadIdx.x;
-    p.active = p.s < g.count;
-    p.c = p.active ? g.cell[p.s] : make_int4(0, 0, 0, 0);
-    p.scene = g.scenes + p.c.w;
-    p.k = g.constants[p.scene->constants];
-    return p;
-}
+using namespace gather_detail;
 
 // ------------------------------------------------------------------ density + lambda
+// density (density/density.cu:18-40) and lambda (pbf/pbf.cu:95-127) of one particle in one walk.
 struct DensityLambdaOp {
     const float4* __restrict__ pos;
     f3 x;
@@ -115,28 +38,25 @@ struct DensityLambdaOp {
     float denominator;
     uint32_t neighbors;
 
-    __device__ __forceinline__ bool accept(const uint32_t t) const {
-        const float4 q = pos[t];
-        const f3 d = x - xyz(q);
-        return dot(d, d) < k.union_threshold;
-    }
     __device__ __forceinline__ void process(const uint32_t t) {
         const float4 q = pos[t];
-        const f3 d = x - xyz(q);
-        const float r2 = dot(d, d);
-        if (r2 < k.h2) density += q.w * poly6_inside(r2, k);
+        const f3 d = sub(x, xyz(q));
+        const float r2 = squared(d);
+        if (r2 < k.h2) density = __fmaf_rn(q.w, poly6_inside(r2, k), density);
         if (t == self) return;
         if (r2 < k.h2) ++neighbors;
-        const float distance = sqrtf(r2);
+        const float distance = __fsqrt_rn(r2);
         if (distance == 0.0F || distance >= k.h) return;
         const f3 gradient = spiky_gradient_at(d, distance, k);
-        const float coefficient = q.w / rest_density;
-        gradient_sum = gradient_sum + times(gradient, coefficient);
-        denominator += coefficient * coefficient * dot(gradient, gradient);
+        const float coefficient = __fdiv_rn(q.w, rest_density);
+        gradient_sum = fma3(coefficient, gradient, gradient_sum);
+        denominator = __fmaf_rn(__fmul_rn(coefficient, coefficient), sq_xfirst(gradient), denominator);
     }
 };
 
 __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLambdaArgs a) {
+    __shared__ WarpScratch scratch[kWarpsPerBlock];
+    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     DensityLambdaOp op;
     op.pos = a.pos;
@@ -150,18 +70,18 @@ __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLam
     op.gradient_sum = mk(0.0F, 0.0F, 0.0F);
     op.denominator = pa.y;  // relaxation
     op.neighbors = 0;
-    Walker w;
-    w.init(a.g.cell_offsets, p.scene->grid, p.c, p.active);
-    gather(op, w, p.active);
+    scan<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, ListWriter{a.list_entries, a.list_counts, a.list_capacity});
     if (!p.active) return;
-    const float denominator = op.denominator + dot(op.gradient_sum, op.gradient_sum);
-    a.lambda[p.s] = -(op.density / op.rest_density - 1.0F) / denominator;
+    const float denominator = __fadd_rn(op.denominator, sq_yfirst(op.gradient_sum));
+    a.lambda[p.s] = __fdiv_rn(-__fsub_rn(__fdiv_rn(op.density, op.rest_density), 1.0F), denominator);
     if (a.density) a.density[p.s] = op.density;
     if (a.gsum_denom) a.gsum_denom[p.s] = make_float4(op.gradient_sum.x, op.gradient_sum.y, op.gradient_sum.z, denominator);
     if (a.neighbor_count) a.neighbor_count[p.s] = op.neighbors;
 }
 
 // ------------------------------------------------------- correction + project
+// correction (pbf/pbf.cu:254-288) and project (pbf/pbf.cu:417-431); on the last iteration
+// also reconstruct (pbf/pbf.cu:456-460) and the write-back of next_state.positions.
 struct CorrectionOp {
     const float4* __restrict__ pos;
     const float* __restrict__ lambda;
@@ -174,34 +94,31 @@ struct CorrectionOp {
     KernelConstants k;
     f3 correction;
 
-    __device__ __forceinline__ bool accept(const uint32_t t) const {
-        if (t == self) return false;
-        const float4 q = pos[t];
-        const f3 d = x - xyz(q);
-        const float r2 = dot(d, d);
-        return r2 > 0.0F && r2 < k.spiky_threshold;
-    }
     __device__ __forceinline__ void process(const uint32_t t) {
+        if (t == self) return;
         const float4 q = pos[t];
-        const f3 d = x - xyz(q);
-        const float r2 = dot(d, d);
-        const float distance = sqrtf(r2);
+        const f3 d = sub(x, xyz(q));
+        const float r2 = squared(d);
+        const float distance = __fsqrt_rn(r2);
         if (distance == 0.0F || distance >= k.h) return;
-        // s_corr of pbf/pbf.cu:56-71; with zero strength it is -strength * ratio^n = -0 inside
-        // the poly6 support and 0 outside, which is what the fast branch yields.
+        // s_corr (pbf/pbf.cu:56-71).  With zero strength it is -strength * ratio^n, i.e. -0 inside
+        // the poly6 support and 0 outside, which the fast branch yields without powf.
         float artificial;
         if (artificial_full) {
             const float weight = r2 >= k.h2 ? 0.0F : poly6_inside(r2, k);
-            artificial = weight == 0.0F ? 0.0F : -strength * powf(weight / reference_weight, exponent);
+            artificial = weight == 0.0F ? 0.0F : __fmul_rn(-strength, powf(__fdiv_rn(weight, reference_weight), exponent));
         } else {
             artificial = r2 < k.h2 ? -strength : 0.0F;
         }
-        const float coefficient = q.w / rest_density;
-        correction = correction + times(spiky_gradient_at(d, distance, k), coefficient * (lambda_i + lambda[t] + artificial));
+        const float coefficient = __fdiv_rn(q.w, rest_density);
+        const float factor = __fmul_rn(coefficient, __fadd_rn(__fadd_rn(lambda_i, lambda[t]), artificial));
+        correction = fma3(factor, spiky_gradient_at(d, distance, k), correction);
     }
 };
 
 __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs a) {
+    __shared__ WarpScratch scratch[kWarpsPerBlock];
+    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     CorrectionOp op;
     op.pos = a.pos;
@@ -219,12 +136,10 @@ __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs
     op.artificial_full = pb.x != 0.0F;
     op.reference_weight = op.artificial_full ? poly6(mk(pb.z, 0.0F, 0.0F), p.k) : 1.0F;
     op.correction = mk(0.0F, 0.0F, 0.0F);
-    Walker w;
-    w.init(a.g.cell_offsets, p.scene->grid, p.c, p.active);
-    gather(op, w, p.active);
+    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list_entries, a.list_counts, a.list_capacity);
     if (!p.active) return;
     const Box& box = p.scene->box;
-    const f3 candidate = op.x + op.correction;
+    const f3 candidate = add(op.x, op.correction);
     uint32_t mask = 0u;
     if (candidate.x < box.min_x || candidate.x > box.max_x) mask |= 1u;
     if (candidate.y < box.min_y || candidate.y > box.max_y) mask |= 2u;
@@ -236,7 +151,7 @@ __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs
     if (a.last) {
         const uint32_t i = a.sorted_index[p.s];
         const f3 previous = mk(a.previous_positions.x[i], a.previous_positions.y[i], a.previous_positions.z[i]);
-        const f3 velocity = times(projected - previous, p.scene->inverse_time_step);
+        const f3 velocity = scale(sub(projected, previous), p.scene->inverse_time_step);
         a.velocity[p.s] = make_float4(velocity.x, velocity.y, velocity.z, 0.0F);
         a.out_positions.x[i] = projected.x;
         a.out_positions.y[i] = projected.y;
@@ -245,34 +160,27 @@ __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs
 }
 
 // ---------------------------------------------------------------- vorticity
-struct SpikyAccept {
+// vorticity (pbf/pbf.cu:476-497) and its magnitude (pbf/pbf.cu:565-569).
+struct VorticityOp {
     const float4* __restrict__ pos;
-    f3 x;
+    const float4* __restrict__ velocity;
+    f3 x, v;
     uint32_t self;
     KernelConstants k;
-    __device__ __forceinline__ bool accept(const uint32_t t) const {
-        if (t == self) return false;
-        const float4 q = pos[t];
-        const f3 d = x - xyz(q);
-        const float r2 = dot(d, d);
-        return r2 > 0.0F && r2 < k.spiky_threshold;
-    }
-};
-
-struct VorticityOp : SpikyAccept {
-    const float4* __restrict__ velocity;
-    f3 v;
     f3 vorticity;
+
     __device__ __forceinline__ void process(const uint32_t t) {
-        const float4 q = pos[t];
-        const f3 d = x - xyz(q);
-        const float distance = sqrtf(dot(d, d));
+        if (t == self) return;
+        const f3 d = sub(x, xyz(pos[t]));
+        const float distance = __fsqrt_rn(squared(d));
         if (distance == 0.0F || distance >= k.h) return;
-        vorticity = vorticity + cross(xyz(velocity[t]) - v, spiky_gradient_at(d, distance, k));
+        vorticity = add(vorticity, cross_f(sub(xyz(velocity[t]), v), spiky_gradient_at(d, distance, k)));
     }
 };
 
 __global__ void __launch_bounds__(kBlock) vorticity_kernel(const VorticityArgs a) {
+    __shared__ WarpScratch scratch[kWarpsPerBlock];
+    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     VorticityOp op;
     op.pos = a.pos;
@@ -282,28 +190,34 @@ __global__ void __launch_bounds__(kBlock) vorticity_kernel(const VorticityArgs a
     op.x = p.active ? xyz(a.pos[p.s]) : mk(0, 0, 0);
     op.v = p.active ? xyz(a.velocity[p.s]) : mk(0, 0, 0);
     op.vorticity = mk(0.0F, 0.0F, 0.0F);
-    Walker w;
-    w.init(a.g.cell_offsets, p.scene->grid, p.c, p.active);
-    gather(op, w, p.active);
+    scan<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, ListWriter{a.list_entries, a.list_counts, a.list_capacity});
     if (!p.active) return;
-    a.vorticity[p.s] = make_float4(op.vorticity.x, op.vorticity.y, op.vorticity.z, norm(op.vorticity));
+    a.vorticity[p.s] = make_float4(op.vorticity.x, op.vorticity.y, op.vorticity.z, __fsqrt_rn(sq_xfirst(op.vorticity)));
 }
 
 // ------------------------------------------------------- normal + confinement
-struct NormalOp : SpikyAccept {
+// normal (pbf/pbf.cu:571-593) and confinement (pbf/pbf.cu:674-678).
+struct NormalOp {
+    const float4* __restrict__ pos;
     const float4* __restrict__ vorticity;
+    f3 x;
     float magnitude;
+    uint32_t self;
+    KernelConstants k;
     f3 gradient;
+
     __device__ __forceinline__ void process(const uint32_t t) {
-        const float4 q = pos[t];
-        const f3 d = x - xyz(q);
-        const float distance = sqrtf(dot(d, d));
+        if (t == self) return;
+        const f3 d = sub(x, xyz(pos[t]));
+        const float distance = __fsqrt_rn(squared(d));
         if (distance == 0.0F || distance >= k.h) return;
-        gradient = gradient + times(spiky_gradient_at(d, distance, k), vorticity[t].w - magnitude);
+        gradient = fma3(__fsub_rn(vorticity[t].w, magnitude), spiky_gradient_at(d, distance, k), gradient);
     }
 };
 
 __global__ void __launch_bounds__(kBlock) normal_kernel(const NormalArgs a) {
+    __shared__ WarpScratch scratch[kWarpsPerBlock];
+    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     NormalOp op;
     op.pos = a.pos;
@@ -314,20 +228,19 @@ __global__ void __launch_bounds__(kBlock) normal_kernel(const NormalArgs a) {
     op.x = p.active ? xyz(a.pos[p.s]) : mk(0, 0, 0);
     op.magnitude = wi.w;
     op.gradient = mk(0.0F, 0.0F, 0.0F);
-    Walker w;
-    w.init(a.g.cell_offsets, p.scene->grid, p.c, p.active);
-    gather(op, w, p.active);
+    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list_entries, a.list_counts, a.list_capacity);
     if (!p.active) return;
-    const float normalizer = norm(op.gradient);
-    const f3 normal = normalizer > 0.0F ? times(op.gradient, 1.0F / normalizer) : mk(0.0F, 0.0F, 0.0F);
+    const float normalizer = __fsqrt_rn(sq_yfirst(op.gradient));
+    const f3 normal = normalizer > 0.0F ? scale(op.gradient, __fdiv_rn(1.0F, normalizer)) : mk(0.0F, 0.0F, 0.0F);
     a.normal[p.s] = make_float4(normal.x, normal.y, normal.z, normalizer);
     const float4 pa = a.g.params_a[p.s];
     const f3 v = xyz(a.velocity[p.s]);
-    const f3 confined = v + times(cross(normal, xyz(wi)), p.scene->time_step * pa.w);
+    const f3 confined = fma3(__fmul_rn(p.scene->time_step, pa.w), cross_f(normal, xyz(wi)), v);
     a.confined[p.s] = make_float4(confined.x, confined.y, confined.z, 0.0F);
 }
 
 // ---------------------------------------------------------------------- XSPH
+// XSPH (pbf/pbf.cu:700-721) and the write-back of next_state.velocities.
 struct XsphOp {
     const float4* __restrict__ pos;
     const float4* __restrict__ confined;
@@ -335,22 +248,19 @@ struct XsphOp {
     uint32_t self;
     KernelConstants k;
     f3 smoothing;
-    __device__ __forceinline__ bool accept(const uint32_t t) const {
-        if (t == self) return false;
-        const float4 q = pos[t];
-        const f3 d = x - xyz(q);
-        return dot(d, d) < k.h2;
-    }
+
     __device__ __forceinline__ void process(const uint32_t t) {
-        const float4 q = pos[t];
-        const f3 d = x - xyz(q);
-        const float r2 = dot(d, d);
+        if (t == self) return;
+        const f3 d = sub(x, xyz(pos[t]));
+        const float r2 = squared(d);
         if (r2 >= k.h2) return;
-        smoothing = smoothing + times(xyz(confined[t]) - v, poly6_inside(r2, k));
+        smoothing = fma3(poly6_inside(r2, k), sub(xyz(confined[t]), v), smoothing);
     }
 };
 
 __global__ void __launch_bounds__(kBlock) xsph_kernel(const XsphArgs a) {
+    __shared__ WarpScratch scratch[kWarpsPerBlock];
+    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     XsphOp op;
     op.pos = a.pos;
@@ -360,12 +270,10 @@ __global__ void __launch_bounds__(kBlock) xsph_kernel(const XsphArgs a) {
     op.x = p.active ? xyz(a.pos[p.s]) : mk(0, 0, 0);
     op.v = p.active ? xyz(a.confined[p.s]) : mk(0, 0, 0);
     op.smoothing = mk(0.0F, 0.0F, 0.0F);
-    Walker w;
-    w.init(a.g.cell_offsets, p.scene->grid, p.c, p.active);
-    gather(op, w, p.active);
+    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list_entries, a.list_counts, a.list_capacity);
     if (!p.active) return;
     const float viscosity = a.g.params_a[p.s].z;
-    const f3 out = op.v + times(op.smoothing, viscosity);
+    const f3 out = fma3(viscosity, op.smoothing, op.v);
     const uint32_t i = a.sorted_index[p.s];
     a.out_velocities.x[i] = out.x;
     a.out_velocities.y[i] = out.y;
@@ -377,13 +285,15 @@ __global__ void constants_kernel(const float* __restrict__ radii, const uint32_t
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float h = radii[i];
-    const float squared_radius = h * h;
+    const float squared_radius = __fmul_rn(h, h);
     KernelConstants k;
     k.h = h;
     k.h2 = squared_radius;
-    k.poly6_denominator = 64.0F * kPi * squared_radius * squared_radius * squared_radius * h * h * h;
-    k.poly6_grad_denominator = 32.0F * kPi * squared_radius * squared_radius * squared_radius * h * h * h;
-    k.spiky_coefficient = -45.0F / (kPi * powf(h, 6.0F));
+    k.poly6_denominator = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(64.0F * kPi, squared_radius), squared_radius),
+                                                                     squared_radius), h), h), h);
+    k.poly6_grad_denominator = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(32.0F * kPi, squared_radius), squared_radius),
+                                                                          squared_radius), h), h), h);
+    k.spiky_coefficient = __fdiv_rn(-45.0F, __fmul_rn(kPi, powf(h, 6.0F)));
     // Smallest float r2 with sqrtf(r2) >= h; sqrtf is monotone, so bisect on the bit pattern.
     uint32_t lo = 0u, hi = 0x7f800000u;
     while (hi - lo > 1u) {
@@ -393,7 +303,18 @@ __global__ void constants_kernel(const float* __restrict__ radii, const uint32_t
     }
     k.spiky_threshold = __uint_as_float(hi);
     k.union_threshold = fmaxf(k.h2, k.spiky_threshold);
-    k.poly6_radial_coefficient = 315.0F / (64.0F * kPi * powf(h, 9.0F));
+    // Smallest float r2 with sqrt((double)r2) >= h (the FP64 Hessian's support test).
+    lo = 0u;
+    hi = 0x7f800000u;
+    while (hi - lo > 1u) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        if (sqrt(static_cast<double>(__uint_as_float(mid))) >= static_cast<double>(h)) hi = mid;
+        else lo = mid;
+    }
+    k.hessian_threshold = __uint_as_float(hi);
+    k.adjoint_threshold = fmaxf(k.spiky_threshold, k.hessian_threshold);
+    k.list_threshold = fmaxf(k.union_threshold, k.hessian_threshold);
+    k.poly6_radial_coefficient = __fdiv_rn(315.0F, __fmul_rn(64.0F * kPi, powf(h, 9.0F)));
     k.spiky_coefficient_d = -45.0 / (static_cast<double>(kPi) * pow(static_cast<double>(h), 6.0));
     out[i] = k;
 }
@@ -434,7 +355,7 @@ __global__ void reconstruct_kernel(const uint32_t count, const SceneDesc* __rest
     const SceneDesc& sc = scenes[cell[s].w];
     const uint32_t i = sorted_index[s];
     const f3 x = xyz(positions[s]);
-    const f3 v = times(x - mk(previous.x[i], previous.y[i], previous.z[i]), sc.inverse_time_step);
+    const f3 v = scale(sub(x, mk(previous.x[i], previous.y[i], previous.z[i])), sc.inverse_time_step);
     velocity[s] = make_float4(v.x, v.y, v.z, 0.0F);
     out.x[i] = x.x;
     out.y[i] = x.y;

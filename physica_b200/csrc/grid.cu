@@ -36,13 +36,14 @@ __global__ void predict_key_kernel(const uint32_t count, const SceneDesc* __rest
     const f3 a = mk(controls.x[i], controls.y[i], controls.z[i]);
     const f3 x = mk(positions.x[i], positions.y[i], positions.z[i]);
     const float dt = sc.time_step;
-    const f3 predicted_velocity = v + times(gravity + a, dt);
-    const f3 xs = x + times(predicted_velocity, dt);
+    const f3 predicted_velocity = fma3(dt, add(gravity, a), v);
+    const f3 xs = fma3(dt, predicted_velocity, x);
     predicted[i] = make_float4(xs.x, xs.y, xs.z, masses[i]);
     const Grid& g = sc.grid;
-    const int cx = clamp_cell((xs.x - g.key_min_x - g.time * g.key_vel_x) / g.cell_size, g.cells_x);
-    const int cy = clamp_cell((xs.y - g.key_min_y - g.time * g.key_vel_y) / g.cell_size, g.cells_y);
-    const int cz = clamp_cell((xs.z - g.key_min_z - g.time * g.key_vel_z) / g.cell_size, g.cells_z);
+    // (x - minimum - time * velocity) / h, the product fused into the subtraction
+    const int cx = clamp_cell(__fdiv_rn(__fmaf_rn(-g.time, g.key_vel_x, __fsub_rn(xs.x, g.key_min_x)), g.cell_size), g.cells_x);
+    const int cy = clamp_cell(__fdiv_rn(__fmaf_rn(-g.time, g.key_vel_y, __fsub_rn(xs.y, g.key_min_y)), g.cell_size), g.cells_y);
+    const int cz = clamp_cell(__fdiv_rn(__fmaf_rn(-g.time, g.key_vel_z, __fsub_rn(xs.z, g.key_min_z)), g.cell_size), g.cells_z);
     const uint32_t key = g.cell_base + (static_cast<uint32_t>(cz) * g.cells_y + static_cast<uint32_t>(cy)) * g.cells_x +
                          static_cast<uint32_t>(cx);
     keys[i] = key;
@@ -168,9 +169,9 @@ __global__ void reorder_kernel(const uint32_t count, const SceneDesc* __restrict
     const uint32_t scene = scene_of ? scene_of[i] : 0u;
     const Grid& g = scenes[scene].grid;
     // gather-side cell of x* (neighborhood/device.cuh:44-48)
-    const int cx = clamp_cell((xs.x - g.origin_x) / g.cell_size, g.cells_x);
-    const int cy = clamp_cell((xs.y - g.origin_y) / g.cell_size, g.cells_y);
-    const int cz = clamp_cell((xs.z - g.origin_z) / g.cell_size, g.cells_z);
+    const int cx = clamp_cell(__fdiv_rn(__fsub_rn(xs.x, g.origin_x), g.cell_size), g.cells_x);
+    const int cy = clamp_cell(__fdiv_rn(__fsub_rn(xs.y, g.origin_y), g.cell_size), g.cells_y);
+    const int cz = clamp_cell(__fdiv_rn(__fsub_rn(xs.z, g.origin_z), g.cell_size), g.cells_z);
     cell[s] = make_int4(cx, cy, cz, static_cast<int>(scene));
     params_a[s] = make_float4(params.rest_densities[i], params.relaxation[i], params.xsph[i], params.vorticity[i]);
     params_b[s] = make_float4(params.strength[i], params.exponent[i], params.radius[i], 0.0F);

@@ -77,5 +77,7 @@ struct SortedState {
 };
 
 constexpr uint32_t kMaxIterations = 64;
+// Stored neighbour-list capacity per particle (a longer list is rebuilt by scanning).
+constexpr uint32_t kListCapacity = 64;
 
 }  // namespace pbf

@@ -55,6 +55,9 @@ struct DensityLambdaArgs {
     float* density;            // optional record
     float4* gsum_denom;        // optional record: gradient sum S and denominator D
     uint32_t* neighbor_count;  // optional: poly6 in-radius neighbours, self excluded
+    uint32_t* list_entries;    // neighbour list of this iterate, written for later passes
+    uint32_t* list_counts;
+    uint32_t list_capacity;
 };
 
 struct CorrectionArgs {
@@ -68,6 +71,9 @@ struct CorrectionArgs {
     const uint32_t* sorted_index;
     MutField3 out_positions;   // original order (next_state.positions)
     float4* velocity;          // reconstructed velocity (sorted)
+    const uint32_t* list_entries;
+    const uint32_t* list_counts;
+    uint32_t list_capacity;
 };
 
 struct VorticityArgs {
@@ -75,6 +81,9 @@ struct VorticityArgs {
     const float4* pos;
     const float4* velocity;
     float4* vorticity;         // (omega, |omega|)
+    uint32_t* list_entries;
+    uint32_t* list_counts;
+    uint32_t list_capacity;
 };
 
 struct NormalArgs {
@@ -84,6 +93,9 @@ struct NormalArgs {
     const float4* vorticity;
     float4* normal;            // (N, normalizer)
     float4* confined;          // confined velocity
+    const uint32_t* list_entries;
+    const uint32_t* list_counts;
+    uint32_t list_capacity;
 };
 
 struct XsphArgs {
@@ -92,6 +104,9 @@ struct XsphArgs {
     const float4* confined;
     const uint32_t* sorted_index;
     MutField3 out_velocities;  // original order (next_state.velocities)
+    const uint32_t* list_entries;
+    const uint32_t* list_counts;
+    uint32_t list_capacity;
 };
 
 cudaError_t launch_constants(cudaStream_t stream, const float* support_radii, uint32_t n, KernelConstants* out);
@@ -107,6 +122,11 @@ cudaError_t launch_reconstruct(cudaStream_t stream, uint32_t count, const SceneD
 
 // FP64 dst[f][i] += src[f][i] for up to six fields.
 cudaError_t launch_accumulate(cudaStream_t stream, size_t count, const double* const* src, double* const* dst, int fields);
+
+// Neumaier-compensated FP64 sums of `segments` ranges (first/count device arrays; null: one range
+// [0, single_count)).
+cudaError_t launch_segment_sums(cudaStream_t stream, const double* values, const uint32_t* first, const uint32_t* count,
+                                uint32_t segments, uint32_t single_count, double* out);
 
 // Inspection helpers: scatter sorted arrays back to original order.
 cudaError_t launch_unsort_float4(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const float4* in,

@@ -1,0 +1,152 @@
+"""GPU tests of the adjoint: one substep against the reference's VJP kernels and the FP64 oracle,
+central finite differences of the FP64 forward, and a checkpointed multi-step rollout."""
+import numpy as np
+import pytest
+import torch
+
+from physica_b200 import pbf, scenes, trajectory
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ("masses", "rest_densities", "relaxation", "artificial_pressure_strength", "artificial_pressure_exponent",
+         "artificial_pressure_radius", "xsph_viscosity", "vorticity_confinement")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda(cuda_lib):
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    yield
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    s = np.abs(b).max()
+    return float(np.abs(a - b).max() / s) if s > 0 else float(np.abs(a - b).max())
+
+
+def my_vjp(sc, nxa, nva, checkpoint_interval=1):
+    solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable,
+                                                          checkpoint_interval=checkpoint_interval)
+    cache = solver.allocate_step_cache()
+    nxt = solver.allocate_state()
+    solver.forward_step(state, control, params, nxt, cache)
+    na = pbf.StateAdjoint(torch.from_numpy(nxa).cuda(), torch.from_numpy(nva).cuda())
+    pa, ca, qa = solver.allocate_state_adjoint(), solver.allocate_control_adjoint(), solver.allocate_parameter_adjoint()
+    solver.vjp_step(state, control, params, nxt, cache, na, pa, ca, qa)
+    torch.cuda.synchronize()
+    return {"position": pa.positions.cpu().numpy(), "velocity": pa.velocities.cpu().numpy(),
+            "control": ca.external_accelerations.cpu().numpy(), **{k: qa.tensors[k].cpu().numpy() for k in NAMES}}
+
+
+def _scene(lattice=(10, 10, 10), seed=12):
+    return scenes.dam_break(lattice, (0, 0, 0), (1, 2, 1), seed, 4, velocity_sigma=0.1)
+
+
+def test_vjp_matches_reference_vjp():
+    """The adjoint of one substep equals the reference's vjp_step to FP64 rounding."""
+    from oracle import reference
+    if not reference.available():
+        pytest.skip("reference kernels (oracle/_ref) not built")
+    sc = _scene()
+    rng = np.random.default_rng(5)
+    nxa, nva = rng.normal(size=(3, sc.count)), rng.normal(size=(3, sc.count))
+    mine = my_vjp(sc, nxa, nva)
+    ref = reference.ReferencePBF(sc, checkpoint_interval=2, differentiable=True)
+    x = torch.from_numpy(sc.positions).cuda().contiguous()
+    v = torch.from_numpy(sc.velocities).cuda().contiguous()
+    xo, vo = torch.zeros_like(x), torch.zeros_like(v)
+    ref.forward_step(x, v, xo, vo, 0)
+    z3 = lambda: torch.zeros((3, sc.count), dtype=torch.float64, device="cuda")
+    prev = {"positions": z3(), "velocities": z3()}
+    ctrl = z3()
+    pa = {k: torch.zeros(sc.count, dtype=torch.float64, device="cuda") for k in NAMES}
+    ref.vjp_step(x, v, {"positions": torch.from_numpy(nxa).cuda(), "velocities": torch.from_numpy(nva).cuda()},
+                 prev, ctrl, pa)
+    theirs = {"position": prev["positions"].cpu().numpy(), "velocity": prev["velocities"].cpu().numpy(),
+              "control": ctrl.cpu().numpy(), **{k: pa[k].cpu().numpy() for k in NAMES}}
+    for k in ("position", "velocity", "control", "masses", "rest_densities", "relaxation",
+              "artificial_pressure_strength", "xsph_viscosity", "vorticity_confinement"):
+        assert rel(mine[k], theirs[k]) < 1e-9, (k, rel(mine[k], theirs[k]))
+
+
+def test_vjp_matches_fp64_oracle():
+    from oracle import oracle
+    sc = _scene()
+    rng = np.random.default_rng(6)
+    nxa, nva = rng.normal(size=(3, sc.count)), rng.normal(size=(3, sc.count))
+    mine = my_vjp(sc, nxa, nva)
+    o = oracle.vjp_step(sc, sc.positions, sc.velocities, nxa, nva)
+    for k in ("position", "velocity", "control", "xsph_viscosity", "vorticity_confinement", "relaxation"):
+        assert rel(mine[k], o[k]) < 1e-3, (k, rel(mine[k], o[k]))
+
+
+def test_vjp_directional_derivative_matches_central_differences():
+    """<dL/dv0, dv> of the CUDA adjoint equals the central difference of the FP64 forward (1e-3 relative)."""
+    from oracle import oracle
+    sc = _scene((8, 8, 8), 13)
+    rng = np.random.default_rng(7)
+    wx, wv = rng.normal(size=(3, sc.count)), rng.normal(size=(3, sc.count))
+    mine = my_vjp(sc, wx, wv)
+    x0, v0 = sc.positions.astype(np.float64), sc.velocities.astype(np.float64)
+
+    def loss(x, v):
+        x1, v1 = oracle.forward_step(sc, x, v)
+        return float((wx * x1).sum() + (wv * v1).sum())
+
+    for target, grad in (("v", mine["velocity"]), ("x", mine["position"])):
+        dirn = rng.normal(size=(3, sc.count))
+        eps = 1e-6
+        if target == "v":
+            fd = (loss(x0, v0 + eps * dirn) - loss(x0, v0 - eps * dirn)) / (2 * eps)
+        else:
+            fd = (loss(x0 + eps * dirn, v0) - loss(x0 - eps * dirn, v0)) / (2 * eps)
+        ad = float((grad * dirn).sum())
+        assert ad == pytest.approx(fd, rel=1e-3), (target, ad, fd)
+
+
+def test_vjp_independent_of_checkpoint_interval():
+    sc = _scene((8, 8, 8), 14)
+    rng = np.random.default_rng(8)
+    nxa, nva = rng.normal(size=(3, sc.count)), rng.normal(size=(3, sc.count))
+    a = my_vjp(sc, nxa, nva, 1)
+    b = my_vjp(sc, nxa, nva, 3)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_rollout_gradient_matches_fp64_finite_differences():
+    """Checkpointed 8-step rollout: dL/dv0 (directional) and dL/dc of the scalar XSPH viscosity."""
+    from oracle import oracle
+    sc = scenes.dam_break((8, 8, 8), (0, 0, 0), (1, 2, 1), 15, 3, velocity_sigma=0.1)
+    targets = scenes.target_cloud(15, sc.count)
+    steps, every = 8, 3
+    solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
+    g = trajectory.loss_and_gradients(solver, state, control, params, torch.from_numpy(targets).cuda(), steps, every)
+
+    def rollout_loss(v0, c=None):
+        x, v = sc.positions.astype(np.float64), v0
+        p = oracle.Parameters(sc, c) if c is not None else None
+        for k in range(steps):
+            x, v = oracle.forward_step(sc, x, v, step_index=k, params=p)
+        d = x - targets.astype(np.float64)
+        return float((d * d).sum() / sc.count)
+
+    rng = np.random.default_rng(9)
+    dirn = rng.normal(size=(3, sc.count))
+    v0 = sc.velocities.astype(np.float64)
+    eps = 1e-6
+    fd = (rollout_loss(v0 + eps * dirn) - rollout_loss(v0 - eps * dirn)) / (2 * eps)
+    ad = float((g.initial_velocities.cpu().numpy() * dirn).sum())
+    assert ad == pytest.approx(fd, rel=1e-3)
+    c = float(sc.xsph_viscosity[0])
+    dc = 1e-3 * c
+    fdc = (rollout_loss(v0, c + dc) - rollout_loss(v0, c - dc)) / (2 * dc)
+    assert g.scalar["xsph_viscosity"] == pytest.approx(fdc, rel=1e-3)
+    assert g.loss == pytest.approx(rollout_loss(v0), rel=1e-4)
+
+
+def test_compensated_sum_is_exact_for_a_hard_case():
+    solver, state, control, params = pbf.solver_for_scene(scenes.dam_break((2, 2, 2), (0, 0, 0), (1, 2, 1), 1, 1))
+    vals = torch.tensor([1e16, 1.0, -1e16, 3.0] * 1000, dtype=torch.float64, device="cuda")
+    assert trajectory.compensated_sum(solver, vals).item() == 4000.0

@@ -1,0 +1,292 @@
+"""GPU parity of the CUDA solver (called through the C ABI) against the reference's own kernels,
+the committed golden fixtures and the FP64 host oracle.
+
+Integer work (keys, stable order, cell offsets, neighbour counts) is compared bit for bit;
+FP32 per-pass outputs given identical inputs are compared bit for bit against the reference;
+trajectories are compared to 1e-4 h after 100 steps; the FP64 oracle is the tolerance check.
+"""
+import ctypes
+import pathlib
+
+import numpy as np
+import pytest
+import torch
+
+from physica_b200 import pbf, scenes
+
+pytestmark = pytest.mark.gpu
+GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
+F = pbf.IterationField
+C = pbf.CacheField
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda(cuda_lib):
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    yield
+
+
+def reference_or_skip():
+    from oracle import reference
+    if not reference.available():
+        pytest.skip("reference kernels (oracle/_ref) not built")
+    return reference
+
+
+def step(solver, state, control, params, cache):
+    nxt = solver.allocate_state()
+    solver.forward_step(state, control, params, nxt, cache)
+    return nxt
+
+
+def bits_equal(a, b):
+    a = a.detach().cpu().contiguous()
+    b = b.detach().cpu().contiguous()
+    if a.dtype == torch.float32:
+        return int((a.view(torch.int32) != b.view(torch.int32)).sum())
+    return int((a != b).sum())
+
+
+# ----------------------------------------------------------------------------- grid
+@pytest.mark.parametrize("lattice,seed", [((12, 12, 12), 1), ((17, 9, 13), 2)])
+def test_grid_matches_oracle(lattice, seed):
+    """Keys, stable sorted order and cell offsets equal the FP32 oracle grid of x*."""
+    from oracle import oracle
+    sc = scenes.dam_break(lattice, (0, 0, 0), (1, 2, 1), seed, 2)
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    step(solver, state, control, params, cache)
+    xs = cache.read(C.PREDICTED_POSITIONS).cpu().numpy()
+    keys, srt, off, dims = oracle.grid_f32(sc, xs, float(np.float32(1) * np.float32(sc.time_step)))
+    assert np.array_equal(cache.read(C.SORTED_PARTICLE_INDICES).cpu().numpy().astype(np.uint32), srt)
+    assert np.array_equal(cache.read(C.CELL_OFFSETS).cpu().numpy().astype(np.uint32), off)
+    assert np.array_equal(cache.read(C.SORTED_KEYS).cpu().numpy().astype(np.uint64), keys[srt].astype(np.uint64))
+    assert tuple(cache.read(C.GRID_RESOLUTION).tolist()) == dims
+
+
+def test_neighbor_counts_match_oracle():
+    from oracle import oracle
+    sc = scenes.plain_small(lattice=(16, 16, 16))
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    step(solver, state, control, params, cache)
+    xs = cache.read(C.PREDICTED_POSITIONS).cpu().numpy()
+    counts = oracle.neighbor_counts_f32(sc, xs, xs, float(np.float32(sc.time_step)))
+    assert np.array_equal(cache.read(C.NEIGHBOR_COUNTS).cpu().numpy().astype(np.uint32), counts)
+
+
+# ------------------------------------------------------------------ reference kernels
+def _ref_pass_fn(reference):
+    lib = reference.load()
+    lib.ref_pass_topology.argtypes = [ctypes.c_void_p, ctypes.c_void_p * 3, ctypes.c_uint64]
+    lib.ref_pass.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p * 9, ctypes.c_void_p * 2,
+                             ctypes.POINTER(reference.RefParams), ctypes.c_void_p * 6, ctypes.c_void_p * 2,
+                             ctypes.c_void_p, ctypes.c_uint64]
+
+    def p3(t):
+        return [t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr()]
+
+    def run(ref, pas, in3=(), sin=(), out3=(), sout=(), mask=None, step_index=1):
+        a = sum((p3(t) for t in in3), []) + [0] * (9 - 3 * len(in3))
+        s = [t.data_ptr() for t in sin] + [0] * (2 - len(sin))
+        o = sum((p3(t) for t in out3), []) + [0] * (6 - 3 * len(out3))
+        so = [t.data_ptr() for t in sout] + [0] * (2 - len(sout))
+        torch.cuda.synchronize()
+        rc = lib.ref_pass(ref.handle, pas, (ctypes.c_void_p * 9)(*a), (ctypes.c_void_p * 2)(*s),
+                          ctypes.byref(ref._pstruct()), (ctypes.c_void_p * 6)(*o), (ctypes.c_void_p * 2)(*so),
+                          ctypes.c_void_p(mask.data_ptr() if mask is not None else 0), step_index)
+        assert rc == 0
+
+    def topology(ref, xs, step_index):
+        assert lib.ref_pass_topology(ref.handle, (ctypes.c_void_p * 3)(*p3(xs)), step_index) == 0
+
+    return run, topology
+
+
+@pytest.mark.parametrize("warm_steps", [0, 15])
+def test_every_pass_bit_exact_against_reference(warm_steps):
+    """Each fused pass, fed the same inputs as the reference kernel it replaces, is bit-identical."""
+    reference = reference_or_skip()
+    run, topology = _ref_pass_fn(reference)
+    sc = scenes.plain_small(lattice=(20, 20, 20))
+    solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
+    cache = solver.allocate_step_cache()
+    for _ in range(warm_steps):
+        nxt = step(solver, state, control, params, cache)
+        solver.copy_state(nxt, state)
+    nxt = step(solver, state, control, params, cache)
+    torch.cuda.synchronize()
+    ref = reference.ReferencePBF(sc)
+    n, K = sc.count, sc.pressure_iterations
+    f1 = lambda: torch.zeros(n, dtype=torch.float32, device="cuda")
+    f3 = lambda: torch.zeros((3, n), dtype=torch.float32, device="cuda")
+    topology(ref, cache.read_iteration(F.POSITIONS, 0), state.step_index + 1)
+    bad = {}
+    for k in range(K):
+        xk = cache.read_iteration(F.POSITIONS, k)
+        rho, lam = cache.read_iteration(F.DENSITIES, k), cache.read_iteration(F.LAMBDAS, k)
+        r_rho = f1(); run(ref, 0, in3=[xk], sout=[r_rho])
+        r_S, r_D, r_l = f3(), f1(), f1(); run(ref, 1, in3=[xk], sin=[rho], out3=[r_S], sout=[r_D, r_l])
+        r_c = f3(); run(ref, 2, in3=[xk], sin=[lam], out3=[r_c])
+        r_x, r_m = f3(), torch.zeros(n, dtype=torch.int32, device="cuda")
+        run(ref, 3, in3=[xk, r_c], out3=[r_x], mask=r_m, step_index=state.step_index + 1)
+        for name, mine, theirs in (("density", rho, r_rho), ("gradient_sum", cache.read_iteration(F.GRADIENT_SUMS, k), r_S),
+                                   ("denominator", cache.read_iteration(F.DENOMINATORS, k), r_D), ("lambda", lam, r_l),
+                                   ("positions", cache.read_iteration(F.POSITIONS, k + 1), r_x),
+                                   ("mask", cache.read_iteration(F.COLLISION_MASKS, k), r_m)):
+            bad[f"it{k}.{name}"] = bits_equal(mine, theirs)
+    xK = cache.read_iteration(F.POSITIONS, K)
+    vr = cache.read(C.RECONSTRUCTED_VELOCITIES)
+    r_vr = f3(); run(ref, 8, in3=[state.positions, xK], out3=[r_vr])
+    w = cache.read(C.VORTICITIES)
+    r_w = f3(); run(ref, 4, in3=[xK, vr], out3=[r_w])
+    r_mag, r_N, r_nz = f1(), f3(), f1(); run(ref, 5, in3=[xK, w], out3=[r_N], sout=[r_mag, r_nz])
+    N = cache.read(C.VORTICITY_NORMALS)
+    r_vc = f3(); run(ref, 6, in3=[vr, w, N], out3=[r_vc])
+    vc = cache.read(C.CONFINED_VELOCITIES)
+    r_v = f3(); run(ref, 7, in3=[xK, vc], out3=[r_v])
+    for name, mine, theirs in (("reconstruct", vr, r_vr), ("vorticity", w, r_w),
+                               ("magnitude", cache.read(C.VORTICITY_MAGNITUDES), r_mag), ("normal", N, r_N),
+                               ("normalizer", cache.read(C.VORTICITY_NORMALIZERS), r_nz), ("confinement", vc, r_vc),
+                               ("xsph", nxt.velocities, r_v)):
+        bad[name] = bits_equal(mine, theirs)
+    assert all(v == 0 for v in bad.values()), {k: v for k, v in bad.items() if v}
+
+
+def _trajectory(sc, steps, reference):
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    ref = reference.ReferencePBF(sc)
+    cur, nxt = state, solver.allocate_state()
+    xr, vr = state.positions.clone(), state.velocities.clone()
+    xr2, vr2 = torch.zeros_like(xr), torch.zeros_like(vr)
+    errs = {}
+    for k in range(steps):
+        solver.forward_step(cur, control, params, nxt, cache)
+        torch.cuda.synchronize()
+        ref.forward_step(xr, vr, xr2, vr2, k)
+        cur, nxt = nxt, cur
+        xr, xr2, vr, vr2 = xr2, xr, vr2, vr
+        if k + 1 in (1, 10, steps):
+            torch.cuda.synchronize()
+            errs[k + 1] = (float((cur.positions - xr).abs().max()), float((cur.velocities - vr).abs().max()),
+                           bits_equal(cur.positions, xr) + bits_equal(cur.velocities, vr))
+    return errs
+
+
+def test_trajectory_matches_reference_after_100_steps():
+    """32,768-particle dam break, 100 steps: positions and velocities within 1e-4 h of the reference."""
+    reference = reference_or_skip()
+    sc = scenes.plain_small()
+    errs = _trajectory(sc, 100, reference)
+    h = sc.support_radius
+    for k, (ex, ev, nbits) in errs.items():
+        assert ex <= 1e-4 * h, (k, ex, ev, nbits)
+        assert ev <= 1e-4 * h / sc.time_step, (k, ex, ev, nbits)
+    assert errs[100][2] == 0, errs   # and in fact bit for bit
+
+
+def test_batched_scene_layout_trajectory_matches_reference():
+    """A truncated-lattice scene (the batched scenes' shape) over 30 steps, bit for bit."""
+    reference = reference_or_skip()
+    sc = scenes.batched_scene(3001, 77, 4)
+    errs = _trajectory(sc, 30, reference)
+    assert errs[30][2] == 0, errs
+
+
+# -------------------------------------------------------------------- golden fixtures
+def test_forward_matches_reference_golden():
+    """The committed reference outputs (tests/golden/reference_step_small.npz) are reproduced exactly."""
+    path = GOLDEN / "reference_step_small.npz"
+    if not path.exists():
+        pytest.skip("golden fixture not generated yet")
+    g = np.load(path)
+    sc = scenes.dam_break(tuple(g["lattice"]), tuple(g["box_min"]), tuple(g["box_max"]), int(g["seed"]),
+                          int(g["iterations"]))
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    nxt = step(solver, state, control, params, cache)
+    assert np.array_equal(cache.read(C.SORTED_PARTICLE_INDICES).cpu().numpy(), g["sorted_indices"].astype(np.int32))
+    assert np.array_equal(cache.read(C.CELL_OFFSETS).cpu().numpy(), g["cell_offsets"].astype(np.int32))
+    assert np.array_equal(cache.read(C.PREDICTED_POSITIONS).cpu().numpy(), g["predicted"])
+    assert np.array_equal(cache.read(C.FIRST_DENSITIES).cpu().numpy(), g["first_densities"])
+    assert np.array_equal(cache.read(C.FIRST_LAMBDAS).cpu().numpy(), g["first_lambdas"])
+    assert np.array_equal(nxt.positions.cpu().numpy(), g["x1"])
+    assert np.array_equal(nxt.velocities.cpu().numpy(), g["v1"])
+    cur = nxt
+    for k in range(1, 10):
+        n2 = step(solver, cur, control, params, cache)
+        cur = n2
+    assert np.array_equal(cur.positions.cpu().numpy(), g["x10"])
+    assert np.array_equal(cur.velocities.cpu().numpy(), g["v10"])
+
+
+# ----------------------------------------------------------------------- FP64 oracle
+def test_forward_against_fp64_oracle():
+    from oracle import oracle
+    sc = scenes.plain_small(lattice=(14, 14, 14))
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    nxt = step(solver, state, control, params, cache)
+    x1, v1 = oracle.forward_step(sc, sc.positions, sc.velocities)
+    h = sc.support_radius
+    assert np.abs(nxt.positions.cpu().numpy() - x1).max() < 1e-4 * h
+    assert np.abs(nxt.velocities.cpu().numpy() - v1).max() < 1e-4 * h / sc.time_step
+
+
+# ------------------------------------------------------------------------ edge cases
+@pytest.mark.parametrize("case", ["single", "ragged", "one_cell", "outside_grid", "two_coincident"])
+def test_edge_cases_match_oracle(case):
+    from oracle import oracle
+    if case == "single":
+        sc = scenes.dam_break((1, 1, 1), (0, 0, 0), (1, 2, 1), 3, 3)
+    elif case == "ragged":
+        sc = scenes.batched_scene(1001, 5, 3)     # not a multiple of the block or warp size
+    elif case == "one_cell":
+        sc = scenes.dam_break((4, 4, 4), (0, 0, 0), (1, 2, 1), 4, 3)
+        rng = np.random.default_rng(3)
+        sc.positions[:] = (np.array([[0.5], [0.5], [0.5]]) + rng.uniform(0, 0.02, sc.positions.shape)).astype(np.float32)
+    elif case == "outside_grid":
+        sc = scenes.dam_break((6, 6, 6), (0, 0, 0), (1, 2, 1), 6, 3)
+        sc.positions[0, :20] -= 0.5                # left of the box: clamped into edge cells
+        sc.positions[1, 20:40] += 3.0              # above the box
+    else:
+        sc = scenes.dam_break((4, 4, 4), (0, 0, 0), (1, 2, 1), 7, 3)
+        sc.positions[:, 1] = sc.positions[:, 0]    # two particles at the same point (zero distance)
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    nxt = step(solver, state, control, params, cache)
+    x1, v1 = oracle.forward_step(sc, sc.positions, sc.velocities)
+    got_x, got_v = nxt.positions.cpu().numpy(), nxt.velocities.cpu().numpy()
+    assert np.all(np.isfinite(got_x)) and np.all(np.isfinite(got_v))
+    h = sc.support_radius
+    tol = 1e-4 * h if case != "one_cell" else 2e-3 * h      # a 64-particle clump is stiff
+    assert np.abs(got_x - x1).max() < tol
+    xs = cache.read(C.PREDICTED_POSITIONS).cpu().numpy()
+    keys, srt, off, _ = oracle.grid_f32(sc, xs, float(np.float32(sc.time_step)))
+    assert np.array_equal(cache.read(C.SORTED_PARTICLE_INDICES).cpu().numpy().astype(np.uint32), srt)
+
+
+def test_host_buffer_entry_matches_device_entry():
+    sc = scenes.plain_small(lattice=(10, 10, 10))
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    nxt = step(solver, state, control, params, cache)
+    hx = torch.from_numpy(sc.positions.copy()).pin_memory()
+    hv = torch.from_numpy(sc.velocities.copy()).pin_memory()
+    ox, ov = torch.empty_like(hx).pin_memory(), torch.empty_like(hv).pin_memory()
+    assert solver.forward_step_host(hx, hv, control, params, ox, ov, cache) == 1
+    assert np.array_equal(ox.numpy(), nxt.positions.cpu().numpy())
+    assert np.array_equal(ov.numpy(), nxt.velocities.cpu().numpy())
+
+
+def test_vjp_requires_differentiable_mode():
+    sc = scenes.plain_small(lattice=(4, 4, 4))
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    nxt = step(solver, state, control, params, cache)
+    with pytest.raises(pbf.PBFError) as e:
+        solver.vjp_step(state, control, params, nxt, cache, solver.allocate_state_adjoint(),
+                        solver.allocate_state_adjoint(), solver.allocate_control_adjoint(),
+                        solver.allocate_parameter_adjoint())
+    assert e.value.status == 4
