@@ -50,48 +50,100 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and throttle-reason samples taken while the timed region runs.
+
+    A thread reads NVML (the source nvidia-smi prints) every 10 ms between start() and stop(), so
+    even a timed region of a few hundred milliseconds has dozens of samples; if NVML cannot be
+    loaded, nvidia-smi -lms 100 runs for the same window instead.  Reading clocks changes nothing.
+    """
+
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+                   "hw_power_brake_slowdown": 0x80}
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.path = pathlib.Path(f"/tmp/pbf_clocks_{os.getpid()}.csv")
+        self.samples = []     # (sm_mhz, reason bits)
+        self.max_mhz = None
+        self.source = None
+        self._stop = None
+        self._thread = None
+        self._proc = None
+        self._path = pathlib.Path(f"/tmp/pbf_clocks_{os.getpid()}.csv")
 
-    def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
         except Exception:
-            self.proc = None
-        return self
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
-    def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
+    def start(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self._stop = threading.Event()
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(reasons(h))))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.01)
+
+            self.source = "nvml"
+            self._thread = threading.Thread(target=run, daemon=True)
+            self._thread.start()
+        except Exception:
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
             try:
-                self.proc.wait(timeout=5)
+                self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                               "--format=csv,noheader,nounits", "-lms", "100"],
+                                              stdout=open(self._path, "w"), stderr=subprocess.DEVNULL)
+                self.source = "nvidia-smi"
             except Exception:
-                self.proc.kill()
+                self._proc = None
+
+    def stop(self):
+        if self._thread:
+            self._stop.set()
+            self._thread.join(timeout=5)
+            self._thread = None
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+            self._proc = None
+            try:
+                for r in self._path.read_text().strip().splitlines():
+                    f = [x.strip() for x in r.split(",")]
+                    if len(f) < 9 or not f[1].replace(".", "").isdigit():
+                        continue
+                    bits = 0
+                    for name, col in (("hw_slowdown", 5), ("hw_thermal_slowdown", 6), ("sw_thermal_slowdown", 7),
+                                      ("sw_power_cap", 8)):
+                        if f[col].startswith("Active"):
+                            bits |= self.REASON_BITS[name]
+                    self.samples.append((float(f[1]), bits))
+                    if f[2].replace(".", "").isdigit():
+                        self.max_mhz = float(f[2])
+            except Exception:
+                pass
 
     def summary(self):
-        try:
-            rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.strip()]
-        except Exception:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if len(r) > 2 and r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if len(r) > 2 and r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in rows:
-            for k, name in enumerate(names):
-                if len(r) > 5 + k and "Active" in r[5 + k] and "Not" not in r[5 + k]:
-                    reasons.add(name)
-        load = sorted(sm)[len(sm) // 4:] if sm else []
-        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
-                "samples": len(rows), "reasons": sorted(reasons)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "samples": 0, "reasons": ["unsampled"], "source": self.source}
+        reasons = sorted(name for name, bit in self.REASON_BITS.items() if any(b & bit for _, b in self.samples))
+        return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "samples": len(self.samples), "reasons": reasons, "source": self.source}
 
 
 def setup_dist():
@@ -120,11 +172,13 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
-def timed(step, steps, warmup, world, stream, flush):
+def timed(step, steps, warmup, world, stream, flush, clocks=None):
     for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     barrier(world)
+    if clocks is not None:
+        clocks.start()
     events = []
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -137,6 +191,8 @@ def timed(step, steps, warmup, world, stream, flush):
         b.record(stream)
         events.append((a, b))
     torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.stop()
     barrier(world)
     wall = time.perf_counter() - t0
     ms = sum(a.elapsed_time(b) for a, b in events)
@@ -162,8 +218,8 @@ def bench_b200(args, world, rank):
         holder["cur"], holder["nxt"] = holder["nxt"], holder["cur"]
 
     launches0 = pbf.launch_count()
-    with Clocks(torch.cuda.current_device()) as clk:
-        ms, wall = timed(step, args.steps, args.warmup, world, stream, flush)
+    clk = Clocks(torch.cuda.current_device())
+    ms, wall = timed(step, args.steps, args.warmup, world, stream, flush, clk)
     launches = pbf.launch_count() - launches0
     per_step_launches = launches / (args.steps + args.warmup)
     ms_max = max_over_ranks(ms, world)
@@ -181,9 +237,9 @@ def bench_b200(args, world, rank):
     neighbors = float(cache.read(CacheField.NEIGHBOR_COUNTS).double().mean())
     K = sc.pressure_iterations
     cells = solver.cells
-    bytes_per_particle = {"density_lambda": 16, "correction_project": 28, "vorticity": 36, "normal_confinement": 48,
+    bytes_per_particle = {"list_scan": 16, "density_lambda": 16, "correction_project": 28, "vorticity": 36, "normal_confinement": 48,
                           "xsph": 48}
-    flops_per_pair = {"density_lambda": 14 + 30, "correction_project": 25, "vorticity": 34, "normal_confinement": 26,
+    flops_per_pair = {"list_scan": 9, "density_lambda": 14 + 30, "correction_project": 25, "vorticity": 34, "normal_confinement": 26,
                       "xsph": 21}
     hbm, hbm_src = peaks()
     top = max((p for p in passes if p["name"] in bytes_per_particle), key=lambda p: p["ms"], default=None)
@@ -240,6 +296,10 @@ def bench_b200(args, world, rank):
     if not args.no_grad:
         grad = bench_grad(args, world, rank)
 
+    batched = None
+    if not args.no_batch:
+        batched = bench_batch(args, world, rank)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(sc)
@@ -253,7 +313,7 @@ def bench_b200(args, world, rank):
                    "l2": "flushed between timed steps (256 MiB write)", "wall_s": round(wall, 3)},
         "roofline": roofline, "step_roofline": step_roofline, "per_pass": per_pass,
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(round(per_step_launches * args.steps)),
-        "clocks": clk.summary(), "grad_steps_per_s": grad,
+        "clocks": clk.summary(), "grad_steps_per_s": grad, "batched_scenes": batched,
     }
 
 
@@ -290,13 +350,15 @@ def bench_grad(args, world, rank):
     solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
     targets = torch.from_numpy(sc.targets).cuda()
     steps = 20
-    trajectory.loss_and_gradients(solver, state, control, params, targets, 10, 10)   # warm-up
+    solver.set_graph_mode(True)
+    rollout = trajectory.Rollout(solver, control, params, steps, 10)   # buffers allocated once, outside the timing
+    trajectory.loss_and_gradients(solver, state, control, params, targets, steps, rollout=rollout)   # warm-up
     torch.cuda.synchronize()
     barrier(world)
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
     a.record(solver.stream)
-    g = trajectory.loss_and_gradients(solver, state, control, params, targets, steps, 10)
+    g = trajectory.loss_and_gradients(solver, state, control, params, targets, steps, rollout=rollout)
     b.record(solver.stream)
     torch.cuda.synchronize()
     ms = max_over_ranks(a.elapsed_time(b), world)
@@ -304,6 +366,47 @@ def bench_grad(args, world, rank):
             "config": {"workload": "differentiable_64k: 65,536 particles (32x64x32 lattice), v0 ~ N(0, 0.1), "
                                    "4 iterations, target-cloud loss", "rollout_steps": steps,
                        "trajectory_checkpoint_every": 10}, "loss": g.loss}
+
+
+def bench_batch(args, world, rank):
+    """256 independent scenes (2,048-65,536 particles, log-uniform): one batched launch sequence per
+    substep against one solver per scene, both on the same stream with CUDA events."""
+    from physica_b200 import pbf, scenes
+    scs = scenes.batched_forward(seed=4 + rank)
+    total = sum(s.count for s in scs)
+    batch, state, control, params = pbf.batch_for_scenes(scs)
+    batch.set_graph_mode(True)
+    nxt = batch.allocate_state()
+    holder = {"cur": state, "nxt": nxt}
+
+    def batched_step():
+        batch.forward_step(holder["cur"], control, params, holder["nxt"])
+        holder["cur"], holder["nxt"] = holder["nxt"], holder["cur"]
+
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    steps = max(3, min(args.steps, 10))
+    ms_b, _ = timed(batched_step, steps, 3, world, batch.stream, flush)
+    ms_b = max_over_ranks(ms_b, world) / steps
+
+    solvers = []
+    for sc in scs:
+        solver, st, ctl, prm = pbf.solver_for_scene(sc)
+        solver.set_graph_mode(True)
+        solvers.append([solver, st, solver.allocate_state(), ctl, prm, solver.allocate_step_cache()])
+
+    def loop_step():
+        for e in solvers:
+            e[0].forward_step(e[1], e[3], e[4], e[2], e[5])
+            e[1], e[2] = e[2], e[1]
+
+    ms_l, _ = timed(loop_step, steps, 3, world, solvers[0][0].stream, flush)
+    ms_l = max_over_ranks(ms_l, world) / steps
+    return {"unit": UNIT, "batched": round(world * total / (ms_b * 1e-3), 1),
+            "per_scene_solvers": round(world * total / (ms_l * 1e-3), 1), "speedup": round(ms_l / ms_b, 3),
+            "batched_ms_per_step": round(ms_b, 4), "per_scene_ms_per_step": round(ms_l, 4),
+            "config": {"workload": "batched_forward_256: 256 dam-break scenes, counts log-uniform in [2048, 65536], "
+                                   "4 iterations", "particles_per_gpu": total, "scenes_per_gpu": len(scs),
+                       "graphs": True}}
 
 
 def cpu_baseline(sc):
@@ -339,12 +442,13 @@ def bench_reference(args, world, rank):
         holder["v"], holder["vo"] = holder["vo"], holder["v"]
         holder["k"] += 1
 
-    with Clocks(torch.cuda.current_device()) as clk:
-        ms, wall = timed(step, args.steps, args.warmup, world, stream, flush)
+    clk = Clocks(torch.cuda.current_device())
+    ms, wall = timed(step, args.steps, args.warmup, world, stream, flush, clk)
     ms_max = max_over_ranks(ms, world)
     ms_per_step = ms_max / args.steps
     value = world * n / (ms_per_step * 1e-3)
     grad = None if args.no_grad else bench_reference_grad(world, rank)
+    batched = None if args.no_batch else bench_reference_batch(args, world, rank)
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
@@ -358,8 +462,64 @@ def bench_reference(args, world, rank):
                                    "compiled from its sources) replaying PBF::forward_step on the same B200; the reference "
                                    "has no CPU implementation of this path"},
         "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "clocks": clk.summary(), "grad_steps_per_s": grad,
+        "clocks": clk.summary(), "grad_steps_per_s": grad, "batched_scenes": batched,
     }
+
+
+def bench_reference_batch(args, world, rank):
+    """The 256-scene batched workload through the reference: one reference solver per scene, each on
+    its own stream as the reference's solvers are, stepped in turn (the reference has no batched form)."""
+    from oracle import reference
+    from physica_b200 import scenes
+    scs = scenes.batched_forward(seed=4 + rank)
+    total = sum(s.count for s in scs)
+    entries = []
+    for sc in scs:
+        ref = reference.ReferencePBF(sc)
+        x = torch.from_numpy(sc.positions).cuda().contiguous()
+        v = torch.from_numpy(sc.velocities).cuda().contiguous()
+        entries.append({"ref": ref, "x": x, "v": v, "xo": torch.zeros_like(x), "vo": torch.zeros_like(v), "k": 0})
+    torch.cuda.synchronize()
+
+    def step():
+        for e in entries:
+            e["ref"].forward_step(e["x"], e["v"], e["xo"], e["vo"], e["k"], synchronize=False)
+            e["x"], e["xo"] = e["xo"], e["x"]
+            e["v"], e["vo"] = e["vo"], e["v"]
+            e["k"] += 1
+
+    # each reference solver owns a non-blocking stream: the timed window opens with an event on the
+    # first stream that every other stream waits on, and closes after the first stream waits on all
+    streams = [torch.cuda.ExternalStream(e["ref"].stream) for e in entries]
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    steps = max(3, min(args.steps, 10))
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    total_ms = 0.0
+    for _ in range(steps):
+        flush.add_(1.0)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(streams[0])
+        for st in streams[1:]:
+            st.wait_event(a)
+        step()
+        for st in streams[1:]:
+            done = torch.cuda.Event()
+            done.record(st)
+            streams[0].wait_event(done)
+        b.record(streams[0])
+        b.synchronize()
+        total_ms += a.elapsed_time(b)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(total_ms, world) / steps
+    return {"unit": UNIT, "per_scene_solvers": round(world * total / (ms * 1e-3), 1), "per_scene_ms_per_step": round(ms, 4),
+            "config": {"workload": "batched_forward_256: 256 dam-break scenes, counts log-uniform in [2048, 65536], "
+                                   "4 iterations", "particles_per_gpu": total, "scenes_per_gpu": len(scs)}}
 
 
 def bench_reference_grad(world, rank):
@@ -424,6 +584,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -272,6 +272,12 @@ int pbf_profile_read(pbf_solver* solver, pbf_pass_time* passes, uint32_t capacit
 int pbf_batch_profile_enable(pbf_batch* batch, int enable);
 int pbf_batch_profile_read(pbf_batch* batch, pbf_pass_time* passes, uint32_t capacity, uint32_t* count);
 
+/* ---- CUDA-graph replay of the forward substep: the launch sequence is captured once per set of
+ *      state / control / parameter / cache buffers and replayed with one graph launch per call
+ *      (default off for a solver, on for a batch).  No reference counterpart. ---- */
+int pbf_set_graph_mode(pbf_solver* solver, int enable);
+int pbf_batch_set_graph_mode(pbf_batch* batch, int enable);
+
 /* ---- misc ---- */
 int pbf_synchronize(pbf_solver* solver);
 int pbf_batch_synchronize(pbf_batch* batch);

@@ -38,12 +38,6 @@ namespace {
 
 using namespace gather_detail;
 
-struct StoredList {
-    const uint32_t* entries;
-    const uint32_t* counts;
-    uint32_t capacity;
-};
-
 // Caller-side FP64 outputs (original order); null pointers are skipped.
 struct ParamAdjoint {
     double* masses;
@@ -145,6 +139,8 @@ struct XsphVjpOp {
     d3 pc, vc;
     double cc;
 
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
         if (t == self) return;
         const f3 d = sub(x, xyz(pos[t]));
@@ -166,8 +162,6 @@ struct XsphVjpOp {
 };
 
 __global__ void __launch_bounds__(kBlock) xsph_vjp_kernel(const XsphVjpArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     XsphVjpOp op;
     op.pos = a.pos;
@@ -184,7 +178,7 @@ __global__ void __launch_bounds__(kBlock) xsph_vjp_kernel(const XsphVjpArgs a) {
     op.pc = {0.0, 0.0, 0.0};
     op.vc = op.ob;
     op.cc = 0.0;
-    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list.entries, a.list.counts, a.list.capacity);
+    replay(op, p, a.g, a.list);
     if (!p.active) return;
     const uint32_t i = a.sorted_index[p.s];
     a.x[p.s] = st3(ld3(a.x[p.s]) + op.pc);
@@ -225,6 +219,8 @@ struct NormalVjpOp {
     d3 pc;
     double mc;
 
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
         if (t == self) return;
         const f3 d = sub(x, xyz(pos[t]));
@@ -245,8 +241,6 @@ struct NormalVjpOp {
 };
 
 __global__ void __launch_bounds__(kBlock) normal_vjp_kernel(const NormalVjpArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     NormalVjpOp op;
     op.pos = a.pos;
@@ -260,7 +254,7 @@ __global__ void __launch_bounds__(kBlock) normal_vjp_kernel(const NormalVjpArgs 
     op.eb = p.active ? ld3(a.eta[p.s]) : d3{0, 0, 0};
     op.pc = {0.0, 0.0, 0.0};
     op.mc = 0.0;
-    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list.entries, a.list.counts, a.list.capacity);
+    replay(op, p, a.g, a.list);
     if (!p.active) return;
     a.x[p.s] = st3(ld3(a.x[p.s]) + op.pc);
     if (wi.w > 0.0F) a.vorticity_adjoint[p.s] = st3(ld3(a.vorticity_adjoint[p.s]) + times(xyz(wi), op.mc / wi.w));
@@ -289,6 +283,8 @@ struct VorticityVjpOp {
     KernelConstants k;
     d3 pc, vc;
 
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
         if (t == self) return;
         const f3 d = sub(x, xyz(pos[t]));
@@ -309,8 +305,6 @@ struct VorticityVjpOp {
 };
 
 __global__ void __launch_bounds__(kBlock) vorticity_vjp_kernel(const VorticityVjpArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     VorticityVjpOp op;
     op.pos = a.pos;
@@ -323,7 +317,7 @@ __global__ void __launch_bounds__(kBlock) vorticity_vjp_kernel(const VorticityVj
     op.wb = p.active ? ld3(a.vorticity_adjoint[p.s]) : d3{0, 0, 0};
     op.pc = {0.0, 0.0, 0.0};
     op.vc = {0.0, 0.0, 0.0};
-    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list.entries, a.list.counts, a.list.capacity);
+    replay(op, p, a.g, a.list);
     if (!p.active) return;
     const uint32_t i = a.sorted_index[p.s];
     d3 xb = ld3(a.x[p.s]) + op.pc;
@@ -365,6 +359,8 @@ struct CorrectionVjpOp {
     d3 pc;
     double lc, mc, rc, sc, ec, qc;
 
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
         if (t == self) return;
         const float4 q = pos[t];
@@ -402,8 +398,6 @@ struct CorrectionVjpOp {
 };
 
 __global__ void __launch_bounds__(kBlock) correction_vjp_kernel(const CorrectionVjpArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     CorrectionVjpOp op;
     op.pos = a.pos;
@@ -426,7 +420,7 @@ __global__ void __launch_bounds__(kBlock) correction_vjp_kernel(const Correction
     op.ob = p.active ? ld3(a.correction[p.s]) : d3{0, 0, 0};
     op.pc = {0.0, 0.0, 0.0};
     op.lc = op.mc = op.rc = op.sc = op.ec = op.qc = 0.0;
-    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list.entries, a.list.counts, a.list.capacity);
+    replay(op, p, a.g, a.list);
     if (!p.active) return;
     const uint32_t i = a.sorted_index[p.s];
     a.x[p.s] = st3(ld3(a.x[p.s]) + op.pc);
@@ -468,6 +462,8 @@ struct LambdaVjpOp {
     double mc;
     f3 self_gradient;
 
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
         if (t == self) return;
         const float4 q = pos[t];
@@ -508,6 +504,8 @@ struct LambdaVjpSecondOp {
     KernelConstants k;
     double rc;
 
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
         if (t == self) return;
         const float4 q = pos[t];
@@ -522,8 +520,6 @@ struct LambdaVjpSecondOp {
 };
 
 __global__ void __launch_bounds__(kBlock) lambda_vjp_kernel(const LambdaVjpArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     LambdaVjpOp op;
     op.pos = a.pos;
@@ -547,7 +543,7 @@ __global__ void __launch_bounds__(kBlock) lambda_vjp_kernel(const LambdaVjpArgs 
     op.pc = {0.0, 0.0, 0.0};
     op.mc = 0.0;
     op.self_gradient = mk(0.0F, 0.0F, 0.0F);
-    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list.entries, a.list.counts, a.list.capacity);
+    replay(op, p, a.g, a.list);
     double rc = lb * rho / (static_cast<double>(gi.w) * pa.x * pa.x);
     rc -= dot(op.sb, op.self_gradient) / pa.x;
     LambdaVjpSecondOp second;
@@ -558,7 +554,7 @@ __global__ void __launch_bounds__(kBlock) lambda_vjp_kernel(const LambdaVjpArgs 
     second.self = p.s;
     second.k = p.k;
     second.rc = rc;
-    replay<true>(second, p, a.g, a.pos, p.k.list_threshold, ws, a.list.entries, a.list.counts, a.list.capacity);
+    replay(second, p, a.g, a.list);
     if (!p.active) return;
     const uint32_t i = a.sorted_index[p.s];
     a.x[p.s] = st3(ld3(a.x[p.s]) + op.pc);
@@ -590,6 +586,8 @@ struct DensityVjpOp {
     d3 pc;
     double mc;
 
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
         const float4 q = pos[t];
         const f3 d = sub(x, xyz(q));
@@ -602,8 +600,6 @@ struct DensityVjpOp {
 };
 
 __global__ void __launch_bounds__(kBlock) density_vjp_kernel(const DensityVjpArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
     DensityVjpOp op;
     op.pos = a.pos;
@@ -615,7 +611,7 @@ __global__ void __launch_bounds__(kBlock) density_vjp_kernel(const DensityVjpArg
     op.ob = p.active ? a.density_adjoint[p.s] : 0.0;
     op.pc = {0.0, 0.0, 0.0};
     op.mc = 0.0;
-    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list.entries, a.list.counts, a.list.capacity);
+    replay(op, p, a.g, a.list);
     if (!p.active) return;
     const uint32_t i = a.sorted_index[p.s];
     const d3 xb = ld3(a.x[p.s]) + op.pc;

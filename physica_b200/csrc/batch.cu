@@ -22,6 +22,7 @@ int pbf_batch_create(const pbf_domain_configuration* scenes, const uint32_t scen
         auto b = std::make_unique<pbf_batch>();
         const int rc = b->engine.init(scenes, scene_count, configuration, mode, static_cast<cudaStream_t>(cuda_stream));
         if (rc) return rc;
+        b->engine.set_graphs(true);   // one graph launch per substep
         *batch = b.release();
         return PBF_SUCCESS;
     } catch (...) {
@@ -117,6 +118,12 @@ int pbf_batch_scene_sums(pbf_batch* batch, const double* values, double* result)
     return batch->engine.check(pbf::launch_segment_sums(batch->engine.stream(), values, batch->scene_first, batch->scene_count, n, 0,
                                                         result),
                                "batch scene sums");
+}
+
+int pbf_batch_set_graph_mode(pbf_batch* batch, const int enable) {
+    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
+    batch->engine.set_graphs(enable != 0);
+    return PBF_SUCCESS;
 }
 
 int pbf_batch_profile_enable(pbf_batch* batch, const int enable) {

@@ -116,6 +116,7 @@ int pbf_free_step_cache(pbf_step_cache* cache) {
     if (!cache) return PBF_SUCCESS;
     return guarded([&] {
         cudaStreamSynchronize(cache->solver->engine.stream());
+        cache->solver->engine.forget(&cache->record);
         delete cache;
         return static_cast<int>(PBF_SUCCESS);
     });
@@ -288,6 +289,12 @@ int pbf_sum_compensated(pbf_solver* solver, const double* values, const uint32_t
     if (!solver || !result || (count && !values)) return null_arg("solver/values/result");
     return solver->engine.check(pbf::launch_segment_sums(solver->engine.stream(), values, nullptr, nullptr, 1, count, result),
                                 "sum_compensated");
+}
+
+int pbf_set_graph_mode(pbf_solver* solver, const int enable) {
+    if (!solver) return null_arg("solver");
+    solver->engine.set_graphs(enable != 0);
+    return PBF_SUCCESS;
 }
 
 int pbf_profile_enable(pbf_solver* solver, const int enable) {

@@ -5,6 +5,7 @@
 //   K x [density+lambda, correction+project(+reconstruct on the last)]  2K kernels
 //   vorticity(+magnitude), normal(+confinement), XSPH(+write-back)      3 kernels
 // All launches are asynchronous on the engine's stream; nothing synchronises.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -25,7 +26,7 @@ void count_launch(const unsigned n) { g_launches.fetch_add(n, std::memory_order_
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 const char* pass_name(const int pass) {
-    static const char* names[kPassCount] = {"grid_build", "density_lambda", "correction_project", "vorticity",
+    static const char* names[kPassCount] = {"grid_build", "list_scan", "density_lambda", "correction_project", "vorticity",
                                             "normal_confinement", "xsph", "adjoint_seed", "xsph_vjp", "normal_vjp",
                                             "vorticity_vjp", "correction_vjp", "lambda_vjp", "density_vjp"};
     return pass >= 0 && pass < kPassCount ? names[pass] : "unknown";
@@ -112,6 +113,9 @@ int Engine::check(const cudaError_t e, const char* what) {
 void destroy_adjoint_workspace(void* workspace);
 
 Engine::~Engine() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    drop_graphs();
+    if (capture_stream_) cudaStreamDestroy(capture_stream_);
     destroy_adjoint_workspace(adjoint_);
     adjoint_ = nullptr;
     arena_.release();
@@ -212,18 +216,13 @@ int Engine::init(const pbf_domain_configuration* scenes, const uint32_t scene_co
         e = cudaStreamSynchronize(stream_);
         if (int rc = check(e, "synchronise")) return rc;
     }
-    table_step_ = ~0ull;
-    return check(cudaStreamSynchronize(stream_), "engine initialisation");
-}
-
-int Engine::update_scene_table(const uint64_t step_index) {
-    if (table_step_ == step_index) return PBF_SUCCESS;
-    for (size_t s = 0; s < scenes_.size(); ++s) {
+    // Time-independent scene table; the per-step fields are derived on the device from a step counter.
+    std::vector<SceneStatic> statics(scene_count);
+    for (uint32_t s = 0; s < scene_count; ++s) {
         const SceneHost& h = scenes_[s];
         const pbf_domain_configuration& c = h.config;
         SceneDesc& d = scene_table_[s];
-        // The step computes state step_index + 1 (pbf/pbf.cpp:170, 178): time = float(step + 1) * dt.
-        const float time = static_cast<float>(step_index + 1u) * c.time_step;
+        d = SceneDesc{};
         d.grid.cells_x = h.dims[0];
         d.grid.cells_y = h.dims[1];
         d.grid.cells_z = h.dims[2];
@@ -234,32 +233,52 @@ int Engine::update_scene_table(const uint64_t step_index) {
         d.grid.key_vel_x = c.boundary.velocity.x;
         d.grid.key_vel_y = c.boundary.velocity.y;
         d.grid.key_vel_z = c.boundary.velocity.z;
-        d.grid.time = time;
         d.grid.cell_size = c.support_radius;
-        // gather-side origin (neighborhood/neighborhood.cpp:83-88)
-        d.grid.origin_x = c.boundary.minimum.x + time * c.boundary.velocity.x;
-        d.grid.origin_y = c.boundary.minimum.y + time * c.boundary.velocity.y;
-        d.grid.origin_z = c.boundary.minimum.z + time * c.boundary.velocity.z;
-        // collision box (pbf/pbf.cpp:17-31)
-        d.box.min_x = c.boundary.minimum.x + time * c.boundary.velocity.x + c.particle_radius;
-        d.box.min_y = c.boundary.minimum.y + time * c.boundary.velocity.y + c.particle_radius;
-        d.box.min_z = c.boundary.minimum.z + time * c.boundary.velocity.z + c.particle_radius;
-        d.box.max_x = c.boundary.maximum.x + time * c.boundary.velocity.x - c.particle_radius;
-        d.box.max_y = c.boundary.maximum.y + time * c.boundary.velocity.y - c.particle_radius;
-        d.box.max_z = c.boundary.maximum.z + time * c.boundary.velocity.z - c.particle_radius;
         d.first = h.first;
         d.count = c.particle_count;
         d.time_step = c.time_step;
-        d.inverse_time_step = 1.0F / c.time_step;
+        d.inverse_time_step = 1.0F / c.time_step;   // pbf/pbf.cpp:184, evaluated on the host in float
         d.gravity_x = c.gravity.x;
         d.gravity_y = c.gravity.y;
         d.gravity_z = c.gravity.z;
-        d.constants = static_cast<uint32_t>(s);
+        d.constants = s;
+        statics[s] = {c.boundary.minimum.x, c.boundary.minimum.y, c.boundary.minimum.z, c.boundary.maximum.x,
+                      c.boundary.maximum.y, c.boundary.maximum.z, c.boundary.velocity.x, c.boundary.velocity.y,
+                      c.boundary.velocity.z, c.particle_radius};
     }
-    const cudaError_t e = cudaMemcpyAsync(d_scenes_, scene_table_.data(), scene_table_.size() * sizeof(SceneDesc),
-                                          cudaMemcpyHostToDevice, stream_);
-    if (e == cudaSuccess) table_step_ = step_index;
-    return check(e, "upload scene table");
+    d_static_ = arena_.alloc<SceneStatic>(scene_count, e);
+    d_step_ = arena_.alloc<unsigned long long>(1, e);
+    if (int rc = check(e, "device allocation")) return rc;
+    e = cudaMemcpyAsync(d_scenes_, scene_table_.data(), scene_count * sizeof(SceneDesc), cudaMemcpyHostToDevice, stream_);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_static_, statics.data(), scene_count * sizeof(SceneStatic), cudaMemcpyHostToDevice, stream_);
+    if (int rc = check(e, "upload scene table")) return rc;
+    host_step_ = ~0ull;
+    if (int rc = check(cudaStreamCreateWithFlags(&capture_stream_, cudaStreamNonBlocking), "capture stream")) return rc;
+    return check(cudaStreamSynchronize(stream_), "engine initialisation");
+}
+
+bool Engine::GraphKey::operator==(const GraphKey& o) const {
+    if (record != o.record) return false;
+    for (int k = 0; k < 16; ++k)
+        if (p[k] != o.p[k]) return false;
+    return true;
+}
+
+void Engine::drop_graphs() {
+    for (auto& g : graph_cache_) cudaGraphExecDestroy(g.exec);
+    graph_cache_.clear();
+}
+
+void Engine::forget(const StepRecord* record) {
+    for (size_t k = 0; k < graph_cache_.size();) {
+        if (graph_cache_[k].key.record == record) {
+            cudaGraphExecDestroy(graph_cache_[k].exec);
+            graph_cache_.erase(graph_cache_.begin() + static_cast<long>(k));
+        } else {
+            ++k;
+        }
+    }
 }
 
 int Engine::allocate_record(StepRecord& r) {
@@ -333,7 +352,82 @@ int Engine::forward(const pbf_particle_state* state, const pbf_control* control,
             return PBF_ERROR_INVALID_ARGUMENT;
         }
     }
-    if (int rc = update_scene_table(state->step_index)) return rc;
+    // The device step counter holds the index of the state being advanced.
+    if (host_step_ != state->step_index) {
+        if (int rc = check(launch_set_step(stream_, d_step_, state->step_index), "step counter")) return rc;
+        host_step_ = state->step_index;
+    }
+    int rc = PBF_SUCCESS;
+    if (graphs_ && !timer_.enabled()) {
+        GraphKey key{};
+        const void* ptrs[16] = {state->positions.x, state->positions.y, state->positions.z, state->velocities.x,
+                                state->velocities.y, state->velocities.z, control->external_accelerations.x,
+                                control->external_accelerations.y, control->external_accelerations.z, parameters->masses,
+                                parameters->rest_densities, parameters->relaxation, parameters->xsph_viscosity,
+                                next_state->positions.x, next_state->velocities.x, parameters->vorticity_confinement};
+        for (int k = 0; k < 16; ++k) key.p[k] = ptrs[k];
+        key.record = &r;
+        cudaGraphExec_t exec = nullptr;
+        unsigned captured_launches = 0;
+        for (size_t k = 0; k < graph_cache_.size(); ++k) {
+            const GraphEntry& g = graph_cache_[k];
+            if (g.key == key && g.extra[0] == parameters->artificial_pressure_strength &&
+                g.extra[1] == parameters->artificial_pressure_exponent && g.extra[2] == parameters->artificial_pressure_radius &&
+                g.extra[3] == next_state->positions.y && g.extra[4] == next_state->positions.z &&
+                g.extra[5] == next_state->velocities.y && g.extra[6] == next_state->velocities.z) {
+                exec = g.exec;
+                captured_launches = g.launches;
+                // least recently used entries sit at the front
+                std::rotate(graph_cache_.begin() + static_cast<long>(k), graph_cache_.begin() + static_cast<long>(k) + 1,
+                            graph_cache_.end());
+                break;
+            }
+        }
+        if (!exec) {
+            cudaGraph_t graph = nullptr;
+            if ((rc = check(cudaStreamBeginCapture(capture_stream_, cudaStreamCaptureModeThreadLocal), "begin capture")))
+                return rc;
+            const uint64_t before = launch_count();
+            rc = launch_forward(capture_stream_, state, control, parameters, next_state, r);
+            captured_launches = static_cast<unsigned>(launch_count() - before);
+            const cudaError_t ce = cudaStreamEndCapture(capture_stream_, &graph);
+            if (rc) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
+            if ((rc = check(ce, "end capture"))) return rc;
+            rc = check(cudaGraphInstantiate(&exec, graph, 0), "instantiate graph");
+            cudaGraphDestroy(graph);
+            if (rc) return rc;
+            if (graph_cache_.size() >= kGraphCacheEntries) {
+                cudaGraphExecDestroy(graph_cache_.front().exec);
+                graph_cache_.erase(graph_cache_.begin());
+            }
+            GraphEntry entry{key, exec, {parameters->artificial_pressure_strength, parameters->artificial_pressure_exponent,
+                                         parameters->artificial_pressure_radius, next_state->positions.y,
+                                         next_state->positions.z, next_state->velocities.y, next_state->velocities.z},
+                             captured_launches};
+            graph_cache_.push_back(entry);
+        } else {
+            count_launch(captured_launches);   // the replayed kernels (capture counted them the first time)
+        }
+        rc = check(cudaGraphLaunch(exec, stream_), "graph launch");
+    } else {
+        rc = launch_forward(stream_, state, control, parameters, next_state, r);
+    }
+    if (rc) return rc;
+    host_step_ = state->step_index + 1u;
+    next_state->step_index = state->step_index + 1u;
+    r.valid = true;
+    r.step_index = state->step_index;
+    return PBF_SUCCESS;
+}
+
+int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state, const pbf_control* control,
+                           const pbf_parameters* parameters, pbf_particle_state* next_state, StepRecord& r) {
+    if (int rc = check(launch_scene_time(stream, d_static_, d_scenes_, d_step_, static_cast<uint32_t>(scenes_.size())),
+                       "scene table"))
+        return rc;
     const bool diff = differentiable();
     const uint32_t K = iterations_;
     GridBuildArgs g{};
@@ -359,9 +453,9 @@ int Engine::forward(const pbf_particle_state* state, const pbf_control* control,
     g.topology = r.topology;
     g.params_a = r.params_a;
     g.params_b = r.params_b;
-    timer_.begin(stream_, kPassGrid);
-    if (int rc = check(launch_grid_build(stream_, g), "grid build")) return rc;
-    timer_.end(stream_, kPassGrid);
+    timer_.begin(stream, kPassGrid);
+    if (int rc = check(launch_grid_build(stream, g), "grid build")) return rc;
+    timer_.end(stream, kPassGrid);
 
     const GatherCommon gc{count_, d_scenes_, d_constants_, r.cell_offsets, r.cell, r.params_a, r.params_b};
     const Field3 previous{state->positions.x, state->positions.y, state->positions.z};
@@ -371,44 +465,47 @@ int Engine::forward(const pbf_particle_state* state, const pbf_control* control,
         float4* xk1 = const_cast<float4*>(r.iterate(k + 1, K, diff));
         float* lam = diff ? r.lambda[k] : (k == 0 ? r.first_lambda : r.lambda[0]);
         const uint32_t l = diff ? k : 0u;
+        const StoredList list{r.list_entries[l], r.list_counts[l], r.list_capacity};
+        timer_.begin(stream, kPassListScan);
+        if (int rc = check(launch_list_scan(stream, ListScanArgs{gc, xk, list}), "neighbour list scan")) return rc;
+        timer_.end(stream, kPassListScan);
         DensityLambdaArgs d{gc, xk, lam, diff ? r.density[k] : (k == 0 ? r.first_density : nullptr),
-                            diff ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr,
-                            r.list_entries[l], r.list_counts[l], r.list_capacity};
-        timer_.begin(stream_, kPassDensityLambda);
-        if (int rc = check(launch_density_lambda(stream_, d, block_), "density/lambda")) return rc;
-        timer_.end(stream_, kPassDensityLambda);
+                            diff ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr, list};
+        timer_.begin(stream, kPassDensityLambda);
+        if (int rc = check(launch_density_lambda(stream, d, block_), "density/lambda")) return rc;
+        timer_.end(stream, kPassDensityLambda);
         CorrectionArgs c{gc, xk, lam, xk1, diff ? r.mask[k] : nullptr, k + 1 == K ? 1 : 0, previous, r.sorted_index,
-                         out_positions, r.velocity, r.list_entries[l], r.list_counts[l], r.list_capacity};
-        timer_.begin(stream_, kPassCorrection);
-        if (int rc = check(launch_correction(stream_, c, block_), "correction/project")) return rc;
-        timer_.end(stream_, kPassCorrection);
+                         out_positions, r.velocity, list};
+        timer_.begin(stream, kPassCorrection);
+        if (int rc = check(launch_correction(stream, c, block_), "correction/project")) return rc;
+        timer_.end(stream, kPassCorrection);
     }
     const float4* xK = r.iterate(K, K, diff);
     if (K == 0) {
-        if (int rc = check(launch_reconstruct(stream_, count_, d_scenes_, r.cell, r.topology, previous, r.sorted_index,
+        if (int rc = check(launch_reconstruct(stream, count_, d_scenes_, r.cell, r.topology, previous, r.sorted_index,
                                               out_positions, r.velocity),
                            "reconstruct"))
             return rc;
     }
     const uint32_t lp = diff ? K : 0u;
-    VorticityArgs v{gc, xK, r.velocity, r.vorticity, r.list_entries[lp], r.list_counts[lp], r.list_capacity};
-    timer_.begin(stream_, kPassVorticity);
-    if (int rc = check(launch_vorticity(stream_, v, block_), "vorticity")) return rc;
-    timer_.end(stream_, kPassVorticity);
-    NormalArgs nm{gc, xK, r.velocity, r.vorticity, r.normal, r.confined, r.list_entries[lp], r.list_counts[lp],
-                  r.list_capacity};
-    timer_.begin(stream_, kPassNormal);
-    if (int rc = check(launch_normal(stream_, nm, block_), "normal/confinement")) return rc;
-    timer_.end(stream_, kPassNormal);
+    const StoredList post{r.list_entries[lp], r.list_counts[lp], r.list_capacity};
+    timer_.begin(stream, kPassListScan);
+    if (int rc = check(launch_list_scan(stream, ListScanArgs{gc, xK, post}), "neighbour list scan")) return rc;
+    timer_.end(stream, kPassListScan);
+    VorticityArgs v{gc, xK, r.velocity, r.vorticity, post};
+    timer_.begin(stream, kPassVorticity);
+    if (int rc = check(launch_vorticity(stream, v, block_), "vorticity")) return rc;
+    timer_.end(stream, kPassVorticity);
+    NormalArgs nm{gc, xK, r.velocity, r.vorticity, r.normal, r.confined, post};
+    timer_.begin(stream, kPassNormal);
+    if (int rc = check(launch_normal(stream, nm, block_), "normal/confinement")) return rc;
+    timer_.end(stream, kPassNormal);
     XsphArgs x{gc, xK, r.confined, r.sorted_index, {next_state->velocities.x, next_state->velocities.y, next_state->velocities.z},
-               r.list_entries[lp], r.list_counts[lp], r.list_capacity};
-    timer_.begin(stream_, kPassXsph);
-    if (int rc = check(launch_xsph(stream_, x, block_), "xsph")) return rc;
-    timer_.end(stream_, kPassXsph);
-    next_state->step_index = state->step_index + 1u;
-    r.valid = true;
-    r.step_index = state->step_index;
-    return PBF_SUCCESS;
+               post};
+    timer_.begin(stream, kPassXsph);
+    if (int rc = check(launch_xsph(stream, x, block_), "xsph")) return rc;
+    timer_.end(stream, kPassXsph);
+    return check(launch_advance_step(stream, d_step_), "step counter");
 }
 
 int Engine::read(const StepRecord& r, const pbf_cache_field field, void* destination, const size_t bytes) {

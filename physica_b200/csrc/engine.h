@@ -94,6 +94,7 @@ struct StepRecord {
 
 enum PassId : int {
     kPassGrid = 0,
+    kPassListScan,
     kPassDensityLambda,
     kPassCorrection,
     kPassVorticity,
@@ -164,10 +165,36 @@ public:
 
     int check(cudaError_t e, const char* what);
     PassTimer& timer() { return timer_; }
+    // Replay the forward launch sequence as a CUDA graph, captured once per buffer set.
+    void set_graphs(bool on) { graphs_ = on; }
+    bool graphs() const { return graphs_; }
+    void forget(const StepRecord* record);
 
 private:
+    struct GraphKey {
+        const void* p[16];
+        const StepRecord* record;
+        bool operator==(const GraphKey& o) const;
+    };
+    struct GraphEntry {
+        GraphKey key;
+        cudaGraphExec_t exec;
+        const void* extra[7];   // the remaining parameter / next-state pointers
+        unsigned launches;      // kernels in the captured sequence
+    };
+    int launch_forward(cudaStream_t s, const pbf_particle_state* state, const pbf_control* control,
+                       const pbf_parameters* parameters, pbf_particle_state* next_state, StepRecord& record);
+    void drop_graphs();
+    // Instantiated forward graphs kept per solver (one per buffer set; least recently used dropped).
+    static constexpr size_t kGraphCacheEntries = 32;
+
     PassTimer timer_;
-    int update_scene_table(uint64_t step_index);
+    bool graphs_ = false;
+    cudaStream_t capture_stream_ = nullptr;
+    std::vector<GraphEntry> graph_cache_;
+    SceneStatic* d_static_ = nullptr;
+    unsigned long long* d_step_ = nullptr;
+    uint64_t host_step_ = ~0ull;   // step index the device counter holds
 
     uint32_t count_ = 0;
     uint64_t cells_ = 0;
@@ -187,7 +214,6 @@ private:
     uint32_t* arrival_ = nullptr;
     uint32_t* unordered_ = nullptr;
     uint32_t* tile_sums_ = nullptr;
-    uint64_t table_step_ = ~0ull;
     friend struct AdjointWorkspace;
     void* adjoint_ = nullptr;  // AdjointWorkspace*, differentiable mode
 };

@@ -25,6 +25,89 @@ namespace {
 
 using namespace gather_detail;
 
+// --------------------------------------------------------------- list scan
+// Builds the ordered neighbour list of every particle over the positions `pos` (gather.cuh).
+__global__ void __launch_bounds__(kBlock) list_scan_kernel(const ListScanArgs a) {
+    __shared__ float4 home_s[kWarpsPerBlock][32];
+    __shared__ uint32_t first_s[kWarpsPerBlock][32];
+    __shared__ uint32_t base_s[kWarpsPerBlock][32];
+    const uint32_t w = threadIdx.x >> 5, lane = lane_id();
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = s < a.g.count;
+    const int4 c = active ? a.g.cell[s] : make_int4(0, 0, 0, 0);
+    const float threshold = active ? a.g.constants[a.g.scenes[c.w].constants].list_threshold : 0.0F;
+    const uint32_t warp_first = s - lane;
+    const int nact = __popc(__ballot_sync(kFull, active));
+    home_s[w][lane] = active ? a.pos[s] : make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+    const int px = __shfl_up_sync(kFull, c.x, 1), py = __shfl_up_sync(kFull, c.y, 1);
+    const int pz = __shfl_up_sync(kFull, c.z, 1), pw = __shfl_up_sync(kFull, c.w, 1);
+    const bool start = active && (lane == 0 || px != c.x || py != c.y || pz != c.z || pw != c.w);
+    uint32_t starts = __ballot_sync(kFull, start);
+    const unsigned lower = (1u << lane) - 1u;
+    const uint32_t cap = a.list.capacity;
+    uint32_t* __restrict__ entries = a.list.entries + static_cast<size_t>(s >> 5) * cap * 32u;
+    uint32_t n = 0;
+    __syncwarp();
+    while (starts) {
+        const int ra = __ffs(starts) - 1;
+        starts &= starts - 1u;
+        const int rb = starts ? __ffs(starts) - 1 : nact;
+        const int hx = __shfl_sync(kFull, c.x, ra), hy = __shfl_sync(kFull, c.y, ra);
+        const int hz = __shfl_sync(kFull, c.z, ra), hw = __shfl_sync(kFull, c.w, ra);
+        const float thr = __shfl_sync(kFull, threshold, ra);
+        const Grid& grid = a.g.scenes[hw].grid;
+        uint32_t first = 0, cnt = 0;
+        if (lane < 27u) {
+            const int x = hx + static_cast<int>(lane) / 9 - 1;
+            const int y = hy + (static_cast<int>(lane) / 3) % 3 - 1;
+            const int z = hz + static_cast<int>(lane) % 3 - 1;
+            if (x >= 0 && y >= 0 && z >= 0 && x < static_cast<int>(grid.cells_x) && y < static_cast<int>(grid.cells_y) &&
+                z < static_cast<int>(grid.cells_z)) {
+                const uint32_t cell = grid.cell_base +
+                                      (static_cast<uint32_t>(z) * grid.cells_y + static_cast<uint32_t>(y)) * grid.cells_x +
+                                      static_cast<uint32_t>(x);
+                first = a.g.cell_offsets[cell];
+                cnt = a.g.cell_offsets[cell + 1u] - first;
+            }
+        }
+        uint32_t inc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, inc, o);
+            if (lane >= static_cast<uint32_t>(o)) inc += v;
+        }
+        const uint32_t total = __shfl_sync(kFull, inc, 31);
+        __syncwarp();
+        first_s[w][lane] = first;
+        base_s[w][lane] = lane < 27u ? inc - cnt : total;
+        __syncwarp();
+        for (uint32_t u0 = 0; u0 < total; u0 += 32u) {
+            const uint32_t u = u0 + lane;
+            const bool valid = u < total;
+            uint32_t o = 0;
+#pragma unroll
+            for (uint32_t step = 16; step > 0; step >>= 1)
+                if (base_s[w][o + step] <= u) o += step;
+            const uint32_t t = first_s[w][o] + (u - base_s[w][o]);
+            const float4 q = valid ? a.pos[t] : make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+            for (int h = ra; h < rb; ++h) {
+                const float4 xh = home_s[w][h];
+                const float r2 = squared(mk(__fsub_rn(xh.x, q.x), __fsub_rn(xh.y, q.y), __fsub_rn(xh.z, q.z)));
+                const bool in = valid && r2 < thr;
+                const unsigned m = __ballot_sync(kFull, in);
+                if (m) {
+                    const uint32_t nh = __shfl_sync(kFull, n, h);
+                    const uint32_t k = nh + __popc(m & lower);
+                    if (in && k < cap) entries[static_cast<size_t>(k) * 32u + static_cast<uint32_t>(h)] = t;
+                    if (static_cast<int>(lane) == h) n += __popc(m);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (active) a.list.counts[s] = n <= cap ? n : kOverflow;
+}
+
 // ------------------------------------------------------------------ density + lambda
 // density (density/density.cu:18-40) and lambda (pbf/pbf.cu:95-127) of one particle in one walk.
 struct DensityLambdaOp {
@@ -38,8 +121,8 @@ struct DensityLambdaOp {
     float denominator;
     uint32_t neighbors;
 
-    __device__ __forceinline__ void process(const uint32_t t) {
-        const float4 q = pos[t];
+    __device__ __forceinline__ float4 prefetch(const uint32_t t) const { return pos[t]; }
+    __device__ __forceinline__ void apply(const uint32_t t, const float4 q) {
         const f3 d = sub(x, xyz(q));
         const float r2 = squared(d);
         if (r2 < k.h2) density = __fmaf_rn(q.w, poly6_inside(r2, k), density);
@@ -52,26 +135,25 @@ struct DensityLambdaOp {
         gradient_sum = fma3(coefficient, gradient, gradient_sum);
         denominator = __fmaf_rn(__fmul_rn(coefficient, coefficient), sq_xfirst(gradient), denominator);
     }
+    __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
 __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLambdaArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
+    if (!p.active) return;
     DensityLambdaOp op;
     op.pos = a.pos;
     op.self = p.s;
     op.k = p.k;
-    const float4 xi = p.active ? a.pos[p.s] : make_float4(0, 0, 0, 0);
-    const float4 pa = p.active ? a.g.params_a[p.s] : make_float4(1, 0, 0, 0);
+    const float4 xi = a.pos[p.s];
+    const float4 pa = a.g.params_a[p.s];
     op.x = xyz(xi);
     op.rest_density = pa.x;
     op.density = 0.0F;
     op.gradient_sum = mk(0.0F, 0.0F, 0.0F);
     op.denominator = pa.y;  // relaxation
     op.neighbors = 0;
-    scan<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, ListWriter{a.list_entries, a.list_counts, a.list_capacity});
-    if (!p.active) return;
+    replay(op, p, a.g, a.list);
     const float denominator = __fadd_rn(op.denominator, sq_yfirst(op.gradient_sum));
     a.lambda[p.s] = __fdiv_rn(-__fsub_rn(__fdiv_rn(op.density, op.rest_density), 1.0F), denominator);
     if (a.density) a.density[p.s] = op.density;
@@ -82,6 +164,11 @@ __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLam
 // ------------------------------------------------------- correction + project
 // correction (pbf/pbf.cu:254-288) and project (pbf/pbf.cu:417-431); on the last iteration
 // also reconstruct (pbf/pbf.cu:456-460) and the write-back of next_state.positions.
+struct PositionLambda {
+    float4 q;
+    float lambda;
+};
+
 struct CorrectionOp {
     const float4* __restrict__ pos;
     const float* __restrict__ lambda;
@@ -94,10 +181,10 @@ struct CorrectionOp {
     KernelConstants k;
     f3 correction;
 
-    __device__ __forceinline__ void process(const uint32_t t) {
+    __device__ __forceinline__ PositionLambda prefetch(const uint32_t t) const { return {pos[t], lambda[t]}; }
+    __device__ __forceinline__ void apply(const uint32_t t, const PositionLambda in) {
         if (t == self) return;
-        const float4 q = pos[t];
-        const f3 d = sub(x, xyz(q));
+        const f3 d = sub(x, xyz(in.q));
         const float r2 = squared(d);
         const float distance = __fsqrt_rn(r2);
         if (distance == 0.0F || distance >= k.h) return;
@@ -110,34 +197,33 @@ struct CorrectionOp {
         } else {
             artificial = r2 < k.h2 ? -strength : 0.0F;
         }
-        const float coefficient = __fdiv_rn(q.w, rest_density);
-        const float factor = __fmul_rn(coefficient, __fadd_rn(__fadd_rn(lambda_i, lambda[t]), artificial));
+        const float coefficient = __fdiv_rn(in.q.w, rest_density);
+        const float factor = __fmul_rn(coefficient, __fadd_rn(__fadd_rn(lambda_i, in.lambda), artificial));
         correction = fma3(factor, spiky_gradient_at(d, distance, k), correction);
     }
+    __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
 __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
+    if (!p.active) return;
     CorrectionOp op;
     op.pos = a.pos;
     op.lambda = a.lambda;
     op.self = p.s;
     op.k = p.k;
-    const float4 xi = p.active ? a.pos[p.s] : make_float4(0, 0, 0, 0);
-    const float4 pa = p.active ? a.g.params_a[p.s] : make_float4(1, 0, 0, 0);
-    const float4 pb = p.active ? a.g.params_b[p.s] : make_float4(0, 0, 0, 0);
+    const float4 xi = a.pos[p.s];
+    const float4 pa = a.g.params_a[p.s];
+    const float4 pb = a.g.params_b[p.s];
     op.x = xyz(xi);
     op.rest_density = pa.x;
-    op.lambda_i = p.active ? a.lambda[p.s] : 0.0F;
+    op.lambda_i = a.lambda[p.s];
     op.strength = pb.x;
     op.exponent = pb.y;
     op.artificial_full = pb.x != 0.0F;
     op.reference_weight = op.artificial_full ? poly6(mk(pb.z, 0.0F, 0.0F), p.k) : 1.0F;
     op.correction = mk(0.0F, 0.0F, 0.0F);
-    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list_entries, a.list_counts, a.list_capacity);
-    if (!p.active) return;
+    replay(op, p, a.g, a.list);
     const Box& box = p.scene->box;
     const f3 candidate = add(op.x, op.correction);
     uint32_t mask = 0u;
@@ -161,6 +247,11 @@ __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs
 
 // ---------------------------------------------------------------- vorticity
 // vorticity (pbf/pbf.cu:476-497) and its magnitude (pbf/pbf.cu:565-569).
+struct PositionVector {
+    float4 q;
+    float4 v;
+};
+
 struct VorticityOp {
     const float4* __restrict__ pos;
     const float4* __restrict__ velocity;
@@ -169,34 +260,39 @@ struct VorticityOp {
     KernelConstants k;
     f3 vorticity;
 
-    __device__ __forceinline__ void process(const uint32_t t) {
+    __device__ __forceinline__ PositionVector prefetch(const uint32_t t) const { return {pos[t], velocity[t]}; }
+    __device__ __forceinline__ void apply(const uint32_t t, const PositionVector in) {
         if (t == self) return;
-        const f3 d = sub(x, xyz(pos[t]));
+        const f3 d = sub(x, xyz(in.q));
         const float distance = __fsqrt_rn(squared(d));
         if (distance == 0.0F || distance >= k.h) return;
-        vorticity = add(vorticity, cross_f(sub(xyz(velocity[t]), v), spiky_gradient_at(d, distance, k)));
+        vorticity = add(vorticity, cross_f(sub(xyz(in.v), v), spiky_gradient_at(d, distance, k)));
     }
+    __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
 __global__ void __launch_bounds__(kBlock) vorticity_kernel(const VorticityArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
+    if (!p.active) return;
     VorticityOp op;
     op.pos = a.pos;
     op.velocity = a.velocity;
     op.self = p.s;
     op.k = p.k;
-    op.x = p.active ? xyz(a.pos[p.s]) : mk(0, 0, 0);
-    op.v = p.active ? xyz(a.velocity[p.s]) : mk(0, 0, 0);
+    op.x = xyz(a.pos[p.s]);
+    op.v = xyz(a.velocity[p.s]);
     op.vorticity = mk(0.0F, 0.0F, 0.0F);
-    scan<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, ListWriter{a.list_entries, a.list_counts, a.list_capacity});
-    if (!p.active) return;
+    replay(op, p, a.g, a.list);
     a.vorticity[p.s] = make_float4(op.vorticity.x, op.vorticity.y, op.vorticity.z, __fsqrt_rn(sq_xfirst(op.vorticity)));
 }
 
 // ------------------------------------------------------- normal + confinement
 // normal (pbf/pbf.cu:571-593) and confinement (pbf/pbf.cu:674-678).
+struct PositionScalar {
+    float4 q;
+    float w;
+};
+
 struct NormalOp {
     const float4* __restrict__ pos;
     const float4* __restrict__ vorticity;
@@ -206,30 +302,30 @@ struct NormalOp {
     KernelConstants k;
     f3 gradient;
 
-    __device__ __forceinline__ void process(const uint32_t t) {
+    __device__ __forceinline__ PositionScalar prefetch(const uint32_t t) const { return {pos[t], vorticity[t].w}; }
+    __device__ __forceinline__ void apply(const uint32_t t, const PositionScalar in) {
         if (t == self) return;
-        const f3 d = sub(x, xyz(pos[t]));
+        const f3 d = sub(x, xyz(in.q));
         const float distance = __fsqrt_rn(squared(d));
         if (distance == 0.0F || distance >= k.h) return;
-        gradient = fma3(__fsub_rn(vorticity[t].w, magnitude), spiky_gradient_at(d, distance, k), gradient);
+        gradient = fma3(__fsub_rn(in.w, magnitude), spiky_gradient_at(d, distance, k), gradient);
     }
+    __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
 __global__ void __launch_bounds__(kBlock) normal_kernel(const NormalArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
+    if (!p.active) return;
     NormalOp op;
     op.pos = a.pos;
     op.vorticity = a.vorticity;
     op.self = p.s;
     op.k = p.k;
-    const float4 wi = p.active ? a.vorticity[p.s] : make_float4(0, 0, 0, 0);
-    op.x = p.active ? xyz(a.pos[p.s]) : mk(0, 0, 0);
+    const float4 wi = a.vorticity[p.s];
+    op.x = xyz(a.pos[p.s]);
     op.magnitude = wi.w;
     op.gradient = mk(0.0F, 0.0F, 0.0F);
-    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list_entries, a.list_counts, a.list_capacity);
-    if (!p.active) return;
+    replay(op, p, a.g, a.list);
     const float normalizer = __fsqrt_rn(sq_yfirst(op.gradient));
     const f3 normal = normalizer > 0.0F ? scale(op.gradient, __fdiv_rn(1.0F, normalizer)) : mk(0.0F, 0.0F, 0.0F);
     a.normal[p.s] = make_float4(normal.x, normal.y, normal.z, normalizer);
@@ -249,29 +345,29 @@ struct XsphOp {
     KernelConstants k;
     f3 smoothing;
 
-    __device__ __forceinline__ void process(const uint32_t t) {
+    __device__ __forceinline__ PositionVector prefetch(const uint32_t t) const { return {pos[t], confined[t]}; }
+    __device__ __forceinline__ void apply(const uint32_t t, const PositionVector in) {
         if (t == self) return;
-        const f3 d = sub(x, xyz(pos[t]));
+        const f3 d = sub(x, xyz(in.q));
         const float r2 = squared(d);
         if (r2 >= k.h2) return;
-        smoothing = fma3(poly6_inside(r2, k), sub(xyz(confined[t]), v), smoothing);
+        smoothing = fma3(poly6_inside(r2, k), sub(xyz(in.v), v), smoothing);
     }
+    __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
 __global__ void __launch_bounds__(kBlock) xsph_kernel(const XsphArgs a) {
-    __shared__ WarpScratch scratch[kWarpsPerBlock];
-    WarpScratch& ws = scratch[threadIdx.x >> 5];
     const Particle p = locate(a.g);
+    if (!p.active) return;
     XsphOp op;
     op.pos = a.pos;
     op.confined = a.confined;
     op.self = p.s;
     op.k = p.k;
-    op.x = p.active ? xyz(a.pos[p.s]) : mk(0, 0, 0);
-    op.v = p.active ? xyz(a.confined[p.s]) : mk(0, 0, 0);
+    op.x = xyz(a.pos[p.s]);
+    op.v = xyz(a.confined[p.s]);
     op.smoothing = mk(0.0F, 0.0F, 0.0F);
-    replay<true>(op, p, a.g, a.pos, p.k.list_threshold, ws, a.list_entries, a.list_counts, a.list_capacity);
-    if (!p.active) return;
+    replay(op, p, a.g, a.list);
     const float viscosity = a.g.params_a[p.s].z;
     const f3 out = fma3(viscosity, op.smoothing, op.v);
     const uint32_t i = a.sorted_index[p.s];
@@ -368,6 +464,13 @@ inline unsigned grid_of(const uint32_t n, const unsigned block) { return (n + bl
 
 cudaError_t launch_constants(cudaStream_t stream, const float* radii, const uint32_t n, KernelConstants* out) {
     constants_kernel<<<grid_of(n, 64), 64, 0, stream>>>(radii, n, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a) {
+    if (a.g.count == 0) return cudaSuccess;
+    list_scan_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }

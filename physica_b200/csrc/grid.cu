@@ -185,9 +185,57 @@ __global__ void sorted_keys_kernel(const uint32_t count, const uint32_t* __restr
     out[s] = keys[sorted_index[s]];
 }
 
+__global__ void set_step_kernel(unsigned long long* step, const unsigned long long value) { *step = value; }
+__global__ void advance_step_kernel(unsigned long long* step) { *step += 1ull; }
+
+// Per-step scene fields from the device step counter (the step advances state `step` to `step + 1`):
+// time = float(step + 1) * dt (pbf/pbf.cpp:18, neighborhood/neighborhood.cu:55), the gather origin
+// (neighborhood/neighborhood.cpp:83-88) and the collision box (pbf/pbf.cpp:17-31), each with the
+// float operation order of the reference's host code.
+__global__ void scene_time_kernel(const SceneStatic* __restrict__ statics, SceneDesc* __restrict__ scenes,
+                                  const unsigned long long* __restrict__ step, const uint32_t count) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    const SceneStatic st = statics[s];
+    SceneDesc& d = scenes[s];
+    const float time = __fmul_rn(__ull2float_rn(*step + 1ull), d.time_step);
+    const float ox = __fadd_rn(st.min_x, __fmul_rn(time, st.vel_x));
+    const float oy = __fadd_rn(st.min_y, __fmul_rn(time, st.vel_y));
+    const float oz = __fadd_rn(st.min_z, __fmul_rn(time, st.vel_z));
+    d.grid.time = time;
+    d.grid.origin_x = ox;
+    d.grid.origin_y = oy;
+    d.grid.origin_z = oz;
+    d.box.min_x = __fadd_rn(ox, st.particle_radius);
+    d.box.min_y = __fadd_rn(oy, st.particle_radius);
+    d.box.min_z = __fadd_rn(oz, st.particle_radius);
+    d.box.max_x = __fsub_rn(__fadd_rn(st.max_x, __fmul_rn(time, st.vel_x)), st.particle_radius);
+    d.box.max_y = __fsub_rn(__fadd_rn(st.max_y, __fmul_rn(time, st.vel_y)), st.particle_radius);
+    d.box.max_z = __fsub_rn(__fadd_rn(st.max_z, __fmul_rn(time, st.vel_z)), st.particle_radius);
+}
+
 inline unsigned blocks_for(const uint64_t n, const unsigned threads) { return static_cast<unsigned>((n + threads - 1) / threads); }
 
 }  // namespace
+
+cudaError_t launch_set_step(cudaStream_t stream, unsigned long long* step, const uint64_t value) {
+    set_step_kernel<<<1, 1, 0, stream>>>(step, value);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advance_step(cudaStream_t stream, unsigned long long* step) {
+    advance_step_kernel<<<1, 1, 0, stream>>>(step);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scene_time(cudaStream_t stream, const SceneStatic* statics, SceneDesc* scenes, const unsigned long long* step,
+                              const uint32_t count) {
+    scene_time_kernel<<<blocks_for(count, 128), 128, 0, stream>>>(statics, scenes, step, count);
+    count_launch();
+    return cudaGetLastError();
+}
 
 size_t scan_tile_count(const uint64_t n) { return static_cast<size_t>((n + kScanTile - 1) / kScanTile); }
 

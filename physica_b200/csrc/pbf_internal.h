@@ -37,6 +37,13 @@ struct SceneDesc {
     uint32_t constants;        // index into the KernelConstants table
 };
 
+// Time-independent box data of one scene, from which the device derives the per-step fields.
+struct SceneStatic {
+    float min_x, min_y, min_z, max_x, max_y, max_z;
+    float vel_x, vel_y, vel_z;
+    float particle_radius;
+};
+
 // Per-particle parameters gathered into sorted order once per substep.
 //   a = (rest density, relaxation, xsph viscosity, vorticity confinement)
 //   b = (artificial pressure strength, exponent, radius, unused)
@@ -78,6 +85,6 @@ struct SortedState {
 
 constexpr uint32_t kMaxIterations = 64;
 // Stored neighbour-list capacity per particle (a longer list is rebuilt by scanning).
-constexpr uint32_t kListCapacity = 64;
+constexpr uint32_t kListCapacity = 96;
 
 }  // namespace pbf

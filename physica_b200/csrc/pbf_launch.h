@@ -37,6 +37,13 @@ cudaError_t launch_grid_build(cudaStream_t stream, const GridBuildArgs& args);
 cudaError_t launch_sorted_keys(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const uint32_t* keys,
                                unsigned long long* out);
 
+// A stored neighbour list (warp-interleaved entries + per-particle counts).
+struct StoredList {
+    uint32_t* entries;
+    uint32_t* counts;
+    uint32_t capacity;
+};
+
 // Common inputs of every neighbour-gather pass.
 struct GatherCommon {
     uint32_t count;
@@ -55,9 +62,7 @@ struct DensityLambdaArgs {
     float* density;            // optional record
     float4* gsum_denom;        // optional record: gradient sum S and denominator D
     uint32_t* neighbor_count;  // optional: poly6 in-radius neighbours, self excluded
-    uint32_t* list_entries;    // neighbour list of this iterate, written for later passes
-    uint32_t* list_counts;
-    uint32_t list_capacity;
+    StoredList list;
 };
 
 struct CorrectionArgs {
@@ -71,9 +76,7 @@ struct CorrectionArgs {
     const uint32_t* sorted_index;
     MutField3 out_positions;   // original order (next_state.positions)
     float4* velocity;          // reconstructed velocity (sorted)
-    const uint32_t* list_entries;
-    const uint32_t* list_counts;
-    uint32_t list_capacity;
+    StoredList list;
 };
 
 struct VorticityArgs {
@@ -81,9 +84,7 @@ struct VorticityArgs {
     const float4* pos;
     const float4* velocity;
     float4* vorticity;         // (omega, |omega|)
-    uint32_t* list_entries;
-    uint32_t* list_counts;
-    uint32_t list_capacity;
+    StoredList list;
 };
 
 struct NormalArgs {
@@ -93,9 +94,7 @@ struct NormalArgs {
     const float4* vorticity;
     float4* normal;            // (N, normalizer)
     float4* confined;          // confined velocity
-    const uint32_t* list_entries;
-    const uint32_t* list_counts;
-    uint32_t list_capacity;
+    StoredList list;
 };
 
 struct XsphArgs {
@@ -104,11 +103,21 @@ struct XsphArgs {
     const float4* confined;
     const uint32_t* sorted_index;
     MutField3 out_velocities;  // original order (next_state.velocities)
-    const uint32_t* list_entries;
-    const uint32_t* list_counts;
-    uint32_t list_capacity;
+    StoredList list;
 };
 
+struct ListScanArgs {
+    GatherCommon g;
+    const float4* pos;
+    StoredList list;
+};
+
+cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a);
+// Device step counter and the per-step scene fields derived from it (time, grid origin, collision box).
+cudaError_t launch_set_step(cudaStream_t stream, unsigned long long* step, uint64_t value);
+cudaError_t launch_advance_step(cudaStream_t stream, unsigned long long* step);
+cudaError_t launch_scene_time(cudaStream_t stream, const SceneStatic* statics, SceneDesc* scenes, const unsigned long long* step,
+                              uint32_t count);
 cudaError_t launch_constants(cudaStream_t stream, const float* support_radii, uint32_t n, KernelConstants* out);
 cudaError_t launch_density_lambda(cudaStream_t stream, const DensityLambdaArgs& a, unsigned block);
 cudaError_t launch_correction(cudaStream_t stream, const CorrectionArgs& a, unsigned block);

@@ -165,6 +165,12 @@ def library() -> ctypes.CDLL:
         lib.pbf_batch_reserve_caches.argtypes = [vp, ctypes.c_uint32]
         lib.pbf_batch_set_launch_shape.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32]
         lib.pbf_batch_synchronize.argtypes = [vp]
+        lib.pbf_batch_scene_sums.argtypes = [vp, vp, vp]
+        lib.pbf_batch_set_graph_mode.argtypes = [vp, ctypes.c_int]
+        lib.pbf_set_graph_mode.argtypes = [vp, ctypes.c_int]
+        lib.pbf_sum_compensated.argtypes = [vp, vp, ctypes.c_uint32, vp]
+        lib.pbf_profile_enable.argtypes = [vp, ctypes.c_int]
+        lib.pbf_batch_profile_enable.argtypes = [vp, ctypes.c_int]
         _lib = lib
     return _lib
 
@@ -491,6 +497,117 @@ class PBF:
 
     def synchronize(self):
         check(library().pbf_synchronize(self.handle))
+
+    def set_graph_mode(self, enable: bool = True):
+        """Replay the forward launch sequence as a CUDA graph per buffer set."""
+        check(library().pbf_set_graph_mode(self.handle, 1 if enable else 0))
+
+
+class Batch:
+    """Many independent scenes advanced together (pbf_batch_*).
+
+    Particle arrays are the scenes' arrays concatenated in scene order; `particle_range(s)` gives a
+    scene's slice.  Each scene evolves exactly as a separate PBF solver would.
+    """
+
+    def __init__(self, domain_configurations: list, configuration: Configuration = Configuration(),
+                 mode: ExecutionMode = ExecutionMode.forward, stream: torch.cuda.Stream | None = None,
+                 device: torch.device | str = "cuda"):
+        lib = library()
+        self.device = torch.device(device)
+        self.mode = ExecutionMode(mode)
+        self.stream = stream or torch.cuda.current_stream(self.device)
+        self._dcs = [d.to_c() for d in domain_configurations]
+        arr = (DomainConfigurationC * len(self._dcs))(*self._dcs)
+        self._arr = arr
+        cc = ConfigurationC(configuration.pressure_iterations, configuration.checkpoint_interval)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(lib.pbf_batch_create(arr, len(self._dcs), ctypes.byref(cc), int(self.mode),
+                                       ctypes.c_void_p(self.stream.cuda_stream), ctypes.byref(h)))
+        self.handle = h
+        self.scene_count = len(self._dcs)
+        self.ranges = []
+        for s in range(self.scene_count):
+            off, cnt = ctypes.c_uint32(), ctypes.c_uint32()
+            check(lib.pbf_batch_particle_offset(self.handle, s, ctypes.byref(off), ctypes.byref(cnt)))
+            self.ranges.append((int(off.value), int(cnt.value)))
+        self.count = sum(c for _, c in self.ranges)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            library().pbf_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def particle_range(self, scene: int) -> slice:
+        off, cnt = self.ranges[scene]
+        return slice(off, off + cnt)
+
+    def _vec(self, dtype=torch.float32):
+        return torch.zeros((3, self.count), dtype=dtype, device=self.device)
+
+    def allocate_state(self) -> State:
+        return State(self._vec(), self._vec(), 0)
+
+    def allocate_state_adjoint(self) -> StateAdjoint:
+        return StateAdjoint(self._vec(torch.float64), self._vec(torch.float64))
+
+    def allocate_control_adjoint(self) -> Control:
+        return Control(self._vec(torch.float64))
+
+    def allocate_parameter_adjoint(self) -> Parameters:
+        return Parameters({n: torch.zeros(self.count, dtype=torch.float64, device=self.device) for n in PARAMETER_NAMES})
+
+    def reserve_caches(self, slots: int):
+        check(library().pbf_batch_reserve_caches(self.handle, slots))
+
+    def forward_step(self, state: State, control: Control, parameters: Parameters, next_state: State, cache_slot: int = 0):
+        nc = next_state.c()
+        check(library().pbf_batch_forward_step(self.handle, ctypes.byref(state.c()), ctypes.byref(control.c()),
+                                               ctypes.byref(parameters.c()), ctypes.byref(nc), cache_slot))
+        next_state.step_index = int(nc.step_index)
+
+    def vjp_step(self, state, control, parameters, next_state, cache_slot, next_state_adjoint, previous_state_adjoint,
+                 control_adjoint, parameter_adjoint):
+        check(library().pbf_batch_vjp_step(self.handle, ctypes.byref(state.c()), ctypes.byref(control.c()),
+                                           ctypes.byref(parameters.c()), ctypes.byref(next_state.c()), cache_slot,
+                                           ctypes.byref(next_state_adjoint.c()), ctypes.byref(previous_state_adjoint.c()),
+                                           ctypes.byref(control_adjoint.c()), ctypes.byref(parameter_adjoint.c())))
+
+    def scene_sums(self, values: torch.Tensor) -> torch.Tensor:
+        """Compensated FP64 per-scene sums of a per-particle FP64 vector."""
+        out = torch.empty(self.scene_count, dtype=torch.float64, device=self.device)
+        check(library().pbf_batch_scene_sums(self.handle, ctypes.c_void_p(values.data_ptr()), ctypes.c_void_p(out.data_ptr())))
+        return out
+
+    def set_graph_mode(self, enable: bool = True):
+        check(library().pbf_batch_set_graph_mode(self.handle, 1 if enable else 0))
+
+    def synchronize(self):
+        check(library().pbf_batch_synchronize(self.handle))
+
+
+def batch_for_scenes(scene_list, mode=ExecutionMode.forward, checkpoint_interval=2, device="cuda"):
+    """A batch, its concatenated state, control and parameters for synthetic scenes (physica_b200.scenes)."""
+    import numpy as np
+    iters = {s.pressure_iterations for s in scene_list}
+    if len(iters) != 1:
+        raise ValueError("all scenes of a batch share the Jacobi iteration count")
+    batch = Batch([DomainConfiguration.from_scene(s) for s in scene_list],
+                  Configuration(iters.pop(), checkpoint_interval), mode, device=device)
+    cat = lambda key: torch.from_numpy(np.concatenate([getattr(s, key) for s in scene_list], axis=-1)).to(batch.device)
+    state = State(cat("positions").contiguous(), cat("velocities").contiguous(), 0)
+    control = Control(cat("controls").contiguous())
+    params = Parameters({n: torch.zeros(batch.count, dtype=torch.float32, device=batch.device) for n in PARAMETER_NAMES})
+    for k in scene_list[0].parameter_arrays():
+        params.tensors[k].copy_(torch.from_numpy(np.concatenate([s.parameter_arrays()[k] for s in scene_list])))
+    return batch, state, control, params
 
 
 def solver_for_scene(scene, mode=ExecutionMode.forward, checkpoint_interval=2, device="cuda"):

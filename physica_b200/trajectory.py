@@ -21,10 +21,6 @@ import torch
 from . import pbf
 
 
-def _new_like(state: pbf.State) -> pbf.State:
-    return pbf.State(torch.empty_like(state.positions), torch.empty_like(state.velocities), state.step_index)
-
-
 def compensated_sum(solver: pbf.PBF, values: torch.Tensor) -> torch.Tensor:
     """Neumaier-compensated FP64 sum of a device vector (deterministic)."""
     out = torch.empty(1, dtype=torch.float64, device=values.device)
@@ -44,7 +40,11 @@ class Gradients:
 
 
 class Rollout:
-    """Forward `steps` substeps from `state0`, then the reverse sweep with recompute."""
+    """Forward `steps` substeps from `state0`, then the reverse sweep with recompute.
+
+    Every buffer (step caches, checkpoints, segment states, adjoints) is allocated once here and
+    reused by later calls, so the tensors of a returned `Gradients` are overwritten by the next
+    backward sweep of the same rollout; copy them to keep them."""
 
     def __init__(self, solver: pbf.PBF, control: pbf.Control, parameters: pbf.Parameters, steps: int,
                  checkpoint_every: int = 10):
@@ -58,46 +58,57 @@ class Rollout:
         self.steps = steps
         self.every = checkpoint_every
         self.caches = [solver.allocate_step_cache() for _ in range(min(checkpoint_every, steps))]
-        self.checkpoints: list[pbf.State] = []
+        segments = (steps + checkpoint_every - 1) // checkpoint_every
+        self.checkpoints: list[pbf.State] = [solver.allocate_state() for _ in range(segments)]
+        # segment states are reused by every segment, so their buffers (and any CUDA graph keyed on
+        # them) repeat from call to call
+        self.segment = [solver.allocate_state() for _ in range(min(checkpoint_every, steps) + 1)]
+        self.adjoints = [solver.allocate_state_adjoint() for _ in range(2)]
+        self.control_adjoint = solver.allocate_control_adjoint()
+        self.parameter_adjoint = solver.allocate_parameter_adjoint()
         self.final: pbf.State | None = None
 
     def forward(self, state0: pbf.State) -> pbf.State:
         """Run the rollout, keeping a state every `checkpoint_every` steps."""
         s = self.solver
-        self.checkpoints = []
-        cur = _new_like(state0)
-        s.copy_state(state0, cur)
-        nxt = _new_like(state0)
         for k in range(self.steps):
-            if k % self.every == 0:
-                cp = _new_like(cur)
-                s.copy_state(cur, cp)
-                self.checkpoints.append(cp)
-            s.forward_step(cur, self.control, self.parameters, nxt, self.caches[k % self.every])
-            cur, nxt = nxt, cur
-        self.final = cur
-        return cur
+            j = k % self.every
+            if j == 0:
+                # a new segment starts from the previous segment's last state
+                source = state0 if k == 0 else self.segment[self.every]
+                s.copy_state(source, self.checkpoints[k // self.every])
+                s.copy_state(source, self.segment[0])
+            s.forward_step(self.segment[j], self.control, self.parameters, self.segment[j + 1], self.caches[j])
+        last = (self.steps - 1) % self.every + 1
+        self.final = self.segment[last]
+        return self.final
 
     def backward(self, final_position_adjoint: torch.Tensor, final_velocity_adjoint: torch.Tensor | None = None,
                  scalar_parameters=("xsph_viscosity",)) -> Gradients:
         """Reverse sweep: dL/d(initial state), dL/d(control), per-particle and scalar parameter adjoints."""
         s = self.solver
-        adj = s.allocate_state_adjoint()
+        adj, prev = self.adjoints
         adj.positions.copy_(final_position_adjoint)
         if final_velocity_adjoint is not None:
             adj.velocities.copy_(final_velocity_adjoint)
-        control_adj = s.allocate_control_adjoint()
-        param_adj = s.allocate_parameter_adjoint()
-        prev = s.allocate_state_adjoint()
+        else:
+            adj.velocities.zero_()
+        control_adj = self.control_adjoint
+        param_adj = self.parameter_adjoint
+        control_adj.external_accelerations.zero_()
+        for t in param_adj.tensors.values():
+            t.zero_()
         segments = len(self.checkpoints)
         for seg in reversed(range(segments)):
             begin = seg * self.every
             end = min(begin + self.every, self.steps)
-            states = [self.checkpoints[seg]]
-            for k in range(begin, end):
-                nxt = _new_like(states[-1])
-                s.forward_step(states[-1], self.control, self.parameters, nxt, self.caches[k - begin])
-                states.append(nxt)
+            states = self.segment
+            s.copy_state(self.checkpoints[seg], states[0])
+            # the last segment's step caches still hold its forward steps
+            if seg != segments - 1:
+                for k in range(begin, end):
+                    s.forward_step(states[k - begin], self.control, self.parameters, states[k - begin + 1],
+                                   self.caches[k - begin])
             for k in reversed(range(begin, end)):
                 j = k - begin
                 prev.positions.zero_()
@@ -106,6 +117,7 @@ class Rollout:
                            control_adj, param_adj)
                 adj, prev = prev, adj
         scalar = {name: compensated_sum(s, param_adj.tensors[name]) for name in scalar_parameters}
+        self.adjoints = [adj, prev]
         return Gradients(loss=float("nan"), initial_positions=adj.positions, initial_velocities=adj.velocities,
                          controls=control_adj.external_accelerations, parameters=param_adj,
                          scalar={k: float(v.item()) for k, v in scalar.items()})
@@ -120,9 +132,9 @@ def target_loss(positions: torch.Tensor, targets: torch.Tensor):
 
 
 def loss_and_gradients(solver: pbf.PBF, state0: pbf.State, control: pbf.Control, parameters: pbf.Parameters,
-                       targets: torch.Tensor, steps: int, checkpoint_every: int = 10) -> Gradients:
-    """Rollout, target loss and its gradients in one call."""
-    r = Rollout(solver, control, parameters, steps, checkpoint_every)
+                       targets: torch.Tensor, steps: int, checkpoint_every: int = 10, rollout: Rollout | None = None) -> Gradients:
+    """Rollout, target loss and its gradients in one call (pass `rollout` to reuse its buffers)."""
+    r = rollout or Rollout(solver, control, parameters, steps, checkpoint_every)
     final = r.forward(state0)
     loss, dx = target_loss(final.positions, targets)
     g = r.backward(dx)

@@ -1,0 +1,86 @@
+"""GPU tests of the batched form: every scene of a batch evolves exactly as its own solver, forward
+and adjoint, with or without CUDA-graph replay."""
+import numpy as np
+import pytest
+import torch
+
+from physica_b200 import pbf, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda(cuda_lib):
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    yield
+
+
+def _scenes(velocity_sigma=0.0):
+    counts = [2048, 3001, 777, 5000, 1]
+    return [scenes.batched_scene(c, 100 + k, 3, velocity_sigma=velocity_sigma) for k, c in enumerate(counts)]
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_batched_forward_equals_per_scene_solvers(graphs):
+    scs = _scenes()
+    batch, state, control, params = pbf.batch_for_scenes(scs)
+    batch.set_graph_mode(graphs)
+    nxt = batch.allocate_state()
+    cur = state
+    for k in range(6):
+        batch.forward_step(cur, control, params, nxt)
+        cur, nxt = nxt, cur
+    torch.cuda.synchronize()
+    for s, sc in enumerate(scs):
+        solver, st, ctl, prm = pbf.solver_for_scene(sc)
+        cache = solver.allocate_step_cache()
+        a, b = st, solver.allocate_state()
+        for k in range(6):
+            solver.forward_step(a, ctl, prm, b, cache)
+            a, b = b, a
+        sl = batch.particle_range(s)
+        assert torch.equal(cur.positions[:, sl], a.positions), s
+        assert torch.equal(cur.velocities[:, sl], a.velocities), s
+    assert cur.step_index == 6
+
+
+def test_graph_replay_equals_direct_launches():
+    sc = scenes.plain_small(lattice=(12, 12, 12))
+    out = []
+    for graphs in (False, True):
+        solver, state, control, params = pbf.solver_for_scene(sc)
+        solver.set_graph_mode(graphs)
+        cache = solver.allocate_step_cache()
+        cur, nxt = state, solver.allocate_state()
+        for k in range(8):
+            solver.forward_step(cur, control, params, nxt, cache)
+            cur, nxt = nxt, cur
+        out.append((cur.positions.clone(), cur.velocities.clone()))
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+
+
+def test_batched_vjp_equals_per_scene_vjp():
+    scs = _scenes(0.1)[:3]
+    batch, state, control, params = pbf.batch_for_scenes(scs, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
+    nxt = batch.allocate_state()
+    batch.forward_step(state, control, params, nxt, 0)
+    rng = np.random.default_rng(4)
+    nxa = torch.from_numpy(rng.normal(size=(3, batch.count))).cuda()
+    nva = torch.from_numpy(rng.normal(size=(3, batch.count))).cuda()
+    na = pbf.StateAdjoint(nxa, nva)
+    pa, ca, qa = batch.allocate_state_adjoint(), batch.allocate_control_adjoint(), batch.allocate_parameter_adjoint()
+    batch.vjp_step(state, control, params, nxt, 0, na, pa, ca, qa)
+    sums = batch.scene_sums(qa.tensors["xsph_viscosity"]).cpu().numpy()
+    for s, sc in enumerate(scs):
+        sl = batch.particle_range(s)
+        solver, st, ctl, prm = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
+        cache = solver.allocate_step_cache()
+        b = solver.allocate_state()
+        solver.forward_step(st, ctl, prm, b, cache)
+        a1 = pbf.StateAdjoint(nxa[:, sl].contiguous(), nva[:, sl].contiguous())
+        p1, c1, q1 = solver.allocate_state_adjoint(), solver.allocate_control_adjoint(), solver.allocate_parameter_adjoint()
+        solver.vjp_step(st, ctl, prm, b, cache, a1, p1, c1, q1)
+        assert torch.equal(pa.positions[:, sl], p1.positions), s
+        assert torch.equal(pa.velocities[:, sl], p1.velocities), s
+        assert torch.equal(qa.tensors["xsph_viscosity"][sl], q1.tensors["xsph_viscosity"]), s
+        assert sums[s] == pytest.approx(float(q1.tensors["xsph_viscosity"].sum()), rel=1e-12)
