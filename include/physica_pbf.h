@@ -278,6 +278,30 @@ int pbf_batch_profile_read(pbf_batch* batch, pbf_pass_time* passes, uint32_t cap
 int pbf_set_graph_mode(pbf_solver* solver, int enable);
 int pbf_batch_set_graph_mode(pbf_batch* batch, int enable);
 
+/* ---- forward substep without any device allocation.  No counterpart in the reference.
+ *
+ *  For callers that cannot call cudaMalloc where they advance the fluid: hosts with a fixed
+ *  device-memory budget that hand out no memory after start-up, plugins running while their host
+ *  captures a CUDA graph (an allocation inside a global-mode capture is an error), code whose
+ *  device memory belongs to another allocator.  The caller passes the scene, its inputs and its
+ *  outputs (device pointers, as for pbf_forward_step); every intermediate buffer lives in one
+ *  library-owned device array of at most PBF_PREALLOCATED_SCRATCH_BYTES that every GPU loading
+ *  this library holds until the process exits.  Scenes above PBF_PREALLOCATED_MAX_PARTICLES
+ *  particles or PBF_PREALLOCATED_MAX_CELLS grid cells return PBF_ERROR_CAPACITY; boundary
+ *  particles return PBF_ERROR_UNSUPPORTED.  Forward mode only; no step cache is kept.
+ *  Results are bit-identical to pbf_forward_step on a forward-mode solver of the same scene.
+ *  The first call on a device (that device current) looks up the array's device address; make it
+ *  before any stream capture.  All calls on a device share the array and it keeps the last call's
+ *  contents (the call clears what must start at zero): calls whose GPU work overlaps, on different
+ *  streams or host threads, race and give undefined results, so order them on one stream.
+ *  `cuda_stream` is a cudaStream_t (NULL: the legacy default stream). ---- */
+#define PBF_PREALLOCATED_MAX_PARTICLES 32768u
+#define PBF_PREALLOCATED_MAX_CELLS 262144u
+#define PBF_PREALLOCATED_SCRATCH_BYTES 20971520u   /* 20 MiB */
+int pbf_forward_step_preallocated(const pbf_domain_configuration* domain, const pbf_configuration* configuration,
+                                  const pbf_particle_state* state, const pbf_control* control,
+                                  const pbf_parameters* parameters, pbf_particle_state* next_state, void* cuda_stream);
+
 /* ---- misc ---- */
 int pbf_synchronize(pbf_solver* solver);
 int pbf_batch_synchronize(pbf_batch* batch);
