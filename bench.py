@@ -29,6 +29,7 @@ import time
 ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+import numpy as np  # noqa: E402
 import torch  # noqa: E402
 import torch.distributed as dist  # noqa: E402
 
@@ -217,6 +218,12 @@ def bench_b200(args, world, rank):
         solver.forward_step(holder["cur"], control, params, holder["nxt"], cache)
         holder["cur"], holder["nxt"] = holder["nxt"], holder["cur"]
 
+    if args.launch_shape:   # a fixed shape (e.g. to profile one kernel variant); else the autotuner picks it
+        v, b = args.launch_shape.split(":")
+        shape, tuned_ms = pbf.LaunchShape(["per_lane", "cooperative"].index(v), int(b)), float("nan")
+        solver.launch_shape = shape
+    else:
+        shape, tuned_ms = solver.autotune(state, control, params, repeats=2)   # outside the timing
     launches0 = pbf.launch_count()
     clk = Clocks(torch.cuda.current_device())
     ms, wall = timed(step, args.steps, args.warmup, world, stream, flush, clk)
@@ -299,6 +306,9 @@ def bench_b200(args, world, rank):
     batched = None
     if not args.no_batch:
         batched = bench_batch(args, world, rank)
+    batched_grad = None
+    if not args.no_batch and not args.no_grad:
+        batched_grad = bench_batch_grad(args, world, rank)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -310,10 +320,13 @@ def bench_b200(args, world, rank):
         "config": {"workload": "dam_break_1m: 1,048,576 particles (128x64x128 lattice, spacing 0.5h, h=0.025), "
                                "box [0,4]^3, 8 Jacobi iterations, dt=1/120, XSPH c=0.01, vorticity eps=1e-4",
                    "particles_per_gpu": n, "pressure_iterations": K, "cells": cells, "replicas": world,
-                   "l2": "flushed between timed steps (256 MiB write)", "wall_s": round(wall, 3)},
+                   "l2": "flushed between timed steps (256 MiB write)", "wall_s": round(wall, 3),
+                   "launch_shape": {"list_scan": ["per_lane", "cooperative"][shape.list_scan], "block": shape.block_size,
+                                    "autotune_ms_per_step": None if math.isnan(tuned_ms) else round(tuned_ms, 4)}},
         "roofline": roofline, "step_roofline": step_roofline, "per_pass": per_pass,
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(round(per_step_launches * args.steps)),
         "clocks": clk.summary(), "grad_steps_per_s": grad, "batched_scenes": batched,
+        "batched_grad_steps_per_s": batched_grad,
     }
 
 
@@ -375,6 +388,7 @@ def bench_batch(args, world, rank):
     scs = scenes.batched_forward(seed=4 + rank)
     total = sum(s.count for s in scs)
     batch, state, control, params = pbf.batch_for_scenes(scs)
+    shape, _ = batch.autotune(state, control, params, repeats=2)
     batch.set_graph_mode(True)
     nxt = batch.allocate_state()
     holder = {"cur": state, "nxt": nxt}
@@ -406,7 +420,55 @@ def bench_batch(args, world, rank):
             "batched_ms_per_step": round(ms_b, 4), "per_scene_ms_per_step": round(ms_l, 4),
             "config": {"workload": "batched_forward_256: 256 dam-break scenes, counts log-uniform in [2048, 65536], "
                                    "4 iterations", "particles_per_gpu": total, "scenes_per_gpu": len(scs),
-                       "graphs": True}}
+                       "graphs": True, "launch_shape": {"list_scan": ["per_lane", "cooperative"][shape.list_scan],
+                                                         "block": shape.block_size}}}
+
+
+def bench_batch_grad(args, world, rank):
+    """32 differentiable scenes (16,384-131,072 particles, uniform), each with its own target-cloud
+    loss: one checkpointed batched rollout against one rollout per scene, CUDA events on the stream."""
+    import gc
+    from physica_b200 import pbf, scenes, trajectory
+    scs = scenes.batched_adjoint(seed=5 + rank)
+    total = sum(s.count for s in scs)
+    steps, every = 20, 10
+    diff = pbf.ExecutionMode.differentiable
+
+    def timed_rollout(solver, state, control, params, targets):
+        rollout = trajectory.Rollout(solver, control, params, steps, every)
+        trajectory.loss_and_gradients(solver, state, control, params, targets, steps, rollout=rollout)   # warm-up
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(solver.stream)
+        trajectory.loss_and_gradients(solver, state, control, params, targets, steps, rollout=rollout)
+        b.record(solver.stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    batch, state, control, params = pbf.batch_for_scenes(scs, mode=diff)
+    batch.set_graph_mode(True)
+    targets = torch.from_numpy(np.concatenate([s.targets for s in scs], axis=1)).cuda()
+    barrier(world)
+    ms_b = max_over_ranks(timed_rollout(batch, state, control, params, targets), world)
+    del batch, state, control, params, targets
+    gc.collect()
+    torch.cuda.synchronize()
+    ms_l = 0.0
+    for sc in scs:   # one scene at a time (its buffers allocated outside its timing)
+        solver, st, ctl, prm = pbf.solver_for_scene(sc, mode=diff)
+        solver.set_graph_mode(True)
+        ms_l += timed_rollout(solver, st, ctl, prm, torch.from_numpy(sc.targets).cuda())
+        del solver, st, ctl, prm
+        gc.collect()
+    ms_l = max_over_ranks(ms_l, world)
+    return {"unit": "grad-steps/s", "batched": round(world * steps / (ms_b * 1e-3), 3),
+            "per_scene_rollouts": round(world * steps / (ms_l * 1e-3), 3), "speedup": round(ms_l / ms_b, 3),
+            "particle_grad_steps_per_s": round(world * total * steps / (ms_b * 1e-3), 1),
+            "config": {"workload": "batched_adjoint_32: 32 dam-break scenes, counts uniform in [16384, 131072], "
+                                   "v0 ~ N(0, 0.1), 4 iterations, per-scene target-cloud loss and dL/dc_s",
+                       "particles_per_gpu": total, "scenes_per_gpu": len(scs), "rollout_steps": steps,
+                       "trajectory_checkpoint_every": every, "graphs": True}}
 
 
 def cpu_baseline(sc):
@@ -585,6 +647,8 @@ def main():
     ap.add_argument("--no-grad", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--launch-shape", default="", help="fixed list-scan variant and block, e.g. per_lane:128 "
+                                                        "(default: autotuned)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -150,6 +150,10 @@ typedef struct {
 typedef struct pbf_solver pbf_solver;          /* PBF (pbf/pbf.ixx:14-141) */
 typedef struct pbf_step_cache pbf_step_cache;  /* PBF::StepCache (pbf/pbf.ixx:54-70) */
 typedef struct pbf_batch pbf_batch;            /* many independent scenes in one launch sequence (no reference counterpart) */
+typedef struct pbf_launch_shape {
+    uint32_t list_scan;    /* 0: per-lane walk, 1: warp-cooperative scan */
+    uint32_t block_size;   /* 32, 64, 96 or 128 */
+} pbf_launch_shape;
 
 /* Fields of a step cache that pbf_step_cache_read copies out, in ORIGINAL particle order
  * unless stated otherwise.  Each maps to a StepCache / Neighborhood member. */
@@ -197,7 +201,9 @@ int pbf_free_step_cache(pbf_step_cache* cache);
 int pbf_forward_step(pbf_solver* solver, const pbf_particle_state* state, const pbf_control* control,
                      const pbf_parameters* parameters, pbf_particle_state* next_state, pbf_step_cache* cache);
 
-/* ---- PBF::jvp_step (pbf/pbf.cpp:193-215) ---- */
+/* ---- PBF::jvp_step (pbf/pbf.cpp:193-215): forward-mode FP32 tangents of the substep that `cache`
+ *      holds (pbf_forward_step of `state` on a differentiable solver).  `parameter_tangent` may be
+ *      NULL, and so may any of its pointers: a zero tangent.  next_state_tangent is overwritten. ---- */
 int pbf_jvp_step(pbf_solver* solver, const pbf_particle_state* state, const pbf_control* control,
                  const pbf_parameters* parameters, const pbf_particle_state* next_state, const pbf_step_cache* cache,
                  const pbf_particle_state_tangent* state_tangent, const pbf_control* control_tangent,
@@ -247,8 +253,11 @@ int pbf_batch_vjp_step(pbf_batch* batch, const pbf_particle_state* state, const 
                        const pbf_particle_state_adjoint* next_state_adjoint,
                        pbf_particle_state_adjoint* previous_state_adjoint, pbf_control_adjoint* control_adjoint,
                        pbf_parameter_adjoint* parameter_adjoint);
+int pbf_batch_jvp_step(pbf_batch* batch, const pbf_particle_state* state, const pbf_control* control,
+                       const pbf_parameters* parameters, const pbf_particle_state* next_state, uint32_t cache_slot,
+                       const pbf_particle_state_tangent* state_tangent, const pbf_control* control_tangent,
+                       const pbf_parameter_tangent* parameter_tangent, pbf_particle_state_tangent* next_state_tangent);
 int pbf_batch_reserve_caches(pbf_batch* batch, uint32_t cache_slots);
-int pbf_batch_set_launch_shape(pbf_batch* batch, uint32_t bucket, uint32_t block_size);
 
 /* ---- compensated FP64 sum of a per-particle adjoint (Neumaier summation in a fixed, deterministic
  *      order), e.g. dL/dc for a scalar parameter shared by all particles: dL/dc = sum_i dL/dc_i.
@@ -301,6 +310,24 @@ int pbf_batch_set_graph_mode(pbf_batch* batch, int enable);
 int pbf_forward_step_preallocated(const pbf_domain_configuration* domain, const pbf_configuration* configuration,
                                   const pbf_particle_state* state, const pbf_control* control,
                                   const pbf_parameters* parameters, pbf_particle_state* next_state, void* cuda_stream);
+
+/* ---- launch shape of the neighbour-list and gather kernels, and its autotuner.  No reference
+ *      counterpart.  Every shape gives bit-identical results; only the speed changes.
+ *      list_scan: 0 = each lane walks its own 27 cells, 1 = a warp walks each home cell's
+ *      candidates once; block_size: 32, 64, 96 or 128 threads.  pbf_autotune times all eight
+ *      shapes on `repeats` forward steps from `state` (writing `scratch_state` and the cache, which
+ *      then hold that step), keeps the fastest, returns it in `chosen` (may be NULL) and its time
+ *      per step in `milliseconds_per_step` (may be NULL).  It synchronises the stream. ---- */
+int pbf_set_launch_shape(pbf_solver* solver, const pbf_launch_shape* shape);
+int pbf_get_launch_shape(pbf_solver* solver, pbf_launch_shape* shape);
+int pbf_autotune(pbf_solver* solver, const pbf_particle_state* state, const pbf_control* control,
+                 const pbf_parameters* parameters, pbf_particle_state* scratch_state, pbf_step_cache* cache,
+                 uint32_t repeats, pbf_launch_shape* chosen, float* milliseconds_per_step);
+int pbf_batch_set_launch_shape(pbf_batch* batch, const pbf_launch_shape* shape);
+int pbf_batch_get_launch_shape(pbf_batch* batch, pbf_launch_shape* shape);
+int pbf_batch_autotune(pbf_batch* batch, const pbf_particle_state* state, const pbf_control* control,
+                       const pbf_parameters* parameters, pbf_particle_state* scratch_state, uint32_t cache_slot,
+                       uint32_t repeats, pbf_launch_shape* chosen, float* milliseconds_per_step);
 
 /* ---- misc ---- */
 int pbf_synchronize(pbf_solver* solver);

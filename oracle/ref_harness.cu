@@ -112,6 +112,11 @@ struct Harness {
     DVec current_position_adjoint, next_position_adjoint, correction_adjoint, reconstructed_velocity_adjoint,
         vorticity_adjoint, vorticity_normal_adjoint, confined_velocity_adjoint;
     double *lambda_adjoint, *density_adjoint;
+    // tangent workspace of PBF::jvp_step (allocated on first use)
+    bool tangents_ready = false;
+    Vec current_position_tangent, next_position_tangent, gradient_sum_tangent, correction_tangent,
+        reconstructed_velocity_tangent, vorticity_tangent, vorticity_normal_tangent, confined_velocity_tangent, jvp_positions;
+    float *density_tangent, *denominator_tangent, *lambda_tangent, *vorticity_magnitude_tangent;
     // empty boundary set
     float* empty_f = nullptr;
 
@@ -387,6 +392,83 @@ int ref_vjp_step(void* handle, const ref_state_in* state, const ref_params* p, c
     }
     cd::pbf::launch_predict_vjp(s, n, h->cfg.time_step, h->cdv(h->current_position_adjoint), prev_x, prev_v,
                                 cd::VectorView<double>{control_adjoint[0], control_adjoint[1], control_adjoint[2]});
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+// PBF::jvp_step (pbf/pbf.cpp:193-215), after ref_forward_step of the same state.  Tangents are
+// FP32 device SoA; `pt` holds the parameter tangents in the ref_params layout.
+int ref_jvp_step(void* handle, const ref_state_in* state, const ref_params* p, const ref_state_in* tangent,
+                 const float* const* control_tangent, const ref_params* pt, const ref_state_out* next_tangent) {
+    auto* h = static_cast<Harness*>(handle);
+    if (!h->cfg.differentiable) return 4;
+    (void)state;
+    const ::cuda::stream_ref s{h->stream};
+    const uint32_t n = h->cfg.particle_count;
+    const float hr = h->cfg.support_radius;
+    if (!h->tangents_ready) {
+        h->current_position_tangent = h->vec();
+        h->next_position_tangent = h->vec();
+        h->gradient_sum_tangent = h->vec();
+        h->correction_tangent = h->vec();
+        h->reconstructed_velocity_tangent = h->vec();
+        h->vorticity_tangent = h->vec();
+        h->vorticity_normal_tangent = h->vec();
+        h->confined_velocity_tangent = h->vec();
+        h->jvp_positions = h->vec();
+        h->density_tangent = h->alloc<float>(n);
+        h->denominator_tangent = h->alloc<float>(n);
+        h->lambda_tangent = h->alloc<float>(n);
+        h->vorticity_magnitude_tangent = h->alloc<float>(n);
+        for (void* q : h->allocations)
+            if (!q) return 2;
+        h->tangents_ready = true;
+    }
+    const cd::ParticleParameterView pv = param_view(*p);
+    const cd::ParticleParameterTangentView ptv{pt->masses, pt->rest_densities, nullptr, nullptr};
+    const cd::ConstVectorView<float> xd{tangent->px, tangent->py, tangent->pz}, vd{tangent->vx, tangent->vy, tangent->vz},
+        ad{control_tangent[0], control_tangent[1], control_tangent[2]};
+    Iteration& it = h->forward_iteration;
+    cd::pbf::launch_predict_jvp(s, n, h->cfg.time_step, xd, vd, ad, h->mv(h->current_position_tangent));
+    h->copy(h->predicted, h->jvp_positions);
+    for (uint32_t k = 0; k < h->cfg.pressure_iterations; ++k) {
+        cd::density_forward(s, n, hr, true, h->cv(h->predicted), h->cv(h->jvp_positions), pv, h->neighborhood(), h->boundary(),
+                            it.densities);
+        cd::density_jvp(s, n, hr, true, h->cv(h->predicted), h->cv(h->jvp_positions), h->cv(h->current_position_tangent), pv, ptv,
+                        h->neighborhood(), h->boundary(), h->density_tangent);
+        cd::pbf::launch_lambda_forward(s, n, hr, h->cv(h->predicted), h->cv(h->jvp_positions), pv, h->neighborhood(),
+                                       h->boundary(), it.densities, p->relaxation, h->mv(it.gradient_sums), it.denominators,
+                                       it.lambdas);
+        cd::pbf::launch_lambda_jvp(s, n, hr, h->cv(h->predicted), h->cv(h->jvp_positions), h->cv(h->current_position_tangent), pv,
+                                   ptv, h->neighborhood(), h->boundary(), it.densities, h->density_tangent, p->relaxation,
+                                   pt->relaxation, h->mv(h->gradient_sum_tangent), h->denominator_tangent, h->lambda_tangent);
+        cd::pbf::launch_correction_forward(s, n, hr, h->cv(h->predicted), h->cv(h->jvp_positions), pv, h->neighborhood(),
+                                           h->boundary(), it.lambdas, p->strength, p->exponent, p->radius, h->mv(it.corrections));
+        cd::pbf::launch_correction_jvp(s, n, hr, h->cv(h->predicted), h->cv(h->jvp_positions), h->cv(h->current_position_tangent),
+                                       pv, ptv, h->neighborhood(), h->boundary(), it.lambdas, h->lambda_tangent, p->strength,
+                                       pt->strength, p->exponent, pt->exponent, p->radius, pt->radius,
+                                       h->mv(h->correction_tangent));
+        cd::pbf::launch_project_forward(s, n, h->collision_box(h->step_index + 1u), h->cv(h->jvp_positions),
+                                        h->cv(it.corrections), it.masks, h->mv(h->jvp_positions));
+        cd::pbf::launch_project_jvp(s, n, it.masks, h->cv(h->current_position_tangent), h->cv(h->correction_tangent),
+                                    h->mv(h->next_position_tangent));
+        std::swap(h->current_position_tangent, h->next_position_tangent);
+    }
+    cd::pbf::launch_reconstruct_jvp(s, n, 1.0F / h->cfg.time_step, xd, h->cv(h->current_position_tangent),
+                                    h->mv(h->reconstructed_velocity_tangent));
+    cd::pbf::launch_vorticity_jvp(s, n, hr, h->cv(h->predicted), h->cv(h->corrected), h->cv(h->reconstructed),
+                                  h->cv(h->current_position_tangent), h->cv(h->reconstructed_velocity_tangent), h->neighborhood(),
+                                  h->mv(h->vorticity_tangent));
+    cd::pbf::launch_normal_jvp(s, n, hr, h->cv(h->predicted), h->cv(h->corrected), h->cv(h->vorticities),
+                               h->cv(h->current_position_tangent), h->cv(h->vorticity_tangent), h->neighborhood(), h->magnitudes,
+                               h->cv(h->normals), h->normalizers, h->vorticity_magnitude_tangent,
+                               h->mv(h->vorticity_normal_tangent));
+    cd::pbf::launch_confinement_jvp(s, n, h->cfg.time_step, h->cv(h->vorticities), h->cv(h->normals), p->vorticity,
+                                    h->cv(h->reconstructed_velocity_tangent), h->cv(h->vorticity_tangent),
+                                    h->cv(h->vorticity_normal_tangent), pt->vorticity, h->mv(h->confined_velocity_tangent));
+    cd::pbf::launch_xsph_jvp(s, n, hr, h->cv(h->predicted), h->cv(h->corrected), h->cv(h->confined),
+                             h->cv(h->current_position_tangent), h->cv(h->confined_velocity_tangent), h->neighborhood(), p->xsph,
+                             pt->xsph, cd::VectorView<float>{next_tangent->vx, next_tangent->vy, next_tangent->vz});
+    h->copy(h->current_position_tangent, Vec{next_tangent->px, next_tangent->py, next_tangent->pz});
     return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }
 

@@ -61,6 +61,7 @@ def load():
         lib.ref_create.argtypes = [P(RefConfig), P(vp)]
         lib.ref_destroy.argtypes = [vp]
         lib.ref_forward_step.argtypes = [vp, P(RefStateIn), P(vp), P(RefParams), P(RefStateOut), ctypes.c_uint64]
+        lib.ref_jvp_step.argtypes = [vp, P(RefStateIn), P(RefParams), P(RefStateIn), P(vp), P(RefParams), P(RefStateOut)]
         lib.ref_vjp_step.argtypes = [vp, P(RefStateIn), P(RefParams), P(RefAdjointState), P(RefAdjointState), P(vp),
                                      P(RefParamAdjoint)]
         lib.ref_read.argtypes = [vp, ctypes.c_int, vp]
@@ -163,6 +164,25 @@ class ReferencePBF:
                               ctypes.byref(pa), ca, ctypes.byref(pp))
         if rc:
             raise RuntimeError(f"ref_vjp_step failed: {rc}")
+        lib.ref_synchronize(self.handle)
+
+    def jvp_step(self, x, v, tangent, control_tangent, param_tangent, next_tangent):
+        """PBF::jvp_step after forward_step of (x, v).  tangent / next_tangent: dicts with (3, N)
+        float32 CUDA tensors "positions" and "velocities"; param_tangent: dict of float32 (N,) tensors."""
+        lib = load()
+        sin = RefStateIn(_p(x[0]), _p(x[1]), _p(x[2]), _p(v[0]), _p(v[1]), _p(v[2]))
+        tin = RefStateIn(*[_p(tangent[k][a]) for k in ("positions", "velocities") for a in range(3)])
+        tout = RefStateOut(*[_p(next_tangent[k][a]) for k in ("positions", "velocities") for a in range(3)])
+        ct = (ctypes.c_void_p * 3)(*[control_tangent[a].data_ptr() for a in range(3)])
+        g = param_tangent
+        pt = RefParams(_p(g["masses"]), _p(g["rest_densities"]), _p(g["relaxation"]),
+                       _p(g["artificial_pressure_strength"]), _p(g["artificial_pressure_exponent"]),
+                       _p(g["artificial_pressure_radius"]), _p(g["xsph_viscosity"]), _p(g["vorticity_confinement"]))
+        torch.cuda.synchronize(self.device)
+        rc = lib.ref_jvp_step(self.handle, ctypes.byref(sin), ctypes.byref(self._pstruct()), ctypes.byref(tin), ct,
+                              ctypes.byref(pt), ctypes.byref(tout))
+        if rc:
+            raise RuntimeError(f"ref_jvp_step failed: {rc}")
         lib.ref_synchronize(self.handle)
 
     def read(self, field: str) -> torch.Tensor:

@@ -83,15 +83,47 @@ int pbf_batch_vjp_step(pbf_batch* batch, const pbf_particle_state* state, const 
                                  previous_state_adjoint, control_adjoint, parameter_adjoint);
 }
 
-int pbf_batch_set_launch_shape(pbf_batch* batch, const uint32_t bucket, const uint32_t block_size) {
-    (void)bucket;
-    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
-    if (block_size != 128) {
-        pbf::set_error("only 128-thread blocks are built");
-        return PBF_ERROR_UNSUPPORTED;
+int pbf_batch_jvp_step(pbf_batch* batch, const pbf_particle_state* state, const pbf_control* control,
+                       const pbf_parameters* parameters, const pbf_particle_state* next_state, const uint32_t cache_slot,
+                       const pbf_particle_state_tangent* state_tangent, const pbf_control* control_tangent,
+                       const pbf_parameter_tangent* parameter_tangent, pbf_particle_state_tangent* next_state_tangent) {
+    (void)control;
+    (void)parameters;
+    (void)next_state;
+    if (!batch || cache_slot >= batch->caches.size()) return PBF_ERROR_INVALID_ARGUMENT;
+    if (!batch->engine.differentiable()) return PBF_ERROR_NOT_DIFFERENTIABLE;
+    return batch->engine.tangent(state, *batch->caches[cache_slot], state_tangent, control_tangent, parameter_tangent,
+                                 next_state_tangent);
+}
+
+int pbf_batch_set_launch_shape(pbf_batch* batch, const pbf_launch_shape* shape) {
+    if (!batch || !shape) return PBF_ERROR_INVALID_ARGUMENT;
+    const pbf::LaunchShape s{shape->list_scan, shape->block_size};
+    if (!pbf::valid_shape(s)) {
+        pbf::set_error("launch shape: list_scan must be 0 or 1 and block_size one of 32, 64, 96, 128");
+        return PBF_ERROR_INVALID_ARGUMENT;
     }
-    batch->engine.set_block(block_size);
+    batch->engine.set_shape(s);
     return PBF_SUCCESS;
+}
+
+int pbf_batch_get_launch_shape(pbf_batch* batch, pbf_launch_shape* shape) {
+    if (!batch || !shape) return PBF_ERROR_INVALID_ARGUMENT;
+    shape->list_scan = batch->engine.shape().scan;
+    shape->block_size = batch->engine.shape().block;
+    return PBF_SUCCESS;
+}
+
+int pbf_batch_autotune(pbf_batch* batch, const pbf_particle_state* state, const pbf_control* control,
+                       const pbf_parameters* parameters, pbf_particle_state* scratch_state, const uint32_t cache_slot,
+                       const uint32_t repeats, pbf_launch_shape* chosen, float* milliseconds_per_step) {
+    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
+    if (int rc = pbf_batch_reserve_caches(batch, cache_slot + 1)) return rc;
+    if (!state || !control || !parameters || !scratch_state) return PBF_ERROR_INVALID_ARGUMENT;
+    const int rc = batch->engine.autotune(state, control, parameters, scratch_state, *batch->caches[cache_slot], repeats,
+                                          milliseconds_per_step);
+    if (rc) return rc;
+    return chosen ? pbf_batch_get_launch_shape(batch, chosen) : PBF_SUCCESS;
 }
 
 int pbf_batch_scene_sums(pbf_batch* batch, const double* values, double* result) {

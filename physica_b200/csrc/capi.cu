@@ -137,16 +137,18 @@ int pbf_jvp_step(pbf_solver* solver, const pbf_particle_state* state, const pbf_
                  const pbf_parameters* parameters, const pbf_particle_state* next_state, const pbf_step_cache* cache,
                  const pbf_particle_state_tangent* state_tangent, const pbf_control* control_tangent,
                  const pbf_parameter_tangent* parameter_tangent, pbf_particle_state_tangent* next_state_tangent) {
-    (void)state; (void)control; (void)parameters; (void)next_state; (void)state_tangent; (void)control_tangent;
-    (void)parameter_tangent; (void)next_state_tangent;
+    (void)control;
+    (void)parameters;
+    (void)next_state;
     if (!solver) return null_arg("solver");
     if (!cache) return null_arg("cache");
-    if (!solver->engine.differentiable()) {
-        pbf::set_error("jvp_step needs a solver created in PBF_EXECUTION_DIFFERENTIABLE mode");
-        return PBF_ERROR_NOT_DIFFERENTIABLE;
+    if (cache->solver != solver) {
+        pbf::set_error("step cache belongs to another solver");
+        return PBF_ERROR_INVALID_ARGUMENT;
     }
-    pbf::set_error("jvp_step is not available in this build");
-    return PBF_ERROR_UNSUPPORTED;
+    return guarded([&] {
+        return solver->engine.tangent(state, cache->record, state_tangent, control_tangent, parameter_tangent, next_state_tangent);
+    });
 }
 
 int pbf_vjp_step(pbf_solver* solver, const pbf_particle_state* state, const pbf_control* control,
@@ -295,6 +297,43 @@ int pbf_set_graph_mode(pbf_solver* solver, const int enable) {
     if (!solver) return null_arg("solver");
     solver->engine.set_graphs(enable != 0);
     return PBF_SUCCESS;
+}
+
+int pbf_set_launch_shape(pbf_solver* solver, const pbf_launch_shape* shape) {
+    if (!solver) return null_arg("solver");
+    if (!shape) return null_arg("shape");
+    const pbf::LaunchShape s{shape->list_scan, shape->block_size};
+    if (!pbf::valid_shape(s)) {
+        pbf::set_error("launch shape: list_scan must be 0 or 1 and block_size one of 32, 64, 96, 128");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    solver->engine.set_shape(s);
+    return PBF_SUCCESS;
+}
+
+int pbf_get_launch_shape(pbf_solver* solver, pbf_launch_shape* shape) {
+    if (!solver) return null_arg("solver");
+    if (!shape) return null_arg("shape");
+    shape->list_scan = solver->engine.shape().scan;
+    shape->block_size = solver->engine.shape().block;
+    return PBF_SUCCESS;
+}
+
+int pbf_autotune(pbf_solver* solver, const pbf_particle_state* state, const pbf_control* control,
+                 const pbf_parameters* parameters, pbf_particle_state* scratch_state, pbf_step_cache* cache,
+                 const uint32_t repeats, pbf_launch_shape* chosen, float* milliseconds_per_step) {
+    if (!solver) return null_arg("solver");
+    if (!cache) return null_arg("cache");
+    if (cache->solver != solver) {
+        pbf::set_error("step cache belongs to another solver");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (!state || !control || !parameters || !scratch_state) return null_arg("state/control/parameters/scratch_state");
+    const int rc = guarded([&] {
+        return solver->engine.autotune(state, control, parameters, scratch_state, cache->record, repeats, milliseconds_per_step);
+    });
+    if (rc) return rc;
+    return chosen ? pbf_get_launch_shape(solver, chosen) : PBF_SUCCESS;
 }
 
 int pbf_profile_enable(pbf_solver* solver, const int enable) {

@@ -28,7 +28,9 @@ uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 const char* pass_name(const int pass) {
     static const char* names[kPassCount] = {"grid_build", "list_scan", "density_lambda", "correction_project", "vorticity",
                                             "normal_confinement", "xsph", "adjoint_seed", "xsph_vjp", "normal_vjp",
-                                            "vorticity_vjp", "correction_vjp", "lambda_vjp", "density_vjp"};
+                                            "vorticity_vjp", "correction_vjp", "lambda_vjp", "density_vjp",
+                                            "tangent_seed", "density_lambda_jvp", "correction_jvp", "vorticity_jvp",
+                                            "normal_jvp", "xsph_jvp"};
     return pass >= 0 && pass < kPassCount ? names[pass] : "unknown";
 }
 
@@ -111,6 +113,7 @@ int Engine::check(const cudaError_t e, const char* what) {
 }
 
 void destroy_adjoint_workspace(void* workspace);
+void destroy_tangent_workspace(void* workspace);
 
 Engine::~Engine() {
     if (stream_) cudaStreamSynchronize(stream_);
@@ -118,6 +121,8 @@ Engine::~Engine() {
     if (capture_stream_) cudaStreamDestroy(capture_stream_);
     destroy_adjoint_workspace(adjoint_);
     adjoint_ = nullptr;
+    destroy_tangent_workspace(tangent_);
+    tangent_ = nullptr;
     arena_.release();
 }
 
@@ -467,17 +472,17 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
         const uint32_t l = diff ? k : 0u;
         const StoredList list{r.list_entries[l], r.list_counts[l], r.list_capacity};
         timer_.begin(stream, kPassListScan);
-        if (int rc = check(launch_list_scan(stream, ListScanArgs{gc, xk, list}), "neighbour list scan")) return rc;
+        if (int rc = check(launch_list_scan(stream, ListScanArgs{gc, xk, list}, shape_), "neighbour list scan")) return rc;
         timer_.end(stream, kPassListScan);
         DensityLambdaArgs d{gc, xk, lam, diff ? r.density[k] : (k == 0 ? r.first_density : nullptr),
                             diff ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr, list};
         timer_.begin(stream, kPassDensityLambda);
-        if (int rc = check(launch_density_lambda(stream, d, block_), "density/lambda")) return rc;
+        if (int rc = check(launch_density_lambda(stream, d, shape_.block), "density/lambda")) return rc;
         timer_.end(stream, kPassDensityLambda);
         CorrectionArgs c{gc, xk, lam, xk1, diff ? r.mask[k] : nullptr, k + 1 == K ? 1 : 0, previous, r.sorted_index,
                          out_positions, r.velocity, list};
         timer_.begin(stream, kPassCorrection);
-        if (int rc = check(launch_correction(stream, c, block_), "correction/project")) return rc;
+        if (int rc = check(launch_correction(stream, c, shape_.block), "correction/project")) return rc;
         timer_.end(stream, kPassCorrection);
     }
     const float4* xK = r.iterate(K, K, diff);
@@ -490,22 +495,70 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
     const uint32_t lp = diff ? K : 0u;
     const StoredList post{r.list_entries[lp], r.list_counts[lp], r.list_capacity};
     timer_.begin(stream, kPassListScan);
-    if (int rc = check(launch_list_scan(stream, ListScanArgs{gc, xK, post}), "neighbour list scan")) return rc;
+    if (int rc = check(launch_list_scan(stream, ListScanArgs{gc, xK, post}, shape_), "neighbour list scan")) return rc;
     timer_.end(stream, kPassListScan);
     VorticityArgs v{gc, xK, r.velocity, r.vorticity, post};
     timer_.begin(stream, kPassVorticity);
-    if (int rc = check(launch_vorticity(stream, v, block_), "vorticity")) return rc;
+    if (int rc = check(launch_vorticity(stream, v, shape_.block), "vorticity")) return rc;
     timer_.end(stream, kPassVorticity);
     NormalArgs nm{gc, xK, r.velocity, r.vorticity, r.normal, r.confined, post};
     timer_.begin(stream, kPassNormal);
-    if (int rc = check(launch_normal(stream, nm, block_), "normal/confinement")) return rc;
+    if (int rc = check(launch_normal(stream, nm, shape_.block), "normal/confinement")) return rc;
     timer_.end(stream, kPassNormal);
     XsphArgs x{gc, xK, r.confined, r.sorted_index, {next_state->velocities.x, next_state->velocities.y, next_state->velocities.z},
                post};
     timer_.begin(stream, kPassXsph);
-    if (int rc = check(launch_xsph(stream, x, block_), "xsph")) return rc;
+    if (int rc = check(launch_xsph(stream, x, shape_.block), "xsph")) return rc;
     timer_.end(stream, kPassXsph);
     return check(launch_advance_step(stream, d_step_), "step counter");
+}
+
+int Engine::autotune(const pbf_particle_state* state, const pbf_control* control, const pbf_parameters* parameters,
+                     pbf_particle_state* next_state, StepRecord& record, const uint32_t repeats, float* best_ms) {
+    const uint32_t reps = repeats ? repeats : 1u;
+    const LaunchShape previous = shape_;
+    const bool graphs = graphs_;
+    graphs_ = false;
+    LaunchShape best = previous;
+    float best_time = -1.0F;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    int rc = check(cudaEventCreate(&start), "autotune event");
+    if (!rc) rc = check(cudaEventCreate(&stop), "autotune event");
+    const uint32_t scans[2] = {kScanPerLane, kScanCooperative};
+    const uint32_t blocks[4] = {32u, 64u, 96u, 128u};
+    for (int v = 0; v < 2 && !rc; ++v) {
+        for (int b = 0; b < 4 && !rc; ++b) {
+            LaunchShape candidate;
+            candidate.scan = scans[v];
+            candidate.block = blocks[b];
+            shape_ = candidate;
+            pbf_particle_state out = *next_state;
+            if ((rc = forward(state, control, parameters, &out, record))) break;   // warm-up
+            if ((rc = check(cudaEventRecord(start, stream_), "autotune event"))) break;
+            for (uint32_t k = 0; k < reps && !rc; ++k) {
+                out = *next_state;
+                rc = forward(state, control, parameters, &out, record);
+            }
+            if (rc) break;
+            if ((rc = check(cudaEventRecord(stop, stream_), "autotune event"))) break;
+            if ((rc = check(cudaEventSynchronize(stop), "autotune event"))) break;
+            float ms = 0.0F;
+            if ((rc = check(cudaEventElapsedTime(&ms, start, stop), "autotune event"))) break;
+            ms /= static_cast<float>(reps);
+            if (best_time < 0.0F || ms < best_time) {
+                best_time = ms;
+                best = candidate;
+            }
+        }
+    }
+    if (start) cudaEventDestroy(start);
+    if (stop) cudaEventDestroy(stop);
+    graphs_ = graphs;
+    shape_ = rc ? previous : best;
+    drop_graphs();
+    if (!rc && best_ms) *best_ms = best_time;
+    if (!rc) next_state->step_index = state->step_index + 1u;
+    return rc;
 }
 
 int Engine::read(const StepRecord& r, const pbf_cache_field field, void* destination, const size_t bytes) {

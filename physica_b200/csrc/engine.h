@@ -107,6 +107,12 @@ enum PassId : int {
     kPassCorrectionVjp,
     kPassLambdaVjp,
     kPassDensityVjp,
+    kPassTangentSeed,
+    kPassDensityLambdaJvp,
+    kPassCorrectionJvp,
+    kPassVorticityJvp,
+    kPassNormalJvp,
+    kPassXsphJvp,
     kPassCount
 };
 
@@ -147,6 +153,10 @@ public:
     int allocate_record(StepRecord& r);
     int forward(const pbf_particle_state* state, const pbf_control* control, const pbf_parameters* parameters,
                 pbf_particle_state* next_state, StepRecord& record);
+    // Forward-mode tangent of the substep recorded in `record` (jvp.cu).
+    int tangent(const pbf_particle_state* state, const StepRecord& record, const pbf_particle_state_tangent* state_tangent,
+                const pbf_control* control_tangent, const pbf_parameter_tangent* parameter_tangent,
+                pbf_particle_state_tangent* next_state_tangent);
     int reverse(const pbf_particle_state* state, const pbf_control* control, const pbf_parameters* parameters,
                 const StepRecord& record, const pbf_particle_state_adjoint* next_adjoint,
                 pbf_particle_state_adjoint* previous_adjoint, pbf_control_adjoint* control_adjoint,
@@ -161,7 +171,16 @@ public:
     bool differentiable() const { return mode_ == PBF_EXECUTION_DIFFERENTIABLE; }
     cudaStream_t stream() const { return stream_; }
     const std::vector<SceneHost>& scenes() const { return scenes_; }
-    void set_block(unsigned block) { block_ = block; }
+    // Launch shape of the list and gather kernels (bit-identical results for every shape).
+    void set_shape(const LaunchShape& shape) {
+        shape_ = shape;
+        drop_graphs();
+    }
+    const LaunchShape& shape() const { return shape_; }
+    // Times every candidate shape on `repeats` forward steps from `state` (writing `next_state` and
+    // the record) and keeps the fastest; returns its per-step milliseconds in `best_ms`.
+    int autotune(const pbf_particle_state* state, const pbf_control* control, const pbf_parameters* parameters,
+                 pbf_particle_state* next_state, StepRecord& record, uint32_t repeats, float* best_ms);
 
     int check(cudaError_t e, const char* what);
     PassTimer& timer() { return timer_; }
@@ -202,7 +221,7 @@ private:
     uint32_t checkpoint_interval_ = 1;
     pbf_execution_mode mode_ = PBF_EXECUTION_FORWARD;
     cudaStream_t stream_ = nullptr;
-    unsigned block_ = 128;
+    LaunchShape shape_{};
     std::vector<SceneHost> scenes_;
     std::vector<SceneDesc> scene_table_;
     DeviceArena arena_;
@@ -216,6 +235,7 @@ private:
     uint32_t* tile_sums_ = nullptr;
     friend struct AdjointWorkspace;
     void* adjoint_ = nullptr;  // AdjointWorkspace*, differentiable mode
+    void* tangent_ = nullptr;  // TangentWorkspace*, differentiable mode
 };
 
 int read_profile(Engine& engine, pbf_pass_time* passes, uint32_t capacity, uint32_t* count);

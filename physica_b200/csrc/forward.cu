@@ -27,6 +27,53 @@ using namespace gather_detail;
 
 // --------------------------------------------------------------- list scan
 // Builds the ordered neighbour list of every particle over the positions `pos` (gather.cuh).
+// Per-lane list scan: every lane walks its own 27 stencil cells in the reference's order and
+// appends its hits; lanes of one home cell read the same candidates at the same time (one
+// broadcast load).  Same lists as list_scan_kernel.
+__global__ void __launch_bounds__(kBlock) list_walk_kernel(const ListScanArgs a) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.g.count) return;
+    const int4 c = a.g.cell[s];
+    const SceneDesc* scene = a.g.scenes + c.w;
+    const float thr = a.g.constants[scene->constants].list_threshold;
+    const int cx = static_cast<int>(scene->grid.cells_x), cy = static_cast<int>(scene->grid.cells_y);
+    const int cz = static_cast<int>(scene->grid.cells_z);
+    const uint32_t cell_base = scene->grid.cell_base;
+    const float4 xi = a.pos[s];
+    const uint32_t cap = a.list.capacity;
+    uint32_t* __restrict__ entries = a.list.entries + list_row(s, cap);
+    const uint32_t* __restrict__ offsets = a.g.cell_offsets;
+    const float4* __restrict__ pos = a.pos;
+    uint32_t n = 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int x = c.x + dx;
+        if (x < 0 || x >= cx) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = c.y + dy;
+            if (y < 0 || y >= cy) continue;
+#pragma unroll
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int z = c.z + dz;
+                if (z < 0 || z >= cz) continue;
+                const uint32_t cell = cell_base + (static_cast<uint32_t>(z) * static_cast<uint32_t>(cy) + static_cast<uint32_t>(y)) *
+                                                      static_cast<uint32_t>(cx) +
+                                      static_cast<uint32_t>(x);
+                const uint32_t end = offsets[cell + 1u];
+#pragma unroll 4
+                for (uint32_t t = offsets[cell]; t < end; ++t) {
+                    const float4 q = pos[t];
+                    const float r2 = squared(mk(__fsub_rn(xi.x, q.x), __fsub_rn(xi.y, q.y), __fsub_rn(xi.z, q.z)));
+                    if (r2 < thr) {
+                        if (n < cap) entries[static_cast<size_t>(n) * 32u] = t;
+                        ++n;
+                    }
+                }
+            }
+        }
+    }
+    a.list.counts[s] = n <= cap ? n : kOverflow;
+}
+
 __global__ void __launch_bounds__(kBlock) list_scan_kernel(const ListScanArgs a) {
     __shared__ float4 home_s[kWarpsPerBlock][32];
     __shared__ uint32_t first_s[kWarpsPerBlock][32];
@@ -110,6 +157,22 @@ __global__ void __launch_bounds__(kBlock) list_scan_kernel(const ListScanArgs a)
 
 // ------------------------------------------------------------------ density + lambda
 // density (density/density.cu:18-40) and lambda (pbf/pbf.cu:95-127) of one particle in one walk.
+// m_j / rho0_i for a run of neighbours: most neighbours share a mass, so the last quotient is
+// kept and reused while the mass bits repeat (same operands, same correctly rounded quotient).
+struct MassRatio {
+    uint32_t mass_bits;
+    float quotient;
+    __device__ __forceinline__ void reset(const float mass, const float rest_density) {
+        mass_bits = __float_as_uint(mass);
+        quotient = __fdiv_rn(mass, rest_density);
+    }
+    __device__ __forceinline__ float operator()(const float mass, const float rest_density) {
+        const uint32_t bits = __float_as_uint(mass);
+        if (bits != mass_bits) reset(mass, rest_density);
+        return quotient;
+    }
+};
+
 struct DensityLambdaOp {
     const float4* __restrict__ pos;
     f3 x;
@@ -120,6 +183,7 @@ struct DensityLambdaOp {
     f3 gradient_sum;
     float denominator;
     uint32_t neighbors;
+    MassRatio ratio;
 
     __device__ __forceinline__ float4 prefetch(const uint32_t t) const { return pos[t]; }
     __device__ __forceinline__ void apply(const uint32_t t, const float4 q) {
@@ -131,7 +195,7 @@ struct DensityLambdaOp {
         const float distance = __fsqrt_rn(r2);
         if (distance == 0.0F || distance >= k.h) return;
         const f3 gradient = spiky_gradient_at(d, distance, k);
-        const float coefficient = __fdiv_rn(q.w, rest_density);
+        const float coefficient = ratio(q.w, rest_density);
         gradient_sum = fma3(coefficient, gradient, gradient_sum);
         denominator = __fmaf_rn(__fmul_rn(coefficient, coefficient), sq_xfirst(gradient), denominator);
     }
@@ -153,6 +217,7 @@ __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLam
     op.gradient_sum = mk(0.0F, 0.0F, 0.0F);
     op.denominator = pa.y;  // relaxation
     op.neighbors = 0;
+    op.ratio.reset(xi.w, op.rest_density);
     replay(op, p, a.g, a.list);
     const float denominator = __fadd_rn(op.denominator, sq_yfirst(op.gradient_sum));
     a.lambda[p.s] = __fdiv_rn(-__fsub_rn(__fdiv_rn(op.density, op.rest_density), 1.0F), denominator);
@@ -180,6 +245,7 @@ struct CorrectionOp {
     bool artificial_full;
     KernelConstants k;
     f3 correction;
+    MassRatio ratio;
 
     __device__ __forceinline__ PositionLambda prefetch(const uint32_t t) const { return {pos[t], lambda[t]}; }
     __device__ __forceinline__ void apply(const uint32_t t, const PositionLambda in) {
@@ -197,7 +263,7 @@ struct CorrectionOp {
         } else {
             artificial = r2 < k.h2 ? -strength : 0.0F;
         }
-        const float coefficient = __fdiv_rn(in.q.w, rest_density);
+        const float coefficient = ratio(in.q.w, rest_density);
         const float factor = __fmul_rn(coefficient, __fadd_rn(__fadd_rn(lambda_i, in.lambda), artificial));
         correction = fma3(factor, spiky_gradient_at(d, distance, k), correction);
     }
@@ -217,6 +283,7 @@ __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs
     const float4 pb = a.g.params_b[p.s];
     op.x = xyz(xi);
     op.rest_density = pa.x;
+    op.ratio.reset(xi.w, op.rest_density);
     op.lambda_i = a.lambda[p.s];
     op.strength = pb.x;
     op.exponent = pb.y;
@@ -468,44 +535,64 @@ cudaError_t launch_constants(cudaStream_t stream, const float* radii, const uint
     return cudaGetLastError();
 }
 
-cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a) {
+bool valid_shape(const LaunchShape& shape) {
+    return (shape.scan == kScanPerLane || shape.scan == kScanCooperative) && shape.block >= 32u &&
+           shape.block <= static_cast<uint32_t>(kBlock) && shape.block % 32u == 0u;
+}
+
+namespace {
+unsigned block_of(const unsigned block) {
+    return block >= 32u && block <= static_cast<unsigned>(kBlock) && block % 32u == 0u ? block : static_cast<unsigned>(kBlock);
+}
+}  // namespace
+
+cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a, const LaunchShape& shape) {
     if (a.g.count == 0) return cudaSuccess;
-    list_scan_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    const unsigned block = block_of(shape.block);
+    if (shape.scan == kScanCooperative)
+        list_scan_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    else
+        list_walk_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_density_lambda(cudaStream_t stream, const DensityLambdaArgs& a, unsigned) {
+cudaError_t launch_density_lambda(cudaStream_t stream, const DensityLambdaArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
-    density_lambda_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    const unsigned block = block_of(block_size);
+    density_lambda_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_correction(cudaStream_t stream, const CorrectionArgs& a, unsigned) {
+cudaError_t launch_correction(cudaStream_t stream, const CorrectionArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
-    correction_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    const unsigned block = block_of(block_size);
+    correction_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_vorticity(cudaStream_t stream, const VorticityArgs& a, unsigned) {
+cudaError_t launch_vorticity(cudaStream_t stream, const VorticityArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
-    vorticity_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    const unsigned block = block_of(block_size);
+    vorticity_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_normal(cudaStream_t stream, const NormalArgs& a, unsigned) {
+cudaError_t launch_normal(cudaStream_t stream, const NormalArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
-    normal_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    const unsigned block = block_of(block_size);
+    normal_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_xsph(cudaStream_t stream, const XsphArgs& a, unsigned) {
+cudaError_t launch_xsph(cudaStream_t stream, const XsphArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
-    xsph_kernel<<<grid_of(a.g.count, kBlock), kBlock, 0, stream>>>(a);
+    const unsigned block = block_of(block_size);
+    xsph_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }

@@ -16,7 +16,7 @@
 // lanes is one coalesced transaction.  A list longer than the capacity is marked overflowed.
 //
 // Replay (replay): each lane drains its own list in order with a pass's per-pair arithmetic, the
-// next entry's loads issued before the current entry is processed.  An overflowed particle walks
+// next entry's loads (and the index after it) issued before the current entry is processed.  An overflowed particle walks
 // its stencil directly (same order, every candidate offered to the pass), which gives the same sums.
 #pragma once
 
@@ -83,13 +83,17 @@ __device__ __forceinline__ void replay(Op& op, const Particle& p, const GatherCo
     }
     const uint32_t* __restrict__ entries = list.entries + list_row(p.s, list.capacity);
     if (n == 0) return;
+    // Two-stage pipeline: the index of entry k+1 and the data of entry k are in flight while
+    // entry k-1 is applied.
     uint32_t t = entries[0];
+    uint32_t tn = n > 1u ? entries[32] : 0u;
     auto data = op.prefetch(t);
     for (uint32_t k = 1; k < n; ++k) {
-        const uint32_t tn = entries[static_cast<size_t>(k) * 32u];
+        const uint32_t tnn = k + 1u < n ? entries[static_cast<size_t>(k + 1u) * 32u] : 0u;
         const auto next = op.prefetch(tn);
         op.apply(t, data);
         t = tn;
+        tn = tnn;
         data = next;
     }
     op.apply(t, data);

@@ -112,7 +112,19 @@ struct ListScanArgs {
     StoredList list;
 };
 
-cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a);
+// Launch shape of the neighbour-list and gather kernels.  Every shape gives bit-identical results
+// (the per-particle arithmetic and its order do not depend on it); the autotuner picks the fastest.
+enum ListScanVariant : uint32_t {
+    kScanPerLane = 0,       // every lane walks its own 27 cells (run-mates share each load)
+    kScanCooperative = 1,   // a warp walks each home-cell run's candidates once, 32 at a time
+};
+struct LaunchShape {
+    uint32_t scan = kScanPerLane;
+    uint32_t block = 128;   // threads per block of the list and gather kernels: 32, 64, 96 or 128
+};
+bool valid_shape(const LaunchShape& shape);
+
+cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a, const LaunchShape& shape = LaunchShape{});
 // Device step counter and the per-step scene fields derived from it (time, grid origin, collision box).
 cudaError_t launch_set_step(cudaStream_t stream, unsigned long long* step, uint64_t value);
 cudaError_t launch_advance_step(cudaStream_t stream, unsigned long long* step);

@@ -78,6 +78,25 @@ class ParametersC(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name in PARAMETER_NAMES]
 
 
+class LaunchShapeC(ctypes.Structure):
+    _fields_ = [("list_scan", ctypes.c_uint32), ("block_size", ctypes.c_uint32)]
+
+
+@dataclasses.dataclass
+class LaunchShape:
+    """Launch shape of the neighbour-list and gather kernels (results are identical for every shape).
+    list_scan: 0 = per-lane walk, 1 = warp-cooperative scan; block_size: 32, 64, 96 or 128."""
+    list_scan: int = 0
+    block_size: int = 128
+
+    def to_c(self) -> "LaunchShapeC":
+        return LaunchShapeC(self.list_scan, self.block_size)
+
+    @staticmethod
+    def from_c(c: "LaunchShapeC") -> "LaunchShape":
+        return LaunchShape(int(c.list_scan), int(c.block_size))
+
+
 class HostStateC(ctypes.Structure):
     _fields_ = [("positions", ctypes.c_void_p * 3), ("velocities", ctypes.c_void_p * 3), ("step_index", ctypes.c_uint64)]
 
@@ -162,8 +181,17 @@ def library() -> ctypes.CDLL:
         lib.pbf_batch_vjp_step.argtypes = [vp, P(ParticleStateC), P(ControlC), P(ParametersC), P(ParticleStateC),
                                            ctypes.c_uint32, P(StateAdjointC), P(StateAdjointC), P(ControlC),
                                            P(ParametersC)]
+        lib.pbf_batch_jvp_step.argtypes = [vp, P(ParticleStateC), P(ControlC), P(ParametersC), P(ParticleStateC),
+                                           ctypes.c_uint32, P(StateAdjointC), P(ControlC), P(ParametersC), P(StateAdjointC)]
         lib.pbf_batch_reserve_caches.argtypes = [vp, ctypes.c_uint32]
-        lib.pbf_batch_set_launch_shape.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32]
+        lib.pbf_set_launch_shape.argtypes = [vp, P(LaunchShapeC)]
+        lib.pbf_get_launch_shape.argtypes = [vp, P(LaunchShapeC)]
+        lib.pbf_autotune.argtypes = [vp, P(ParticleStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
+                                     ctypes.c_uint32, P(LaunchShapeC), P(ctypes.c_float)]
+        lib.pbf_batch_set_launch_shape.argtypes = [vp, P(LaunchShapeC)]
+        lib.pbf_batch_get_launch_shape.argtypes = [vp, P(LaunchShapeC)]
+        lib.pbf_batch_autotune.argtypes = [vp, P(ParticleStateC), P(ControlC), P(ParametersC), P(ParticleStateC),
+                                           ctypes.c_uint32, ctypes.c_uint32, P(LaunchShapeC), P(ctypes.c_float)]
         lib.pbf_batch_synchronize.argtypes = [vp]
         lib.pbf_batch_scene_sums.argtypes = [vp, vp, vp]
         lib.pbf_batch_set_graph_mode.argtypes = [vp, ctypes.c_int]
@@ -502,6 +530,27 @@ class PBF:
         """Replay the forward launch sequence as a CUDA graph per buffer set."""
         check(library().pbf_set_graph_mode(self.handle, 1 if enable else 0))
 
+    @property
+    def launch_shape(self) -> LaunchShape:
+        c = LaunchShapeC()
+        check(library().pbf_get_launch_shape(self.handle, ctypes.byref(c)))
+        return LaunchShape.from_c(c)
+
+    @launch_shape.setter
+    def launch_shape(self, shape: LaunchShape):
+        check(library().pbf_set_launch_shape(self.handle, ctypes.byref(shape.to_c())))
+
+    def autotune(self, state: State, control: Control, parameters: Parameters, repeats: int = 2):
+        """Time every launch shape on forward steps from `state` and keep the fastest.
+        Returns (shape, milliseconds per step)."""
+        scratch = self.allocate_state()
+        cache = self.allocate_step_cache()
+        c, ms = LaunchShapeC(), ctypes.c_float()
+        check(library().pbf_autotune(self.handle, ctypes.byref(state.c()), ctypes.byref(control.c()),
+                                     ctypes.byref(parameters.c()), ctypes.byref(scratch.c()), cache.handle, repeats,
+                                     ctypes.byref(c), ctypes.byref(ms)))
+        return LaunchShape.from_c(c), float(ms.value)
+
 
 class Batch:
     """Many independent scenes advanced together (pbf_batch_*).
@@ -580,6 +629,16 @@ class Batch:
                                            ctypes.byref(next_state_adjoint.c()), ctypes.byref(previous_state_adjoint.c()),
                                            ctypes.byref(control_adjoint.c()), ctypes.byref(parameter_adjoint.c())))
 
+    def jvp_step(self, state, control, parameters, next_state, cache_slot, state_tangent, control_tangent,
+                 parameter_tangent, next_state_tangent):
+        check(library().pbf_batch_jvp_step(self.handle, ctypes.byref(state.c()), ctypes.byref(control.c()),
+                                           ctypes.byref(parameters.c()), ctypes.byref(next_state.c()), cache_slot,
+                                           ctypes.byref(state_tangent.c()), ctypes.byref(control_tangent.c()),
+                                           ctypes.byref(parameter_tangent.c()), ctypes.byref(next_state_tangent.c())))
+
+    def allocate_state_tangent(self) -> StateTangent:
+        return StateTangent(self._vec(), self._vec())
+
     def scene_sums(self, values: torch.Tensor) -> torch.Tensor:
         """Compensated FP64 per-scene sums of a per-particle FP64 vector."""
         out = torch.empty(self.scene_count, dtype=torch.float64, device=self.device)
@@ -588,6 +647,26 @@ class Batch:
 
     def set_graph_mode(self, enable: bool = True):
         check(library().pbf_batch_set_graph_mode(self.handle, 1 if enable else 0))
+
+    @property
+    def launch_shape(self) -> LaunchShape:
+        c = LaunchShapeC()
+        check(library().pbf_batch_get_launch_shape(self.handle, ctypes.byref(c)))
+        return LaunchShape.from_c(c)
+
+    @launch_shape.setter
+    def launch_shape(self, shape: LaunchShape):
+        check(library().pbf_batch_set_launch_shape(self.handle, ctypes.byref(shape.to_c())))
+
+    def autotune(self, state: State, control: Control, parameters: Parameters, repeats: int = 2, cache_slot: int = 0):
+        """Time every launch shape on batched forward steps from `state` and keep the fastest.
+        Returns (shape, milliseconds per step)."""
+        scratch = self.allocate_state()
+        c, ms = LaunchShapeC(), ctypes.c_float()
+        check(library().pbf_batch_autotune(self.handle, ctypes.byref(state.c()), ctypes.byref(control.c()),
+                                           ctypes.byref(parameters.c()), ctypes.byref(scratch.c()), cache_slot, repeats,
+                                           ctypes.byref(c), ctypes.byref(ms)))
+        return LaunchShape.from_c(c), float(ms.value)
 
     def synchronize(self):
         check(library().pbf_batch_synchronize(self.handle))

@@ -84,3 +84,22 @@ def test_batched_vjp_equals_per_scene_vjp():
         assert torch.equal(pa.velocities[:, sl], p1.velocities), s
         assert torch.equal(qa.tensors["xsph_viscosity"][sl], q1.tensors["xsph_viscosity"]), s
         assert sums[s] == pytest.approx(float(q1.tensors["xsph_viscosity"].sum()), rel=1e-12)
+
+
+def test_batched_rollout_gradients_equal_per_scene_rollouts():
+    """A checkpointed rollout of a differentiable batch gives every scene exactly the loss, dL/dv0
+    and dL/dc of that scene's own rollout."""
+    from physica_b200 import trajectory
+    scs = [scenes.batched_scene(c, 400 + k, 3, velocity_sigma=0.1) for k, c in enumerate((900, 2100, 1500))]
+    targets = [scenes.target_cloud(500 + k, sc.count) for k, sc in enumerate(scs)]
+    batch, state, control, params = pbf.batch_for_scenes(scs, mode=pbf.ExecutionMode.differentiable)
+    t_all = torch.from_numpy(np.concatenate(targets, axis=1)).cuda()
+    g = trajectory.loss_and_gradients(batch, state, control, params, t_all, 5, 2)
+    torch.cuda.synchronize()
+    for s, sc in enumerate(scs):
+        solver, st, ctl, prm = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable)
+        gs = trajectory.loss_and_gradients(solver, st, ctl, prm, torch.from_numpy(targets[s]).cuda(), 5, 2)
+        sl = batch.particle_range(s)
+        assert g.loss[s] == gs.loss
+        assert torch.equal(g.initial_velocities[:, sl], gs.initial_velocities), s
+        assert g.scalar["xsph_viscosity"][s] == gs.scalar["xsph_viscosity"], s

@@ -1,0 +1,78 @@
+"""GPU tests of the launch shapes and the autotuner: every shape of the list and gather kernels
+gives bit-identical substeps, for one scene and for a batch, and the autotuner keeps a valid shape."""
+import itertools
+
+import pytest
+import torch
+
+from physica_b200 import pbf, scenes
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [pbf.LaunchShape(v, b) for v, b in itertools.product((0, 1), (32, 64, 96, 128))]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda(cuda_lib):
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    yield
+
+
+def _run(solver, state, control, params, steps):
+    cache = solver.allocate_step_cache()
+    cur = pbf.State(state.positions.clone(), state.velocities.clone(), state.step_index)
+    nxt = solver.allocate_state()
+    for _ in range(steps):
+        solver.forward_step(cur, control, params, nxt, cache)
+        cur, nxt = nxt, cur
+    torch.cuda.synchronize()
+    return cur.positions.clone(), cur.velocities.clone()
+
+
+def test_every_shape_gives_identical_substeps():
+    sc = scenes.dam_break((14, 14, 14), (0, 0, 0), (1, 2, 1), 31, 3, velocity_sigma=0.1)
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    results = []
+    for shape in SHAPES:
+        solver.launch_shape = shape
+        assert solver.launch_shape == shape
+        results.append(_run(solver, state, control, params, 5))
+    for shape, (x, v) in zip(SHAPES[1:], results[1:]):
+        assert torch.equal(x, results[0][0]), shape
+        assert torch.equal(v, results[0][1]), shape
+
+
+def test_invalid_shapes_are_rejected():
+    solver, _, _, _ = pbf.solver_for_scene(scenes.dam_break((4, 4, 4), (0, 0, 0), (1, 2, 1), 32, 2))
+    for bad in (pbf.LaunchShape(2, 128), pbf.LaunchShape(0, 48), pbf.LaunchShape(0, 256), pbf.LaunchShape(1, 0)):
+        with pytest.raises(pbf.PBFError):
+            solver.launch_shape = bad
+
+
+def test_autotune_keeps_a_valid_shape_and_identical_results():
+    sc = scenes.dam_break((16, 16, 16), (0, 0, 0), (1, 2, 1), 33, 3)
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    before = _run(solver, state, control, params, 3)
+    shape, ms = solver.autotune(state, control, params, repeats=1)
+    assert shape in SHAPES and ms > 0.0
+    assert solver.launch_shape == shape
+    after = _run(solver, state, control, params, 3)
+    assert torch.equal(before[0], after[0]) and torch.equal(before[1], after[1])
+
+
+def test_batch_autotune_and_shapes_give_identical_substeps():
+    scs = [scenes.batched_scene(c, 200 + k, 3) for k, c in enumerate((1500, 4000, 257))]
+    batch, state, control, params = pbf.batch_for_scenes(scs)
+    out = []
+    for shape in (pbf.LaunchShape(0, 128), pbf.LaunchShape(1, 64)):
+        batch.launch_shape = shape
+        cur = pbf.State(state.positions.clone(), state.velocities.clone(), 0)
+        nxt = batch.allocate_state()
+        for _ in range(4):
+            batch.forward_step(cur, control, params, nxt)
+            cur, nxt = nxt, cur
+        torch.cuda.synchronize()
+        out.append((cur.positions.clone(), cur.velocities.clone()))
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+    shape, ms = batch.autotune(state, control, params, repeats=1)
+    assert shape in SHAPES and ms > 0.0
