@@ -606,15 +606,24 @@ int Engine::read(const StepRecord& r, const pbf_cache_field field, void* destina
     auto w = [&](const float4* src) { return launch_unsort_float4(stream_, n, r.sorted_index, src, 0, nullptr, nullptr, nullptr, f); };
     cudaError_t e = cudaSuccess;
     switch (field) {
-        case PBF_CACHE_SORTED_PARTICLE_INDICES:
-            e = cudaMemcpyAsync(destination, r.sorted_index, need, cudaMemcpyDeviceToDevice, stream_);
-            break;
+        // the grid is exported in the reference's layout (x-fastest cell index), converted from the
+        // z-fastest layout the solver sorts by
         case PBF_CACHE_CELL_OFFSETS:
-            e = cudaMemcpyAsync(destination, r.cell_offsets, need, cudaMemcpyDeviceToDevice, stream_);
+            e = launch_reference_offsets(stream_, scene_table_.data(), static_cast<uint32_t>(scene_table_.size()), cells_,
+                                         r.cell_offsets, static_cast<uint32_t*>(destination), tile_sums_);
             break;
-        case PBF_CACHE_SORTED_KEYS:
-            e = launch_sorted_keys(stream_, n, r.sorted_index, r.keys, static_cast<unsigned long long*>(destination));
+        case PBF_CACHE_SORTED_PARTICLE_INDICES:
+        case PBF_CACHE_SORTED_KEYS: {
+            if (!export_offsets_) export_offsets_ = arena_.alloc<uint32_t>(cells_ + 1, e);
+            if (e == cudaSuccess)
+                e = launch_reference_offsets(stream_, scene_table_.data(), static_cast<uint32_t>(scene_table_.size()), cells_,
+                                             r.cell_offsets, export_offsets_, tile_sums_);
+            if (e == cudaSuccess)
+                e = launch_reference_order(stream_, n, d_scenes_, r.cell, r.sorted_index, r.keys, r.cell_offsets, export_offsets_,
+                                           field == PBF_CACHE_SORTED_PARTICLE_INDICES ? static_cast<uint32_t*>(destination) : nullptr,
+                                           field == PBF_CACHE_SORTED_KEYS ? static_cast<unsigned long long*>(destination) : nullptr);
             break;
+        }
         case PBF_CACHE_PREDICTED_POSITIONS: e = vec(r.topology); break;
         case PBF_CACHE_CORRECTED_POSITIONS: e = vec(r.iterate(iterations_, iterations_, diff)); break;
         case PBF_CACHE_RECONSTRUCTED_VELOCITIES: e = vec(r.velocity); break;

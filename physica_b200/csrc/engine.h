@@ -212,6 +212,7 @@ private:
     cudaStream_t capture_stream_ = nullptr;
     std::vector<GraphEntry> graph_cache_;
     SceneStatic* d_static_ = nullptr;
+    uint32_t* export_offsets_ = nullptr;   // reference-layout cell offsets for exports (allocated on first use)
     unsigned long long* d_step_ = nullptr;
     uint64_t host_step_ = ~0ull;   // step index the device counter holds
 

@@ -8,15 +8,12 @@
 //   normal (pbf/pbf.cu:571-593) + confinement (pbf/pbf.cu:674-678)     -> normal_kernel
 //   XSPH (pbf/pbf.cu:700-721) + write-back of next_state               -> xsph_kernel
 //
-// One thread owns one cell-sorted particle.  It walks the 27 stencil cells in the
-// reference order (x offset outer, z inner; particles of a cell in ascending original
-// index, which is their sorted order) and, in a first phase, keeps only candidates whose
-// squared distance is below the pass's exact support threshold, appending their sorted
-// slots to a per-thread list in shared memory.  The list is drained in order with the
-// reference's per-pair expressions, so every per-particle sum is accumulated in the
-// reference's order and equals it bit for bit; skipped candidates contribute an exact
-// zero in the reference.  The list keeps the costly per-pair math (sqrt, divisions)
-// convergent across the warp instead of running under a 15%-taken branch.
+// A list-scan kernel first writes, for every particle, the sorted slots of its neighbours inside
+// the union of all supports, in the reference's stencil order (gather.cuh); each gather pass then
+// replays the list with the reference's per-pair expressions, so every per-particle sum is
+// accumulated in the reference's order and equals it bit for bit (skipped candidates contribute
+// an exact zero in the reference).  Separating the cheap candidate tests from the costly per-pair
+// math (sqrt, divisions) keeps that math convergent across the warp.
 #include "gather.cuh"
 
 namespace pbf {
@@ -27,7 +24,7 @@ using namespace gather_detail;
 
 // --------------------------------------------------------------- list scan
 // Builds the ordered neighbour list of every particle over the positions `pos` (gather.cuh).
-// Per-lane list scan: every lane walks its own 27 stencil cells in the reference's order and
+// Per-lane list scan: every lane walks its own nine stencil columns in the reference's order and
 // appends its hits; lanes of one home cell read the same candidates at the same time (one
 // broadcast load).  Same lists as list_scan_kernel.
 __global__ void __launch_bounds__(kBlock) list_walk_kernel(const ListScanArgs a) {
@@ -36,37 +33,31 @@ __global__ void __launch_bounds__(kBlock) list_walk_kernel(const ListScanArgs a)
     const int4 c = a.g.cell[s];
     const SceneDesc* scene = a.g.scenes + c.w;
     const float thr = a.g.constants[scene->constants].list_threshold;
-    const int cx = static_cast<int>(scene->grid.cells_x), cy = static_cast<int>(scene->grid.cells_y);
-    const int cz = static_cast<int>(scene->grid.cells_z);
-    const uint32_t cell_base = scene->grid.cell_base;
+    const Grid grid = scene->grid;
+    const int cx = static_cast<int>(grid.cells_x), cy = static_cast<int>(grid.cells_y), cz = static_cast<int>(grid.cells_z);
+    const uint32_t z_lo = static_cast<uint32_t>(c.z > 0 ? c.z - 1 : 0);
+    const uint32_t z_hi = static_cast<uint32_t>(c.z + 1 < cz ? c.z + 1 : cz - 1);
     const float4 xi = a.pos[s];
     const uint32_t cap = a.list.capacity;
     uint32_t* __restrict__ entries = a.list.entries + list_row(s, cap);
     const uint32_t* __restrict__ offsets = a.g.cell_offsets;
     const float4* __restrict__ pos = a.pos;
     uint32_t n = 0;
+    // nine stencil columns, x-offset outer; each column's three cells are one contiguous range
     for (int dx = -1; dx <= 1; ++dx) {
         const int x = c.x + dx;
         if (x < 0 || x >= cx) continue;
         for (int dy = -1; dy <= 1; ++dy) {
             const int y = c.y + dy;
             if (y < 0 || y >= cy) continue;
-#pragma unroll
-            for (int dz = -1; dz <= 1; ++dz) {
-                const int z = c.z + dz;
-                if (z < 0 || z >= cz) continue;
-                const uint32_t cell = cell_base + (static_cast<uint32_t>(z) * static_cast<uint32_t>(cy) + static_cast<uint32_t>(y)) *
-                                                      static_cast<uint32_t>(cx) +
-                                      static_cast<uint32_t>(x);
-                const uint32_t end = offsets[cell + 1u];
+            const uint32_t end = offsets[cell_index(grid, x, y, z_hi) + 1u];
 #pragma unroll 4
-                for (uint32_t t = offsets[cell]; t < end; ++t) {
-                    const float4 q = pos[t];
-                    const float r2 = squared(mk(__fsub_rn(xi.x, q.x), __fsub_rn(xi.y, q.y), __fsub_rn(xi.z, q.z)));
-                    if (r2 < thr) {
-                        if (n < cap) entries[static_cast<size_t>(n) * 32u] = t;
-                        ++n;
-                    }
+            for (uint32_t t = offsets[cell_index(grid, x, y, z_lo)]; t < end; ++t) {
+                const float4 q = pos[t];
+                const float r2 = squared(mk(__fsub_rn(xi.x, q.x), __fsub_rn(xi.y, q.y), __fsub_rn(xi.z, q.z)));
+                if (r2 < thr) {
+                    if (n < cap) entries[static_cast<size_t>(n) * 32u] = t;
+                    ++n;
                 }
             }
         }
@@ -103,18 +94,17 @@ __global__ void __launch_bounds__(kBlock) list_scan_kernel(const ListScanArgs a)
         const int hz = __shfl_sync(kFull, c.z, ra), hw = __shfl_sync(kFull, c.w, ra);
         const float thr = __shfl_sync(kFull, threshold, ra);
         const Grid& grid = a.g.scenes[hw].grid;
+        // lane o < 9 holds stencil column o (x-offset outer): cells z-1..z+1, one contiguous range
         uint32_t first = 0, cnt = 0;
-        if (lane < 27u) {
-            const int x = hx + static_cast<int>(lane) / 9 - 1;
-            const int y = hy + (static_cast<int>(lane) / 3) % 3 - 1;
-            const int z = hz + static_cast<int>(lane) % 3 - 1;
-            if (x >= 0 && y >= 0 && z >= 0 && x < static_cast<int>(grid.cells_x) && y < static_cast<int>(grid.cells_y) &&
-                z < static_cast<int>(grid.cells_z)) {
-                const uint32_t cell = grid.cell_base +
-                                      (static_cast<uint32_t>(z) * grid.cells_y + static_cast<uint32_t>(y)) * grid.cells_x +
-                                      static_cast<uint32_t>(x);
-                first = a.g.cell_offsets[cell];
-                cnt = a.g.cell_offsets[cell + 1u] - first;
+        if (lane < 9u) {
+            const int x = hx + static_cast<int>(lane) / 3 - 1;
+            const int y = hy + static_cast<int>(lane) % 3 - 1;
+            const int cz = static_cast<int>(grid.cells_z);
+            if (x >= 0 && y >= 0 && x < static_cast<int>(grid.cells_x) && y < static_cast<int>(grid.cells_y)) {
+                const uint32_t z_lo = static_cast<uint32_t>(hz > 0 ? hz - 1 : 0);
+                const uint32_t z_hi = static_cast<uint32_t>(hz + 1 < cz ? hz + 1 : cz - 1);
+                first = a.g.cell_offsets[cell_index(grid, x, y, z_lo)];
+                cnt = a.g.cell_offsets[cell_index(grid, x, y, z_hi) + 1u] - first;
             }
         }
         uint32_t inc = cnt;
@@ -126,14 +116,14 @@ __global__ void __launch_bounds__(kBlock) list_scan_kernel(const ListScanArgs a)
         const uint32_t total = __shfl_sync(kFull, inc, 31);
         __syncwarp();
         first_s[w][lane] = first;
-        base_s[w][lane] = lane < 27u ? inc - cnt : total;
+        base_s[w][lane] = lane < 9u ? inc - cnt : total;
         __syncwarp();
         for (uint32_t u0 = 0; u0 < total; u0 += 32u) {
             const uint32_t u = u0 + lane;
             const bool valid = u < total;
             uint32_t o = 0;
 #pragma unroll
-            for (uint32_t step = 16; step > 0; step >>= 1)
+            for (uint32_t step = 8; step > 0; step >>= 1)
                 if (base_s[w][o + step] <= u) o += step;
             const uint32_t t = first_s[w][o] + (u - base_s[w][o]);
             const float4 q = valid ? a.pos[t] : make_float4(0.0F, 0.0F, 0.0F, 0.0F);

@@ -3,13 +3,16 @@
 // Every per-particle sum of the reference runs over the particles of the 27 stencil cells of the
 // particle's home cell in a fixed order: stencil cells x offset outer, z offset inner
 // (pbf/pbf.cu:105-110), and within a cell ascending original index, which is the sorted order.
+// Cells are sorted z fastest (cell_index), so the three cells of each (x, y) stencil column are
+// one contiguous range of the sorted array and the stencil is nine ranges.
 // Candidates whose squared distance is at or beyond the list threshold contribute exact zeros to
 // every sum of every pass, so each particle only needs its in-support candidates, in that order.
 //
-// Scan (list_scan_kernel): a warp owns 32 consecutive sorted particles.  Lanes that share a home
-// cell form a run; for each run the warp lays the run's 27 cell ranges end to end (an exclusive
-// warp scan of their lengths) and walks them 32 candidates at a time, one candidate per lane, so a
-// candidate is loaded once per run.  Each home particle of the run tests the 32 candidates against
+// Scan, per lane (list_walk_kernel): each lane walks its own nine column ranges and appends its
+// hits.  Scan, cooperative (list_scan_kernel): a warp owns 32 consecutive sorted particles.
+// Lanes that share a home cell form a run; for each run the warp lays the run's nine column
+// ranges end to end (an exclusive warp scan of their lengths) and walks them 32 candidates at a
+// time, one candidate per lane, so a candidate is loaded once per run.  Each home particle of the run tests the 32 candidates against
 // its position (a shared-memory broadcast); a ballot and a prefix popcount give every hit its slot
 // in the home particle's list, written straight to device memory.  Lists are warp-interleaved:
 // entry k of the warp's 32 particles is one 128-byte line, so a later read of entry k by the 32
@@ -59,15 +62,14 @@ __device__ __forceinline__ size_t list_row(const uint32_t s, const uint32_t capa
 template <class Op>
 __device__ void walk(Op& op, const Particle& p, const GatherCommon& g) {
     const Grid& grid = p.scene->grid;
-    for (int o = 0; o < 27; ++o) {
-        const int x = p.c.x + o / 9 - 1, y = p.c.y + (o / 3) % 3 - 1, z = p.c.z + o % 3 - 1;
-        if (x < 0 || y < 0 || z < 0 || x >= static_cast<int>(grid.cells_x) || y >= static_cast<int>(grid.cells_y) ||
-            z >= static_cast<int>(grid.cells_z))
-            continue;
-        const uint32_t c = grid.cell_base + (static_cast<uint32_t>(z) * grid.cells_y + static_cast<uint32_t>(y)) * grid.cells_x +
-                           static_cast<uint32_t>(x);
-        const uint32_t end = g.cell_offsets[c + 1u];
-        for (uint32_t t = g.cell_offsets[c]; t < end; ++t) op.process(t);
+    const int cz = static_cast<int>(grid.cells_z);
+    const uint32_t z_lo = static_cast<uint32_t>(p.c.z > 0 ? p.c.z - 1 : 0);
+    const uint32_t z_hi = static_cast<uint32_t>(p.c.z + 1 < cz ? p.c.z + 1 : cz - 1);
+    for (int o = 0; o < 9; ++o) {   // stencil columns, x-offset outer; cells z-1..z+1 are contiguous
+        const int x = p.c.x + o / 3 - 1, y = p.c.y + o % 3 - 1;
+        if (x < 0 || y < 0 || x >= static_cast<int>(grid.cells_x) || y >= static_cast<int>(grid.cells_y)) continue;
+        const uint32_t end = g.cell_offsets[cell_index(grid, x, y, z_hi) + 1u];
+        for (uint32_t t = g.cell_offsets[cell_index(grid, x, y, z_lo)]; t < end; ++t) op.process(t);
     }
 }
 

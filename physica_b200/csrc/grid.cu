@@ -44,8 +44,7 @@ __global__ void predict_key_kernel(const uint32_t count, const SceneDesc* __rest
     const int cx = clamp_cell(__fdiv_rn(__fmaf_rn(-g.time, g.key_vel_x, __fsub_rn(xs.x, g.key_min_x)), g.cell_size), g.cells_x);
     const int cy = clamp_cell(__fdiv_rn(__fmaf_rn(-g.time, g.key_vel_y, __fsub_rn(xs.y, g.key_min_y)), g.cell_size), g.cells_y);
     const int cz = clamp_cell(__fdiv_rn(__fmaf_rn(-g.time, g.key_vel_z, __fsub_rn(xs.z, g.key_min_z)), g.cell_size), g.cells_z);
-    const uint32_t key = g.cell_base + (static_cast<uint32_t>(cz) * g.cells_y + static_cast<uint32_t>(cy)) * g.cells_x +
-                         static_cast<uint32_t>(cx);
+    const uint32_t key = cell_index(g, static_cast<uint32_t>(cx), static_cast<uint32_t>(cy), static_cast<uint32_t>(cz));
     keys[i] = key;
     arrival[i] = atomicAdd(histogram + key, 1u);
 }
@@ -177,12 +176,33 @@ __global__ void reorder_kernel(const uint32_t count, const SceneDesc* __restrict
     params_b[s] = make_float4(params.strength[i], params.exponent[i], params.radius[i], 0.0F);
 }
 
-// Sorted keys as the reference stores them (uint64), for inspection.
-__global__ void sorted_keys_kernel(const uint32_t count, const uint32_t* __restrict__ sorted_index,
-                                   const uint32_t* __restrict__ keys, unsigned long long* __restrict__ out) {
+// ---- export in the reference's grid layout (cell index x fastest) ----
+// Particle count of every cell of one scene, stored at the cell's reference index.
+__global__ void reference_counts_kernel(const Grid g, const uint32_t* __restrict__ cell_offsets, uint32_t* __restrict__ out) {
+    const uint32_t local = blockIdx.x * blockDim.x + threadIdx.x;
+    if (local >= g.cells_x * g.cells_y * g.cells_z) return;
+    const uint32_t z = local % g.cells_z, y = (local / g.cells_z) % g.cells_y, x = local / (g.cells_z * g.cells_y);
+    const uint32_t c = g.cell_base + local;
+    out[reference_cell_index(g, x, y, z)] = cell_offsets[c + 1u] - cell_offsets[c];
+}
+
+// Slot of every particle in the reference's sorted order (cells by reference index, ascending
+// original index within a cell), with its original index and its reference key.
+__global__ void reference_order_kernel(const uint32_t count, const SceneDesc* __restrict__ scenes, const int4* __restrict__ cell,
+                                       const uint32_t* __restrict__ sorted_index, const uint32_t* __restrict__ keys,
+                                       const uint32_t* __restrict__ cell_offsets, const uint32_t* __restrict__ reference_offsets,
+                                       uint32_t* __restrict__ out_index, unsigned long long* __restrict__ out_keys) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= count) return;
-    out[s] = keys[sorted_index[s]];
+    const uint32_t i = sorted_index[s];
+    const uint32_t key = keys[i];
+    const Grid& g = scenes[cell[s].w].grid;
+    const uint32_t local = key - g.cell_base;
+    const uint32_t z = local % g.cells_z, y = (local / g.cells_z) % g.cells_y, x = local / (g.cells_z * g.cells_y);
+    const uint32_t reference = reference_cell_index(g, x, y, z);
+    const uint32_t slot = reference_offsets[reference] + (s - cell_offsets[key]);
+    if (out_index) out_index[slot] = i;
+    if (out_keys) out_keys[slot] = reference;
 }
 
 __global__ void set_step_kernel(unsigned long long* step, const unsigned long long value) { *step = value; }
@@ -265,10 +285,36 @@ cudaError_t launch_grid_build(cudaStream_t stream, const GridBuildArgs& a) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_sorted_keys(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const uint32_t* keys,
-                               unsigned long long* out) {
+cudaError_t launch_exclusive_scan(cudaStream_t stream, uint32_t* data, const uint64_t n, uint32_t* tile_sums) {
+    const unsigned tiles = static_cast<unsigned>(scan_tile_count(n));
+    scan_reduce_kernel<<<tiles, kScanThreads, 0, stream>>>(data, n, tile_sums);
+    scan_tiles_kernel<<<1, kScanThreads, 0, stream>>>(tile_sums, tiles);
+    scan_apply_kernel<<<tiles, kScanThreads, 0, stream>>>(data, n, tile_sums);
+    count_launch(3);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reference_offsets(cudaStream_t stream, const SceneDesc* host_scenes, const uint32_t scene_count,
+                                     const uint64_t cells, const uint32_t* cell_offsets, uint32_t* reference_offsets,
+                                     uint32_t* tile_sums) {
+    cudaError_t e = cudaMemsetAsync(reference_offsets, 0, (cells + 1) * sizeof(uint32_t), stream);
+    for (uint32_t s = 0; s < scene_count && e == cudaSuccess; ++s) {
+        const Grid& g = host_scenes[s].grid;
+        const uint32_t n = g.cells_x * g.cells_y * g.cells_z;
+        reference_counts_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(g, cell_offsets, reference_offsets);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return e;
+    return launch_exclusive_scan(stream, reference_offsets, cells + 1, tile_sums);
+}
+
+cudaError_t launch_reference_order(cudaStream_t stream, const uint32_t count, const SceneDesc* scenes, const int4* cell,
+                                   const uint32_t* sorted_index, const uint32_t* keys, const uint32_t* cell_offsets,
+                                   const uint32_t* reference_offsets, uint32_t* out_index, unsigned long long* out_keys) {
     if (count == 0) return cudaSuccess;
-    sorted_keys_kernel<<<blocks_for(count, 256), 256, 0, stream>>>(count, sorted_index, keys, out);
+    reference_order_kernel<<<blocks_for(count, 256), 256, 0, stream>>>(count, scenes, cell, sorted_index, keys, cell_offsets,
+                                                                       reference_offsets, out_index, out_keys);
     count_launch();
     return cudaGetLastError();
 }

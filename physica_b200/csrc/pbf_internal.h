@@ -20,6 +20,21 @@ struct Grid {
     float cell_size;           // support radius
 };
 
+// Linear cell index of the particle sort used here: z fastest, then y, then x.  The cells
+// (x, y, z-1), (x, y, z), (x, y, z+1) of a stencil column are then adjacent in the cell-sorted
+// particle array, so every column of the 27-cell stencil is one contiguous range, visited in the
+// reference's order (neighbour cells x-offset outer, z-offset inner, pbf/pbf.cu:105-110; within a
+// cell ascending original index).  Exported grids use the reference's x-fastest index
+// (reference_cell_index, neighborhood/neighborhood.cu:20-39).
+__host__ __device__ __forceinline__ uint32_t cell_index(const Grid& g, const uint32_t x, const uint32_t y, const uint32_t z) {
+    return g.cell_base + (x * g.cells_y + y) * g.cells_z + z;
+}
+
+__host__ __device__ __forceinline__ uint32_t reference_cell_index(const Grid& g, const uint32_t x, const uint32_t y,
+                                                                   const uint32_t z) {
+    return g.cell_base + (z * g.cells_y + y) * g.cells_x + x;
+}
+
 // Collision box of one scene at the step being computed (pbf/pbf.cpp:17-31).
 struct Box {
     float min_x, min_y, min_z, max_x, max_y, max_z;

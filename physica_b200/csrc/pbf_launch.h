@@ -34,8 +34,14 @@ struct GridBuildArgs {
 
 size_t scan_tile_count(uint64_t n);
 cudaError_t launch_grid_build(cudaStream_t stream, const GridBuildArgs& args);
-cudaError_t launch_sorted_keys(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const uint32_t* keys,
-                               unsigned long long* out);
+cudaError_t launch_exclusive_scan(cudaStream_t stream, uint32_t* data, uint64_t n, uint32_t* tile_sums);
+// Cell offsets in the reference's grid layout (x-fastest cell index) from this layout's offsets.
+cudaError_t launch_reference_offsets(cudaStream_t stream, const SceneDesc* host_scenes, uint32_t scene_count, uint64_t cells,
+                                     const uint32_t* cell_offsets, uint32_t* reference_offsets, uint32_t* tile_sums);
+// The reference's sorted order: original indices and uint64 reference keys by reference slot.
+cudaError_t launch_reference_order(cudaStream_t stream, uint32_t count, const SceneDesc* scenes, const int4* cell,
+                                   const uint32_t* sorted_index, const uint32_t* keys, const uint32_t* cell_offsets,
+                                   const uint32_t* reference_offsets, uint32_t* out_index, unsigned long long* out_keys);
 
 // A stored neighbour list (warp-interleaved entries + per-particle counts).
 struct StoredList {
