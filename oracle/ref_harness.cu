@@ -117,8 +117,11 @@ struct Harness {
     Vec current_position_tangent, next_position_tangent, gradient_sum_tangent, correction_tangent,
         reconstructed_velocity_tangent, vorticity_tangent, vorticity_normal_tangent, confined_velocity_tangent, jvp_positions;
     float *density_tangent, *denominator_tangent, *lambda_tangent, *vorticity_magnitude_tangent;
-    // empty boundary set
+    // boundary particles (empty unless ref_set_boundary was called)
     float* empty_f = nullptr;
+    uint32_t boundary_count = 0;
+    Vec boundary_positions, boundary_velocities;
+    float* boundary_volumes = nullptr;
 
     template <class T>
     T* alloc(size_t n) {
@@ -146,9 +149,13 @@ struct Harness {
 
     cd::NeighborhoodView neighborhood() const {
         return {sorted_keys, sorted_indices, cell_offsets, sorted_boundary_keys, sorted_boundary_indices, boundary_cell_offsets,
-                cfg.particle_count, 0u, cells_x, cells_y, cells_z, origin[0], origin[1], origin[2], cfg.support_radius};
+                cfg.particle_count, boundary_count, cells_x, cells_y, cells_z, origin[0], origin[1], origin[2], cfg.support_radius};
     }
-    cd::BoundaryView boundary() const { return {empty_f, empty_f, empty_f, empty_f, empty_f, empty_f, empty_f, 0u, boundary_time}; }
+    cd::BoundaryView boundary() const {
+        if (boundary_count == 0) return {empty_f, empty_f, empty_f, empty_f, empty_f, empty_f, empty_f, 0u, boundary_time};
+        return {boundary_positions.x, boundary_positions.y, boundary_positions.z, boundary_velocities.x, boundary_velocities.y,
+                boundary_velocities.z, boundary_volumes, boundary_count, boundary_time};
+    }
 
     // pbf/pbf.cpp:17-31
     cd::Box collision_box(const uint64_t step) const {
@@ -186,9 +193,12 @@ struct Harness {
     void build(const uint64_t step, const Vec& positions) {
         const cd::Box box{cfg.box_min[0], cfg.box_min[1], cfg.box_min[2], cfg.box_max[0], cfg.box_max[1], cfg.box_max[2],
                           cfg.box_velocity[0], cfg.box_velocity[1], cfg.box_velocity[2], cfg.no_slip};
-        cd::build_neighborhood(::cuda::stream_ref{stream}, cfg.particle_count, 0u, cfg.support_radius, cfg.time_step, step, box,
-                               cv(positions), cd::ConstVectorView<float>{empty_f, empty_f, empty_f},
-                               cd::ConstVectorView<float>{empty_f, empty_f, empty_f}, unsorted_keys, unsorted_indices,
+        const bool b = boundary_count > 0;
+        cd::build_neighborhood(::cuda::stream_ref{stream}, cfg.particle_count, boundary_count, cfg.support_radius, cfg.time_step,
+                               step, box, cv(positions),
+                               b ? cv(boundary_positions) : cd::ConstVectorView<float>{empty_f, empty_f, empty_f},
+                               b ? cv(boundary_velocities) : cd::ConstVectorView<float>{empty_f, empty_f, empty_f},
+                               unsorted_keys, unsorted_indices,
                                unsorted_boundary_keys, unsorted_boundary_indices, sort_scratch, sort_scratch_bytes,
                                boundary_scratch, boundary_scratch_bytes, sorted_keys, sorted_indices, cell_offsets,
                                sorted_boundary_keys, sorted_boundary_indices, boundary_cell_offsets);
@@ -278,6 +288,34 @@ int ref_create(const ref_config* cfg, void** handle) {
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) { delete h; return 3; }
     *handle = h;
     return 0;
+}
+
+// Boundary particles (host arrays; copied): positions, velocities (x, y, z) and volumes.
+int ref_set_boundary(void* handle, const float* const* positions, const float* const* velocities, const float* volumes,
+                     const uint32_t count) {
+    auto* h = static_cast<Harness*>(handle);
+    h->boundary_count = count;
+    if (count == 0) return 0;
+    h->boundary_positions = {h->alloc<float>(count), h->alloc<float>(count), h->alloc<float>(count)};
+    h->boundary_velocities = {h->alloc<float>(count), h->alloc<float>(count), h->alloc<float>(count)};
+    h->boundary_volumes = h->alloc<float>(count);
+    h->unsorted_boundary_keys = h->alloc<uint64_t>(count);
+    h->sorted_boundary_keys = h->alloc<uint64_t>(count);
+    h->unsorted_boundary_indices = h->alloc<uint32_t>(count);
+    h->sorted_boundary_indices = h->alloc<uint32_t>(count);
+    h->boundary_scratch_bytes = cd::radix_sort_storage_size(count);
+    h->boundary_scratch = h->alloc<uint8_t>(h->boundary_scratch_bytes);
+    for (void* q : h->allocations)
+        if (!q) return 2;
+    const size_t b = count * sizeof(float);
+    float* const dp[3] = {h->boundary_positions.x, h->boundary_positions.y, h->boundary_positions.z};
+    float* const dv[3] = {h->boundary_velocities.x, h->boundary_velocities.y, h->boundary_velocities.z};
+    for (int a = 0; a < 3; ++a) {
+        cudaMemcpy(dp[a], positions[a], b, cudaMemcpyHostToDevice);
+        cudaMemcpy(dv[a], velocities[a], b, cudaMemcpyHostToDevice);
+    }
+    cudaMemcpy(h->boundary_volumes, volumes, b, cudaMemcpyHostToDevice);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 3;
 }
 
 int ref_destroy(void* handle) {

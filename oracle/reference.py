@@ -9,6 +9,7 @@ from __future__ import annotations
 import ctypes
 import pathlib
 
+import numpy as np
 import torch
 
 HERE = pathlib.Path(__file__).resolve().parent
@@ -61,6 +62,7 @@ def load():
         lib.ref_create.argtypes = [P(RefConfig), P(vp)]
         lib.ref_destroy.argtypes = [vp]
         lib.ref_forward_step.argtypes = [vp, P(RefStateIn), P(vp), P(RefParams), P(RefStateOut), ctypes.c_uint64]
+        lib.ref_set_boundary.argtypes = [vp, P(vp), P(vp), vp, ctypes.c_uint32]
         lib.ref_jvp_step.argtypes = [vp, P(RefStateIn), P(RefParams), P(RefStateIn), P(vp), P(RefParams), P(RefStateOut)]
         lib.ref_vjp_step.argtypes = [vp, P(RefStateIn), P(RefParams), P(RefAdjointState), P(RefAdjointState), P(vp),
                                      P(RefParamAdjoint)]
@@ -112,6 +114,14 @@ class ReferencePBF:
         self.params = {k: torch.from_numpy(v).to(self.device) for k, v in scene.parameter_arrays().items()}
         self.controls = torch.from_numpy(scene.controls).to(self.device).contiguous()
         self.n = n
+        b = getattr(scene, "boundary", None)
+        if b is not None and len(b["volumes"]):
+            keep = [np.ascontiguousarray(b[k], dtype=np.float32) for k in ("positions", "velocities", "volumes")]
+            pp = (ctypes.c_void_p * 3)(*[keep[0][a].ctypes.data for a in range(3)])
+            vv = (ctypes.c_void_p * 3)(*[keep[1][a].ctypes.data for a in range(3)])
+            rc = lib.ref_set_boundary(h, pp, vv, ctypes.c_void_p(keep[2].ctypes.data), len(b["volumes"]))
+            if rc:
+                raise RuntimeError(f"ref_set_boundary failed: {rc}")
 
     @property
     def stream(self):

@@ -346,7 +346,9 @@ struct CorrectionVjpArgs {
 };
 
 struct CorrectionVjpOp {
+    static constexpr bool kBoundary = true;
     const float4* __restrict__ pos;
+    const float4* __restrict__ boundary;
     const float* __restrict__ lambda;
     const double4* __restrict__ correction;
     const float4* __restrict__ params_a;
@@ -363,6 +365,10 @@ struct CorrectionVjpOp {
     __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
         if (t == self) return;
+        if (t & kBoundaryBit) {
+            boundary_term(boundary[t & ~kBoundaryBit]);
+            return;
+        }
         const float4 q = pos[t];
         const f3 d = sub(x, xyz(q));
         const float r2 = squared(d);
@@ -395,12 +401,30 @@ struct CorrectionVjpOp {
         lc += rscalar;
         mc += dot(rob, times(rg, rmultiplier / rrest));
     }
+    // boundary particle (position at the step's time, volume): pbf.cu:390-405
+    __device__ __forceinline__ void boundary_term(const float4 q) {
+        const f3 d = sub(x, xyz(q));
+        const float r2 = squared(d);
+        if (r2 == 0.0F || r2 >= k.adjoint_threshold) return;
+        const f3 gradient = spiky_gradient(d, k);
+        const ArtificialPressure ap = artificial_pressure(d, k, strength, exponent, radius);
+        const float volume = q.w;
+        const float multiplier = lambda_i + ap.value;
+        const double scalar_adjoint = volume * dot(ob, gradient);
+        pc = pc + spiky_hessian_product(d, times(ob, volume * multiplier), k);
+        pc = pc + times(ap.gradient, scalar_adjoint);
+        lc += scalar_adjoint;
+        sc += scalar_adjoint * ap.d_strength;
+        ec += scalar_adjoint * ap.d_exponent;
+        qc += scalar_adjoint * ap.d_radius;
+    }
 };
 
 __global__ void __launch_bounds__(kBlock) correction_vjp_kernel(const CorrectionVjpArgs a) {
     const Particle p = locate(a.g);
     CorrectionVjpOp op;
     op.pos = a.pos;
+    op.boundary = a.g.boundary;
     op.lambda = a.lambda;
     op.correction = a.correction;
     op.params_a = a.g.params_a;
@@ -447,7 +471,9 @@ struct LambdaVjpArgs {
 };
 
 struct LambdaVjpOp {
+    static constexpr bool kBoundary = true;
     const float4* __restrict__ pos;
+    const float4* __restrict__ boundary;
     const float* __restrict__ density;
     const float4* __restrict__ gsum;
     const double* __restrict__ lambda_adjoint;
@@ -466,6 +492,15 @@ struct LambdaVjpOp {
     __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
         if (t == self) return;
+        if (t & kBoundaryBit) {
+            // boundary particle: Hessian of V_b W applied to the self-gradient adjoint (pbf.cu:226-230)
+            const float4 q = boundary[t & ~kBoundaryBit];
+            const f3 d = sub(x, xyz(q));
+            const float r2 = squared(d);
+            if (r2 == 0.0F || r2 >= k.adjoint_threshold) return;
+            pc = pc + spiky_hessian_product(d, times(sb, static_cast<double>(q.w)), k);
+            return;
+        }
         const float4 q = pos[t];
         const f3 d = sub(x, xyz(q));
         const float r2 = squared(d);
@@ -507,7 +542,7 @@ struct LambdaVjpSecondOp {
     __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
     __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
-        if (t == self) return;
+        if (t == self || (t & kBoundaryBit)) return;   // fluid neighbours only (pbf.cu:233-246)
         const float4 q = pos[t];
         const f3 d = sub(x, xyz(q));
         const float r2 = squared(d);
@@ -523,6 +558,7 @@ __global__ void __launch_bounds__(kBlock) lambda_vjp_kernel(const LambdaVjpArgs 
     const Particle p = locate(a.g);
     LambdaVjpOp op;
     op.pos = a.pos;
+    op.boundary = a.g.boundary;
     op.density = a.density;
     op.gsum = a.gsum;
     op.lambda_adjoint = a.lambda_adjoint;
@@ -577,18 +613,30 @@ struct DensityVjpArgs {
 };
 
 struct DensityVjpOp {
+    static constexpr bool kBoundary = true;
     const float4* __restrict__ pos;
+    const float4* __restrict__ boundary;
     const double* __restrict__ density_adjoint;
     f3 x;
-    float mass;
+    float mass, rest_density;
     double ob;
     KernelConstants k;
     d3 pc;
-    double mc;
+    double mc, rc;
 
     __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
     __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
     __device__ __forceinline__ void process(const uint32_t t) {
+        if (t & kBoundaryBit) {
+            // boundary particle: rho0_i V_b W (density/density.cu:93-98)
+            const float4 q = boundary[t & ~kBoundaryBit];
+            const f3 d = sub(x, xyz(q));
+            if (squared(d) >= k.h2) return;
+            const float volume = q.w;
+            pc = pc + times(poly6_gradient(d, k), ob * rest_density * volume);
+            rc += ob * volume * poly6(d, k);
+            return;
+        }
         const float4 q = pos[t];
         const f3 d = sub(x, xyz(q));
         if (squared(d) >= k.h2) return;
@@ -603,20 +651,23 @@ __global__ void __launch_bounds__(kBlock) density_vjp_kernel(const DensityVjpArg
     const Particle p = locate(a.g);
     DensityVjpOp op;
     op.pos = a.pos;
+    op.boundary = a.g.boundary;
     op.density_adjoint = a.density_adjoint;
     op.k = p.k;
     const float4 xi = p.active ? a.pos[p.s] : make_float4(0, 0, 0, 0);
     op.x = xyz(xi);
     op.mass = xi.w;
+    op.rest_density = p.active ? a.g.params_a[p.s].x : 1.0F;
     op.ob = p.active ? a.density_adjoint[p.s] : 0.0;
     op.pc = {0.0, 0.0, 0.0};
     op.mc = 0.0;
+    op.rc = 0.0;
     replay(op, p, a.g, a.list);
     if (!p.active) return;
     const uint32_t i = a.sorted_index[p.s];
     const d3 xb = ld3(a.x[p.s]) + op.pc;
     add_to(a.pa.masses, i, op.mc);
-    add_to(a.pa.rest_densities, i, 0.0);
+    add_to(a.pa.rest_densities, i, op.rc);
     finish(a.tail, p.s, i, xb, p.scene->time_step);
 }
 
@@ -753,7 +804,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
               parameter_adjoint->artificial_pressure_radius, parameter_adjoint->xsph_viscosity,
               parameter_adjoint->vorticity_confinement};
     }
-    const GatherCommon gc{n, d_scenes_, d_constants_, r.cell_offsets, r.cell, r.params_a, r.params_b};
+    const GatherCommon gc = gather_common(r);
     const AdjField3 prev_x{previous_adjoint->positions.x, previous_adjoint->positions.y, previous_adjoint->positions.z};
     const AdjField3 prev_v{previous_adjoint->velocities.x, previous_adjoint->velocities.y, previous_adjoint->velocities.z};
     const AdjField3 ctrl{control_adjoint->external_accelerations.x, control_adjoint->external_accelerations.y,

@@ -167,8 +167,8 @@ int Engine::init(const pbf_domain_configuration* scenes, const uint32_t scene_co
                 set_error("boundary_particles is null but boundary_particle_count > 0");
                 return PBF_ERROR_INVALID_ARGUMENT;
             }
-            set_error("boundary particles are not supported by this build");
-            return PBF_ERROR_UNSUPPORTED;
+            // domain/domain.cpp: the boundary set is copied at construction
+            h.boundary.assign(c.boundary_particles, c.boundary_particles + c.boundary_particle_count);
         }
         const float mins[3] = {c.boundary.minimum.x, c.boundary.minimum.y, c.boundary.minimum.z};
         const float maxs[3] = {c.boundary.maximum.x, c.boundary.maximum.y, c.boundary.maximum.z};
@@ -220,6 +220,40 @@ int Engine::init(const pbf_domain_configuration* scenes, const uint32_t scene_co
         if (int rc = check(e, "upload scene table")) return rc;
         e = cudaStreamSynchronize(stream_);
         if (int rc = check(e, "synchronise")) return rc;
+    }
+    // Boundary particles of every scene, concatenated.
+    uint64_t boundary_total = 0;
+    for (const SceneHost& h : scenes_) boundary_total += h.boundary.size();
+    if (boundary_total >= (1ull << 31)) {
+        set_error("boundary particles must stay below 2^31");
+        return PBF_ERROR_CAPACITY;
+    }
+    boundary_count_ = static_cast<uint32_t>(boundary_total);
+    if (boundary_count_ > 0) {
+        std::vector<float4> rest, velocity;
+        std::vector<uint32_t> scene_of;
+        for (uint32_t s = 0; s < scene_count; ++s)
+            for (const pbf_boundary_particle& b : scenes_[s].boundary) {
+                rest.push_back(make_float4(b.position.x, b.position.y, b.position.z, b.volume));
+                velocity.push_back(make_float4(b.velocity.x, b.velocity.y, b.velocity.z, 0.0F));
+                scene_of.push_back(s);
+            }
+        boundary_rest_ = arena_.alloc<float4>(boundary_count_, e);
+        boundary_velocity_ = arena_.alloc<float4>(boundary_count_, e);
+        boundary_keys_ = arena_.alloc<uint32_t>(boundary_count_, e);
+        boundary_arrival_ = arena_.alloc<uint32_t>(boundary_count_, e);
+        boundary_unordered_ = arena_.alloc<uint32_t>(boundary_count_, e);
+        if (scene_count > 1) boundary_scene_ = arena_.alloc<uint32_t>(boundary_count_, e);
+        if (int rc = check(e, "device allocation")) return rc;
+        e = cudaMemcpyAsync(boundary_rest_, rest.data(), rest.size() * sizeof(float4), cudaMemcpyHostToDevice, stream_);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(boundary_velocity_, velocity.data(), velocity.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                                stream_);
+        if (e == cudaSuccess && boundary_scene_)
+            e = cudaMemcpyAsync(boundary_scene_, scene_of.data(), scene_of.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                stream_);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);   // the host vectors go out of scope
+        if (int rc = check(e, "upload boundary particles")) return rc;
     }
     // Time-independent scene table; the per-step fields are derived on the device from a step counter.
     std::vector<SceneStatic> statics(scene_count);
@@ -331,6 +365,10 @@ int Engine::allocate_record(StepRecord& r) {
         r.list_entries[l] = r.arena.alloc<uint32_t>(padded * r.list_capacity, e);
         r.list_counts[l] = r.arena.alloc<uint32_t>(n, e);
     }
+    if (boundary_count_ > 0) {
+        r.boundary_offsets = r.arena.alloc<uint32_t>(cells_ + 1, e);
+        r.boundary = r.arena.alloc<float4>(boundary_count_, e);
+    }
     r.valid = false;
     if (int rc = check(e, "step cache allocation")) return rc;
     return check(cudaStreamSynchronize(stream_), "step cache allocation");
@@ -428,6 +466,15 @@ int Engine::forward(const pbf_particle_state* state, const pbf_control* control,
     return PBF_SUCCESS;
 }
 
+GatherCommon Engine::gather_common(const StepRecord& r) const {
+    GatherCommon gc{count_, d_scenes_, d_constants_, r.cell_offsets, r.cell, r.params_a, r.params_b};
+    if (boundary_count_ > 0) {
+        gc.boundary_offsets = r.boundary_offsets;
+        gc.boundary = r.boundary;
+    }
+    return gc;
+}
+
 int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state, const pbf_control* control,
                            const pbf_parameters* parameters, pbf_particle_state* next_state, StepRecord& r) {
     if (int rc = check(launch_scene_time(stream, d_static_, d_scenes_, d_step_, static_cast<uint32_t>(scenes_.size())),
@@ -460,9 +507,14 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
     g.params_b = r.params_b;
     timer_.begin(stream, kPassGrid);
     if (int rc = check(launch_grid_build(stream, g), "grid build")) return rc;
+    if (boundary_count_ > 0) {
+        BoundaryBuildArgs b{boundary_count_, cells_, d_scenes_, boundary_scene_, boundary_rest_, boundary_velocity_,
+                            boundary_keys_, boundary_arrival_, boundary_unordered_, tile_sums_, r.boundary_offsets, r.boundary};
+        if (int rc = check(launch_boundary_build(stream, b), "boundary grid build")) return rc;
+    }
     timer_.end(stream, kPassGrid);
 
-    const GatherCommon gc{count_, d_scenes_, d_constants_, r.cell_offsets, r.cell, r.params_a, r.params_b};
+    const GatherCommon gc = gather_common(r);
     const Field3 previous{state->positions.x, state->positions.y, state->positions.z};
     const MutField3 out_positions{next_state->positions.x, next_state->positions.y, next_state->positions.z};
     for (uint32_t k = 0; k < K; ++k) {
@@ -472,7 +524,7 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
         const uint32_t l = diff ? k : 0u;
         const StoredList list{r.list_entries[l], r.list_counts[l], r.list_capacity};
         timer_.begin(stream, kPassListScan);
-        if (int rc = check(launch_list_scan(stream, ListScanArgs{gc, xk, list}, shape_), "neighbour list scan")) return rc;
+        if (int rc = check(launch_list_scan(stream, ListScanArgs{gc, xk, list, 1}, shape_), "neighbour list scan")) return rc;
         timer_.end(stream, kPassListScan);
         DensityLambdaArgs d{gc, xk, lam, diff ? r.density[k] : (k == 0 ? r.first_density : nullptr),
                             diff ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr, list};

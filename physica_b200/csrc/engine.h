@@ -83,6 +83,9 @@ struct StepRecord {
     std::vector<uint32_t*> list_entries;
     std::vector<uint32_t*> list_counts;
     uint32_t list_capacity = 0;
+    // Boundary particles of the step (only when the scenes have some).
+    uint32_t* boundary_offsets = nullptr;   // cells + 1
+    float4* boundary = nullptr;             // (position at the step's time, volume), cell-sorted
 
     const float4* iterate(uint32_t k, uint32_t K, bool differentiable) const {
         if (k == 0) return topology;
@@ -213,6 +216,16 @@ private:
     std::vector<GraphEntry> graph_cache_;
     SceneStatic* d_static_ = nullptr;
     uint32_t* export_offsets_ = nullptr;   // reference-layout cell offsets for exports (allocated on first use)
+    // Boundary particles of all scenes, concatenated in scene order (original order).
+    uint32_t boundary_count_ = 0;
+    float4* boundary_rest_ = nullptr;       // (position at t = 0, volume)
+    float4* boundary_velocity_ = nullptr;
+    uint32_t* boundary_scene_ = nullptr;    // boundary particle -> scene (several scenes only)
+    uint32_t* boundary_keys_ = nullptr;
+    uint32_t* boundary_arrival_ = nullptr;
+    uint32_t* boundary_unordered_ = nullptr;
+    // The gather inputs shared by every pass of a step recorded in `r`.
+    GatherCommon gather_common(const StepRecord& r) const;
     unsigned long long* d_step_ = nullptr;
     uint64_t host_step_ = ~0ull;   // step index the device counter holds
 

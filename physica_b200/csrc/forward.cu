@@ -43,6 +43,42 @@ __global__ void __launch_bounds__(kBlock) list_walk_kernel(const ListScanArgs a)
     const uint32_t* __restrict__ offsets = a.g.cell_offsets;
     const float4* __restrict__ pos = a.pos;
     uint32_t n = 0;
+    if (a.boundary && a.g.boundary_offsets) {
+        // cell by cell: each cell's fluid particles, then its boundary particles (pbf/pbf.cu:111-121)
+        const uint32_t* __restrict__ boffsets = a.g.boundary_offsets;
+        const float4* __restrict__ bpos = a.g.boundary;
+        for (int dx = -1; dx <= 1; ++dx) {
+            const int x = c.x + dx;
+            if (x < 0 || x >= cx) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int y = c.y + dy;
+                if (y < 0 || y >= cy) continue;
+                for (uint32_t z = z_lo; z <= z_hi; ++z) {
+                    const uint32_t cell = cell_index(grid, x, y, z);
+                    const uint32_t end = offsets[cell + 1u];
+                    for (uint32_t t = offsets[cell]; t < end; ++t) {
+                        const float4 q = pos[t];
+                        const float r2 = squared(mk(__fsub_rn(xi.x, q.x), __fsub_rn(xi.y, q.y), __fsub_rn(xi.z, q.z)));
+                        if (r2 < thr) {
+                            if (n < cap) entries[static_cast<size_t>(n) * 32u] = t;
+                            ++n;
+                        }
+                    }
+                    const uint32_t bend = boffsets[cell + 1u];
+                    for (uint32_t b = boffsets[cell]; b < bend; ++b) {
+                        const float4 q = bpos[b];
+                        const float r2 = squared(mk(__fsub_rn(xi.x, q.x), __fsub_rn(xi.y, q.y), __fsub_rn(xi.z, q.z)));
+                        if (r2 < thr) {
+                            if (n < cap) entries[static_cast<size_t>(n) * 32u] = b | kBoundaryBit;
+                            ++n;
+                        }
+                    }
+                }
+            }
+        }
+        a.list.counts[s] = n <= cap ? n : kOverflow;
+        return;
+    }
     // nine stencil columns, x-offset outer; each column's three cells are one contiguous range
     for (int dx = -1; dx <= 1; ++dx) {
         const int x = c.x + dx;
@@ -164,7 +200,9 @@ struct MassRatio {
 };
 
 struct DensityLambdaOp {
+    static constexpr bool kBoundary = true;
     const float4* __restrict__ pos;
+    const float4* __restrict__ boundary;
     f3 x;
     uint32_t self;
     float rest_density;
@@ -175,10 +213,21 @@ struct DensityLambdaOp {
     uint32_t neighbors;
     MassRatio ratio;
 
-    __device__ __forceinline__ float4 prefetch(const uint32_t t) const { return pos[t]; }
+    __device__ __forceinline__ float4 prefetch(const uint32_t t) const {
+        return (t & kBoundaryBit) ? boundary[t & ~kBoundaryBit] : pos[t];
+    }
     __device__ __forceinline__ void apply(const uint32_t t, const float4 q) {
         const f3 d = sub(x, xyz(q));
         const float r2 = squared(d);
+        if (t & kBoundaryBit) {
+            // boundary particle b: density += rho0_i V_b W (density/density.cu:34-37),
+            // S += V_b grad W (pbf/pbf.cu:118-121); no denominator term
+            if (r2 < k.h2) density = __fmaf_rn(__fmul_rn(rest_density, q.w), poly6_inside(r2, k), density);
+            const float distance = __fsqrt_rn(r2);
+            if (distance == 0.0F || distance >= k.h) return;
+            gradient_sum = fma3(q.w, spiky_gradient_at(d, distance, k), gradient_sum);
+            return;
+        }
         if (r2 < k.h2) density = __fmaf_rn(q.w, poly6_inside(r2, k), density);
         if (t == self) return;
         if (r2 < k.h2) ++neighbors;
@@ -197,6 +246,7 @@ __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLam
     if (!p.active) return;
     DensityLambdaOp op;
     op.pos = a.pos;
+    op.boundary = a.g.boundary;
     op.self = p.s;
     op.k = p.k;
     const float4 xi = a.pos[p.s];
@@ -225,7 +275,9 @@ struct PositionLambda {
 };
 
 struct CorrectionOp {
+    static constexpr bool kBoundary = true;
     const float4* __restrict__ pos;
+    const float4* __restrict__ boundary;
     const float* __restrict__ lambda;
     f3 x;
     uint32_t self;
@@ -237,7 +289,10 @@ struct CorrectionOp {
     f3 correction;
     MassRatio ratio;
 
-    __device__ __forceinline__ PositionLambda prefetch(const uint32_t t) const { return {pos[t], lambda[t]}; }
+    __device__ __forceinline__ PositionLambda prefetch(const uint32_t t) const {
+        if (t & kBoundaryBit) return {boundary[t & ~kBoundaryBit], 0.0F};
+        return {pos[t], lambda[t]};
+    }
     __device__ __forceinline__ void apply(const uint32_t t, const PositionLambda in) {
         if (t == self) return;
         const f3 d = sub(x, xyz(in.q));
@@ -253,6 +308,12 @@ struct CorrectionOp {
         } else {
             artificial = r2 < k.h2 ? -strength : 0.0F;
         }
+        if (t & kBoundaryBit) {
+            // boundary particle b: V_b (lambda_i + s_corr) grad W (pbf/pbf.cu:278-285)
+            const float factor = __fmul_rn(in.q.w, __fadd_rn(lambda_i, artificial));
+            correction = fma3(factor, spiky_gradient_at(d, distance, k), correction);
+            return;
+        }
         const float coefficient = ratio(in.q.w, rest_density);
         const float factor = __fmul_rn(coefficient, __fadd_rn(__fadd_rn(lambda_i, in.lambda), artificial));
         correction = fma3(factor, spiky_gradient_at(d, distance, k), correction);
@@ -265,6 +326,7 @@ __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs
     if (!p.active) return;
     CorrectionOp op;
     op.pos = a.pos;
+    op.boundary = a.g.boundary;
     op.lambda = a.lambda;
     op.self = p.s;
     op.k = p.k;
@@ -539,7 +601,8 @@ unsigned block_of(const unsigned block) {
 cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a, const LaunchShape& shape) {
     if (a.g.count == 0) return cudaSuccess;
     const unsigned block = block_of(shape.block);
-    if (shape.scan == kScanCooperative)
+    // the cooperative scan lists fluid particles only; lists with boundary particles use the walk
+    if (shape.scan == kScanCooperative && !(a.boundary && a.g.boundary_offsets))
         list_scan_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     else
         list_walk_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);

@@ -23,6 +23,8 @@
 // its stencil directly (same order, every candidate offered to the pass), which gives the same sums.
 #pragma once
 
+#include <type_traits>
+
 #include "pbf_internal.h"
 #include "pbf_launch.h"
 
@@ -33,6 +35,16 @@ constexpr int kWarpsPerBlock = 4;
 constexpr int kBlock = 32 * kWarpsPerBlock;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kOverflow = 0xffffffffu;
+// A list entry with this bit set is a boundary particle (slot in the cell-sorted boundary array).
+constexpr uint32_t kBoundaryBit = 0x80000000u;
+
+// Passes with boundary terms (density, lambda, correction and their derivatives) declare
+// `static constexpr bool kBoundary = true`; their overflow walk then visits each cell's boundary
+// particles after its fluid particles, as the reference's cell loops do (pbf/pbf.cu:111-121).
+template <class T, class = void>
+struct takes_boundary : std::false_type {};
+template <class T>
+struct takes_boundary<T, std::void_t<decltype(T::kBoundary)>> : std::integral_constant<bool, T::kBoundary> {};
 
 struct Particle {
     uint32_t s;
@@ -62,6 +74,22 @@ __device__ __forceinline__ size_t list_row(const uint32_t s, const uint32_t capa
 template <class Op>
 __device__ void walk(Op& op, const Particle& p, const GatherCommon& g) {
     const Grid& grid = p.scene->grid;
+    if constexpr (takes_boundary<Op>::value) {
+        if (g.boundary_offsets) {   // cell by cell: fluid particles, then boundary particles
+            for (int o = 0; o < 27; ++o) {
+                const int x = p.c.x + o / 9 - 1, y = p.c.y + (o / 3) % 3 - 1, z = p.c.z + o % 3 - 1;
+                if (x < 0 || y < 0 || z < 0 || x >= static_cast<int>(grid.cells_x) || y >= static_cast<int>(grid.cells_y) ||
+                    z >= static_cast<int>(grid.cells_z))
+                    continue;
+                const uint32_t c = cell_index(grid, x, y, z);
+                const uint32_t end = g.cell_offsets[c + 1u];
+                for (uint32_t t = g.cell_offsets[c]; t < end; ++t) op.process(t);
+                const uint32_t bend = g.boundary_offsets[c + 1u];
+                for (uint32_t b = g.boundary_offsets[c]; b < bend; ++b) op.process(b | kBoundaryBit);
+            }
+            return;
+        }
+    }
     const int cz = static_cast<int>(grid.cells_z);
     const uint32_t z_lo = static_cast<uint32_t>(p.c.z > 0 ? p.c.z - 1 : 0);
     const uint32_t z_hi = static_cast<uint32_t>(p.c.z + 1 < cz ? p.c.z + 1 : cz - 1);

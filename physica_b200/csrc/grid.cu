@@ -176,6 +176,44 @@ __global__ void reorder_kernel(const uint32_t count, const SceneDesc* __restrict
     params_b[s] = make_float4(params.strength[i], params.exponent[i], params.radius[i], 0.0F);
 }
 
+// ---- boundary particles (neighborhood/neighborhood.cu:63-69, key_kernel with moving positions) ----
+// Key of a boundary particle at the step's time: x = p + t v (fused as the reference compiles
+// `x += time * velocity`), then the fluid's cell formula; histogram of keys.
+__global__ void boundary_key_kernel(const uint32_t count, const SceneDesc* __restrict__ scenes,
+                                    const uint32_t* __restrict__ scene_of, const float4* __restrict__ rest,
+                                    const float4* __restrict__ velocity, uint32_t* __restrict__ keys,
+                                    uint32_t* __restrict__ arrival, uint32_t* __restrict__ histogram) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= count) return;
+    const Grid& g = scenes[scene_of ? scene_of[b] : 0u].grid;
+    const float4 p = rest[b], v = velocity[b];
+    const f3 xs = mk(__fmaf_rn(g.time, v.x, p.x), __fmaf_rn(g.time, v.y, p.y), __fmaf_rn(g.time, v.z, p.z));
+    const int cx = clamp_cell(__fdiv_rn(__fmaf_rn(-g.time, g.key_vel_x, __fsub_rn(xs.x, g.key_min_x)), g.cell_size), g.cells_x);
+    const int cy = clamp_cell(__fdiv_rn(__fmaf_rn(-g.time, g.key_vel_y, __fsub_rn(xs.y, g.key_min_y)), g.cell_size), g.cells_y);
+    const int cz = clamp_cell(__fdiv_rn(__fmaf_rn(-g.time, g.key_vel_z, __fsub_rn(xs.z, g.key_min_z)), g.cell_size), g.cells_z);
+    const uint32_t key = cell_index(g, static_cast<uint32_t>(cx), static_cast<uint32_t>(cy), static_cast<uint32_t>(cz));
+    keys[b] = key;
+    arrival[b] = atomicAdd(histogram + key, 1u);
+}
+
+// Stable order inside each cell (ascending boundary index) and the sorted (position at t, volume).
+__global__ void boundary_reorder_kernel(const uint32_t count, const SceneDesc* __restrict__ scenes,
+                                        const uint32_t* __restrict__ scene_of, const uint32_t* __restrict__ keys,
+                                        const uint32_t* __restrict__ cell_offsets, const uint32_t* __restrict__ unordered,
+                                        const float4* __restrict__ rest, const float4* __restrict__ velocity,
+                                        float4* __restrict__ sorted) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= count) return;
+    const uint32_t key = keys[b];
+    const uint32_t first = cell_offsets[key], last = cell_offsets[key + 1u];
+    uint32_t rank = 0;
+    for (uint32_t u = first; u < last; ++u) rank += unordered[u] < b ? 1u : 0u;
+    const float t = scenes[scene_of ? scene_of[b] : 0u].grid.time;
+    const float4 p = rest[b], v = velocity[b];
+    // boundary_position (neighborhood/device.cuh:16-22)
+    sorted[first + rank] = make_float4(__fmaf_rn(t, v.x, p.x), __fmaf_rn(t, v.y, p.y), __fmaf_rn(t, v.z, p.z), p.w);
+}
+
 // ---- export in the reference's grid layout (cell index x fastest) ----
 // Particle count of every cell of one scene, stored at the cell's reference index.
 __global__ void reference_counts_kernel(const Grid g, const uint32_t* __restrict__ cell_offsets, uint32_t* __restrict__ out) {
@@ -282,6 +320,21 @@ cudaError_t launch_grid_build(cudaStream_t stream, const GridBuildArgs& a) {
             a.slot_of, a.cell, a.topology, a.params_a, a.params_b);
         count_launch(2);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_boundary_build(cudaStream_t stream, const BoundaryBuildArgs& a) {
+    cudaError_t e = cudaMemsetAsync(a.cell_offsets, 0, (a.cells + 1) * sizeof(uint32_t), stream);
+    if (e != cudaSuccess || a.count == 0) return e;
+    const unsigned tpb = 256;
+    boundary_key_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.scenes, a.scene_of, a.rest, a.velocity, a.keys,
+                                                                      a.arrival, a.cell_offsets);
+    count_launch();
+    if ((e = launch_exclusive_scan(stream, a.cell_offsets, a.cells + 1, a.tile_sums)) != cudaSuccess) return e;
+    scatter_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.keys, a.arrival, a.cell_offsets, a.unordered);
+    boundary_reorder_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.scenes, a.scene_of, a.keys, a.cell_offsets,
+                                                                          a.unordered, a.rest, a.velocity, a.sorted);
+    count_launch(2);
     return cudaGetLastError();
 }
 

@@ -108,7 +108,9 @@ struct DensityLambdaJvpArgs {
 };
 
 struct DensityLambdaJvpOp {
+    static constexpr bool kBoundary = true;
     const float4* __restrict__ pos;
+    const float4* __restrict__ boundary;
     const float4* __restrict__ x_dot;
     const float4* __restrict__ params_a_dot;
     f3 x, xd;
@@ -118,11 +120,24 @@ struct DensityLambdaJvpOp {
     float density_dot, denominator_dot;
     f3 gsum_dot;
 
-    __device__ __forceinline__ Pair prefetch(const uint32_t t) const { return {pos[t], x_dot[t], params_a_dot[t]}; }
+    __device__ __forceinline__ Pair prefetch(const uint32_t t) const {
+        if (t & kBoundaryBit) return {boundary[t & ~kBoundaryBit], make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0)};
+        return {pos[t], x_dot[t], params_a_dot[t]};
+    }
     __device__ __forceinline__ void apply(const uint32_t t, const Pair& in) {
         const f3 d = x - xyz(in.q);
         const f3 dd = xd - xyz(in.qd);
         const float r2 = squared(d);
+        if (t & kBoundaryBit) {
+            // boundary particle b (density/density.cu:59-63, pbf.cu:164-169); it does not move with
+            // the inputs, so the displacement tangent is x_dot_i
+            const float volume = in.q.w;
+            if (r2 < k.h2) density_dot += volume * (rest_dot * poly6_inside(r2, k) + rest * dot(poly6_gradient(d, k), xd));
+            const float distance = sqrtf(r2);
+            if (distance == 0.0F || distance >= k.h) return;
+            gsum_dot = gsum_dot + times(spiky_gradient_tangent(d, xd, distance, k), volume);
+            return;
+        }
         const float mass_dot = in.aux.x;
         if (r2 < k.h2) density_dot += mass_dot * poly6_inside(r2, k) + in.q.w * dot(poly6_gradient(d, k), dd);
         if (t == self) return;
@@ -145,6 +160,7 @@ __global__ void __launch_bounds__(kBlock) density_lambda_jvp_kernel(const Densit
     if (!p.active) return;
     DensityLambdaJvpOp op;
     op.pos = a.pos;
+    op.boundary = a.g.boundary;
     op.x_dot = a.x_dot;
     op.params_a_dot = a.params_a_dot;
     op.self = p.s;
@@ -192,7 +208,9 @@ struct CorrectionPair {
 };
 
 struct CorrectionJvpOp {
+    static constexpr bool kBoundary = true;
     const float4* __restrict__ pos;
+    const float4* __restrict__ boundary;
     const float4* __restrict__ x_dot;
     const float* __restrict__ lambda;
     const float* __restrict__ lambda_dot;
@@ -206,6 +224,7 @@ struct CorrectionJvpOp {
     f3 result;
 
     __device__ __forceinline__ CorrectionPair prefetch(const uint32_t t) const {
+        if (t & kBoundaryBit) return {boundary[t & ~kBoundaryBit], make_float4(0, 0, 0, 0), 0.0F, 0.0F, 0.0F};
         return {pos[t], x_dot[t], lambda[t], lambda_dot[t], params_a_dot[t].x};
     }
     __device__ __forceinline__ void apply(const uint32_t t, const CorrectionPair& in) {
@@ -219,6 +238,14 @@ struct CorrectionJvpOp {
             const ArtificialPressure ap = artificial_pressure(d, k, strength, exponent, radius);
             art = ap.value;
             art_dot = dot(ap.gradient, dd) + ap.d_strength * strength_dot + ap.d_exponent * exponent_dot + ap.d_radius * radius_dot;
+        }
+        if (t & kBoundaryBit) {
+            // boundary particle b (pbf.cu:321-330)
+            const float multiplier = lambda_i + art;
+            result = result + times(times(spiky_gradient_at(d, distance, k), lambda_dot_i + art_dot) +
+                                        times(spiky_gradient_tangent(d, dd, distance, k), multiplier),
+                                    in.q.w);
+            return;
         }
         const float coefficient = in.q.w / rest;
         const float coefficient_dot = in.mass_dot / rest - in.q.w * rest_dot / (rest * rest);
@@ -235,6 +262,7 @@ __global__ void __launch_bounds__(kBlock) correction_jvp_kernel(const Correction
     if (!p.active) return;
     CorrectionJvpOp op;
     op.pos = a.pos;
+    op.boundary = a.g.boundary;
     op.x_dot = a.x_dot;
     op.lambda = a.lambda;
     op.lambda_dot = a.lambda_dot;
@@ -543,7 +571,7 @@ int Engine::tangent(const pbf_particle_state* state, const StepRecord& r, const 
               parameter_tangent->artificial_pressure_radius, parameter_tangent->xsph_viscosity,
               parameter_tangent->vorticity_confinement};
     }
-    const GatherCommon gc{n, d_scenes_, d_constants_, r.cell_offsets, r.cell, r.params_a, r.params_b};
+    const GatherCommon gc = gather_common(r);
     const unsigned block = shape_.block;
     const unsigned blocks = blocks_of(n, block);
     const MutField3 out_x{next_state_tangent->positions.x, next_state_tangent->positions.y, next_state_tangent->positions.z};

@@ -59,7 +59,29 @@ struct GatherCommon {
     const int4* cell;
     const float4* params_a;
     const float4* params_b;
+    // Boundary particles of the step (null when the scenes have none): cell offsets into the
+    // cell-sorted boundary array and its entries (position at the step's time, volume).
+    const uint32_t* boundary_offsets = nullptr;
+    const float4* boundary = nullptr;
 };
+
+// Boundary particles (neighborhood/neighborhood.cu:63-69): keyed and sorted into the same cells
+// as the fluid at every step, at their position p + t v (neighborhood/device.cuh:16-22).
+struct BoundaryBuildArgs {
+    uint32_t count;
+    uint64_t cells;
+    const SceneDesc* scenes;
+    const uint32_t* scene_of;      // boundary particle -> scene (null: one scene)
+    const float4* rest;            // (position at t = 0, volume), original order
+    const float4* velocity;        // (velocity, 0), original order
+    uint32_t* keys;
+    uint32_t* arrival;
+    uint32_t* unordered;
+    uint32_t* tile_sums;
+    uint32_t* cell_offsets;        // cells + 1
+    float4* sorted;                // (position at the step's time, volume), cell-sorted
+};
+cudaError_t launch_boundary_build(cudaStream_t stream, const BoundaryBuildArgs& args);
 
 struct DensityLambdaArgs {
     GatherCommon g;
@@ -116,6 +138,7 @@ struct ListScanArgs {
     GatherCommon g;
     const float4* pos;
     StoredList list;
+    int boundary = 0;   // also list boundary particles (density, lambda and correction lists)
 };
 
 // Launch shape of the neighbour-list and gather kernels.  Every shape gives bit-identical results

@@ -253,10 +253,16 @@ class DomainConfiguration:
 
     @staticmethod
     def from_scene(scene) -> "DomainConfiguration":
+        particles = []
+        b = getattr(scene, "boundary", None)
+        if b is not None:
+            particles = [(tuple(b["positions"][:, k].tolist()), tuple(b["velocities"][:, k].tolist()), float(b["volumes"][k]))
+                         for k in range(len(b["volumes"]))]
         return DomainConfiguration(
             particle_count=scene.count, time_step=scene.time_step, support_radius=scene.support_radius,
             particle_radius=scene.particle_radius, gravity=tuple(scene.gravity),
-            boundary=BoxBoundary(tuple(scene.box_min), tuple(scene.box_max), tuple(scene.box_velocity), True))
+            boundary=BoxBoundary(tuple(scene.box_min), tuple(scene.box_max), tuple(scene.box_velocity), True),
+            boundary_particles=particles)
 
 
 @dataclasses.dataclass

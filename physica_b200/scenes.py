@@ -71,6 +71,8 @@ class Scene:
     pressure_iterations: int
     name: str = ""
     targets: np.ndarray | None = None  # (3, N) float32 target cloud for the loss
+    # boundary particles: {"positions": (3, B), "velocities": (3, B), "volumes": (B,)} float32
+    boundary: dict | None = None
 
     @property
     def count(self) -> int:
@@ -218,3 +220,26 @@ def batched_adjoint(seed=5, scenes=32, iterations=4) -> list:
         sc.targets = target_cloud(seed * 7919 + s, c, (0.25 * side, 0.0, 0.25 * side), (0.75 * side, 0.5 * side, 0.75 * side))
         out.append(sc)
     return out
+
+
+def with_boundary(scene: Scene, seed: int, floor_velocity=(0.05, 0.0, 0.0)) -> Scene:
+    """The scene plus boundary particles: a moving floor plate under the fluid column (a 0.5h
+    lattice at y = 0.6 spacing, sliding with `floor_velocity`) and a static wall plate at
+    x = 0.4 in front of it, each particle with volume spacing^3 (jittered by +-1%)."""
+    spacing = 0.5 * scene.support_radius
+    lo = np.asarray(scene.positions.min(axis=1), dtype=np.float64)
+    hi = np.asarray(scene.positions.max(axis=1), dtype=np.float64)
+    xs = np.arange(lo[0] - 2 * spacing, hi[0] + 2 * spacing, spacing)
+    zs = np.arange(lo[2] - 2 * spacing, hi[2] + 2 * spacing, spacing)
+    fx, fz = np.meshgrid(xs, zs, indexing="ij")
+    floor = np.stack([fx.ravel(), np.full(fx.size, 0.6 * spacing), fz.ravel()])
+    ys = np.arange(0.5 * spacing, hi[1] + 2 * spacing, spacing)
+    wy, wz = np.meshgrid(ys, zs, indexing="ij")
+    wall = np.stack([np.full(wy.size, hi[0] + 1.5 * spacing), wy.ravel(), wz.ravel()])
+    positions = np.concatenate([floor, wall], axis=1)
+    velocities = np.zeros_like(positions)
+    velocities[:, :floor.shape[1]] = np.asarray(floor_velocity, dtype=np.float64)[:, None]
+    volumes = spacing ** 3 * (1.0 + 0.02 * (uniform01(seed, positions.shape[1], 17) - 0.5))
+    scene.boundary = {"positions": positions.astype(np.float32), "velocities": velocities.astype(np.float32),
+                      "volumes": volumes.astype(np.float32)}
+    return scene
