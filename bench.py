@@ -220,10 +220,11 @@ def bench_b200(args, world, rank):
 
     if args.launch_shape:   # a fixed shape (e.g. to profile one kernel variant); else the autotuner picks it
         v, b = args.launch_shape.split(":")
-        shape, tuned_ms = pbf.LaunchShape(["per_lane", "cooperative"].index(v), int(b)), float("nan")
+        shape, tuned_ms = pbf.LaunchShape(["per_lane", "cooperative"].index(v), int(b), 128), float("nan")
         solver.launch_shape = shape
     else:
         shape, tuned_ms = solver.autotune(state, control, params, repeats=2)   # outside the timing
+    solver.set_graph_mode(True)   # one CUDA graph launch per substep (captured in the warm-up)
     launches0 = pbf.launch_count()
     clk = Clocks(torch.cuda.current_device())
     ms, wall = timed(step, args.steps, args.warmup, world, stream, flush, clk)
@@ -320,8 +321,9 @@ def bench_b200(args, world, rank):
         "config": {"workload": "dam_break_1m: 1,048,576 particles (128x64x128 lattice, spacing 0.5h, h=0.025), "
                                "box [0,4]^3, 8 Jacobi iterations, dt=1/120, XSPH c=0.01, vorticity eps=1e-4",
                    "particles_per_gpu": n, "pressure_iterations": K, "cells": cells, "replicas": world,
-                   "l2": "flushed between timed steps (256 MiB write)", "wall_s": round(wall, 3),
-                   "launch_shape": {"list_scan": ["per_lane", "cooperative"][shape.list_scan], "block": shape.block_size,
+                   "l2": "flushed between timed steps (256 MiB write)", "wall_s": round(wall, 3), "graphs": True,
+                   "launch_shape": {"list_scan": ["per_lane", "cooperative"][shape.list_scan],
+                                    "scan_block": shape.scan_block_size, "block": shape.block_size,
                                     "autotune_ms_per_step": None if math.isnan(tuned_ms) else round(tuned_ms, 4)}},
         "roofline": roofline, "step_roofline": step_roofline, "per_pass": per_pass,
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(round(per_step_launches * args.steps)),
@@ -421,7 +423,7 @@ def bench_batch(args, world, rank):
             "config": {"workload": "batched_forward_256: 256 dam-break scenes, counts log-uniform in [2048, 65536], "
                                    "4 iterations", "particles_per_gpu": total, "scenes_per_gpu": len(scs),
                        "graphs": True, "launch_shape": {"list_scan": ["per_lane", "cooperative"][shape.list_scan],
-                                                         "block": shape.block_size}}}
+                                                         "scan_block": shape.scan_block_size, "block": shape.block_size}}}
 
 
 def bench_batch_grad(args, world, rank):
@@ -647,8 +649,8 @@ def main():
     ap.add_argument("--no-grad", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--launch-shape", default="", help="fixed list-scan variant and block, e.g. per_lane:128 "
-                                                        "(default: autotuned)")
+    ap.add_argument("--launch-shape", default="", help="fixed list-scan variant and its block size, e.g. "
+                                                        "per_lane:128, gather passes at 128 (default: autotuned)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -151,8 +151,9 @@ typedef struct pbf_solver pbf_solver;          /* PBF (pbf/pbf.ixx:14-141) */
 typedef struct pbf_step_cache pbf_step_cache;  /* PBF::StepCache (pbf/pbf.ixx:54-70) */
 typedef struct pbf_batch pbf_batch;            /* many independent scenes in one launch sequence (no reference counterpart) */
 typedef struct pbf_launch_shape {
-    uint32_t list_scan;    /* 0: per-lane walk, 1: warp-cooperative scan */
-    uint32_t block_size;   /* 32, 64, 96 or 128 */
+    uint32_t list_scan;         /* 0: per-lane walk, 1: warp-cooperative scan */
+    uint32_t scan_block_size;   /* threads per block of the list scan: 32, 64, 96 or 128 */
+    uint32_t block_size;        /* threads per block of the gather passes: 32, 64, 96 or 128 */
 } pbf_launch_shape;
 
 /* Fields of a step cache that pbf_step_cache_read copies out, in ORIGINAL particle order
@@ -313,11 +314,14 @@ int pbf_forward_step_preallocated(const pbf_domain_configuration* domain, const 
 
 /* ---- launch shape of the neighbour-list and gather kernels, and its autotuner.  No reference
  *      counterpart.  Every shape gives bit-identical results; only the speed changes.
- *      list_scan: 0 = each lane walks its own 27 cells, 1 = a warp walks each home cell's
- *      candidates once; block_size: 32, 64, 96 or 128 threads.  pbf_autotune times all eight
- *      shapes on `repeats` forward steps from `state` (writing `scratch_state` and the cache, which
- *      then hold that step), keeps the fastest, returns it in `chosen` (may be NULL) and its time
- *      per step in `milliseconds_per_step` (may be NULL).  It synchronises the stream. ---- */
+ *      list_scan: 0 = each lane walks its own stencil, 1 = a warp walks each home cell's
+ *      candidates once; scan_block_size and block_size: 32, 64, 96 or 128 threads.  pbf_autotune
+ *      times the eight list-scan shapes by their scan time, then the gather block sizes by the
+ *      gather passes' time, on `repeats` forward steps from `state` (writing `scratch_state` and
+ *      the cache, which then hold that step); it keeps the fastest shape, returns it in `chosen`
+ *      (may be NULL) and the substep time with it in `milliseconds_per_step` (may be NULL).  It
+ *      synchronises the stream, resets the per-pass profile totals and uses a temporary 256 MiB
+ *      device buffer to evict the L2 cache before every timed step. ---- */
 int pbf_set_launch_shape(pbf_solver* solver, const pbf_launch_shape* shape);
 int pbf_get_launch_shape(pbf_solver* solver, pbf_launch_shape* shape);
 int pbf_autotune(pbf_solver* solver, const pbf_particle_state* state, const pbf_control* control,

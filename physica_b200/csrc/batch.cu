@@ -98,9 +98,9 @@ int pbf_batch_jvp_step(pbf_batch* batch, const pbf_particle_state* state, const 
 
 int pbf_batch_set_launch_shape(pbf_batch* batch, const pbf_launch_shape* shape) {
     if (!batch || !shape) return PBF_ERROR_INVALID_ARGUMENT;
-    const pbf::LaunchShape s{shape->list_scan, shape->block_size};
+    const pbf::LaunchShape s{shape->list_scan, shape->scan_block_size, shape->block_size};
     if (!pbf::valid_shape(s)) {
-        pbf::set_error("launch shape: list_scan must be 0 or 1 and block_size one of 32, 64, 96, 128");
+        pbf::set_error("launch shape: list_scan must be 0 or 1 and the block sizes one of 32, 64, 96, 128");
         return PBF_ERROR_INVALID_ARGUMENT;
     }
     batch->engine.set_shape(s);
@@ -110,6 +110,7 @@ int pbf_batch_set_launch_shape(pbf_batch* batch, const pbf_launch_shape* shape) 
 int pbf_batch_get_launch_shape(pbf_batch* batch, pbf_launch_shape* shape) {
     if (!batch || !shape) return PBF_ERROR_INVALID_ARGUMENT;
     shape->list_scan = batch->engine.shape().scan;
+    shape->scan_block_size = batch->engine.shape().scan_block;
     shape->block_size = batch->engine.shape().block;
     return PBF_SUCCESS;
 }

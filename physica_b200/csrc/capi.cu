@@ -302,9 +302,9 @@ int pbf_set_graph_mode(pbf_solver* solver, const int enable) {
 int pbf_set_launch_shape(pbf_solver* solver, const pbf_launch_shape* shape) {
     if (!solver) return null_arg("solver");
     if (!shape) return null_arg("shape");
-    const pbf::LaunchShape s{shape->list_scan, shape->block_size};
+    const pbf::LaunchShape s{shape->list_scan, shape->scan_block_size, shape->block_size};
     if (!pbf::valid_shape(s)) {
-        pbf::set_error("launch shape: list_scan must be 0 or 1 and block_size one of 32, 64, 96, 128");
+        pbf::set_error("launch shape: list_scan must be 0 or 1 and the block sizes one of 32, 64, 96, 128");
         return PBF_ERROR_INVALID_ARGUMENT;
     }
     solver->engine.set_shape(s);
@@ -315,6 +315,7 @@ int pbf_get_launch_shape(pbf_solver* solver, pbf_launch_shape* shape) {
     if (!solver) return null_arg("solver");
     if (!shape) return null_arg("shape");
     shape->list_scan = solver->engine.shape().scan;
+    shape->scan_block_size = solver->engine.shape().scan_block;
     shape->block_size = solver->engine.shape().block;
     return PBF_SUCCESS;
 }

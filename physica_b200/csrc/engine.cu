@@ -11,6 +11,8 @@
 #include <cstring>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "engine.h"
 
 namespace pbf {
@@ -62,13 +64,16 @@ cudaEvent_t PassTimer::take() {
     return ev;
 }
 
-void PassTimer::begin(cudaStream_t stream, int) {
+// Every pass is also an NVTX range named after it (a no-op unless a profiler is attached).
+void PassTimer::begin(cudaStream_t stream, const int pass) {
+    nvtxRangePushA(pass_name(pass));
     if (!enabled_) return;
     open_ = take();
     cudaEventRecord(open_, stream);
 }
 
 void PassTimer::end(cudaStream_t stream, const int pass) {
+    nvtxRangePop();
     if (!enabled_ || !open_) return;
     cudaEvent_t stop = take();
     cudaEventRecord(stop, stream);
@@ -108,6 +113,7 @@ int read_profile(Engine& engine, pbf_pass_time* passes, const uint32_t capacity,
 
 int Engine::check(const cudaError_t e, const char* what) {
     if (e == cudaSuccess) return PBF_SUCCESS;
+    cudaGetLastError();   // a non-sticky error becomes this call's status; later calls start clean
     set_error(std::string(what) + ": " + cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? PBF_ERROR_OUT_OF_MEMORY : PBF_ERROR_CUDA;
 }
@@ -571,44 +577,76 @@ int Engine::autotune(const pbf_particle_state* state, const pbf_control* control
     const LaunchShape previous = shape_;
     const bool graphs = graphs_;
     graphs_ = false;
-    LaunchShape best = previous;
-    float best_time = -1.0F;
-    cudaEvent_t start = nullptr, stop = nullptr;
-    int rc = check(cudaEventCreate(&start), "autotune event");
-    if (!rc) rc = check(cudaEventCreate(&stop), "autotune event");
-    const uint32_t scans[2] = {kScanPerLane, kScanCooperative};
-    const uint32_t blocks[4] = {32u, 64u, 96u, 128u};
-    for (int v = 0; v < 2 && !rc; ++v) {
-        for (int b = 0; b < 4 && !rc; ++b) {
-            LaunchShape candidate;
-            candidate.scan = scans[v];
-            candidate.block = blocks[b];
-            shape_ = candidate;
-            pbf_particle_state out = *next_state;
-            if ((rc = forward(state, control, parameters, &out, record))) break;   // warm-up
-            if ((rc = check(cudaEventRecord(start, stream_), "autotune event"))) break;
-            for (uint32_t k = 0; k < reps && !rc; ++k) {
-                out = *next_state;
-                rc = forward(state, control, parameters, &out, record);
+    // A temporary buffer larger than the 126 MB L2, rewritten before every timed step so that each
+    // step starts from cold caches as consecutive substeps of a large scene do.
+    constexpr size_t kFlushBytes = size_t{256} << 20;
+    DeviceArena scratch(stream_);
+    cudaError_t fe = cudaSuccess;
+    unsigned char* flush = scratch.alloc<unsigned char>(kFlushBytes, fe);
+    if (int rc = check(fe, "autotune scratch")) {
+        graphs_ = graphs;
+        return rc;
+    }
+    // Per-pass times of `reps` steps with the current shape (after one warm-up step).
+    auto measure = [&](double* pass_ms) -> int {
+        pbf_particle_state out = *next_state;
+        if (int rc = forward(state, control, parameters, &out, record)) return rc;
+        timer_.enable(true);
+        for (uint32_t k = 0; k < reps; ++k) {
+            if (int rc = check(cudaMemsetAsync(flush, static_cast<int>(k + 1u), kFlushBytes, stream_), "autotune flush")) {
+                timer_.enable(false);
+                return rc;
             }
-            if (rc) break;
-            if ((rc = check(cudaEventRecord(stop, stream_), "autotune event"))) break;
-            if ((rc = check(cudaEventSynchronize(stop), "autotune event"))) break;
-            float ms = 0.0F;
-            if ((rc = check(cudaEventElapsedTime(&ms, start, stop), "autotune event"))) break;
-            ms /= static_cast<float>(reps);
-            if (best_time < 0.0F || ms < best_time) {
-                best_time = ms;
-                best = candidate;
+            out = *next_state;
+            if (int rc = forward(state, control, parameters, &out, record)) {
+                timer_.enable(false);
+                return rc;
             }
         }
+        const int rc = timer_.collect(stream_);
+        for (int p = 0; p < kPassCount; ++p) pass_ms[p] = timer_.milliseconds(p) / reps;
+        timer_.enable(false);
+        return rc;
+    };
+    const uint32_t scans[2] = {kScanPerLane, kScanCooperative};
+    const uint32_t blocks[4] = {32u, 64u, 96u, 128u};
+    double ms[kPassCount];
+    int rc = PBF_SUCCESS;
+    // 1. the list scan: variant x block size, by the scan's own time
+    LaunchShape best = previous;
+    best.block = 128u;
+    double best_scan = -1.0;
+    for (int v = 0; v < 2 && !rc; ++v)
+        for (int b = 0; b < 4 && !rc; ++b) {
+            shape_ = best;
+            shape_.scan = scans[v];
+            shape_.scan_block = blocks[b];
+            if ((rc = measure(ms))) break;
+            if (best_scan < 0.0 || ms[kPassListScan] < best_scan) {
+                best_scan = ms[kPassListScan];
+                best.scan = scans[v];
+                best.scan_block = blocks[b];
+            }
+        }
+    // 2. the gather passes' block size, by their summed time
+    double best_gather = -1.0, best_total = 0.0;
+    for (int b = 0; b < 4 && !rc; ++b) {
+        shape_ = best;
+        shape_.block = blocks[b];
+        if ((rc = measure(ms))) break;
+        double gather = 0.0, total = 0.0;
+        for (int p = 0; p < kPassCount; ++p) total += ms[p];
+        for (const int p : {kPassDensityLambda, kPassCorrection, kPassVorticity, kPassNormal, kPassXsph}) gather += ms[p];
+        if (best_gather < 0.0 || gather < best_gather) {
+            best_gather = gather;
+            best_total = total;
+            best.block = blocks[b];
+        }
     }
-    if (start) cudaEventDestroy(start);
-    if (stop) cudaEventDestroy(stop);
     graphs_ = graphs;
     shape_ = rc ? previous : best;
     drop_graphs();
-    if (!rc && best_ms) *best_ms = best_time;
+    if (!rc && best_ms) *best_ms = static_cast<float>(best_total);
     if (!rc) next_state->step_index = state->step_index + 1u;
     return rc;
 }

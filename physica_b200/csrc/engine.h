@@ -32,6 +32,7 @@ public:
         const size_t bytes = count ? count * sizeof(T) : sizeof(T);
         err = cudaMallocAsync(&p, bytes, stream_);
         if (err == cudaSuccess) ptrs_.push_back(p);
+        else cudaGetLastError();   // the status is reported by the caller; clear the runtime's last error
         return static_cast<T*>(p);
     }
     void release() {

@@ -79,24 +79,39 @@ __global__ void __launch_bounds__(kBlock) list_walk_kernel(const ListScanArgs a)
         a.list.counts[s] = n <= cap ? n : kOverflow;
         return;
     }
-    // nine stencil columns, x-offset outer; each column's three cells are one contiguous range
-    for (int dx = -1; dx <= 1; ++dx) {
-        const int x = c.x + dx;
-        if (x < 0 || x >= cx) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int y = c.y + dy;
-            if (y < 0 || y >= cy) continue;
-            const uint32_t end = offsets[cell_index(grid, x, y, z_hi) + 1u];
-#pragma unroll 4
-            for (uint32_t t = offsets[cell_index(grid, x, y, z_lo)]; t < end; ++t) {
-                const float4 q = pos[t];
-                const float r2 = squared(mk(__fsub_rn(xi.x, q.x), __fsub_rn(xi.y, q.y), __fsub_rn(xi.z, q.z)));
-                if (r2 < thr) {
-                    if (n < cap) entries[static_cast<size_t>(n) * 32u] = t;
-                    ++n;
-                }
-            }
+    // Nine stencil columns, x-offset outer; each column's three cells are one contiguous range.
+    // All eighteen range bounds are loaded up front, and candidates are loaded four at a time
+    // before they are tested, so several independent loads are in flight per lane.
+    uint32_t first[9], last[9];
+#pragma unroll
+    for (int o = 0; o < 9; ++o) {
+        const int x = c.x + o / 3 - 1, y = c.y + o % 3 - 1;
+        first[o] = 0u;
+        last[o] = 0u;
+        if (x >= 0 && x < cx && y >= 0 && y < cy) {
+            first[o] = offsets[cell_index(grid, x, y, z_lo)];
+            last[o] = offsets[cell_index(grid, x, y, z_hi) + 1u];
         }
+    }
+    auto test = [&](const float4 q, const uint32_t t) {
+        const float r2 = squared(mk(__fsub_rn(xi.x, q.x), __fsub_rn(xi.y, q.y), __fsub_rn(xi.z, q.z)));
+        if (r2 < thr) {
+            if (n < cap) entries[static_cast<size_t>(n) * 32u] = t;
+            ++n;
+        }
+    };
+#pragma unroll
+    for (int o = 0; o < 9; ++o) {
+        uint32_t t = first[o];
+        const uint32_t end = last[o];
+        for (; t + 4u <= end; t += 4u) {
+            const float4 q0 = pos[t], q1 = pos[t + 1u], q2 = pos[t + 2u], q3 = pos[t + 3u];
+            test(q0, t);
+            test(q1, t + 1u);
+            test(q2, t + 2u);
+            test(q3, t + 3u);
+        }
+        for (; t < end; ++t) test(pos[t], t);
     }
     a.list.counts[s] = n <= cap ? n : kOverflow;
 }
@@ -199,8 +214,11 @@ struct MassRatio {
     }
 };
 
+// WithBoundary: the scene has boundary particles (their entries carry kBoundaryBit); the plain
+// instantiation, launched otherwise, carries no boundary test.
+template <bool WithBoundary>
 struct DensityLambdaOp {
-    static constexpr bool kBoundary = true;
+    static constexpr bool kBoundary = WithBoundary;
     const float4* __restrict__ pos;
     const float4* __restrict__ boundary;
     f3 x;
@@ -214,12 +232,13 @@ struct DensityLambdaOp {
     MassRatio ratio;
 
     __device__ __forceinline__ float4 prefetch(const uint32_t t) const {
-        return (t & kBoundaryBit) ? boundary[t & ~kBoundaryBit] : pos[t];
+        if constexpr (WithBoundary) return (t & kBoundaryBit) ? boundary[t & ~kBoundaryBit] : pos[t];
+        return pos[t];
     }
     __device__ __forceinline__ void apply(const uint32_t t, const float4 q) {
         const f3 d = sub(x, xyz(q));
         const float r2 = squared(d);
-        if (t & kBoundaryBit) {
+        if (WithBoundary && (t & kBoundaryBit)) {
             // boundary particle b: density += rho0_i V_b W (density/density.cu:34-37),
             // S += V_b grad W (pbf/pbf.cu:118-121); no denominator term
             if (r2 < k.h2) density = __fmaf_rn(__fmul_rn(rest_density, q.w), poly6_inside(r2, k), density);
@@ -241,10 +260,11 @@ struct DensityLambdaOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
+template <bool WithBoundary>
 __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLambdaArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
-    DensityLambdaOp op;
+    DensityLambdaOp<WithBoundary> op;
     op.pos = a.pos;
     op.boundary = a.g.boundary;
     op.self = p.s;
@@ -274,8 +294,9 @@ struct PositionLambda {
     float lambda;
 };
 
+template <bool WithBoundary>
 struct CorrectionOp {
-    static constexpr bool kBoundary = true;
+    static constexpr bool kBoundary = WithBoundary;
     const float4* __restrict__ pos;
     const float4* __restrict__ boundary;
     const float* __restrict__ lambda;
@@ -290,7 +311,7 @@ struct CorrectionOp {
     MassRatio ratio;
 
     __device__ __forceinline__ PositionLambda prefetch(const uint32_t t) const {
-        if (t & kBoundaryBit) return {boundary[t & ~kBoundaryBit], 0.0F};
+        if (WithBoundary && (t & kBoundaryBit)) return {boundary[t & ~kBoundaryBit], 0.0F};
         return {pos[t], lambda[t]};
     }
     __device__ __forceinline__ void apply(const uint32_t t, const PositionLambda in) {
@@ -308,7 +329,7 @@ struct CorrectionOp {
         } else {
             artificial = r2 < k.h2 ? -strength : 0.0F;
         }
-        if (t & kBoundaryBit) {
+        if (WithBoundary && (t & kBoundaryBit)) {
             // boundary particle b: V_b (lambda_i + s_corr) grad W (pbf/pbf.cu:278-285)
             const float factor = __fmul_rn(in.q.w, __fadd_rn(lambda_i, artificial));
             correction = fma3(factor, spiky_gradient_at(d, distance, k), correction);
@@ -321,10 +342,11 @@ struct CorrectionOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
+template <bool WithBoundary>
 __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
-    CorrectionOp op;
+    CorrectionOp<WithBoundary> op;
     op.pos = a.pos;
     op.boundary = a.g.boundary;
     op.lambda = a.lambda;
@@ -588,8 +610,8 @@ cudaError_t launch_constants(cudaStream_t stream, const float* radii, const uint
 }
 
 bool valid_shape(const LaunchShape& shape) {
-    return (shape.scan == kScanPerLane || shape.scan == kScanCooperative) && shape.block >= 32u &&
-           shape.block <= static_cast<uint32_t>(kBlock) && shape.block % 32u == 0u;
+    auto ok = [](const uint32_t b) { return b >= 32u && b <= static_cast<uint32_t>(kBlock) && b % 32u == 0u; };
+    return (shape.scan == kScanPerLane || shape.scan == kScanCooperative) && ok(shape.scan_block) && ok(shape.block);
 }
 
 namespace {
@@ -600,7 +622,7 @@ unsigned block_of(const unsigned block) {
 
 cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a, const LaunchShape& shape) {
     if (a.g.count == 0) return cudaSuccess;
-    const unsigned block = block_of(shape.block);
+    const unsigned block = block_of(shape.scan_block);
     // the cooperative scan lists fluid particles only; lists with boundary particles use the walk
     if (shape.scan == kScanCooperative && !(a.boundary && a.g.boundary_offsets))
         list_scan_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
@@ -613,7 +635,10 @@ cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a, const L
 cudaError_t launch_density_lambda(cudaStream_t stream, const DensityLambdaArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
     const unsigned block = block_of(block_size);
-    density_lambda_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    if (a.g.boundary)
+        density_lambda_kernel<true><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    else
+        density_lambda_kernel<false><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }
@@ -621,7 +646,10 @@ cudaError_t launch_density_lambda(cudaStream_t stream, const DensityLambdaArgs& 
 cudaError_t launch_correction(cudaStream_t stream, const CorrectionArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
     const unsigned block = block_of(block_size);
-    correction_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    if (a.g.boundary)
+        correction_kernel<true><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    else
+        correction_kernel<false><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }

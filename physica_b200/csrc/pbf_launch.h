@@ -149,7 +149,8 @@ enum ListScanVariant : uint32_t {
 };
 struct LaunchShape {
     uint32_t scan = kScanPerLane;
-    uint32_t block = 128;   // threads per block of the list and gather kernels: 32, 64, 96 or 128
+    uint32_t scan_block = 128;   // threads per block of the list scan: 32, 64, 96 or 128
+    uint32_t block = 128;        // threads per block of the gather passes: 32, 64, 96 or 128
 };
 bool valid_shape(const LaunchShape& shape);
 

@@ -79,22 +79,24 @@ class ParametersC(ctypes.Structure):
 
 
 class LaunchShapeC(ctypes.Structure):
-    _fields_ = [("list_scan", ctypes.c_uint32), ("block_size", ctypes.c_uint32)]
+    _fields_ = [("list_scan", ctypes.c_uint32), ("scan_block_size", ctypes.c_uint32), ("block_size", ctypes.c_uint32)]
 
 
 @dataclasses.dataclass
 class LaunchShape:
     """Launch shape of the neighbour-list and gather kernels (results are identical for every shape).
-    list_scan: 0 = per-lane walk, 1 = warp-cooperative scan; block_size: 32, 64, 96 or 128."""
+    list_scan: 0 = per-lane walk, 1 = warp-cooperative scan; scan_block_size (list scan) and
+    block_size (gather passes): 32, 64, 96 or 128."""
     list_scan: int = 0
+    scan_block_size: int = 128
     block_size: int = 128
 
     def to_c(self) -> "LaunchShapeC":
-        return LaunchShapeC(self.list_scan, self.block_size)
+        return LaunchShapeC(self.list_scan, self.scan_block_size, self.block_size)
 
     @staticmethod
     def from_c(c: "LaunchShapeC") -> "LaunchShape":
-        return LaunchShape(int(c.list_scan), int(c.block_size))
+        return LaunchShape(int(c.list_scan), int(c.scan_block_size), int(c.block_size))
 
 
 class HostStateC(ctypes.Structure):

@@ -9,7 +9,7 @@ from physica_b200 import pbf, scenes
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [pbf.LaunchShape(v, b) for v, b in itertools.product((0, 1), (32, 64, 96, 128))]
+SHAPES = [pbf.LaunchShape(v, b, g) for v, b, g in itertools.product((0, 1), (32, 64, 96, 128), (32, 64, 96, 128))]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -33,18 +33,19 @@ def test_every_shape_gives_identical_substeps():
     sc = scenes.dam_break((14, 14, 14), (0, 0, 0), (1, 2, 1), 31, 3, velocity_sigma=0.1)
     solver, state, control, params = pbf.solver_for_scene(sc)
     results = []
-    for shape in SHAPES:
+    for shape in SHAPES[::3]:
         solver.launch_shape = shape
         assert solver.launch_shape == shape
         results.append(_run(solver, state, control, params, 5))
-    for shape, (x, v) in zip(SHAPES[1:], results[1:]):
+    for shape, (x, v) in zip(SHAPES[::3][1:], results[1:]):
         assert torch.equal(x, results[0][0]), shape
         assert torch.equal(v, results[0][1]), shape
 
 
 def test_invalid_shapes_are_rejected():
     solver, _, _, _ = pbf.solver_for_scene(scenes.dam_break((4, 4, 4), (0, 0, 0), (1, 2, 1), 32, 2))
-    for bad in (pbf.LaunchShape(2, 128), pbf.LaunchShape(0, 48), pbf.LaunchShape(0, 256), pbf.LaunchShape(1, 0)):
+    for bad in (pbf.LaunchShape(2, 128, 128), pbf.LaunchShape(0, 48, 128), pbf.LaunchShape(0, 128, 256),
+                pbf.LaunchShape(1, 0, 64)):
         with pytest.raises(pbf.PBFError):
             solver.launch_shape = bad
 
@@ -64,7 +65,7 @@ def test_batch_autotune_and_shapes_give_identical_substeps():
     scs = [scenes.batched_scene(c, 200 + k, 3) for k, c in enumerate((1500, 4000, 257))]
     batch, state, control, params = pbf.batch_for_scenes(scs)
     out = []
-    for shape in (pbf.LaunchShape(0, 128), pbf.LaunchShape(1, 64)):
+    for shape in (pbf.LaunchShape(0, 128, 128), pbf.LaunchShape(1, 64, 96)):
         batch.launch_shape = shape
         cur = pbf.State(state.positions.clone(), state.velocities.clone(), 0)
         nxt = batch.allocate_state()
