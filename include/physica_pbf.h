@@ -333,6 +333,20 @@ int pbf_batch_autotune(pbf_batch* batch, const pbf_particle_state* state, const 
                        const pbf_parameters* parameters, pbf_particle_state* scratch_state, uint32_t cache_slot,
                        uint32_t repeats, pbf_launch_shape* chosen, float* milliseconds_per_step);
 
+/* ---- optional input checks.  No reference counterpart (its launchers check nothing,
+ *      pbf/kernels.h:12-46).  While enabled, every forward step also tests its inputs on the
+ *      device and ORs one bit per kind of invalid input into a device word; reading it
+ *      synchronises the stream, returns the bits accumulated since the last read and clears them.
+ *      The step itself still runs (the reference's kernels run on whatever they are given). ---- */
+#define PBF_INPUT_NONFINITE_POSITION 1u
+#define PBF_INPUT_NONFINITE_VELOCITY 2u
+#define PBF_INPUT_NONFINITE_CONTROL 4u
+#define PBF_INPUT_BAD_MASS 8u   /* a mass that is not finite and positive */
+int pbf_set_input_checks(pbf_solver* solver, int enable);
+int pbf_read_input_checks(pbf_solver* solver, uint32_t* flags);
+int pbf_batch_set_input_checks(pbf_batch* batch, int enable);
+int pbf_batch_read_input_checks(pbf_batch* batch, uint32_t* flags);
+
 /* ---- misc ---- */
 int pbf_synchronize(pbf_solver* solver);
 int pbf_batch_synchronize(pbf_batch* batch);

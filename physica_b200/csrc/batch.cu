@@ -96,6 +96,17 @@ int pbf_batch_jvp_step(pbf_batch* batch, const pbf_particle_state* state, const 
                                  next_state_tangent);
 }
 
+int pbf_batch_set_input_checks(pbf_batch* batch, const int enable) {
+    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
+    batch->engine.set_input_checks(enable != 0);
+    return PBF_SUCCESS;
+}
+
+int pbf_batch_read_input_checks(pbf_batch* batch, uint32_t* flags) {
+    if (!batch || !flags) return PBF_ERROR_INVALID_ARGUMENT;
+    return batch->engine.read_input_checks(flags);
+}
+
 int pbf_batch_set_launch_shape(pbf_batch* batch, const pbf_launch_shape* shape) {
     if (!batch || !shape) return PBF_ERROR_INVALID_ARGUMENT;
     const pbf::LaunchShape s{shape->list_scan, shape->scan_block_size, shape->block_size};

@@ -337,6 +337,18 @@ int pbf_autotune(pbf_solver* solver, const pbf_particle_state* state, const pbf_
     return chosen ? pbf_get_launch_shape(solver, chosen) : PBF_SUCCESS;
 }
 
+int pbf_set_input_checks(pbf_solver* solver, const int enable) {
+    if (!solver) return null_arg("solver");
+    solver->engine.set_input_checks(enable != 0);
+    return PBF_SUCCESS;
+}
+
+int pbf_read_input_checks(pbf_solver* solver, uint32_t* flags) {
+    if (!solver) return null_arg("solver");
+    if (!flags) return null_arg("flags");
+    return guarded([&] { return solver->engine.read_input_checks(flags); });
+}
+
 int pbf_profile_enable(pbf_solver* solver, const int enable) {
     if (!solver) return null_arg("solver");
     solver->engine.timer().enable(enable != 0);

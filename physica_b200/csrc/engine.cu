@@ -293,11 +293,13 @@ int Engine::init(const pbf_domain_configuration* scenes, const uint32_t scene_co
     }
     d_static_ = arena_.alloc<SceneStatic>(scene_count, e);
     d_step_ = arena_.alloc<unsigned long long>(1, e);
+    d_input_flags_ = arena_.alloc<uint32_t>(1, e);
     if (int rc = check(e, "device allocation")) return rc;
     e = cudaMemcpyAsync(d_scenes_, scene_table_.data(), scene_count * sizeof(SceneDesc), cudaMemcpyHostToDevice, stream_);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_static_, statics.data(), scene_count * sizeof(SceneStatic), cudaMemcpyHostToDevice, stream_);
     if (int rc = check(e, "upload scene table")) return rc;
+    if (int rc = check(cudaMemsetAsync(d_input_flags_, 0, sizeof(uint32_t), stream_), "input flags")) return rc;
     host_step_ = ~0ull;
     if (int rc = check(cudaStreamCreateWithFlags(&capture_stream_, cudaStreamNonBlocking), "capture stream")) return rc;
     return check(cudaStreamSynchronize(stream_), "engine initialisation");
@@ -472,6 +474,16 @@ int Engine::forward(const pbf_particle_state* state, const pbf_control* control,
     return PBF_SUCCESS;
 }
 
+int Engine::read_input_checks(uint32_t* flags) {
+    uint32_t value = 0;
+    cudaError_t e = cudaMemcpyAsync(&value, d_input_flags_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_input_flags_, 0, sizeof(uint32_t), stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (int rc = check(e, "read input checks")) return rc;
+    *flags = value;
+    return PBF_SUCCESS;
+}
+
 GatherCommon Engine::gather_common(const StepRecord& r) const {
     GatherCommon gc{count_, d_scenes_, d_constants_, r.cell_offsets, r.cell, r.params_a, r.params_b};
     if (boundary_count_ > 0) {
@@ -511,6 +523,7 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
     g.topology = r.topology;
     g.params_a = r.params_a;
     g.params_b = r.params_b;
+    g.input_flags = input_checks_ ? d_input_flags_ : nullptr;
     timer_.begin(stream, kPassGrid);
     if (int rc = check(launch_grid_build(stream, g), "grid build")) return rc;
     if (boundary_count_ > 0) {

@@ -181,6 +181,12 @@ public:
         drop_graphs();
     }
     const LaunchShape& shape() const { return shape_; }
+    // Optional device-side input checks (PBF_INPUT_* bits accumulated until read).
+    void set_input_checks(bool on) {
+        input_checks_ = on;
+        drop_graphs();
+    }
+    int read_input_checks(uint32_t* flags);
     // Times every candidate shape on `repeats` forward steps from `state` (writing `next_state` and
     // the record) and keeps the fastest; returns its per-step milliseconds in `best_ms`.
     int autotune(const pbf_particle_state* state, const pbf_control* control, const pbf_parameters* parameters,
@@ -237,6 +243,8 @@ private:
     pbf_execution_mode mode_ = PBF_EXECUTION_FORWARD;
     cudaStream_t stream_ = nullptr;
     LaunchShape shape_{};
+    bool input_checks_ = false;
+    uint32_t* d_input_flags_ = nullptr;
     std::vector<SceneHost> scenes_;
     std::vector<SceneDesc> scene_table_;
     DeviceArena arena_;

@@ -11,6 +11,7 @@
 // Keys are global across the scenes of a batch (scene cell ranges are disjoint and
 // ordered), so one sort serves one scene or many.
 #include "pbf_internal.h"
+#include "../../include/physica_pbf.h"
 #include "pbf_launch.h"
 
 namespace pbf {
@@ -27,13 +28,22 @@ __global__ void predict_key_kernel(const uint32_t count, const SceneDesc* __rest
                                    const Field3 velocities, const Field3 controls,
                                    const float* __restrict__ masses, float4* __restrict__ predicted,
                                    uint32_t* __restrict__ keys, uint32_t* __restrict__ arrival,
-                                   uint32_t* __restrict__ histogram) {
+                                   uint32_t* __restrict__ histogram, uint32_t* __restrict__ input_flags) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const SceneDesc& sc = scenes[scene_of ? scene_of[i] : 0u];
     const f3 gravity = mk(sc.gravity_x, sc.gravity_y, sc.gravity_z);
     const f3 v = mk(velocities.x[i], velocities.y[i], velocities.z[i]);
     const f3 a = mk(controls.x[i], controls.y[i], controls.z[i]);
+    if (input_flags) {   // optional input checks: one bit per kind of invalid input
+        const float px = positions.x[i], py = positions.y[i], pz = positions.z[i], m = masses[i];
+        uint32_t bad = 0u;
+        if (!isfinite(px) || !isfinite(py) || !isfinite(pz)) bad |= PBF_INPUT_NONFINITE_POSITION;
+        if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z)) bad |= PBF_INPUT_NONFINITE_VELOCITY;
+        if (!isfinite(a.x) || !isfinite(a.y) || !isfinite(a.z)) bad |= PBF_INPUT_NONFINITE_CONTROL;
+        if (!(isfinite(m) && m > 0.0F)) bad |= PBF_INPUT_BAD_MASS;
+        if (bad) atomicOr(input_flags, bad);
+    }
     const f3 x = mk(positions.x[i], positions.y[i], positions.z[i]);
     const float dt = sc.time_step;
     const f3 predicted_velocity = fma3(dt, add(gravity, a), v);
@@ -304,7 +314,8 @@ cudaError_t launch_grid_build(cudaStream_t stream, const GridBuildArgs& a) {
     if (a.count > 0) {
         predict_key_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.scenes, a.scene_of, a.positions,
                                                                          a.velocities, a.controls, a.params.masses,
-                                                                         a.predicted, a.keys, a.arrival, a.cell_offsets);
+                                                                         a.predicted, a.keys, a.arrival, a.cell_offsets,
+                                                                         a.input_flags);
         count_launch();
     }
     const uint64_t n = a.cells + 1;

@@ -30,6 +30,7 @@ struct GridBuildArgs {
     float4* topology;
     float4* params_a;
     float4* params_b;
+    uint32_t* input_flags = nullptr;   // optional input checks (PBF_INPUT_* bits), null when off
 };
 
 size_t scan_tile_count(uint64_t n);

@@ -103,6 +103,12 @@ class HostStateC(ctypes.Structure):
     _fields_ = [("positions", ctypes.c_void_p * 3), ("velocities", ctypes.c_void_p * 3), ("step_index", ctypes.c_uint64)]
 
 
+INPUT_NONFINITE_POSITION = 1
+INPUT_NONFINITE_VELOCITY = 2
+INPUT_NONFINITE_CONTROL = 4
+INPUT_BAD_MASS = 8
+
+
 class CacheField(enum.IntEnum):
     SORTED_PARTICLE_INDICES = 0
     CELL_OFFSETS = 1
@@ -190,6 +196,10 @@ def library() -> ctypes.CDLL:
         lib.pbf_get_launch_shape.argtypes = [vp, P(LaunchShapeC)]
         lib.pbf_autotune.argtypes = [vp, P(ParticleStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
                                      ctypes.c_uint32, P(LaunchShapeC), P(ctypes.c_float)]
+        lib.pbf_set_input_checks.argtypes = [vp, ctypes.c_int]
+        lib.pbf_read_input_checks.argtypes = [vp, P(ctypes.c_uint32)]
+        lib.pbf_batch_set_input_checks.argtypes = [vp, ctypes.c_int]
+        lib.pbf_batch_read_input_checks.argtypes = [vp, P(ctypes.c_uint32)]
         lib.pbf_batch_set_launch_shape.argtypes = [vp, P(LaunchShapeC)]
         lib.pbf_batch_get_launch_shape.argtypes = [vp, P(LaunchShapeC)]
         lib.pbf_batch_autotune.argtypes = [vp, P(ParticleStateC), P(ControlC), P(ParametersC), P(ParticleStateC),
@@ -538,6 +548,16 @@ class PBF:
         """Replay the forward launch sequence as a CUDA graph per buffer set."""
         check(library().pbf_set_graph_mode(self.handle, 1 if enable else 0))
 
+    def set_input_checks(self, enable: bool = True):
+        """Test every forward step's inputs on the device (see read_input_checks)."""
+        check(library().pbf_set_input_checks(self.handle, 1 if enable else 0))
+
+    def read_input_checks(self) -> int:
+        """PBF_INPUT_* bits seen since the last read (synchronises), then cleared."""
+        v = ctypes.c_uint32()
+        check(library().pbf_read_input_checks(self.handle, ctypes.byref(v)))
+        return int(v.value)
+
     @property
     def launch_shape(self) -> LaunchShape:
         c = LaunchShapeC()
@@ -655,6 +675,14 @@ class Batch:
 
     def set_graph_mode(self, enable: bool = True):
         check(library().pbf_batch_set_graph_mode(self.handle, 1 if enable else 0))
+
+    def set_input_checks(self, enable: bool = True):
+        check(library().pbf_batch_set_input_checks(self.handle, 1 if enable else 0))
+
+    def read_input_checks(self) -> int:
+        v = ctypes.c_uint32()
+        check(library().pbf_batch_read_input_checks(self.handle, ctypes.byref(v)))
+        return int(v.value)
 
     @property
     def launch_shape(self) -> LaunchShape:

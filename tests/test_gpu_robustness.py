@@ -112,3 +112,27 @@ def test_vjp_with_a_cache_of_another_step_is_rejected():
         # `cache` holds the step of `state`, not of `nxt`
         solver.vjp_step(nxt, control, params, later, cache, na, solver.allocate_state_adjoint(),
                         solver.allocate_control_adjoint(), solver.allocate_parameter_adjoint())
+
+
+def test_input_checks_flag_invalid_inputs():
+    sc = scenes.dam_break((6, 6, 6), (0, 0, 0), (1, 2, 1), 86, 2)
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    nxt = solver.allocate_state()
+    solver.set_input_checks(True)
+    solver.forward_step(state, control, params, nxt, cache)
+    assert solver.read_input_checks() == 0
+    bad = pbf.State(state.positions.clone(), state.velocities.clone(), 0)
+    bad.velocities[1, 7] = float("nan")
+    bad.positions[0, 3] = float("inf")
+    solver.forward_step(bad, control, params, nxt, cache)
+    flags = solver.read_input_checks()
+    assert flags == pbf.INPUT_NONFINITE_VELOCITY | pbf.INPUT_NONFINITE_POSITION
+    assert solver.read_input_checks() == 0          # cleared by the read
+    params.tensors["masses"][5] = -1.0
+    control.external_accelerations[2, 0] = float("nan")
+    solver.forward_step(state, control, params, nxt, cache)
+    assert solver.read_input_checks() == pbf.INPUT_BAD_MASS | pbf.INPUT_NONFINITE_CONTROL
+    solver.set_input_checks(False)
+    solver.forward_step(bad, control, params, nxt, cache)
+    assert solver.read_input_checks() == 0          # nothing is tested while disabled
