@@ -220,7 +220,7 @@ def bench_b200(args, world, rank):
 
     if args.launch_shape:   # a fixed shape (e.g. to profile one kernel variant); else the autotuner picks it
         v, b = args.launch_shape.split(":")
-        shape, tuned_ms = pbf.LaunchShape(["per_lane", "cooperative"].index(v), int(b), 128), float("nan")
+        shape, tuned_ms = pbf.LaunchShape(["per_lane", "cooperative", "staged"].index(v), int(b), 128), float("nan")
         solver.launch_shape = shape
     else:
         shape, tuned_ms = solver.autotune(state, control, params, repeats=2)   # outside the timing
@@ -322,7 +322,7 @@ def bench_b200(args, world, rank):
                                "box [0,4]^3, 8 Jacobi iterations, dt=1/120, XSPH c=0.01, vorticity eps=1e-4",
                    "particles_per_gpu": n, "pressure_iterations": K, "cells": cells, "replicas": world,
                    "l2": "flushed between timed steps (256 MiB write)", "wall_s": round(wall, 3), "graphs": True,
-                   "launch_shape": {"list_scan": ["per_lane", "cooperative"][shape.list_scan],
+                   "launch_shape": {"list_scan": ["per_lane", "cooperative", "staged"][shape.list_scan],
                                     "scan_block": shape.scan_block_size, "block": shape.block_size,
                                     "autotune_ms_per_step": None if math.isnan(tuned_ms) else round(tuned_ms, 4)}},
         "roofline": roofline, "step_roofline": step_roofline, "per_pass": per_pass,
@@ -422,7 +422,7 @@ def bench_batch(args, world, rank):
             "batched_ms_per_step": round(ms_b, 4), "per_scene_ms_per_step": round(ms_l, 4),
             "config": {"workload": "batched_forward_256: 256 dam-break scenes, counts log-uniform in [2048, 65536], "
                                    "4 iterations", "particles_per_gpu": total, "scenes_per_gpu": len(scs),
-                       "graphs": True, "launch_shape": {"list_scan": ["per_lane", "cooperative"][shape.list_scan],
+                       "graphs": True, "launch_shape": {"list_scan": ["per_lane", "cooperative", "staged"][shape.list_scan],
                                                          "scan_block": shape.scan_block_size, "block": shape.block_size}}}
 
 

@@ -621,7 +621,7 @@ int Engine::autotune(const pbf_particle_state* state, const pbf_control* control
         timer_.enable(false);
         return rc;
     };
-    const uint32_t scans[2] = {kScanPerLane, kScanCooperative};
+    const uint32_t scans[3] = {kScanPerLane, kScanCooperative, kScanStaged};
     const uint32_t blocks[4] = {32u, 64u, 96u, 128u};
     double ms[kPassCount];
     int rc = PBF_SUCCESS;
@@ -629,7 +629,7 @@ int Engine::autotune(const pbf_particle_state* state, const pbf_control* control
     LaunchShape best = previous;
     best.block = 128u;
     double best_scan = -1.0;
-    for (int v = 0; v < 2 && !rc; ++v)
+    for (int v = 0; v < 3 && !rc; ++v)
         for (int b = 0; b < 4 && !rc; ++b) {
             shape_ = best;
             shape_.scan = scans[v];

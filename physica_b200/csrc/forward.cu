@@ -14,6 +14,8 @@
 // accumulated in the reference's order and equals it bit for bit (skipped candidates contribute
 // an exact zero in the reference).  Separating the cheap candidate tests from the costly per-pair
 // math (sqrt, divisions) keeps that math convergent across the warp.
+#include <climits>
+
 #include "gather.cuh"
 
 namespace pbf {
@@ -114,6 +116,103 @@ __global__ void __launch_bounds__(kBlock) list_walk_kernel(const ListScanArgs a)
         for (; t < end; ++t) test(pos[t], t);
     }
     a.list.counts[s] = n <= cap ? n : kOverflow;
+}
+
+// Staged list scan: the lanes of a warp that share a stencil column (same x, y and scene) stage
+// the union of their nine column ranges (cells z_min-1 .. z_max+1 of the group) in shared memory
+// with coalesced loads, then each lane tests its own nine ranges there.  A group whose union
+// exceeds the stage walks global memory instead.  Same lists as the other scans.
+constexpr uint32_t kStageCapacity = 704;   // float4 per warp (44 KB per 128-thread block)
+
+__global__ void __launch_bounds__(kBlock) list_staged_kernel(const ListScanArgs a) {
+    __shared__ float4 stage[kWarpsPerBlock][kStageCapacity];
+    __shared__ uint32_t column_first[kWarpsPerBlock][9];
+    __shared__ uint32_t column_base[kWarpsPerBlock][9];
+    const uint32_t w = threadIdx.x >> 5, lane = lane_id();
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = s < a.g.count;
+    const int4 c = active ? a.g.cell[s] : make_int4(0, 0, 0, 0);
+    const float4 xi = active ? a.pos[s] : make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+    const uint32_t cap = a.list.capacity;
+    uint32_t* __restrict__ entries = a.list.entries + list_row(s, cap);
+    const uint32_t* __restrict__ offsets = a.g.cell_offsets;
+    const float4* __restrict__ pos = a.pos;
+    uint32_t n = 0;
+    uint32_t pending = __ballot_sync(kFull, active);
+    while (pending) {
+        const int leader = __ffs(static_cast<int>(pending)) - 1;
+        const int gx = __shfl_sync(kFull, c.x, leader), gy = __shfl_sync(kFull, c.y, leader);
+        const int gw = __shfl_sync(kFull, c.w, leader);
+        const bool mine = ((pending >> lane) & 1u) != 0u && c.x == gx && c.y == gy && c.w == gw;
+        pending &= ~__ballot_sync(kFull, mine);
+        const SceneDesc* scene = a.g.scenes + gw;
+        const Grid grid = scene->grid;
+        const float thr = a.g.constants[scene->constants].list_threshold;
+        const int cx = static_cast<int>(grid.cells_x), cy = static_cast<int>(grid.cells_y), cz = static_cast<int>(grid.cells_z);
+        const int zmin = __reduce_min_sync(kFull, mine ? c.z : INT_MAX);
+        const int zmax = __reduce_max_sync(kFull, mine ? c.z : INT_MIN);
+        const uint32_t zlo = static_cast<uint32_t>(zmin > 0 ? zmin - 1 : 0);
+        const uint32_t zhi = static_cast<uint32_t>(zmax + 1 < cz ? zmax + 1 : cz - 1);
+        // lane o < 9: the group's union range of stencil column o
+        uint32_t first = 0u, length = 0u;
+        if (lane < 9u) {
+            const int x = gx + static_cast<int>(lane) / 3 - 1, y = gy + static_cast<int>(lane) % 3 - 1;
+            if (x >= 0 && x < cx && y >= 0 && y < cy) {
+                first = offsets[cell_index(grid, x, y, zlo)];
+                length = offsets[cell_index(grid, x, y, zhi) + 1u] - first;
+            }
+        }
+        uint32_t inclusive = length;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, inclusive, o);
+            if (lane >= static_cast<uint32_t>(o)) inclusive += v;
+        }
+        const uint32_t total = __shfl_sync(kFull, inclusive, 8);
+        if (lane < 9u) {
+            column_first[w][lane] = first;
+            column_base[w][lane] = inclusive - length;
+        }
+        __syncwarp();
+        const bool staged = total <= kStageCapacity;
+        if (staged) {
+            for (uint32_t u = lane; u < total; u += 32u) {
+                uint32_t o = 0;   // the column holding staged slot u: last o with base <= u
+#pragma unroll
+                for (uint32_t step = 8; step > 0; step >>= 1)
+                    if (o + step <= 8u && column_base[w][o + step] <= u) o += step;
+                stage[w][u] = pos[column_first[w][o] + (u - column_base[w][o])];
+            }
+        }
+        __syncwarp();
+        if (mine) {
+            const uint32_t z_lo = static_cast<uint32_t>(c.z > 0 ? c.z - 1 : 0);
+            const uint32_t z_hi = static_cast<uint32_t>(c.z + 1 < cz ? c.z + 1 : cz - 1);
+            auto test = [&](const float4 q, const uint32_t t) {
+                const float r2 = squared(mk(__fsub_rn(xi.x, q.x), __fsub_rn(xi.y, q.y), __fsub_rn(xi.z, q.z)));
+                if (r2 < thr) {
+                    if (n < cap) entries[static_cast<size_t>(n) * 32u] = t;
+                    ++n;
+                }
+            };
+#pragma unroll
+            for (int o = 0; o < 9; ++o) {
+                const int x = c.x + o / 3 - 1, y = c.y + o % 3 - 1;
+                if (x < 0 || x >= cx || y < 0 || y >= cy) continue;
+                const uint32_t lo = offsets[cell_index(grid, x, y, z_lo)];
+                const uint32_t hi = offsets[cell_index(grid, x, y, z_hi) + 1u];
+                if (staged) {
+                    // slot t of this column sits at stage index t - first + base
+                    const uint32_t shift = column_base[w][o] - column_first[w][o];
+                    for (uint32_t t = lo; t < hi; ++t) test(stage[w][t + shift], t);
+                } else {
+                    for (uint32_t t = lo; t < hi; ++t) test(pos[t], t);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (active) a.list.counts[s] = n <= cap ? n : kOverflow;
 }
 
 __global__ void __launch_bounds__(kBlock) list_scan_kernel(const ListScanArgs a) {
@@ -611,7 +710,8 @@ cudaError_t launch_constants(cudaStream_t stream, const float* radii, const uint
 
 bool valid_shape(const LaunchShape& shape) {
     auto ok = [](const uint32_t b) { return b >= 32u && b <= static_cast<uint32_t>(kBlock) && b % 32u == 0u; };
-    return (shape.scan == kScanPerLane || shape.scan == kScanCooperative) && ok(shape.scan_block) && ok(shape.block);
+    return (shape.scan == kScanPerLane || shape.scan == kScanCooperative || shape.scan == kScanStaged) &&
+           ok(shape.scan_block) && ok(shape.block);
 }
 
 namespace {
@@ -623,9 +723,13 @@ unsigned block_of(const unsigned block) {
 cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a, const LaunchShape& shape) {
     if (a.g.count == 0) return cudaSuccess;
     const unsigned block = block_of(shape.scan_block);
-    // the cooperative scan lists fluid particles only; lists with boundary particles use the walk
-    if (shape.scan == kScanCooperative && !(a.boundary && a.g.boundary_offsets))
+    // the cooperative and staged scans list fluid particles only; lists with boundary particles
+    // use the per-lane walk
+    const bool fluid_only = !(a.boundary && a.g.boundary_offsets);
+    if (shape.scan == kScanCooperative && fluid_only)
         list_scan_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    else if (shape.scan == kScanStaged && fluid_only)
+        list_staged_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     else
         list_walk_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();

@@ -147,6 +147,7 @@ struct ListScanArgs {
 enum ListScanVariant : uint32_t {
     kScanPerLane = 0,       // every lane walks its own 27 cells (run-mates share each load)
     kScanCooperative = 1,   // a warp walks each home-cell run's candidates once, 32 at a time
+    kScanStaged = 2,        // a warp stages its column group's candidates in shared memory
 };
 struct LaunchShape {
     uint32_t scan = kScanPerLane;

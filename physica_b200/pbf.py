@@ -85,7 +85,8 @@ class LaunchShapeC(ctypes.Structure):
 @dataclasses.dataclass
 class LaunchShape:
     """Launch shape of the neighbour-list and gather kernels (results are identical for every shape).
-    list_scan: 0 = per-lane walk, 1 = warp-cooperative scan; scan_block_size (list scan) and
+    list_scan: 0 = per-lane walk, 1 = warp-cooperative scan, 2 = shared-memory staged walk;
+    scan_block_size (list scan) and
     block_size (gather passes): 32, 64, 96 or 128."""
     list_scan: int = 0
     scan_block_size: int = 128

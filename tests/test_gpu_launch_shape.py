@@ -9,7 +9,7 @@ from physica_b200 import pbf, scenes
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [pbf.LaunchShape(v, b, g) for v, b, g in itertools.product((0, 1), (32, 64, 96, 128), (32, 64, 96, 128))]
+SHAPES = [pbf.LaunchShape(v, b, g) for v, b, g in itertools.product((0, 1, 2), (32, 64, 96, 128), (32, 64, 96, 128))]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -44,7 +44,7 @@ def test_every_shape_gives_identical_substeps():
 
 def test_invalid_shapes_are_rejected():
     solver, _, _, _ = pbf.solver_for_scene(scenes.dam_break((4, 4, 4), (0, 0, 0), (1, 2, 1), 32, 2))
-    for bad in (pbf.LaunchShape(2, 128, 128), pbf.LaunchShape(0, 48, 128), pbf.LaunchShape(0, 128, 256),
+    for bad in (pbf.LaunchShape(3, 128, 128), pbf.LaunchShape(0, 48, 128), pbf.LaunchShape(0, 128, 256),
                 pbf.LaunchShape(1, 0, 64)):
         with pytest.raises(pbf.PBFError):
             solver.launch_shape = bad
@@ -65,7 +65,7 @@ def test_batch_autotune_and_shapes_give_identical_substeps():
     scs = [scenes.batched_scene(c, 200 + k, 3) for k, c in enumerate((1500, 4000, 257))]
     batch, state, control, params = pbf.batch_for_scenes(scs)
     out = []
-    for shape in (pbf.LaunchShape(0, 128, 128), pbf.LaunchShape(1, 64, 96)):
+    for shape in (pbf.LaunchShape(0, 128, 128), pbf.LaunchShape(1, 64, 96), pbf.LaunchShape(2, 128, 64)):
         batch.launch_shape = shape
         cur = pbf.State(state.positions.clone(), state.velocities.clone(), 0)
         nxt = batch.allocate_state()
@@ -74,6 +74,7 @@ def test_batch_autotune_and_shapes_give_identical_substeps():
             cur, nxt = nxt, cur
         torch.cuda.synchronize()
         out.append((cur.positions.clone(), cur.velocities.clone()))
-    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+    for other in out[1:]:
+        assert torch.equal(out[0][0], other[0]) and torch.equal(out[0][1], other[1])
     shape, ms = batch.autotune(state, control, params, repeats=1)
     assert shape in SHAPES and ms > 0.0
