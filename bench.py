@@ -365,6 +365,7 @@ def bench_grad(args, world, rank):
     solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
     targets = torch.from_numpy(sc.targets).cuda()
     steps = 20
+    shape, _ = solver.autotune(state, control, params, repeats=2)
     solver.set_graph_mode(True)
     rollout = trajectory.Rollout(solver, control, params, steps, 10)   # buffers allocated once, outside the timing
     trajectory.loss_and_gradients(solver, state, control, params, targets, steps, rollout=rollout)   # warm-up
@@ -380,7 +381,10 @@ def bench_grad(args, world, rank):
     return {"value": round(world * steps / (ms * 1e-3), 3), "unit": "grad-steps/s",
             "config": {"workload": "differentiable_64k: 65,536 particles (32x64x32 lattice), v0 ~ N(0, 0.1), "
                                    "4 iterations, target-cloud loss", "rollout_steps": steps,
-                       "trajectory_checkpoint_every": 10}, "loss": g.loss}
+                       "trajectory_checkpoint_every": 10, "graphs": True,
+                       "launch_shape": {"list_scan": ["per_lane", "cooperative", "staged"][shape.list_scan],
+                                        "scan_block": shape.scan_block_size, "block": shape.block_size}},
+            "loss": g.loss}
 
 
 def bench_batch(args, world, rank):
@@ -449,6 +453,7 @@ def bench_batch_grad(args, world, rank):
         return a.elapsed_time(b)
 
     batch, state, control, params = pbf.batch_for_scenes(scs, mode=diff)
+    batch.autotune(state, control, params, repeats=1)
     batch.set_graph_mode(True)
     targets = torch.from_numpy(np.concatenate([s.targets for s in scs], axis=1)).cuda()
     barrier(world)
@@ -459,6 +464,7 @@ def bench_batch_grad(args, world, rank):
     ms_l = 0.0
     for sc in scs:   # one scene at a time (its buffers allocated outside its timing)
         solver, st, ctl, prm = pbf.solver_for_scene(sc, mode=diff)
+        solver.autotune(st, ctl, prm, repeats=1)
         solver.set_graph_mode(True)
         ms_l += timed_rollout(solver, st, ctl, prm, torch.from_numpy(sc.targets).cuda())
         del solver, st, ctl, prm

@@ -348,6 +348,19 @@ int pbf_read_input_checks(pbf_solver* solver, uint32_t* flags);
 int pbf_batch_set_input_checks(pbf_batch* batch, int enable);
 int pbf_batch_read_input_checks(pbf_batch* batch, uint32_t* flags);
 
+/* ---- headless frame export.  Replaces the dam-break example's Spectra provider
+ *      (examples/fluids/liquid/pbf-dam-break/spectra/provider.ixx:74-96, spectra/kernels.cu:8-13),
+ *      which copies every frame's positions and velocities as xyz triples and the step cache's
+ *      vorticity magnitudes into viewer buffers: here the buffers are the caller's device memory
+ *      (a file dump or any consumer can read them).  `cache` is the step that produced `state`
+ *      (it supplies the vorticity magnitudes); `vorticity` may be NULL. ---- */
+typedef struct {
+    float* positions;    /* 3N floats: x, y, z of particle 0, then particle 1, ... */
+    float* velocities;   /* 3N floats, same layout */
+    float* vorticity;    /* N floats, |omega| in original particle order, or NULL */
+} pbf_frame;
+int pbf_export_frame(pbf_solver* solver, const pbf_particle_state* state, const pbf_step_cache* cache, pbf_frame* frame);
+
 /* ---- misc ---- */
 int pbf_synchronize(pbf_solver* solver);
 int pbf_batch_synchronize(pbf_batch* batch);

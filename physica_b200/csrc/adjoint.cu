@@ -30,6 +30,7 @@ struct AdjointWorkspace {
     double4* eta = nullptr;               // adjoint of the unnormalised vorticity-magnitude gradient
     double* lambda = nullptr;
     double* density = nullptr;
+    float2* s_corr = nullptr;             // (W(s_corr radius), 1 when the strength is zero and the power stays finite)
 };
 
 void destroy_adjoint_workspace(void* workspace) { delete static_cast<AdjointWorkspace*>(workspace); }
@@ -100,13 +101,27 @@ __device__ __forceinline__ void finish(const Tail& t, const uint32_t s, const ui
 }
 
 // ----------------------------------------------------------------- seed
-__global__ void seed_kernel(const uint32_t count, const uint32_t* __restrict__ sorted_index, const ConstAdjField3 next_x,
-                            const ConstAdjField3 next_v, double4* __restrict__ x, double4* __restrict__ out_v) {
+__global__ void seed_kernel(const GatherCommon g, const uint32_t* __restrict__ sorted_index, const ConstAdjField3 next_x,
+                            const ConstAdjField3 next_v, double4* __restrict__ x, double4* __restrict__ out_v,
+                            float2* __restrict__ s_corr) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= count) return;
+    if (s >= g.count) return;
     const uint32_t i = sorted_index[s];
     x[s] = make_double4(next_x.x[i], next_x.y[i], next_x.z[i], 0.0);
     out_v[s] = make_double4(next_v.x[i], next_v.y[i], next_v.z[i], 0.0);
+    // s_corr of this particle: the reference weight W(radius) and whether its strength is zero
+    // with every power (W/W(radius))^exponent finite.  Then s_corr = -strength * power is a zero
+    // whose sign is that of -strength, and its gradient and its exponent and radius derivatives
+    // vanish; only the strength derivative -power remains (pbf/pbf.cu:56-71).
+    const KernelConstants k = g.constants[g.scenes[g.cell[s].w].constants];
+    const float4 pb = g.params_b[s];
+    const float reference = poly6(mk(pb.z, 0.0F, 0.0F), k);
+    bool zero_strength = pb.x == 0.0F && pb.y >= 0.0F && reference > 0.0F;
+    if (zero_strength) {
+        const float largest = powf(__fdiv_rn(poly6_inside(0.0F, k), reference), pb.y);
+        zero_strength = largest < 1e30F;
+    }
+    s_corr[s] = make_float2(reference, zero_strength ? 1.0F : 0.0F);
 }
 
 // ------------------------------------------------------- XSPH + confinement
@@ -332,12 +347,34 @@ __global__ void __launch_bounds__(kBlock) vorticity_vjp_kernel(const VorticityVj
     finish(a.tail, p.s, i, xb, p.scene->time_step);
 }
 
+// s_corr of a pair whose particle has zero strength (its s_corr table entry is 1): the value is a
+// zero with the sign of -strength (or +0 outside the poly6 support, as the reference's early
+// return), and only the strength derivative -power is non-zero; `weight` is W(d) = W(-d).
+__device__ __forceinline__ ArtificialPressure zero_strength_pressure(const float weight, const float reference,
+                                                                     const float strength, const float exponent,
+                                                                     const bool with_derivative) {
+    ArtificialPressure a;
+    a.d_exponent = a.d_radius = 0.0F;
+    a.gradient = {0.0F, 0.0F, 0.0F};
+    a.value = a.d_strength = 0.0F;
+    if (weight == 0.0F) return a;
+    if (with_derivative) {
+        const float power = powf(__fdiv_rn(weight, reference), exponent);
+        a.value = __fmul_rn(-strength, power);
+        a.d_strength = -power;
+    } else {
+        a.value = -strength;   // -strength * power for a finite power >= 0
+    }
+    return a;
+}
+
 // ------------------------------------------------------------ correction
 struct CorrectionVjpArgs {
     GatherCommon g;
     StoredList list;
     const uint32_t* sorted_index;
     const float4* pos;
+    const float2* s_corr;
     const float* lambda;
     const double4* correction;
     double4* x;
@@ -349,6 +386,9 @@ struct CorrectionVjpOp {
     static constexpr bool kBoundary = true;
     const float4* __restrict__ pos;
     const float4* __restrict__ boundary;
+    const float2* __restrict__ s_corr;
+    float reference_i;
+    bool zero_strength_i;
     const float* __restrict__ lambda;
     const double4* __restrict__ correction;
     const float4* __restrict__ params_a;
@@ -374,29 +414,34 @@ struct CorrectionVjpOp {
         const float r2 = squared(d);
         if (r2 == 0.0F || r2 >= k.adjoint_threshold) return;
         const f3 gradient = spiky_gradient(d, k);
-        const ArtificialPressure ap = artificial_pressure(d, k, strength, exponent, radius);
+        const f3 rg = scale(gradient, -1.0F);   // spiky_gradient(-d), exactly
+        const float weight = r2 >= k.h2 ? 0.0F : poly6_inside(r2, k);   // W(d) = W(-d)
+        const ArtificialPressure ap = zero_strength_i ? zero_strength_pressure(weight, reference_i, strength, exponent, true)
+                                                      : artificial_pressure(d, k, strength, exponent, radius);
+        const float4 pb = params_b[t];
+        const float2 sj = s_corr[t];
+        const ArtificialPressure rap = sj.y != 0.0F ? zero_strength_pressure(weight, sj.x, pb.x, pb.y, false)
+                                                    : artificial_pressure(scale(d, -1.0F), k, pb.x, pb.y, pb.z);
         const float coefficient = q.w / rest_density;
         const float lambda_j = lambda[t];
         const float multiplier = lambda_i + lambda_j + ap.value;
         const double scalar_adjoint = coefficient * dot(ob, gradient);
-        pc = pc + spiky_hessian_product(d, times(ob, coefficient * multiplier), k);
+        const float rrest = params_a[t].x;
+        const float rcoefficient = mass / rrest;
+        const float rmultiplier = lambda_j + lambda_i + rap.value;
+        const d3 rob = ld3(correction[t]);
+        const double rscalar = rcoefficient * dot(rob, rg);
+        d3 hessian, reverse_hessian;   // H(d) applied to both sides' adjoints; H(-d) = H(d)
+        spiky_hessian_products(d, times(ob, coefficient * multiplier), times(rob, rcoefficient * rmultiplier), k, hessian,
+                               reverse_hessian);
+        pc = pc + hessian;
         pc = pc + times(ap.gradient, scalar_adjoint);
         lc += scalar_adjoint;
         rc -= dot(ob, times(gradient, coefficient * multiplier)) / rest_density;
         sc += scalar_adjoint * ap.d_strength;
         ec += scalar_adjoint * ap.d_exponent;
         qc += scalar_adjoint * ap.d_radius;
-
-        const f3 rd = scale(d, -1.0F);
-        const f3 rg = spiky_gradient(rd, k);
-        const float4 pb = params_b[t];
-        const ArtificialPressure rap = artificial_pressure(rd, k, pb.x, pb.y, pb.z);
-        const float rrest = params_a[t].x;
-        const float rcoefficient = mass / rrest;
-        const float rmultiplier = lambda_j + lambda_i + rap.value;
-        const d3 rob = ld3(correction[t]);
-        const double rscalar = rcoefficient * dot(rob, rg);
-        pc = pc + times(spiky_hessian_product(rd, times(rob, rcoefficient * rmultiplier), k), -1.0);
+        pc = pc + times(reverse_hessian, -1.0);
         pc = pc + times(rap.gradient, -rscalar);
         lc += rscalar;
         mc += dot(rob, times(rg, rmultiplier / rrest));
@@ -420,11 +465,16 @@ struct CorrectionVjpOp {
     }
 };
 
-__global__ void __launch_bounds__(kBlock) correction_vjp_kernel(const CorrectionVjpArgs a) {
+// Four resident blocks per SM (at most 128 registers) hide more latency than the unbounded 144.
+__global__ void __launch_bounds__(kBlock, 4) correction_vjp_kernel(const CorrectionVjpArgs a) {
     const Particle p = locate(a.g);
     CorrectionVjpOp op;
     op.pos = a.pos;
     op.boundary = a.g.boundary;
+    op.s_corr = a.s_corr;
+    const float2 si = p.active ? a.s_corr[p.s] : make_float2(1.0F, 0.0F);
+    op.reference_i = si.x;
+    op.zero_strength_i = si.y != 0.0F;
     op.lambda = a.lambda;
     op.correction = a.correction;
     op.params_a = a.g.params_a;
@@ -510,21 +560,21 @@ struct LambdaVjpOp {
         const f3 neighbor_gradient = times(gradient, -coefficient);
         const d3 neighbor_gradient_adjoint = times(neighbor_gradient, 2.0 * db);
         const d3 gradient_adjoint = times(sb - neighbor_gradient_adjoint, coefficient);
-        pc = pc + spiky_hessian_product(d, gradient_adjoint, k);
         self_gradient = fma3(coefficient, gradient, self_gradient);
-
         const float rrest = params_a[t].x;
         const float4 gj = gsum[t];
         const double rconstraint = static_cast<double>(density[t]) / rrest - 1.0;
         const double rdb = lambda_adjoint[t] * rconstraint / (static_cast<double>(gj.w) * gj.w);
         const d3 rsb = times(xyz(gj), 2.0 * rdb);
-        const f3 rd = scale(d, -1.0F);
-        const f3 rg = spiky_gradient(rd, k);
+        const f3 rg = scale(gradient, -1.0F);   // spiky_gradient(-d), exactly
         const float rcoefficient = mass / rrest;
         const f3 rneighbor_gradient = times(rg, -rcoefficient);
         const d3 rneighbor_gradient_adjoint = times(rneighbor_gradient, 2.0 * rdb);
         const d3 rgradient_adjoint = times(rsb - rneighbor_gradient_adjoint, rcoefficient);
-        pc = pc + times(spiky_hessian_product(rd, rgradient_adjoint, k), -1.0);
+        d3 hessian, reverse_hessian;   // H(d) applied to both sides' adjoints; H(-d) = H(d)
+        spiky_hessian_products(d, gradient_adjoint, rgradient_adjoint, k, hessian, reverse_hessian);
+        pc = pc + hessian;
+        pc = pc + times(reverse_hessian, -1.0);
         mc += dot(rsb - rneighbor_gradient_adjoint, rg) / rrest;
     }
 };
@@ -791,6 +841,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
         ws->eta = ws->arena.alloc<double4>(n, e);
         ws->lambda = ws->arena.alloc<double>(n, e);
         ws->density = ws->arena.alloc<double>(n, e);
+        ws->s_corr = ws->arena.alloc<float2>(n, e);
         if (e != cudaSuccess) {
             delete ws;
             return check(e, "adjoint workspace");
@@ -815,8 +866,9 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
 
     timer_.begin(stream_, kPassSeed);
     seed_kernel<<<grid_of(n, 256), 256, 0, stream_>>>(
-        n, r.sorted_index, {next_adjoint->positions.x, next_adjoint->positions.y, next_adjoint->positions.z},
-        {next_adjoint->velocities.x, next_adjoint->velocities.y, next_adjoint->velocities.z}, ws->x[0], ws->output_velocity);
+        gc, r.sorted_index, {next_adjoint->positions.x, next_adjoint->positions.y, next_adjoint->positions.z},
+        {next_adjoint->velocities.x, next_adjoint->velocities.y, next_adjoint->velocities.z}, ws->x[0], ws->output_velocity,
+        ws->s_corr);
     timer_.end(stream_, kPassSeed);
     XsphVjpArgs xa{gc, post_list, r.sorted_index, xK, r.confined, r.vorticity, r.normal, ws->output_velocity, ws->x[0], ws->velocity,
                    ws->vorticity, ws->eta, pa};
@@ -838,7 +890,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
         double4* other = ws->x[(K - k + 1) & 1u];
         const float4* xk = r.iterate(k, K, true);
         const StoredList it_list{r.list_entries[k], r.list_counts[k], r.list_capacity};
-        CorrectionVjpArgs ca{gc, it_list, r.sorted_index, xk, r.lambda[k], ws->correction, acc, ws->lambda, pa};
+        CorrectionVjpArgs ca{gc, it_list, r.sorted_index, xk, ws->s_corr, r.lambda[k], ws->correction, acc, ws->lambda, pa};
         timer_.begin(stream_, kPassCorrectionVjp);
         correction_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(ca);
         timer_.end(stream_, kPassCorrectionVjp);

@@ -337,6 +337,30 @@ int pbf_autotune(pbf_solver* solver, const pbf_particle_state* state, const pbf_
     return chosen ? pbf_get_launch_shape(solver, chosen) : PBF_SUCCESS;
 }
 
+int pbf_export_frame(pbf_solver* solver, const pbf_particle_state* state, const pbf_step_cache* cache, pbf_frame* frame) {
+    if (!solver) return null_arg("solver");
+    if (!state || !frame || !frame->positions || !frame->velocities) return null_arg("state/frame");
+    if (frame->vorticity) {
+        if (!cache) return null_arg("cache (needed for the vorticity magnitudes)");
+        if (cache->solver != solver) {
+            pbf::set_error("step cache belongs to another solver");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        if (!cache->record.valid || cache->record.step_index + 1u != state->step_index) {
+            pbf::set_error("the step cache does not hold the step that produced this state");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+    }
+    const pbf::Field3 x{state->positions.x, state->positions.y, state->positions.z};
+    const pbf::Field3 v{state->velocities.x, state->velocities.y, state->velocities.z};
+    if (solver->engine.count() > 0 && (!x.x || !x.y || !x.z || !v.x || !v.y || !v.z)) return null_arg("state field");
+    const pbf::StepRecord* r = frame->vorticity ? &cache->record : nullptr;
+    return solver->engine.check(pbf::launch_export_frame(solver->engine.stream(), solver->engine.count(), x, v,
+                                                         r ? r->slot_of : nullptr, r ? r->vorticity : nullptr,
+                                                         frame->positions, frame->velocities, frame->vorticity),
+                                "export frame");
+}
+
 int pbf_set_input_checks(pbf_solver* solver, const int enable) {
     if (!solver) return null_arg("solver");
     solver->engine.set_input_checks(enable != 0);

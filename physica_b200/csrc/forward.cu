@@ -700,7 +700,34 @@ __global__ void reconstruct_kernel(const uint32_t count, const SceneDesc* __rest
 
 inline unsigned grid_of(const uint32_t n, const unsigned block) { return (n + block - 1) / block; }
 
+// Headless frame export (the example's Spectra write_vectors kernel and vorticity copy): xyz
+// triples of the state and the step's vorticity magnitudes in original particle order.
+__global__ void export_frame_kernel(const uint32_t count, const Field3 positions, const Field3 velocities,
+                                    const uint32_t* __restrict__ slot_of, const float4* __restrict__ vorticity,
+                                    float* __restrict__ out_positions, float* __restrict__ out_velocities,
+                                    float* __restrict__ out_vorticity) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    out_positions[3u * i] = positions.x[i];
+    out_positions[3u * i + 1u] = positions.y[i];
+    out_positions[3u * i + 2u] = positions.z[i];
+    out_velocities[3u * i] = velocities.x[i];
+    out_velocities[3u * i + 1u] = velocities.y[i];
+    out_velocities[3u * i + 2u] = velocities.z[i];
+    if (out_vorticity) out_vorticity[i] = vorticity[slot_of[i]].w;
+}
+
 }  // namespace
+
+cudaError_t launch_export_frame(cudaStream_t stream, const uint32_t count, const Field3 positions, const Field3 velocities,
+                                const uint32_t* slot_of, const float4* vorticity, float* out_positions, float* out_velocities,
+                                float* out_vorticity) {
+    if (count == 0) return cudaSuccess;
+    export_frame_kernel<<<grid_of(count, 256), 256, 0, stream>>>(count, positions, velocities, slot_of, vorticity, out_positions,
+                                                                  out_velocities, out_vorticity);
+    count_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t launch_constants(cudaStream_t stream, const float* radii, const uint32_t n, KernelConstants* out) {
     constants_kernel<<<grid_of(n, 64), 64, 0, stream>>>(radii, n, out);

@@ -182,6 +182,8 @@ cudaError_t launch_segment_sums(cudaStream_t stream, const double* values, const
                                 uint32_t segments, uint32_t single_count, double* out);
 
 // Inspection helpers: scatter sorted arrays back to original order.
+cudaError_t launch_export_frame(cudaStream_t stream, uint32_t count, Field3 positions, Field3 velocities, const uint32_t* slot_of,
+                                const float4* vorticity, float* out_positions, float* out_velocities, float* out_vorticity);
 cudaError_t launch_unsort_float4(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const float4* in,
                                  int components, float* out_x, float* out_y, float* out_z, float* out_w);
 cudaError_t launch_unsort_mask(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const uint8_t* in,

@@ -156,6 +156,30 @@ __device__ __forceinline__ d3 spiky_hessian_product(const f3 d, const d3 v, cons
 }
 
 // d/dr of poly6 along a radius (pbf/pbf.cu:18-24).
+// H(d) v1 and H(d) v2 (as spiky_hessian_product) sharing one distance, inverse and direction.
+// The spiky Hessian is even, H(-d) = H(d), and every step of the product is sign-symmetric, so
+// H(-d) v equals H(d) v exactly: the reverse term of a pair uses the forward term's setup.
+__device__ __forceinline__ void spiky_hessian_products(const f3 d, const d3 v1, const d3 v2, const KernelConstants& k, d3& out1,
+                                                       d3& out2) {
+    const double r2 = static_cast<double>(squared(d));
+    const double distance = sqrt(r2);
+    if (distance == 0.0 || distance >= k.h) {
+        out1 = out2 = {0.0, 0.0, 0.0};
+        return;
+    }
+    const double inverse = 1.0 / distance;
+    const d3 direction = times(d, inverse);
+    const double difference = k.h - distance;
+    auto product = [&](const d3 v) {
+        const double projection = dot(direction, v);
+        const d3 direction_tangent = times(v - times(direction, projection), inverse);
+        return times(times(direction, -2.0 * difference * projection) + times(direction_tangent, difference * difference),
+                     k.spiky_coefficient_d);
+    };
+    out1 = product(v1);
+    out2 = product(v2);
+}
+
 __device__ __forceinline__ float poly6_radial_derivative(const float radius, const KernelConstants& k) {
     if (radius >= k.h) return 0.0F;
     const float difference = __fmaf_rn(-radius, radius, __fmul_rn(k.h, k.h));

@@ -110,6 +110,10 @@ INPUT_NONFINITE_CONTROL = 4
 INPUT_BAD_MASS = 8
 
 
+class FrameC(ctypes.Structure):
+    _fields_ = [("positions", ctypes.c_void_p), ("velocities", ctypes.c_void_p), ("vorticity", ctypes.c_void_p)]
+
+
 class CacheField(enum.IntEnum):
     SORTED_PARTICLE_INDICES = 0
     CELL_OFFSETS = 1
@@ -197,6 +201,7 @@ def library() -> ctypes.CDLL:
         lib.pbf_get_launch_shape.argtypes = [vp, P(LaunchShapeC)]
         lib.pbf_autotune.argtypes = [vp, P(ParticleStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
                                      ctypes.c_uint32, P(LaunchShapeC), P(ctypes.c_float)]
+        lib.pbf_export_frame.argtypes = [vp, P(ParticleStateC), vp, P(FrameC)]
         lib.pbf_set_input_checks.argtypes = [vp, ctypes.c_int]
         lib.pbf_read_input_checks.argtypes = [vp, P(ctypes.c_uint32)]
         lib.pbf_batch_set_input_checks.argtypes = [vp, ctypes.c_int]
@@ -548,6 +553,21 @@ class PBF:
     def set_graph_mode(self, enable: bool = True):
         """Replay the forward launch sequence as a CUDA graph per buffer set."""
         check(library().pbf_set_graph_mode(self.handle, 1 if enable else 0))
+
+    def export_frame(self, state: State, cache: "StepCache | None" = None) -> dict:
+        """Frame of `state` for a viewer or a file dump: positions and velocities as (N, 3) float32,
+        and, with the step cache that produced `state`, the vorticity magnitudes (N,)."""
+        n = self.count
+        out = {"positions": torch.empty((n, 3), dtype=torch.float32, device=self.device),
+               "velocities": torch.empty((n, 3), dtype=torch.float32, device=self.device)}
+        if cache is not None:
+            out["vorticity"] = torch.empty(n, dtype=torch.float32, device=self.device)
+        f = FrameC(out["positions"].data_ptr() if n else None, out["velocities"].data_ptr() if n else None,
+                   out["vorticity"].data_ptr() if cache is not None and n else None)
+        check(library().pbf_export_frame(self.handle, ctypes.byref(state.c()), cache.handle if cache is not None else None,
+                                         ctypes.byref(f)))
+        out["step"] = state.step_index
+        return out
 
     def set_input_checks(self, enable: bool = True):
         """Test every forward step's inputs on the device (see read_input_checks)."""
