@@ -243,3 +243,41 @@ def with_boundary(scene: Scene, seed: int, floor_velocity=(0.05, 0.0, 0.0)) -> S
     scene.boundary = {"positions": positions.astype(np.float32), "velocities": velocities.astype(np.float32),
                       "volumes": volumes.astype(np.float32)}
     return scene
+
+
+def example_dam_break() -> Scene:
+    """The reference's own dam-break example (examples/fluids/liquid/pbf-dam-break/simulation.ixx):
+    a 16 x 28 x 12 lattice at spacing 0.025 starting at 0.08 (x fastest, then y, then z), h = 0.05,
+    dt = 1/240, particle radius 0.01, gravity -9.81, box [0,0.8] x [0,1.1] x [0,0.5], 5 Jacobi
+    iterations, relaxation 1000, s_corr strength 0 / exponent 4 / radius 0.3h, no XSPH and no
+    vorticity confinement, zero velocities and controls.  No jitter: the example has none."""
+    f32 = np.float32
+    nx, ny, nz = 16, 28, 12
+    spacing, h = f32(0.025), f32(0.050)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    pos = np.stack([f32(0.08) + i.ravel().astype(f32) * spacing, f32(0.08) + j.ravel().astype(f32) * spacing,
+                    f32(0.08) + k.ravel().astype(f32) * spacing]).astype(np.float32)
+    n = pos.shape[1]
+    full = lambda value: np.full(n, value, dtype=np.float32)
+    return Scene(
+        positions=pos,
+        velocities=np.zeros((3, n), dtype=np.float32),
+        controls=np.zeros((3, n), dtype=np.float32),
+        masses=full(f32(1000.0) * spacing * spacing * spacing),
+        rest_densities=full(1000.0),
+        relaxation=full(1000.0),
+        artificial_pressure_strength=full(0.0),
+        artificial_pressure_exponent=full(4.0),
+        artificial_pressure_radius=full(f32(0.3) * h),
+        xsph_viscosity=full(0.0),
+        vorticity_confinement=full(0.0),
+        time_step=float(f32(1.0) / f32(240.0)),
+        support_radius=float(h),
+        particle_radius=float(f32(0.010)),
+        gravity=(0.0, float(f32(-9.81)), 0.0),
+        box_min=(0.0, 0.0, 0.0),
+        box_max=(float(f32(0.8)), float(f32(1.1)), float(f32(0.5))),
+        box_velocity=(0.0, 0.0, 0.0),
+        pressure_iterations=5,
+        name="example_dam_break",
+    )
