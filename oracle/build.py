@@ -1,11 +1,12 @@
 """Build recipe for the oracle -- TEST INFRASTRUCTURE ONLY.
 
 * oracle/lib/libpbf_oracle.so : the FP64 host restatement (gcc + OpenMP).
-* oracle/_ref/libpbf_ref.so   : the reference's own CUDA PBF kernels, compiled from
+* oracle/_ref/libpbf_ref.so   : the reference's own CUDA PBF and SPH kernels, compiled from
   the reference sources (pbf/pbf.cu, density/density.cu, neighborhood/neighborhood.cu,
-  domain/domain.cu of fluids/liquid/particle) with nvcc for sm_100a, plus
-  oracle/ref_harness.cu, which replays PBF::forward_step / PBF::vjp_step
-  (pbf/pbf.cpp:167-258) over the reference's own launch_* functions.  The
+  domain/domain.cu, sph/{common,wcsph,pcisph,iisph,dfsph}.cu of fluids/liquid/particle) with
+  nvcc for sm_100a, plus oracle/ref_harness.cu, which replays PBF::forward_step /
+  PBF::vjp_step (pbf/pbf.cpp:167-258) and SPH<Method>::forward_step (sph/sph.ixx:337-341)
+  over the reference's own launch_* functions.  The
   reference's C++23 module host layer (import std) cannot be compiled by this
   toolchain, so the harness stands in for it.  Built only where the reference
   tree exists; the .so then travels with the repository copy.
@@ -21,7 +22,8 @@ import sys
 HERE = pathlib.Path(__file__).resolve().parent
 REFERENCE = pathlib.Path(os.environ.get("PHYSICA_REFERENCE", "/root/reference"))
 PARTICLE = REFERENCE / "fluids" / "liquid" / "particle"
-REF_SOURCES = ["pbf/pbf.cu", "density/density.cu", "neighborhood/neighborhood.cu", "domain/domain.cu"]
+REF_SOURCES = ["pbf/pbf.cu", "density/density.cu", "neighborhood/neighborhood.cu", "domain/domain.cu",
+               "sph/common.cu", "sph/wcsph.cu", "sph/pcisph.cu", "sph/iisph.cu", "sph/dfsph.cu"]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 

@@ -1,4 +1,4 @@
-// Replay harness of the reference PBF -- TEST INFRASTRUCTURE ONLY.
+// Replay harness of the reference PBF and SPH -- TEST INFRASTRUCTURE ONLY.
 //
 // Linked with the reference's own kernel translation units (pbf/pbf.cu, density/density.cu,
 // neighborhood/neighborhood.cu, domain/domain.cu of fluids/liquid/particle, compiled from the
@@ -8,6 +8,9 @@
 // call for call over the reference's launch_* functions, with plain cudaMalloc buffers in place
 // of cuda::device_buffer.  It exists to produce golden outputs of the reference on a GPU and to
 // time the reference as the baseline arm of bench.py; the product never links it.
+// The SPH section at the end replays SPH<Method>::forward_step (sph/sph.ixx:350-354) and the four
+// methods' forward() (sph/sph.cpp:214-225, 296-312, 409-425, 572-610) over the reference's
+// sph/*.cu launchers in the same way.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -21,6 +24,11 @@
 #include "neighborhood/device.cuh"
 #include "neighborhood/kernels.h"
 #include "pbf/kernels.h"
+#include "sph/dfsph.h"
+#include "sph/iisph.h"
+#include "sph/kernels.h"
+#include "sph/pcisph.h"
+#include "sph/wcsph.h"
 
 namespace cd = physica::fluids::liquid::particle::cuda_detail;
 
@@ -596,5 +604,280 @@ int ref_synchronize(void* handle) {
 
 // Stream of the harness (to time it with events on that stream).
 void* ref_stream(void* handle) { return static_cast<Harness*>(handle)->stream; }
+
+}  // extern "C"
+
+// ================================================================================ SPH
+namespace {
+
+// compute_reference_gradient_norm (sph/sph.cpp:36-58): host float arithmetic over a lattice of
+// spacing 2 r inside the support, evaluated here in the same order and precision.
+float sph_reference_gradient_norm(const float support_radius, const float particle_radius) {
+    const float pi = 3.14159265358979323846F;
+    const float diameter = 2.0F * particle_radius;
+    const float coefficient = 8.0F / (pi * support_radius * support_radius * support_radius);
+    float gx = 0.0F, gy = 0.0F, gz = 0.0F, squared = 0.0F;
+    for (float x = -support_radius; x <= support_radius; x += diameter)
+        for (float y = -support_radius; y <= support_radius; y += diameter)
+            for (float z = -support_radius; z <= support_radius; z += diameter) {
+                const float xx = x * x, yy = y * y, zz = z * z;
+                const float distance = std::sqrt(xx + yy + zz);
+                if (distance == 0.0F || distance >= support_radius) continue;
+                const float q = distance / support_radius;
+                const float derivative = q <= 0.5F ? 18.0F * q * q - 12.0F * q : -6.0F * (1.0F - q) * (1.0F - q);
+                const float scale = coefficient * derivative / (support_radius * distance);
+                gx += scale * x;
+                gy += scale * y;
+                gz += scale * z;
+                squared += scale * scale * (xx + yy + zz);
+            }
+    return gx * gx + gy * gy + gz * gz + squared;
+}
+
+struct SphReplay {
+    Harness* h = nullptr;
+    int method = 0;   // 0 WCSPH, 1 PCISPH, 2 IISPH, 3 DFSPH
+    uint32_t pressure_iterations = 6, divergence_iterations = 4, density_iterations = 6;
+    int warm_start = 1;
+    float reference_gradient_norm = 0.0F;
+    std::vector<void*> allocations;
+    float* densities = nullptr;
+    // WCSPH::Cache (sph/sph.ixx:63-70)
+    float* pressures = nullptr;
+    Vec pressure_acc, viscosity_acc, surface_acc, external_acc, total_acc;
+    // PressureIterationCache `primal` and the iterative methods' caches (sph/sph.ixx:14-21, 114-117, 160-163, 226-232)
+    Vec non_pressure_acc, primal_pressure_acc, predicted_positions, predicted_velocities, divergence_pressure_acc,
+        total_pressure_acc, total_pressure_acceleration;
+    float *primal_pressures = nullptr, *predicted_densities = nullptr;
+
+    template <class T>
+    T* alloc(size_t n) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        allocations.push_back(p);
+        return static_cast<T*>(p);
+    }
+    Vec vec() { const size_t n = h->cfg.particle_count; return {alloc<float>(n), alloc<float>(n), alloc<float>(n)}; }
+    ~SphReplay() {
+        if (h) cudaStreamSynchronize(h->stream);
+        for (void* p : allocations) cudaFree(p);
+    }
+    void clear(float* p) const { cudaMemsetAsync(p, 0, h->cfg.particle_count * sizeof(float), h->stream); }
+    void clear(const Vec& v) const { clear(v.x); clear(v.y); clear(v.z); }
+    void copy(const float* src, float* dst) const {
+        cudaMemcpyAsync(dst, src, h->cfg.particle_count * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
+    }
+    // clear_iteration (sph/sph.cpp:91-97)
+    void clear_primal() const {
+        clear(primal_pressures);
+        clear(predicted_densities);
+        clear(primal_pressure_acc);
+        clear(predicted_positions);
+        clear(predicted_velocities);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+typedef struct {
+    int method;                       // 0 WCSPH, 1 PCISPH, 2 IISPH, 3 DFSPH
+    uint32_t pressure_iterations;     // PCISPH / IISPH
+    uint32_t divergence_iterations;   // DFSPH
+    uint32_t density_iterations;      // DFSPH
+    int pressure_warm_start;          // DFSPH
+} ref_sph_config;
+
+// ParticleParameters (masses, rest densities, viscosities, surface tensions) and the method's
+// Parameters: WCSPH (speed of sound, Tait exponent, boundary surface tension), PCISPH (pressure
+// relaxation), IISPH (Jacobi relaxation), DFSPH (divergence relaxation, density relaxation).
+typedef struct {
+    const float* masses; const float* rest_densities; const float* viscosities; const float* surface_tensions;
+    const float* method0; const float* method1; const float* method2;
+} ref_sph_params;
+
+int ref_sph_create(void* harness, const ref_sph_config* c, void** out) {
+    if (!harness || !c || !out || c->method < 0 || c->method > 3) return 1;
+    auto* r = new SphReplay();
+    r->h = static_cast<Harness*>(harness);
+    r->method = c->method;
+    r->pressure_iterations = c->pressure_iterations;
+    r->divergence_iterations = c->divergence_iterations;
+    r->density_iterations = c->density_iterations;
+    r->warm_start = c->pressure_warm_start;
+    r->reference_gradient_norm = sph_reference_gradient_norm(r->h->cfg.support_radius, r->h->cfg.particle_radius);
+    const size_t n = r->h->cfg.particle_count;
+    r->densities = r->alloc<float>(n);
+    if (r->method == 0) {
+        r->pressures = r->alloc<float>(n);
+        r->pressure_acc = r->vec();
+        r->viscosity_acc = r->vec();
+        r->surface_acc = r->vec();
+        r->external_acc = r->vec();
+        r->total_acc = r->vec();
+    } else {
+        r->non_pressure_acc = r->vec();
+        r->primal_pressures = r->alloc<float>(n);
+        r->predicted_densities = r->alloc<float>(n);
+        r->primal_pressure_acc = r->vec();
+        r->predicted_positions = r->vec();
+        r->predicted_velocities = r->vec();
+        if (r->method == 3) {
+            r->divergence_pressure_acc = r->vec();
+            r->total_pressure_acc = r->vec();
+            r->total_pressure_acceleration = r->vec();
+        }
+    }
+    for (void* p : r->allocations)
+        if (!p) { delete r; return 2; }
+    *out = r;
+    return 0;
+}
+
+int ref_sph_destroy(void* sph) {
+    delete static_cast<SphReplay*>(sph);
+    return 0;
+}
+
+float ref_sph_reference_gradient_norm(void* sph) { return static_cast<SphReplay*>(sph)->reference_gradient_norm; }
+
+// SPH<Method>::forward_step (sph/sph.ixx:350-354).  warm_* / next_warm_*: DFSPH's method state
+// (sph/sph.ixx:202-205), ignored by the other methods.
+int ref_sph_forward_step(void* sph, const ref_state_in* state, const float* const* controls, const ref_sph_params* p,
+                         const float* warm_divergence, const float* warm_density, const ref_state_out* next,
+                         float* next_warm_divergence, float* next_warm_density, const uint64_t step_index) {
+    auto* r = static_cast<SphReplay*>(sph);
+    Harness* h = r->h;
+    const ::cuda::stream_ref s{h->stream};
+    const uint32_t n = h->cfg.particle_count;
+    const float hr = h->cfg.support_radius;
+    const float dt = h->cfg.time_step;
+    const Vec positions{const_cast<float*>(state->px), const_cast<float*>(state->py), const_cast<float*>(state->pz)};
+    const cd::ConstVectorView<float> x{state->px, state->py, state->pz}, v{state->vx, state->vy, state->vz},
+        a{controls[0], controls[1], controls[2]};
+    const cd::VectorView<float> xo{next->px, next->py, next->pz}, vo{next->vx, next->vy, next->vz};
+    const cd::ParticleParameterView pv{p->masses, p->rest_densities, p->viscosities, p->surface_tensions};
+    const cd::Box box = h->collision_box(step_index);
+    h->build(step_index, positions);
+    cd::density_forward(s, n, hr, false, x, x, pv, h->neighborhood(), h->boundary(), r->densities);
+    if (r->method == 0) {   // WCSPH::forward (sph/sph.cpp:214-225)
+        namespace w = cd::wcsph;
+        w::launch_eos_forward(s, n, r->densities, pv, p->method0, p->method1, r->pressures);
+        cd::sph::pressure_forward(s, n, hr, x, pv, h->neighborhood(), h->boundary(), r->densities, r->pressures,
+                                  h->mv(r->pressure_acc));
+        w::launch_artificial_viscosity_forward(s, n, hr, x, v, pv, p->method0, h->neighborhood(), h->boundary(), r->densities,
+                                               h->mv(r->viscosity_acc));
+        w::launch_surface_forward(s, n, hr, h->cfg.particle_radius, x, pv, p->method2, h->neighborhood(), h->boundary(),
+                                  h->mv(r->surface_acc));
+        cd::sph::add(s, n, h->cv(r->pressure_acc), h->cv(r->viscosity_acc), h->mv(r->total_acc));
+        cd::sph::add(s, n, h->cv(r->total_acc), h->cv(r->surface_acc), h->mv(r->total_acc));
+        w::launch_external_forward(s, n, h->cfg.gravity[0], h->cfg.gravity[1], h->cfg.gravity[2], a, h->mv(r->external_acc));
+        cd::sph::add(s, n, h->cv(r->total_acc), h->cv(r->external_acc), h->mv(r->total_acc));
+        cd::sph::integrate_forward(s, n, dt, box, x, v, h->cv(r->total_acc), xo, vo);
+        return cudaGetLastError() == cudaSuccess ? 0 : 3;
+    }
+    cd::sph::non_pressure_forward(s, n, hr, h->cfg.gravity[0], h->cfg.gravity[1], h->cfg.gravity[2], x, v, a, pv,
+                                  h->neighborhood(), h->boundary(), r->densities, h->mv(r->non_pressure_acc));
+    const float rgn = r->reference_gradient_norm;
+    auto predict = [&](const Vec& pressure_acc, const cd::VectorView<float> px, const cd::VectorView<float> pvv) {
+        if (r->method == 1)
+            cd::pcisph::launch_predict_forward(s, n, dt, box, x, v, h->cv(r->non_pressure_acc), h->cv(pressure_acc), px, pvv);
+        else if (r->method == 2)
+            cd::iisph::launch_predict_forward(s, n, dt, box, x, v, h->cv(r->non_pressure_acc), h->cv(pressure_acc), px, pvv);
+        else
+            cd::dfsph::launch_predict_forward(s, n, dt, box, x, v, h->cv(r->non_pressure_acc), h->cv(pressure_acc), px, pvv);
+    };
+    auto pressure = [&]() {
+        cd::sph::pressure_forward(s, n, hr, x, pv, h->neighborhood(), h->boundary(), r->densities, r->primal_pressures,
+                                  h->mv(r->primal_pressure_acc));
+    };
+    auto predicted_density = [&]() {
+        cd::density_forward(s, n, hr, false, x, h->cv(r->predicted_positions), pv, h->neighborhood(), h->boundary(),
+                            r->predicted_densities);
+    };
+    if (r->method == 1 || r->method == 2) {   // PCISPH::forward / IISPH::forward (sph/sph.cpp:296-312, 409-425)
+        r->clear_primal();
+        for (uint32_t it = 1; it <= r->pressure_iterations; ++it) {
+            predict(r->primal_pressure_acc, h->mv(r->predicted_positions), h->mv(r->predicted_velocities));
+            predicted_density();
+            if (r->method == 1)
+                cd::pcisph::launch_pressure_update_forward(s, n, dt, rgn, pv, r->primal_pressures, r->predicted_densities,
+                                                           p->method0, r->primal_pressures);
+            else
+                cd::iisph::launch_jacobi_update_forward(s, n, dt, rgn, pv, r->densities, r->primal_pressures,
+                                                        r->predicted_densities, p->method0, r->primal_pressures);
+            pressure();
+        }
+        predict(r->primal_pressure_acc, xo, vo);
+        return cudaGetLastError() == cudaSuccess ? 0 : 3;
+    }
+    // DFSPH::forward (sph/sph.cpp:572-610)
+    r->clear_primal();
+    if (r->warm_start) r->copy(warm_divergence, r->primal_pressures);
+    pressure();
+    for (uint32_t it = 1; it <= r->divergence_iterations; ++it) {
+        predict(r->primal_pressure_acc, h->mv(r->predicted_positions), h->mv(r->predicted_velocities));
+        predicted_density();
+        cd::dfsph::launch_projection_update_forward(s, n, dt, rgn, pv, r->densities, r->densities, r->primal_pressures,
+                                                    r->predicted_densities, p->method0, r->primal_pressures);
+        pressure();
+    }
+    for (int c = 0; c < 3; ++c) {
+        const float* src[3] = {r->primal_pressure_acc.x, r->primal_pressure_acc.y, r->primal_pressure_acc.z};
+        float* dst[3] = {r->divergence_pressure_acc.x, r->divergence_pressure_acc.y, r->divergence_pressure_acc.z};
+        r->copy(src[c], dst[c]);
+    }
+    r->copy(r->primal_pressures, next_warm_divergence);
+    r->clear_primal();
+    if (r->warm_start) r->copy(warm_density, r->primal_pressures);
+    pressure();
+    for (uint32_t it = 1; it <= r->density_iterations; ++it) {
+        cd::sph::add(s, n, h->cv(r->divergence_pressure_acc), h->cv(r->primal_pressure_acc), h->mv(r->total_pressure_acceleration));
+        predict(r->total_pressure_acceleration, h->mv(r->predicted_positions), h->mv(r->predicted_velocities));
+        predicted_density();
+        cd::dfsph::launch_projection_update_forward(s, n, dt, rgn, pv, r->densities, p->rest_densities, r->primal_pressures,
+                                                    r->predicted_densities, p->method1, r->primal_pressures);
+        pressure();
+    }
+    cd::sph::add(s, n, h->cv(r->divergence_pressure_acc), h->cv(r->primal_pressure_acc), h->mv(r->total_pressure_acc));
+    r->copy(r->primal_pressures, next_warm_density);
+    predict(r->total_pressure_acc, xo, vo);
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+// Copy a field of the last SPH step to device memory (x, y, z: SoA destinations; scalars use x).
+//   0 densities  1 pressures (WCSPH) / last iterate's pressures  2 pressure acceleration
+//   3 viscosity acceleration (WCSPH) / non-pressure acceleration  4 surface acceleration (WCSPH)
+//   5 predicted densities (last iterate)  6 total acceleration (WCSPH) / total pressure acceleration (DFSPH)
+int ref_sph_read(void* sph, const int field, float* x, float* y, float* z) {
+    auto* r = static_cast<SphReplay*>(sph);
+    auto vec3 = [&](const Vec& v) {
+        if (!v.x) return 1;
+        r->copy(v.x, x);
+        r->copy(v.y, y);
+        r->copy(v.z, z);
+        return 0;
+    };
+    auto scalar = [&](const float* f) {
+        if (!f) return 1;
+        r->copy(f, x);
+        return 0;
+    };
+    const bool w = r->method == 0;
+    int rc = 1;
+    switch (field) {
+        case 0: rc = scalar(r->densities); break;
+        case 1: rc = scalar(w ? r->pressures : r->primal_pressures); break;
+        case 2: rc = vec3(w ? r->pressure_acc : r->primal_pressure_acc); break;
+        case 3: rc = vec3(w ? r->viscosity_acc : r->non_pressure_acc); break;
+        case 4: rc = w ? vec3(r->surface_acc) : 1; break;
+        case 5: rc = scalar(r->predicted_densities); break;
+        case 6: rc = vec3(w ? r->total_acc : r->total_pressure_acc); break;
+        default: break;
+    }
+    if (rc) return rc;
+    return cudaStreamSynchronize(r->h->stream) == cudaSuccess ? 0 : 3;
+}
 
 }  // extern "C"

@@ -213,3 +213,114 @@ class ReferencePBF:
         if rc:
             raise RuntimeError(f"ref_read failed: {rc}")
         return out
+
+
+class RefSphConfig(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int), ("pressure_iterations", ctypes.c_uint32), ("divergence_iterations", ctypes.c_uint32),
+                ("density_iterations", ctypes.c_uint32), ("pressure_warm_start", ctypes.c_int)]
+
+
+class RefSphParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("masses", "rest_densities", "viscosities", "surface_tensions", "method0",
+                                               "method1", "method2")]
+
+
+SPH_FIELDS = {"densities": 0, "pressures": 1, "pressure_accelerations": 2, "viscosity_accelerations": 3,
+              "surface_accelerations": 4, "predicted_densities": 5, "total_accelerations": 6}
+SPH_METHOD_PARAMETERS = {0: ("speed_of_sound", "tait_exponent", "boundary_surface_tension"), 1: ("pressure_relaxation",),
+                         2: ("jacobi_relaxation",), 3: ("divergence_relaxation", "density_relaxation")}
+
+
+def _load_sph():
+    lib = load()
+    if not getattr(lib, "_sph_bound", False):
+        vp = ctypes.c_void_p
+        P = ctypes.POINTER
+        lib.ref_sph_create.argtypes = [vp, P(RefSphConfig), P(vp)]
+        lib.ref_sph_destroy.argtypes = [vp]
+        lib.ref_sph_forward_step.argtypes = [vp, P(RefStateIn), P(vp), P(RefSphParams), vp, vp, P(RefStateOut), vp, vp,
+                                             ctypes.c_uint64]
+        lib.ref_sph_read.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+        lib.ref_sph_reference_gradient_norm.argtypes = [vp]
+        lib.ref_sph_reference_gradient_norm.restype = ctypes.c_float
+        lib._sph_bound = True
+    return lib
+
+
+class ReferenceSPH:
+    """The reference SPH<Method>::forward_step replayed by the harness (ref_sph_* in
+    oracle/ref_harness.cu) over the reference's own sph/*.cu kernels, on device tensors.
+    method: 0 WCSPH, 1 PCISPH, 2 IISPH, 3 DFSPH; scene.sph holds the parameter arrays."""
+
+    def __init__(self, scene, method, pressure_iterations=6, divergence_iterations=4, density_iterations=6,
+                 pressure_warm_start=True, device="cuda"):
+        self.base = ReferencePBF(scene, device=device)
+        lib = _load_sph()
+        self.method = int(method)
+        c = RefSphConfig(self.method, pressure_iterations, divergence_iterations, density_iterations,
+                         1 if pressure_warm_start else 0)
+        h = ctypes.c_void_p()
+        rc = lib.ref_sph_create(self.base.handle, ctypes.byref(c), ctypes.byref(h))
+        if rc:
+            raise RuntimeError(f"ref_sph_create failed: {rc}")
+        self.handle = h
+        self.device = self.base.device
+        self.n = scene.count
+        self.params = {k: torch.from_numpy(np.ascontiguousarray(v)).to(self.device) for k, v in scene.sph.items()}
+        self.controls = self.base.controls
+
+    @property
+    def stream(self):
+        return self.base.stream
+
+    @property
+    def reference_gradient_norm(self) -> float:
+        return float(_load_sph().ref_sph_reference_gradient_norm(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _load_sph().ref_sph_destroy(self.handle)
+            self.handle = None
+        self.base.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _pstruct(self):
+        p = self.params
+        names = list(SPH_METHOD_PARAMETERS[self.method]) + [SPH_METHOD_PARAMETERS[self.method][0]] * 3
+        return RefSphParams(_p(p["masses"]), _p(p["rest_densities"]), _p(p["viscosities"]), _p(p["surface_tensions"]),
+                            _p(p[names[0]]), _p(p[names[1]]), _p(p[names[2]]))
+
+    def forward_step(self, x, v, x_out, v_out, step_index, warm=None, warm_out=None, synchronize=True):
+        """x, v, x_out, v_out: (3, N) float32 CUDA tensors; warm / warm_out: DFSPH's (divergence,
+        density) warm-start pressure tensors (N,) float32."""
+        lib = _load_sph()
+        sin = RefStateIn(_p(x[0]), _p(x[1]), _p(x[2]), _p(v[0]), _p(v[1]), _p(v[2]))
+        sout = RefStateOut(_p(x_out[0]), _p(x_out[1]), _p(x_out[2]), _p(v_out[0]), _p(v_out[1]), _p(v_out[2]))
+        ctrl = (ctypes.c_void_p * 3)(self.controls[0].data_ptr(), self.controls[1].data_ptr(), self.controls[2].data_ptr())
+        w = warm if warm is not None else (None, None)
+        wo = warm_out if warm_out is not None else (None, None)
+        args = [ctypes.c_void_p(t.data_ptr()) if t is not None else None for t in (*w, *wo)]
+        params = self._pstruct()
+        self._keep = (sin, sout, ctrl, params)
+        rc = lib.ref_sph_forward_step(self.handle, ctypes.byref(sin), ctrl, ctypes.byref(params), args[0], args[1],
+                                      ctypes.byref(sout), args[2], args[3], step_index)
+        if rc:
+            raise RuntimeError(f"ref_sph_forward_step failed: {rc}")
+        if synchronize:
+            load().ref_synchronize(self.base.handle)
+
+    def read(self, field: str) -> torch.Tensor:
+        code = SPH_FIELDS[field]
+        scalar = code in (0, 1, 5)
+        out = torch.zeros((self.n,) if scalar else (3, self.n), dtype=torch.float32, device=self.device)
+        torch.cuda.synchronize(self.device)
+        ptrs = (out.data_ptr(), None, None) if scalar else (out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr())
+        rc = _load_sph().ref_sph_read(self.handle, code, *[ctypes.c_void_p(p) if p else None for p in ptrs])
+        if rc:
+            raise RuntimeError(f"ref_sph_read failed: {rc}")
+        return out

@@ -22,6 +22,7 @@ LIB = HERE / "lib" / "libphysica_pbf.so"
 OBJ = HERE / "lib" / "obj"
 ARCH = ["-gencode=arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+         "-Xcompiler", "-ffp-contract=off",
          "--expt-relaxed-constexpr", f"-I{ROOT / 'include'}", f"-I{CSRC}"]
 
 

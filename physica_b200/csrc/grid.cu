@@ -28,7 +28,8 @@ __global__ void predict_key_kernel(const uint32_t count, const SceneDesc* __rest
                                    const Field3 velocities, const Field3 controls,
                                    const float* __restrict__ masses, float4* __restrict__ predicted,
                                    uint32_t* __restrict__ keys, uint32_t* __restrict__ arrival,
-                                   uint32_t* __restrict__ histogram, uint32_t* __restrict__ input_flags) {
+                                   uint32_t* __restrict__ histogram, uint32_t* __restrict__ input_flags,
+                                   const int key_current) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const SceneDesc& sc = scenes[scene_of ? scene_of[i] : 0u];
@@ -46,8 +47,8 @@ __global__ void predict_key_kernel(const uint32_t count, const SceneDesc* __rest
     }
     const f3 x = mk(positions.x[i], positions.y[i], positions.z[i]);
     const float dt = sc.time_step;
-    const f3 predicted_velocity = fma3(dt, add(gravity, a), v);
-    const f3 xs = fma3(dt, predicted_velocity, x);
+    // PBF keys the predicted positions (pbf/pbf.cpp:168-170); SPH keys the input positions (sph/sph.ixx:351)
+    const f3 xs = key_current ? x : fma3(dt, fma3(dt, add(gravity, a), v), x);
     predicted[i] = make_float4(xs.x, xs.y, xs.z, masses[i]);
     const Grid& g = sc.grid;
     // (x - minimum - time * velocity) / h, the product fused into the subtraction
@@ -162,7 +163,7 @@ __global__ void reorder_kernel(const uint32_t count, const SceneDesc* __restrict
                                const float4* __restrict__ predicted, const ParamPointers params,
                                uint32_t* __restrict__ sorted_index, uint32_t* __restrict__ slot_of,
                                int4* __restrict__ cell, float4* __restrict__ topology, float4* __restrict__ params_a,
-                               float4* __restrict__ params_b) {
+                               float4* __restrict__ params_b, const Field3 velocities, float4* __restrict__ sorted_velocity) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const uint32_t i = unordered[t];
@@ -184,6 +185,7 @@ __global__ void reorder_kernel(const uint32_t count, const SceneDesc* __restrict
     cell[s] = make_int4(cx, cy, cz, static_cast<int>(scene));
     params_a[s] = make_float4(params.rest_densities[i], params.relaxation[i], params.xsph[i], params.vorticity[i]);
     params_b[s] = make_float4(params.strength[i], params.exponent[i], params.radius[i], 0.0F);
+    if (sorted_velocity) sorted_velocity[s] = make_float4(velocities.x[i], velocities.y[i], velocities.z[i], 0.0F);
 }
 
 // ---- boundary particles (neighborhood/neighborhood.cu:63-69, key_kernel with moving positions) ----
@@ -211,7 +213,7 @@ __global__ void boundary_reorder_kernel(const uint32_t count, const SceneDesc* _
                                         const uint32_t* __restrict__ scene_of, const uint32_t* __restrict__ keys,
                                         const uint32_t* __restrict__ cell_offsets, const uint32_t* __restrict__ unordered,
                                         const float4* __restrict__ rest, const float4* __restrict__ velocity,
-                                        float4* __restrict__ sorted) {
+                                        float4* __restrict__ sorted, float4* __restrict__ sorted_velocity) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= count) return;
     const uint32_t key = keys[b];
@@ -222,6 +224,7 @@ __global__ void boundary_reorder_kernel(const uint32_t count, const SceneDesc* _
     const float4 p = rest[b], v = velocity[b];
     // boundary_position (neighborhood/device.cuh:16-22)
     sorted[first + rank] = make_float4(__fmaf_rn(t, v.x, p.x), __fmaf_rn(t, v.y, p.y), __fmaf_rn(t, v.z, p.z), p.w);
+    if (sorted_velocity) sorted_velocity[first + rank] = v;
 }
 
 // ---- export in the reference's grid layout (cell index x fastest) ----
@@ -257,7 +260,8 @@ __global__ void set_step_kernel(unsigned long long* step, const unsigned long lo
 __global__ void advance_step_kernel(unsigned long long* step) { *step += 1ull; }
 
 // Per-step scene fields from the device step counter (the step advances state `step` to `step + 1`):
-// time = float(step + 1) * dt (pbf/pbf.cpp:18, neighborhood/neighborhood.cu:55), the gather origin
+// time = float(step + 1) * dt (pbf/pbf.cpp:18, neighborhood/neighborhood.cu:55), or float(step) * dt
+// for a grid built at the input step (SPH, sph/sph.ixx:351, sph/sph.cpp:21-35), the gather origin
 // (neighborhood/neighborhood.cpp:83-88) and the collision box (pbf/pbf.cpp:17-31), each with the
 // float operation order of the reference's host code.
 __global__ void scene_time_kernel(const SceneStatic* __restrict__ statics, SceneDesc* __restrict__ scenes,
@@ -266,7 +270,7 @@ __global__ void scene_time_kernel(const SceneStatic* __restrict__ statics, Scene
     if (s >= count) return;
     const SceneStatic st = statics[s];
     SceneDesc& d = scenes[s];
-    const float time = __fmul_rn(__ull2float_rn(*step + 1ull), d.time_step);
+    const float time = __fmul_rn(__ull2float_rn(*step + (st.grid_at_input_step ? 0ull : 1ull)), d.time_step);
     const float ox = __fadd_rn(st.min_x, __fmul_rn(time, st.vel_x));
     const float oy = __fadd_rn(st.min_y, __fmul_rn(time, st.vel_y));
     const float oz = __fadd_rn(st.min_z, __fmul_rn(time, st.vel_z));
@@ -315,7 +319,7 @@ cudaError_t launch_grid_build(cudaStream_t stream, const GridBuildArgs& a) {
         predict_key_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.scenes, a.scene_of, a.positions,
                                                                          a.velocities, a.controls, a.params.masses,
                                                                          a.predicted, a.keys, a.arrival, a.cell_offsets,
-                                                                         a.input_flags);
+                                                                         a.input_flags, a.key_current);
         count_launch();
     }
     const uint64_t n = a.cells + 1;
@@ -328,7 +332,7 @@ cudaError_t launch_grid_build(cudaStream_t stream, const GridBuildArgs& a) {
         scatter_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.keys, a.arrival, a.cell_offsets, a.unordered);
         reorder_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(
             a.count, a.scenes, a.scene_of, a.keys, a.cell_offsets, a.unordered, a.predicted, a.params, a.sorted_index,
-            a.slot_of, a.cell, a.topology, a.params_a, a.params_b);
+            a.slot_of, a.cell, a.topology, a.params_a, a.params_b, a.velocities, a.sorted_velocity);
         count_launch(2);
     }
     return cudaGetLastError();
@@ -344,7 +348,8 @@ cudaError_t launch_boundary_build(cudaStream_t stream, const BoundaryBuildArgs& 
     if ((e = launch_exclusive_scan(stream, a.cell_offsets, a.cells + 1, a.tile_sums)) != cudaSuccess) return e;
     scatter_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.keys, a.arrival, a.cell_offsets, a.unordered);
     boundary_reorder_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.scenes, a.scene_of, a.keys, a.cell_offsets,
-                                                                          a.unordered, a.rest, a.velocity, a.sorted);
+                                                                          a.unordered, a.rest, a.velocity, a.sorted,
+                                                                          a.sorted_velocity);
     count_launch(2);
     return cudaGetLastError();
 }

@@ -57,6 +57,7 @@ struct SceneStatic {
     float min_x, min_y, min_z, max_x, max_y, max_z;
     float vel_x, vel_y, vel_z;
     float particle_radius;
+    uint32_t grid_at_input_step;   // 0: the step's time is (step + 1) dt (PBF); 1: step dt (SPH)
 };
 
 // Per-particle parameters gathered into sorted order once per substep.

@@ -31,6 +31,8 @@ struct GridBuildArgs {
     float4* params_a;
     float4* params_b;
     uint32_t* input_flags = nullptr;   // optional input checks (PBF_INPUT_* bits), null when off
+    int key_current = 0;               // key the input positions instead of the predicted ones (SPH)
+    float4* sorted_velocity = nullptr; // optional (v, 0) in sorted order
 };
 
 size_t scan_tile_count(uint64_t n);
@@ -81,6 +83,7 @@ struct BoundaryBuildArgs {
     uint32_t* tile_sums;
     uint32_t* cell_offsets;        // cells + 1
     float4* sorted;                // (position at the step's time, volume), cell-sorted
+    float4* sorted_velocity = nullptr;   // optional (velocity, 0), cell-sorted
 };
 cudaError_t launch_boundary_build(cudaStream_t stream, const BoundaryBuildArgs& args);
 

@@ -1,0 +1,679 @@
+// Host side of the SPH solvers (include/physica_sph.h): the scene table, the step cache and the
+// launch sequence of SPH<Method>::forward_step (sph/sph.ixx:350-354) for the four methods, over
+// the grid build, boundary build and list scan shared with the PBF substep.
+#include <cmath>
+#include <exception>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/physica_sph.h"
+#include "engine.h"
+#include "sph_launch.h"
+
+namespace pbf {
+namespace sph {
+
+// SPH<Method>::StepCache (sph/sph.ixx:299-303) in sorted order, plus the method's cache fields
+// that the API exports.
+struct SphRecord {
+    DeviceArena arena;
+    bool valid = false;
+    uint64_t step_index = 0;
+    uint32_t* cell_offsets = nullptr;
+    uint32_t* sorted_index = nullptr;
+    uint32_t* slot_of = nullptr;
+    uint32_t* keys = nullptr;
+    int4* cell = nullptr;
+    float4* topology = nullptr;
+    float4* params_a = nullptr;
+    float4* params_b = nullptr;
+    float4* velocity = nullptr;
+    uint32_t* list_entries = nullptr;
+    uint32_t* list_counts = nullptr;
+    uint32_t list_capacity = 0;
+    uint32_t* boundary_offsets = nullptr;
+    float4* boundary = nullptr;
+    float4* boundary_velocity = nullptr;
+    float* density = nullptr;
+    float4* aux = nullptr;
+    float4* non_pressure = nullptr;
+    float4* predicted = nullptr;
+    float4* divergence_acceleration = nullptr;   // DFSPH
+    float4* pressure_acceleration = nullptr;     // the last pressure pass (WCSPH: pressure term)
+    float4* viscosity_acceleration = nullptr;    // WCSPH
+    float4* surface_acceleration = nullptr;      // WCSPH
+    float* pressure[2] = {nullptr, nullptr};
+    float* pressure_term[2] = {nullptr, nullptr};
+    float* predicted_density = nullptr;
+    uint32_t final_pressure = 0;   // which pressure buffer holds the last iterate
+};
+
+class SphEngine {
+public:
+    SphEngine() = default;
+    SphEngine(const SphEngine&) = delete;
+    SphEngine& operator=(const SphEngine&) = delete;
+    ~SphEngine() {
+        if (stream_) cudaStreamSynchronize(stream_);
+    }
+
+    int init(const pbf_domain_configuration* domain, const sph_configuration* configuration, pbf_execution_mode mode,
+             cudaStream_t stream);
+    int allocate(SphRecord& r);
+    int forward(const pbf_particle_state* state, const sph_method_state* method_state, const pbf_control* control,
+                const sph_parameters* parameters, pbf_particle_state* next_state, sph_method_state* next_method_state,
+                SphRecord& r);
+    int read(const SphRecord& r, sph_cache_field field, float* x, float* y, float* z);
+    int check(cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return PBF_SUCCESS;
+        cudaGetLastError();
+        set_error(std::string(what) + ": " + cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? PBF_ERROR_OUT_OF_MEMORY : PBF_ERROR_CUDA;
+    }
+    cudaStream_t stream() const { return stream_; }
+    float reference_gradient_norm() const { return reference_gradient_norm_; }
+    LaunchShape shape{};
+
+private:
+    int launch(cudaStream_t s, const pbf_particle_state* state, const sph_method_state* method_state, const pbf_control* control,
+               const sph_parameters* parameters, pbf_particle_state* next_state, sph_method_state* next_method_state,
+               SphRecord& r);
+
+    sph_configuration config_{};
+    pbf_domain_configuration domain_{};
+    std::vector<pbf_boundary_particle> boundary_host_;
+    uint32_t count_ = 0;
+    uint64_t cells_ = 0;
+    uint32_t dims_[3] = {0, 0, 0};
+    float reference_gradient_norm_ = 0.0F;
+    cudaStream_t stream_ = nullptr;
+    DeviceArena arena_;
+    SceneDesc* d_scenes_ = nullptr;
+    SceneStatic* d_static_ = nullptr;
+    KernelConstants* d_list_constants_ = nullptr;
+    SphConstants* d_constants_ = nullptr;
+    unsigned long long* d_step_ = nullptr;
+    uint64_t host_step_ = ~0ull;
+    float4* scratch_ = nullptr;      // grid build: (x, m) in original order
+    uint32_t* arrival_ = nullptr;
+    uint32_t* unordered_ = nullptr;
+    uint32_t* tile_sums_ = nullptr;
+    uint32_t boundary_count_ = 0;
+    float4* boundary_rest_ = nullptr;
+    float4* boundary_velocity_ = nullptr;
+    uint32_t* boundary_keys_ = nullptr;
+    uint32_t* boundary_arrival_ = nullptr;
+    uint32_t* boundary_unordered_ = nullptr;
+};
+
+namespace {
+bool finite_positive(const float v) { return std::isfinite(v) && v > 0.0F; }
+bool has3(const pbf_vector_field& f) { return f.x && f.y && f.z; }
+}  // namespace
+
+int SphEngine::init(const pbf_domain_configuration* domain, const sph_configuration* configuration, const pbf_execution_mode mode,
+                    cudaStream_t stream) {
+    if (mode == PBF_EXECUTION_DIFFERENTIABLE) {
+        set_error("the SPH solvers are forward-mode only (SPH jvp_step / vjp_step are not provided)");
+        return PBF_ERROR_UNSUPPORTED;
+    }
+    if (mode != PBF_EXECUTION_FORWARD) {
+        set_error("unknown execution mode");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (configuration->method > SPH_METHOD_DFSPH) {
+        set_error("unknown SPH method");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (configuration->checkpoint_interval == 0) {
+        set_error("checkpoint_interval must be at least 1");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (configuration->pressure_iterations > kMaxIterations || configuration->divergence_iterations > kMaxIterations ||
+        configuration->density_iterations > kMaxIterations) {
+        set_error("iteration counts must not exceed " + std::to_string(kMaxIterations));
+        return PBF_ERROR_CAPACITY;
+    }
+    const pbf_domain_configuration& c = *domain;
+    if (!finite_positive(c.time_step) || !finite_positive(c.support_radius) || !std::isfinite(c.particle_radius)) {
+        set_error("time_step and support_radius must be finite and positive");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (c.boundary_particle_count > 0 && !c.boundary_particles) {
+        set_error("boundary_particles is null but boundary_particle_count > 0");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    config_ = *configuration;
+    domain_ = c;
+    domain_.boundary_particles = nullptr;
+    if (c.boundary_particle_count > 0) boundary_host_.assign(c.boundary_particles, c.boundary_particles + c.boundary_particle_count);
+    const float mins[3] = {c.boundary.minimum.x, c.boundary.minimum.y, c.boundary.minimum.z};
+    const float maxs[3] = {c.boundary.maximum.x, c.boundary.maximum.y, c.boundary.maximum.z};
+    cells_ = 1;
+    for (int a = 0; a < 3; ++a) {
+        // neighborhood/neighborhood.cpp:28-32: ceil((max - min) / h) in float
+        const float n = std::ceil((maxs[a] - mins[a]) / c.support_radius);
+        if (!(n >= 1.0F) || n > 1048576.0F) {
+            set_error("box extent / support_radius must be in [1, 2^20] per axis");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        dims_[a] = static_cast<uint32_t>(n);
+        cells_ *= dims_[a];
+    }
+    if (cells_ >= (1ull << 31) || c.particle_count >= (1u << 31) || c.boundary_particle_count >= (1u << 31)) {
+        set_error("cells and particles must each stay below 2^31");
+        return PBF_ERROR_CAPACITY;
+    }
+    count_ = c.particle_count;
+    boundary_count_ = c.boundary_particle_count;
+    stream_ = stream;
+    arena_.set_stream(stream);
+    reference_gradient_norm_ = sph::reference_gradient_norm(c.support_radius, c.particle_radius);
+
+    cudaError_t e = cudaSuccess;
+    d_scenes_ = arena_.alloc<SceneDesc>(1, e);
+    d_static_ = arena_.alloc<SceneStatic>(1, e);
+    d_list_constants_ = arena_.alloc<KernelConstants>(1, e);
+    d_constants_ = arena_.alloc<SphConstants>(1, e);
+    d_step_ = arena_.alloc<unsigned long long>(1, e);
+    float* d_radius = arena_.alloc<float>(1, e);
+    SphSceneInput* d_input = arena_.alloc<SphSceneInput>(1, e);
+    scratch_ = arena_.alloc<float4>(count_, e);
+    arrival_ = arena_.alloc<uint32_t>(count_, e);
+    unordered_ = arena_.alloc<uint32_t>(count_, e);
+    tile_sums_ = arena_.alloc<uint32_t>(scan_tile_count(cells_ + 1), e);
+    if (boundary_count_ > 0) {
+        boundary_rest_ = arena_.alloc<float4>(boundary_count_, e);
+        boundary_velocity_ = arena_.alloc<float4>(boundary_count_, e);
+        boundary_keys_ = arena_.alloc<uint32_t>(boundary_count_, e);
+        boundary_arrival_ = arena_.alloc<uint32_t>(boundary_count_, e);
+        boundary_unordered_ = arena_.alloc<uint32_t>(boundary_count_, e);
+    }
+    if (int rc = check(e, "device allocation")) return rc;
+
+    SceneDesc d{};
+    d.grid.cells_x = dims_[0];
+    d.grid.cells_y = dims_[1];
+    d.grid.cells_z = dims_[2];
+    d.grid.cell_base = 0;
+    d.grid.key_min_x = c.boundary.minimum.x;
+    d.grid.key_min_y = c.boundary.minimum.y;
+    d.grid.key_min_z = c.boundary.minimum.z;
+    d.grid.key_vel_x = c.boundary.velocity.x;
+    d.grid.key_vel_y = c.boundary.velocity.y;
+    d.grid.key_vel_z = c.boundary.velocity.z;
+    d.grid.cell_size = c.support_radius;
+    d.first = 0;
+    d.count = count_;
+    d.time_step = c.time_step;
+    d.inverse_time_step = 1.0F / c.time_step;
+    d.gravity_x = c.gravity.x;
+    d.gravity_y = c.gravity.y;
+    d.gravity_z = c.gravity.z;
+    d.constants = 0;
+    const SceneStatic st{c.boundary.minimum.x, c.boundary.minimum.y, c.boundary.minimum.z, c.boundary.maximum.x,
+                         c.boundary.maximum.y, c.boundary.maximum.z, c.boundary.velocity.x, c.boundary.velocity.y,
+                         c.boundary.velocity.z, c.particle_radius, 1u};
+    const SphSceneInput in{c.support_radius, c.particle_radius, reference_gradient_norm_, c.boundary.velocity.x,
+                           c.boundary.velocity.y, c.boundary.velocity.z, c.boundary.no_slip ? 1u : 0u};
+    e = cudaMemcpyAsync(d_scenes_, &d, sizeof(d), cudaMemcpyHostToDevice, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_static_, &st, sizeof(st), cudaMemcpyHostToDevice, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_input, &in, sizeof(in), cudaMemcpyHostToDevice, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_radius, &c.support_radius, sizeof(float), cudaMemcpyHostToDevice, stream_);
+    if (int rc = check(e, "upload scene table")) return rc;
+    // PBF's constants give the list kernels their fields; the SPH constants then set the list threshold.
+    if (int rc = check(launch_constants(stream_, d_radius, 1, d_list_constants_), "kernel constants")) return rc;
+    if (int rc = check(launch_sph_constants(stream_, d_input, 1, d_constants_, d_list_constants_), "SPH constants")) return rc;
+    if (boundary_count_ > 0) {
+        std::vector<float4> rest, velocity;
+        rest.reserve(boundary_count_);
+        velocity.reserve(boundary_count_);
+        for (const pbf_boundary_particle& b : boundary_host_) {
+            rest.push_back(make_float4(b.position.x, b.position.y, b.position.z, b.volume));
+            velocity.push_back(make_float4(b.velocity.x, b.velocity.y, b.velocity.z, 0.0F));
+        }
+        e = cudaMemcpyAsync(boundary_rest_, rest.data(), rest.size() * sizeof(float4), cudaMemcpyHostToDevice, stream_);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(boundary_velocity_, velocity.data(), velocity.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                                stream_);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);   // the host vectors go out of scope
+        if (int rc = check(e, "upload boundary particles")) return rc;
+    }
+    host_step_ = ~0ull;
+    return check(cudaStreamSynchronize(stream_), "SPH solver initialisation");
+}
+
+int SphEngine::allocate(SphRecord& r) {
+    r.arena.set_stream(stream_);
+    cudaError_t e = cudaSuccess;
+    const uint32_t n = count_;
+    r.cell_offsets = r.arena.alloc<uint32_t>(cells_ + 1, e);
+    r.sorted_index = r.arena.alloc<uint32_t>(n, e);
+    r.slot_of = r.arena.alloc<uint32_t>(n, e);
+    r.keys = r.arena.alloc<uint32_t>(n, e);
+    r.cell = r.arena.alloc<int4>(n, e);
+    r.topology = r.arena.alloc<float4>(n, e);
+    r.params_a = r.arena.alloc<float4>(n, e);
+    r.params_b = r.arena.alloc<float4>(n, e);
+    r.velocity = r.arena.alloc<float4>(n, e);
+    r.list_capacity = kListCapacity;
+    const size_t padded = (static_cast<size_t>(n) + 31u) / 32u * 32u;
+    r.list_entries = r.arena.alloc<uint32_t>(padded * r.list_capacity, e);
+    r.list_counts = r.arena.alloc<uint32_t>(n, e);
+    if (boundary_count_ > 0) {
+        r.boundary_offsets = r.arena.alloc<uint32_t>(cells_ + 1, e);
+        r.boundary = r.arena.alloc<float4>(boundary_count_, e);
+        r.boundary_velocity = r.arena.alloc<float4>(boundary_count_, e);
+    }
+    r.density = r.arena.alloc<float>(n, e);
+    r.aux = r.arena.alloc<float4>(n, e);
+    r.pressure_acceleration = r.arena.alloc<float4>(n, e);
+    r.pressure[0] = r.arena.alloc<float>(n, e);
+    r.pressure_term[0] = r.arena.alloc<float>(n, e);
+    if (config_.method == SPH_METHOD_WCSPH) {
+        r.viscosity_acceleration = r.arena.alloc<float4>(n, e);
+        r.surface_acceleration = r.arena.alloc<float4>(n, e);
+    } else {
+        r.non_pressure = r.arena.alloc<float4>(n, e);
+        r.predicted = r.arena.alloc<float4>(n, e);
+        r.predicted_density = r.arena.alloc<float>(n, e);
+        if (config_.method == SPH_METHOD_DFSPH) {
+            r.divergence_acceleration = r.arena.alloc<float4>(n, e);
+            r.pressure[1] = r.arena.alloc<float>(n, e);
+            r.pressure_term[1] = r.arena.alloc<float>(n, e);
+        }
+    }
+    r.valid = false;
+    if (int rc = check(e, "step cache allocation")) return rc;
+    if (r.predicted_density) {
+        if (int rc = check(cudaMemsetAsync(r.predicted_density, 0, static_cast<size_t>(n) * sizeof(float), stream_), "clear"))
+            return rc;
+    }
+    return check(cudaStreamSynchronize(stream_), "step cache allocation");
+}
+
+int SphEngine::forward(const pbf_particle_state* state, const sph_method_state* method_state, const pbf_control* control,
+                       const sph_parameters* parameters, pbf_particle_state* next_state, sph_method_state* next_method_state,
+                       SphRecord& r) {
+    if (!state || !control || !parameters || !next_state) {
+        set_error("null argument");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    const uint32_t method = config_.method;
+    if (count_ > 0) {
+        if (!has3(state->positions) || !has3(state->velocities) || !has3(control->external_accelerations) ||
+            !has3(next_state->positions) || !has3(next_state->velocities)) {
+            set_error("null field pointer");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        const sph_parameters& p = *parameters;
+        bool ok = p.masses && p.rest_densities && p.viscosities && p.surface_tensions;
+        if (method == SPH_METHOD_WCSPH) ok = ok && p.speed_of_sound && p.tait_exponent && p.boundary_surface_tension;
+        if (method == SPH_METHOD_PCISPH) ok = ok && p.pressure_relaxation;
+        if (method == SPH_METHOD_IISPH) ok = ok && p.jacobi_relaxation;
+        if (method == SPH_METHOD_DFSPH) ok = ok && p.divergence_relaxation && p.density_relaxation;
+        if (!ok) {
+            set_error("null parameter pointer for this method");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        if (method == SPH_METHOD_DFSPH) {
+            if (!next_method_state || !next_method_state->warm_divergence_pressure || !next_method_state->warm_density_pressure ||
+                (config_.pressure_warm_start &&
+                 (!method_state || !method_state->warm_divergence_pressure || !method_state->warm_density_pressure))) {
+                set_error("DFSPH needs its method state (warm-start pressures)");
+                return PBF_ERROR_INVALID_ARGUMENT;
+            }
+        }
+    }
+    if (host_step_ != state->step_index) {
+        if (int rc = check(launch_set_step(stream_, d_step_, state->step_index), "step counter")) return rc;
+        host_step_ = state->step_index;
+    }
+    if (int rc = launch(stream_, state, method_state, control, parameters, next_state, next_method_state, r)) return rc;
+    // the device counter then holds the index of the next state, as the host counter does
+    if (int rc = check(launch_advance_step(stream_, d_step_), "step counter")) return rc;
+    host_step_ = state->step_index + 1u;
+    next_state->step_index = state->step_index + 1u;
+    r.valid = true;
+    r.step_index = state->step_index;
+    return PBF_SUCCESS;
+}
+
+int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph_method_state* method_state,
+                      const pbf_control* control, const sph_parameters* parameters, pbf_particle_state* next_state,
+                      sph_method_state* next_method_state, SphRecord& r) {
+    if (int rc = check(launch_scene_time(s, d_static_, d_scenes_, d_step_, 1), "scene table")) return rc;
+    const sph_parameters& p = *parameters;
+    const uint32_t method = config_.method;
+    // params_a = (rest density, viscosity, surface tension, method 0), params_b = (method 1, method 2, 0)
+    const float* method0 = method == SPH_METHOD_WCSPH    ? p.speed_of_sound
+                           : method == SPH_METHOD_PCISPH ? p.pressure_relaxation
+                           : method == SPH_METHOD_IISPH  ? p.jacobi_relaxation
+                                                         : p.divergence_relaxation;
+    const float* method1 = method == SPH_METHOD_WCSPH ? p.tait_exponent : method == SPH_METHOD_DFSPH ? p.density_relaxation : method0;
+    const float* method2 = method == SPH_METHOD_WCSPH ? p.boundary_surface_tension : method0;
+    GridBuildArgs g{};
+    g.count = count_;
+    g.cells = cells_;
+    g.scenes = d_scenes_;
+    g.scene_of = nullptr;
+    g.positions = {state->positions.x, state->positions.y, state->positions.z};
+    g.velocities = {state->velocities.x, state->velocities.y, state->velocities.z};
+    g.controls = {control->external_accelerations.x, control->external_accelerations.y, control->external_accelerations.z};
+    // ParamPointers slots: (masses, rest densities, relaxation -> viscosities, strength -> method 1,
+    // exponent -> method 2, radius -> method 2, xsph -> surface tensions, vorticity -> method 0)
+    g.params = {p.masses, p.rest_densities, p.viscosities, method1, method2, method2, p.surface_tensions, method0};
+    g.predicted = scratch_;
+    g.keys = r.keys;
+    g.arrival = arrival_;
+    g.cell_offsets = r.cell_offsets;
+    g.tile_sums = tile_sums_;
+    g.unordered = unordered_;
+    g.sorted_index = r.sorted_index;
+    g.slot_of = r.slot_of;
+    g.cell = r.cell;
+    g.topology = r.topology;
+    g.params_a = r.params_a;
+    g.params_b = r.params_b;
+    g.key_current = 1;
+    g.sorted_velocity = r.velocity;
+    if (int rc = check(launch_grid_build(s, g), "grid build")) return rc;
+    if (boundary_count_ > 0) {
+        BoundaryBuildArgs b{boundary_count_, cells_, d_scenes_, nullptr, boundary_rest_, boundary_velocity_, boundary_keys_,
+                            boundary_arrival_, boundary_unordered_, tile_sums_, r.boundary_offsets, r.boundary};
+        b.sorted_velocity = r.boundary_velocity;
+        if (int rc = check(launch_boundary_build(s, b), "boundary grid build")) return rc;
+    }
+    GatherCommon gc{count_, d_scenes_, d_list_constants_, r.cell_offsets, r.cell, r.params_a, r.params_b};
+    if (boundary_count_ > 0) {
+        gc.boundary_offsets = r.boundary_offsets;
+        gc.boundary = r.boundary;
+    }
+    const StoredList list{r.list_entries, r.list_counts, r.list_capacity};
+    if (int rc = check(launch_list_scan(s, ListScanArgs{gc, r.topology, list, 1}, shape), "neighbour list scan")) return rc;
+    SphStep st{gc,
+               d_constants_,
+               r.topology,
+               r.velocity,
+               list,
+               r.boundary_velocity,
+               r.aux,
+               r.non_pressure,
+               r.predicted,
+               r.sorted_index,
+               {control->external_accelerations.x, control->external_accelerations.y, control->external_accelerations.z}};
+    const unsigned block = shape.block;
+    const MutField3 out_x{next_state->positions.x, next_state->positions.y, next_state->positions.z};
+    const MutField3 out_v{next_state->velocities.x, next_state->velocities.y, next_state->velocities.z};
+    const bool warm = method == SPH_METHOD_DFSPH && config_.pressure_warm_start != 0;
+    if (int rc = check(launch_density(s, st, method, r.density, r.pressure[0], r.pressure_term[0],
+                                      warm ? method_state->warm_divergence_pressure : nullptr, block),
+                       "density"))
+        return rc;
+    if (method == SPH_METHOD_WCSPH) {
+        r.final_pressure = 0;
+        return check(launch_wcsph_forces(s, st, r.pressure_term[0], out_x, out_v, r.pressure_acceleration,
+                                         r.viscosity_acceleration, r.surface_acceleration, block),
+                     "WCSPH forces");
+    }
+    if (method == SPH_METHOD_PCISPH || method == SPH_METHOD_IISPH) {
+        const uint32_t K = config_.pressure_iterations;
+        r.final_pressure = 0;
+        if (int rc = check(launch_non_pressure(s, st, K > 0 ? 1 : 2, out_x, out_v, block), "non-pressure acceleration")) return rc;
+        const PressureUpdate update{method, 0u, 0u};
+        for (uint32_t it = 1; it <= K; ++it) {
+            if (int rc = check(launch_predicted_density(s, st, update, r.pressure[0], r.pressure_term[0], r.predicted_density, block),
+                               "predicted density"))
+                return rc;
+            PressurePassArgs a{};
+            a.pressure_term = r.pressure_term[0];
+            a.pressure = r.pressure[0];
+            a.last = it == K ? 1 : 0;
+            a.out_positions = out_x;
+            a.out_velocities = out_v;
+            a.store_acceleration = it == K ? r.pressure_acceleration : nullptr;
+            if (int rc = check(launch_pressure(s, st, a, block), "pressure acceleration")) return rc;
+        }
+        return PBF_SUCCESS;
+    }
+    // DFSPH::forward (sph/sph.cpp:572-610): divergence phase on pressure buffer 0, density phase on
+    // buffer 1; the divergence phase's last pressure pass also loads the density phase's warm start.
+    if (int rc = check(launch_non_pressure(s, st, 0, out_x, out_v, block), "non-pressure acceleration")) return rc;
+    const uint32_t Kd = config_.divergence_iterations, Kr = config_.density_iterations;
+    for (uint32_t it = 0; it <= Kd; ++it) {
+        if (it > 0) {
+            if (int rc = check(launch_predicted_density(s, st, PressureUpdate{SPH_METHOD_DFSPH, 0u, 1u}, r.pressure[0],
+                                                        r.pressure_term[0], r.predicted_density, block),
+                               "predicted density"))
+                return rc;
+        }
+        PressurePassArgs a{};
+        a.pressure_term = r.pressure_term[0];
+        a.pressure = r.pressure[0];
+        a.out_positions = out_x;
+        a.out_velocities = out_v;
+        if (it == Kd) {
+            a.store_acceleration = r.divergence_acceleration;
+            a.warm_out = next_method_state->warm_divergence_pressure;
+            a.next_pressure = r.pressure[1];
+            a.next_pressure_term = r.pressure_term[1];
+            a.next_warm = warm ? method_state->warm_density_pressure : nullptr;
+        }
+        if (int rc = check(launch_pressure(s, st, a, block), "pressure acceleration")) return rc;
+    }
+    for (uint32_t it = 0; it <= Kr; ++it) {
+        if (it > 0) {
+            if (int rc = check(launch_predicted_density(s, st, PressureUpdate{SPH_METHOD_DFSPH, 1u, 0u}, r.pressure[1],
+                                                        r.pressure_term[1], r.predicted_density, block),
+                               "predicted density"))
+                return rc;
+        }
+        PressurePassArgs a{};
+        a.pressure_term = r.pressure_term[1];
+        a.pressure = r.pressure[1];
+        a.base = r.divergence_acceleration;
+        a.out_positions = out_x;
+        a.out_velocities = out_v;
+        if (it == Kr) {
+            a.last = 1;
+            a.warm_out = next_method_state->warm_density_pressure;
+            a.store_acceleration = r.pressure_acceleration;
+        }
+        if (int rc = check(launch_pressure(s, st, a, block), "pressure acceleration")) return rc;
+    }
+    r.final_pressure = 1;
+    return PBF_SUCCESS;
+}
+
+int SphEngine::read(const SphRecord& r, const sph_cache_field field, float* x, float* y, float* z) {
+    if (!r.valid) {
+        set_error("the step cache holds no forward step");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    auto vec = [&](const float4* v) -> int {
+        if (!v) {
+            set_error("this field is not part of this method's cache");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        if (!x || !y || !z) {
+            set_error("null destination");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        return check(launch_unsort_float4(stream_, count_, r.sorted_index, v, 3, x, y, z, nullptr), "read cache");
+    };
+    auto scalar = [&](const float* v) -> int {
+        if (!v) {
+            set_error("this field is not part of this method's cache");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        if (!x) {
+            set_error("null destination");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        return check(launch_unsort_scalar(stream_, count_, r.sorted_index, v, sizeof(float), x), "read cache");
+    };
+    const bool w = config_.method == SPH_METHOD_WCSPH;
+    switch (field) {
+        case SPH_CACHE_DENSITIES: return scalar(r.density);
+        case SPH_CACHE_PRESSURES: return scalar(r.pressure[r.final_pressure]);
+        case SPH_CACHE_PRESSURE_ACCELERATIONS: return vec(r.pressure_acceleration);
+        case SPH_CACHE_VISCOSITY_ACCELERATIONS: return vec(w ? r.viscosity_acceleration : r.non_pressure);
+        case SPH_CACHE_SURFACE_ACCELERATIONS: return vec(r.surface_acceleration);
+        case SPH_CACHE_PREDICTED_DENSITIES: return scalar(r.predicted_density);
+        default: break;
+    }
+    set_error("unknown cache field");
+    return PBF_ERROR_INVALID_ARGUMENT;
+}
+
+}  // namespace sph
+}  // namespace pbf
+
+struct sph_solver {
+    pbf::sph::SphEngine engine;
+};
+
+struct sph_step_cache {
+    sph_solver* solver = nullptr;
+    pbf::sph::SphRecord record;
+};
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        pbf::set_error("host allocation failed");
+        return PBF_ERROR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        pbf::set_error(e.what());
+        return PBF_ERROR_CUDA;
+    } catch (...) {
+        pbf::set_error("unknown failure");
+        return PBF_ERROR_CUDA;
+    }
+}
+
+int null_arg(const char* what) {
+    pbf::set_error(std::string("null argument: ") + what);
+    return PBF_ERROR_INVALID_ARGUMENT;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sph_create(const pbf_domain_configuration* domain, const sph_configuration* configuration, const pbf_execution_mode mode,
+               void* cuda_stream, sph_solver** solver) {
+    if (!solver) return null_arg("solver");
+    *solver = nullptr;
+    if (!domain) return null_arg("domain");
+    if (!configuration) return null_arg("configuration");
+    return guarded([&] {
+        auto s = std::make_unique<sph_solver>();
+        const int rc = s->engine.init(domain, configuration, mode, static_cast<cudaStream_t>(cuda_stream));
+        if (rc) return rc;
+        *solver = s.release();
+        return static_cast<int>(PBF_SUCCESS);
+    });
+}
+
+int sph_destroy(sph_solver* solver) {
+    if (!solver) return PBF_SUCCESS;
+    return guarded([&] {
+        delete solver;
+        return static_cast<int>(PBF_SUCCESS);
+    });
+}
+
+int sph_allocate_step_cache(sph_solver* solver, sph_step_cache** cache) {
+    if (!cache) return null_arg("cache");
+    *cache = nullptr;
+    if (!solver) return null_arg("solver");
+    return guarded([&] {
+        auto c = std::make_unique<sph_step_cache>();
+        c->solver = solver;
+        const int rc = solver->engine.allocate(c->record);
+        if (rc) return rc;
+        *cache = c.release();
+        return static_cast<int>(PBF_SUCCESS);
+    });
+}
+
+int sph_free_step_cache(sph_solver* solver, sph_step_cache* cache) {
+    if (!cache) return PBF_SUCCESS;
+    if (!solver || cache->solver != solver) {
+        pbf::set_error("the step cache belongs to another solver");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    return guarded([&] {
+        cudaStreamSynchronize(solver->engine.stream());
+        delete cache;
+        return static_cast<int>(PBF_SUCCESS);
+    });
+}
+
+int sph_forward_step(sph_solver* solver, const pbf_particle_state* state, const sph_method_state* method_state,
+                     const pbf_control* control, const sph_parameters* parameters, pbf_particle_state* next_state,
+                     sph_method_state* next_method_state, sph_step_cache* cache) {
+    if (!solver) return null_arg("solver");
+    if (!cache) return null_arg("cache");
+    if (cache->solver != solver) {
+        pbf::set_error("the step cache belongs to another solver");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    return guarded([&] {
+        return solver->engine.forward(state, method_state, control, parameters, next_state, next_method_state, cache->record);
+    });
+}
+
+int sph_read_cache(sph_solver* solver, const sph_step_cache* cache, const sph_cache_field field, float* x, float* y, float* z) {
+    if (!solver) return null_arg("solver");
+    if (!cache) return null_arg("cache");
+    if (cache->solver != solver) {
+        pbf::set_error("the step cache belongs to another solver");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    return guarded([&] { return solver->engine.read(cache->record, field, x, y, z); });
+}
+
+int sph_reference_gradient_norm(const sph_solver* solver, float* value) {
+    if (!solver) return null_arg("solver");
+    if (!value) return null_arg("value");
+    *value = solver->engine.reference_gradient_norm();
+    return PBF_SUCCESS;
+}
+
+int sph_set_launch_shape(sph_solver* solver, const pbf_launch_shape* shape) {
+    if (!solver) return null_arg("solver");
+    if (!shape) return null_arg("shape");
+    const pbf::LaunchShape s{shape->list_scan, shape->scan_block_size, shape->block_size};
+    if (!pbf::valid_shape(s)) {
+        pbf::set_error("invalid launch shape");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    solver->engine.shape = s;
+    return PBF_SUCCESS;
+}
+
+int sph_get_launch_shape(const sph_solver* solver, pbf_launch_shape* shape) {
+    if (!solver) return null_arg("solver");
+    if (!shape) return null_arg("shape");
+    shape->list_scan = solver->engine.shape.scan;
+    shape->scan_block_size = solver->engine.shape.scan_block;
+    shape->block_size = solver->engine.shape.block;
+    return PBF_SUCCESS;
+}
+
+int sph_synchronize(sph_solver* solver) {
+    if (!solver) return null_arg("solver");
+    return guarded([&] { return solver->engine.check(cudaStreamSynchronize(solver->engine.stream()), "synchronize"); });
+}
+
+void* sph_stream(const sph_solver* solver) { return solver ? static_cast<void*>(solver->engine.stream()) : nullptr; }
+
+}  // extern "C"

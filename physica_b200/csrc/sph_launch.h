@@ -1,0 +1,122 @@
+// Launcher declarations and argument blocks of the SPH substep kernels (sph.cu).
+//
+// The SPH family of the reference (sph/sph.ixx:39-372: WCSPH, PCISPH, IISPH, DFSPH) runs on the
+// same cell-sorted particles, stencil order and stored neighbour lists as the PBF substep.  The
+// grid is built from the input positions at the input step's time (sph/sph.ixx:351) and every
+// gather uses the cubic spline kernel (density/device.cuh:26-42, 76-79).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pbf_launch.h"
+
+namespace pbf {
+namespace sph {
+
+enum Method : uint32_t { kWcsph = 0, kPcisph = 1, kIisph = 2, kDfsph = 3 };
+
+// Per-scene constants of the SPH kernels, derived on the device from the domain.
+struct SphConstants {
+    float h;                        // support radius
+    float cubic_coefficient;        // 8 / (pi h h h)                        (density/device.cuh:29)
+    float cubic_coefficient_2;      // 2 * cubic_coefficient (exact)         (density/device.cuh:32)
+    float support_threshold;        // smallest r2 with sqrtf(r2) >= h: the cubic kernels vanish at r2 >= this
+    float laplacian_denominator;    // pi h h h h h h                        (density/device.cuh:78)
+    float epsilon_factor;           // 0.01 h: the viscosity denominator is r2 + 0.01 h h (sph/wcsph.cu:157, 169)
+    float diameter;                 // 2 r                                   (sph/wcsph.cu:467)
+    float contact_weight;           // cubic((2 r, 0, 0))                    (sph/wcsph.cu:326)
+    float reference_gradient_norm;  // host value of sph/sph.cpp:36-58
+    float box_vx, box_vy, box_vz;   // box velocity, written on collision    (sph/common.cu:313-319)
+    uint32_t no_slip;
+};
+
+// Sorted per-particle parameters of an SPH step, packed by the grid build:
+//   params_a = (rest density, viscosity, surface tension, method parameter 0)
+//   params_b = (method parameter 1, method parameter 2, 0, 0)
+// Method parameters: WCSPH (speed of sound, Tait exponent, boundary surface tension), PCISPH
+// (pressure relaxation), IISPH (Jacobi relaxation), DFSPH (divergence relaxation, density relaxation).
+
+// Buffers of one SPH step in sorted order.
+struct SphStep {
+    GatherCommon g;
+    const SphConstants* constants;   // per scene (SceneDesc::constants indexes it)
+    const float4* topology;          // (x, mass): positions of the input state
+    const float4* velocity;          // (v, 0)
+    StoredList list;                 // in-support neighbours of every particle (fluid and boundary)
+    const float4* boundary_velocity; // (velocity, 0) of the cell-sorted boundary particles, or null
+    float4* aux;                     // (density, viscosity, speed of sound, 0)
+    float4* non_pressure;            // non-pressure acceleration (iterative methods)
+    float4* predicted;               // (predicted position, mass)
+    const uint32_t* sorted_index;
+    Field3 controls;                 // external accelerations, original order
+};
+
+// Density (cubic) of every particle over its list; WCSPH also evaluates the Tait equation of state
+// (sph/wcsph.cu:92-100) and writes pressure / density^2.  `pressure`, `pressure_term`: sorted
+// outputs (pressure_term = p / rho^2 of the first pressure pass).  warm: DFSPH's warm-start
+// pressures in original order, or null (pressure 0).
+cudaError_t launch_density(cudaStream_t stream, const SphStep& st, uint32_t method, float* density_record, float* pressure,
+                           float* pressure_term, const float* warm, unsigned block);
+
+// WCSPH forces (pressure, artificial viscosity, surface), external acceleration and integration
+// (sph/sph.cpp:214-225) in one pass; writes the next state in original order.
+cudaError_t launch_wcsph_forces(cudaStream_t stream, const SphStep& st, const float* pressure_term, MutField3 out_positions,
+                                MutField3 out_velocities, float4* record_pressure, float4* record_viscosity,
+                                float4* record_surface, unsigned block);
+
+// Non-pressure acceleration (sph/common.cu:14-47) and, for PCISPH / IISPH, the first prediction
+// with the cleared pressure acceleration (sph/sph.cpp:300-303).
+//   mode: 0 acceleration only (DFSPH), 1 also the first predicted positions, 2 the prediction is the
+//   next state (no pressure iteration), written in original order.
+cudaError_t launch_non_pressure(cudaStream_t stream, const SphStep& st, int mode, MutField3 out_positions,
+                                MutField3 out_velocities, unsigned block);
+
+// Predicted density at the predicted positions over the full stencil of the input positions
+// (density::sph_forward(topology = x, positions = x*)), then the method's pressure update.
+//   target: 0 rest density (PCISPH, IISPH, DFSPH density phase), 1 the step's density (DFSPH divergence)
+struct PressureUpdate {
+    uint32_t method;       // kPcisph, kIisph, kDfsph
+    uint32_t relaxation;   // 0: params_a.w, 1: params_b.x
+    uint32_t target;       // 0 rest density, 1 density
+};
+cudaError_t launch_predicted_density(cudaStream_t stream, const SphStep& st, PressureUpdate update, float* pressure,
+                                     float* pressure_term, float* predicted_density_record, unsigned block);
+
+// Pressure acceleration (sph/common.cu:165-194) and the next prediction (sph/pcisph.cu:26-45).
+//   base: an acceleration added to the pressure acceleration before prediction (DFSPH density
+//   phase: the divergence phase's result), or null.
+//   last: write the prediction as the next state (original order) and, when `warm_out` is set,
+//   the pressures (original order).  store_acceleration: keep the pressure acceleration.
+//   next_pressure / next_pressure_term / next_warm: DFSPH's switch to the density phase: load
+//   the density phase's warm-start pressures (original order, or null for 0).
+struct PressurePassArgs {
+    const float* pressure_term;
+    const float* pressure;
+    const float4* base;
+    int last;
+    MutField3 out_positions;
+    MutField3 out_velocities;
+    float* warm_out;
+    float4* store_acceleration;
+    float* next_pressure;
+    float* next_pressure_term;
+    const float* next_warm;
+};
+cudaError_t launch_pressure(cudaStream_t stream, const SphStep& st, const PressurePassArgs& a, unsigned block);
+
+// Constants of every scene (host inputs: support radius, particle radius, box velocity, no-slip
+// flag and the reference gradient norm per scene).
+struct SphSceneInput {
+    float h, particle_radius, reference_gradient_norm;
+    float box_vx, box_vy, box_vz;
+    uint32_t no_slip;
+};
+cudaError_t launch_sph_constants(cudaStream_t stream, const SphSceneInput* inputs, uint32_t n, SphConstants* out,
+                                 KernelConstants* list_constants);
+
+// compute_reference_gradient_norm (sph/sph.cpp:36-58) on the host.
+float reference_gradient_norm(float support_radius, float particle_radius);
+
+}  // namespace sph
+}  // namespace pbf

@@ -73,6 +73,8 @@ class Scene:
     targets: np.ndarray | None = None  # (3, N) float32 target cloud for the loss
     # boundary particles: {"positions": (3, B), "velocities": (3, B), "volumes": (B,)} float32
     boundary: dict | None = None
+    # SPH parameters (sph_dam_break): one (N,) float32 array per SPH<Method>::Parameters field
+    sph: dict | None = None
 
     @property
     def count(self) -> int:
@@ -281,3 +283,45 @@ def example_dam_break() -> Scene:
         pressure_iterations=5,
         name="example_dam_break",
     )
+
+
+SPH_DT = 4.0e-4
+
+
+def sph_parameter_arrays(scene: Scene, *, viscosity=None, surface_tension=0.05, speed_of_sound=20.0,
+                         tait_exponent=7.0, boundary_surface_tension=0.02, relaxation=0.5, method="wcsph") -> dict:
+    """SPH particle and method parameters for a dam-break scene (sph/sph.ixx:45-49, 111, 157,
+    214-217): the scene's masses and rest densities; viscosity 0.05 (Monaghan alpha of WCSPH) or
+    0.001 (kinematic viscosity of the others' Laplacian term); cohesion 0.05; c = 20 m/s and
+    gamma = 7 in the Tait equation; adhesion 0.02; every pressure relaxation 0.5."""
+    n = scene.count
+    full = lambda value: np.full(n, value, dtype=np.float32)
+    if viscosity is None:
+        viscosity = 0.05 if method == "wcsph" else 0.001
+    return {
+        "masses": scene.masses.copy(),
+        "rest_densities": scene.rest_densities.copy(),
+        "viscosities": full(viscosity),
+        "surface_tensions": full(surface_tension),
+        "speed_of_sound": full(speed_of_sound),
+        "tait_exponent": full(tait_exponent),
+        "boundary_surface_tension": full(boundary_surface_tension),
+        "pressure_relaxation": full(relaxation),
+        "jacobi_relaxation": full(relaxation),
+        "divergence_relaxation": full(relaxation),
+        "density_relaxation": full(relaxation),
+    }
+
+
+def sph_dam_break(lattice, box_min, box_max, seed, *, method="wcsph", dt=SPH_DT, velocity_sigma=0.0, name="",
+                  **parameters) -> Scene:
+    """The dam-break lattice of `dam_break` (spacing 0.5 h, particle radius 0.2 h) with SPH
+    parameters and an SPH time step (CFL 0.4 h / c at c = 20 m/s is 5e-4 s)."""
+    scene = dam_break(lattice, box_min, box_max, seed, 0, dt=dt, velocity_sigma=velocity_sigma, name=name)
+    scene.sph = sph_parameter_arrays(scene, method=method, **parameters)
+    return scene
+
+
+def sph_large(seed=6, method="wcsph") -> Scene:
+    """1,048,576-particle SPH dam break (128x64x128 lattice) in a [0,4]^3 box."""
+    return sph_dam_break((128, 64, 128), (0.0, 0.0, 0.0), (4.0, 4.0, 4.0), seed, method=method, name="sph_dam_break_1m")

@@ -14,7 +14,7 @@ def declared_functions():
     names = set()
     for header in (ROOT / "include").glob("*.h"):
         text = header.read_text()
-        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\*?\s+(pbf_[a-z0-9_]+)\s*\(", text, re.M):
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\*?\s+((?:pbf|sph)_[a-z0-9_]+)\s*\(", text, re.M):
             names.add(m.group(1))
     return sorted(names)
 
@@ -22,7 +22,8 @@ def declared_functions():
 def test_header_declares_entry_points():
     names = declared_functions()
     for required in ("pbf_create", "pbf_destroy", "pbf_allocate_step_cache", "pbf_forward_step", "pbf_vjp_step",
-                     "pbf_jvp_step", "pbf_batch_create", "pbf_batch_forward_step", "pbf_forward_step_host"):
+                     "pbf_jvp_step", "pbf_batch_create", "pbf_batch_forward_step", "pbf_forward_step_host",
+                     "sph_create", "sph_forward_step", "sph_allocate_step_cache", "sph_read_cache"):
         assert required in names
 
 
