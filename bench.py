@@ -311,6 +311,7 @@ def bench_b200(args, world, rank):
     if not args.no_batch and not args.no_grad:
         batched_grad = bench_batch_grad(args, world, rank)
 
+    sph_family = None if args.no_sph else bench_sph(args, world, rank)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(sc)
@@ -328,7 +329,7 @@ def bench_b200(args, world, rank):
         "roofline": roofline, "step_roofline": step_roofline, "per_pass": per_pass,
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(round(per_step_launches * args.steps)),
         "clocks": clk.summary(), "grad_steps_per_s": grad, "batched_scenes": batched,
-        "batched_grad_steps_per_s": batched_grad,
+        "batched_grad_steps_per_s": batched_grad, "sph_family": sph_family,
     }
 
 
@@ -479,6 +480,66 @@ def bench_batch_grad(args, world, rank):
                        "trajectory_checkpoint_every": every, "graphs": True}}
 
 
+SPH_METHODS = ("wcsph", "pcisph", "iisph", "dfsph")
+SPH_WORKLOAD = ("sph_dam_break_1m: 1,048,576 particles (128x64x128 lattice, spacing 0.5h, h=0.025), box [0,4]^3, "
+                "dt=4e-4; PCISPH/IISPH 6 pressure iterations, DFSPH 4 divergence + 6 density iterations (the "
+                "reference's defaults), DFSPH warm start from zero")
+
+
+def bench_sph(args, world, rank):
+    """The SPH family's forward substep (SPH<Method>::forward_step) at 1M particles, one solver per method."""
+    from physica_b200 import sph, scenes
+    out = {"unit": UNIT, "config": {"workload": SPH_WORKLOAD, "l2": "flushed between timed steps (256 MiB write)"}}
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    steps = max(3, min(args.steps, 8))
+    for name in SPH_METHODS:
+        sc = scenes.sph_large(seed=6 + rank, method=name)
+        solver, state, control, params = sph.solver_for_scene(sc, sph.Method[name])
+        cache = solver.allocate_step_cache()
+        holder = {"cur": state, "nxt": solver.allocate_state()}
+
+        def step():
+            solver.forward_step(holder["cur"], control, params, holder["nxt"], cache)
+            holder["cur"], holder["nxt"] = holder["nxt"], holder["cur"]
+
+        ms, _ = timed(step, steps, args.warmup, world, solver.stream, flush)
+        ms_per_step = max_over_ranks(ms, world) / steps
+        out[name] = {"value": round(world * sc.count / (ms_per_step * 1e-3), 1), "ms_per_step": round(ms_per_step, 4)}
+        del cache, solver
+        torch.cuda.synchronize()
+    return out
+
+
+def bench_reference_sph(args, world, rank):
+    """The same SPH workloads through the reference's SPH kernels replayed by the harness."""
+    from oracle import reference
+    from physica_b200 import sph, scenes
+    out = {"unit": UNIT, "config": {"workload": SPH_WORKLOAD, "l2": "flushed between timed steps (256 MiB write)"}}
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    steps = max(3, min(args.steps, 8))
+    for name in SPH_METHODS:
+        sc = scenes.sph_large(seed=6 + rank, method=name)
+        ref = reference.ReferenceSPH(sc, int(sph.Method[name]))
+        x = torch.from_numpy(sc.positions).cuda().contiguous()
+        v = torch.from_numpy(sc.velocities).cuda().contiguous()
+        warm = (torch.zeros(sc.count, device="cuda"), torch.zeros(sc.count, device="cuda"))
+        warm_out = (torch.zeros(sc.count, device="cuda"), torch.zeros(sc.count, device="cuda"))
+        h = {"x": x, "v": v, "xo": torch.zeros_like(x), "vo": torch.zeros_like(v), "k": 0, "w": warm, "wo": warm_out}
+        torch.cuda.synchronize()
+
+        def step():
+            ref.forward_step(h["x"], h["v"], h["xo"], h["vo"], h["k"], warm=h["w"], warm_out=h["wo"], synchronize=False)
+            h["x"], h["xo"], h["v"], h["vo"], h["w"], h["wo"] = h["xo"], h["x"], h["vo"], h["v"], h["wo"], h["w"]
+            h["k"] += 1
+
+        ms, _ = timed(step, steps, args.warmup, world, torch.cuda.ExternalStream(ref.stream), flush)
+        ms_per_step = max_over_ranks(ms, world) / steps
+        out[name] = {"value": round(world * sc.count / (ms_per_step * 1e-3), 1), "ms_per_step": round(ms_per_step, 4)}
+        ref.close()
+        torch.cuda.synchronize()
+    return out
+
+
 def cpu_baseline(sc):
     """FP64 host oracle on all host cores: consecutive substeps of the same 1M workload from its
     initial state until at least 10 s of CPU work (at most 4 substeps)."""
@@ -524,6 +585,7 @@ def bench_reference(args, world, rank):
     value = world * n / (ms_per_step * 1e-3)
     grad = None if args.no_grad else bench_reference_grad(world, rank)
     batched = None if args.no_batch else bench_reference_batch(args, world, rank)
+    sph_family = None if args.no_sph else bench_reference_sph(args, world, rank)
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
@@ -537,7 +599,7 @@ def bench_reference(args, world, rank):
                                    "compiled from its sources) replaying PBF::forward_step on the same B200; the reference "
                                    "has no CPU implementation of this path"},
         "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "clocks": clk.summary(), "grad_steps_per_s": grad, "batched_scenes": batched,
+        "clocks": clk.summary(), "grad_steps_per_s": grad, "batched_scenes": batched, "sph_family": sph_family,
     }
 
 
@@ -660,6 +722,7 @@ def main():
     ap.add_argument("--no-grad", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-sph", action="store_true", help="skip the SPH family's substeps")
     ap.add_argument("--launch-shape", default="", help="fixed list-scan variant and its block size, e.g. "
                                                         "per_lane:128, gather passes at 128 (default: autotuned)")
     args = ap.parse_args()

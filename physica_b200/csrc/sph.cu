@@ -90,6 +90,16 @@ __device__ __forceinline__ void predict(const f3 x, const f3 v, const f3 a, cons
     vo = vel;
 }
 
+// Largest |x* - x| of the particles predicted by one pass, as the bits of a non-negative float
+// (their unsigned order is the float order): a warp maximum, then one atomic per warp.
+__device__ __forceinline__ void record_displacement(unsigned int* word, const f3 predicted, const f3 x) {
+    const float d = __fsqrt_rn(sq_xfirst(sub(predicted, x)));
+    const unsigned int bits = __float_as_uint(d);   // d >= 0 or NaN (NaN bits exceed every finite bound)
+    const unsigned int mask = __activemask();
+    const unsigned int m = __reduce_max_sync(mask, bits);
+    if ((threadIdx.x & 31u) == static_cast<unsigned int>(__ffs(mask) - 1)) atomicMax(word, m);
+}
+
 struct Own {
     Particle p;
     f3 x;
@@ -371,7 +381,7 @@ struct NonPressureOp {
 
 template <bool WithBoundary>
 __global__ void __launch_bounds__(kBlock) non_pressure_kernel(const SphStep st, const int mode, const MutField3 out_positions,
-                                                              const MutField3 out_velocities) {
+                                                              const MutField3 out_velocities, const uint32_t displacement_slot) {
     const Own o = own(st);
     if (!o.p.active) return;
     const uint32_t s = o.p.s;
@@ -398,6 +408,7 @@ __global__ void __launch_bounds__(kBlock) non_pressure_kernel(const SphStep st, 
     predict(o.x, op.v, add(op.acceleration, mk(0.0F, 0.0F, 0.0F)), sc.time_step, sc.box, op.k, xo, vo);
     if (mode == 1) {
         st.predicted[s] = make_float4(xo.x, xo.y, xo.z, o.mass);
+        record_displacement(st.displacement + displacement_slot, xo, o.x);
         return;
     }
     out_positions.x[i] = xo.x;
@@ -419,16 +430,21 @@ struct PredictedDensityOp {
     SphConstants k;
     float density;
 
-    __device__ __forceinline__ void process(const uint32_t t) {
+    __device__ __forceinline__ float4 prefetch(const uint32_t t) const {
+        if (WithBoundary && (t & kBoundaryBit)) return boundary[t & ~kBoundaryBit];
+        return predicted[t];
+    }
+    __device__ __forceinline__ void apply(const uint32_t t, const float4 q) {
         const bool is_boundary = WithBoundary && (t & kBoundaryBit);
-        const float4 q = is_boundary ? boundary[t & ~kBoundaryBit] : predicted[t];
         const float distance = __fsqrt_rn(sq_xfirst(sub(x, xyz(q))));
         if (distance >= k.h) return;
         const float w = cubic_inside(distance, k);
         if (is_boundary) density = __fmaf_rn(__fmul_rn(rest_density, q.w), w, density);
         else density = __fmaf_rn(q.w, w, density);
     }
+    __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
+
 
 template <bool WithBoundary>
 __global__ void __launch_bounds__(kBlock) predicted_density_kernel(const SphStep st, const PressureUpdate update,
@@ -443,7 +459,11 @@ __global__ void __launch_bounds__(kBlock) predicted_density_kernel(const SphStep
     op.rest_density = o.pa.x;
     op.k = *o.k;
     op.density = 0.0F;
-    walk(op, o.p, st.g);
+    // Every pair within h at the predicted positions lies within h + 2 max|x* - x| at the input
+    // positions; when that is inside the list's skin, the list holds all of them in stencil order.
+    const float displacement = __uint_as_float(st.displacement[update.displacement_slot]);
+    if (__fmul_rn(2.0F, displacement) <= o.k->skin_bound) replay(op, o.p, st.g, st.list);
+    else walk(op, o.p, st.g);
     const float predicted_density = op.density;
     if (record) record[s] = predicted_density;
     const float rho = st.aux[s].x;
@@ -539,6 +559,7 @@ __global__ void __launch_bounds__(kBlock) pressure_kernel(const PressureKernelAr
     }
     if (!a.p.last) {
         st.predicted[s] = make_float4(xo.x, xo.y, xo.z, o.mass);
+        record_displacement(st.displacement + a.p.displacement_slot, xo, o.x);
         return;
     }
     a.p.out_positions.x[i] = xo.x;
@@ -575,6 +596,11 @@ __global__ void sph_constants_kernel(const SphSceneInput* __restrict__ inputs, c
     const float contact = __fsqrt_rn(sq_xfirst(mk(k.diameter, 0.0F, 0.0F)));
     k.contact_weight = contact >= h ? 0.0F : cubic_inside(contact, k);
     k.reference_gradient_norm = in.reference_gradient_norm;
+    // Skin of the stored lists: they hold the pairs with sqrtf(r2) < h + skin; the predicted
+    // density replays them while 2 max|x* - x| <= skin_bound, a bound kept 0.1% inside the skin
+    // for the roundings of the distances involved.
+    const float skin = __fmul_rn(in.skin, h);
+    k.skin_bound = __fmul_rn(skin, 0.999F);
     k.box_vx = in.box_vx;
     k.box_vy = in.box_vy;
     k.box_vz = in.box_vz;
@@ -583,7 +609,12 @@ __global__ void sph_constants_kernel(const SphSceneInput* __restrict__ inputs, c
     // The list lists every candidate whose squared distance, in any of the passes' roundings, can
     // fall below the support threshold: a few ulps of margin above it.
     KernelConstants& lc = list_constants[i];
-    lc.list_threshold = __uint_as_float(hi + 8u);
+    if (in.skin > 0.0F) {
+        const float outer = __fadd_ru(h, skin);
+        lc.list_threshold = __uint_as_float(__float_as_uint(__fmul_ru(outer, outer)) + 8u);
+    } else {
+        lc.list_threshold = __uint_as_float(hi + 8u);
+    }
 }
 
 inline unsigned grid_of(const uint32_t n, const unsigned block) { return (n + block - 1u) / block; }
@@ -626,11 +657,15 @@ cudaError_t launch_wcsph_forces(cudaStream_t stream, const SphStep& st, const fl
 }
 
 cudaError_t launch_non_pressure(cudaStream_t stream, const SphStep& st, const int mode, const MutField3 out_positions,
-                                const MutField3 out_velocities, const unsigned block) {
+                                const MutField3 out_velocities, const uint32_t displacement_slot, const unsigned block) {
     if (st.g.count == 0) return cudaSuccess;
     const unsigned b = block_of(block);
-    if (st.g.boundary) non_pressure_kernel<true><<<grid_of(st.g.count, b), b, 0, stream>>>(st, mode, out_positions, out_velocities);
-    else non_pressure_kernel<false><<<grid_of(st.g.count, b), b, 0, stream>>>(st, mode, out_positions, out_velocities);
+    if (st.g.boundary)
+        non_pressure_kernel<true><<<grid_of(st.g.count, b), b, 0, stream>>>(st, mode, out_positions, out_velocities,
+                                                                           displacement_slot);
+    else
+        non_pressure_kernel<false><<<grid_of(st.g.count, b), b, 0, stream>>>(st, mode, out_positions, out_velocities,
+                                                                            displacement_slot);
     count_launch();
     return cudaGetLastError();
 }

@@ -47,8 +47,15 @@ struct SphRecord {
     float* pressure[2] = {nullptr, nullptr};
     float* pressure_term[2] = {nullptr, nullptr};
     float* predicted_density = nullptr;
+    unsigned int* displacement = nullptr;   // max |x* - x| of every prediction of the step
     uint32_t final_pressure = 0;   // which pressure buffer holds the last iterate
 };
+
+// List skin of the iterative methods, as a fraction of h: their predicted densities replay the
+// stored lists instead of walking the stencil while twice the largest predicted displacement
+// stays inside it (always exact: otherwise they walk).
+constexpr float kIterativeSkin = 0.1F;
+constexpr uint32_t kDisplacementSlots = 2u * kMaxIterations + 4u;
 
 class SphEngine {
 public:
@@ -217,7 +224,8 @@ int SphEngine::init(const pbf_domain_configuration* domain, const sph_configurat
                          c.boundary.maximum.y, c.boundary.maximum.z, c.boundary.velocity.x, c.boundary.velocity.y,
                          c.boundary.velocity.z, c.particle_radius, 1u};
     const SphSceneInput in{c.support_radius, c.particle_radius, reference_gradient_norm_, c.boundary.velocity.x,
-                           c.boundary.velocity.y, c.boundary.velocity.z, c.boundary.no_slip ? 1u : 0u};
+                           c.boundary.velocity.y, c.boundary.velocity.z, c.boundary.no_slip ? 1u : 0u,
+                           configuration->method == SPH_METHOD_WCSPH ? 0.0F : kIterativeSkin};
     e = cudaMemcpyAsync(d_scenes_, &d, sizeof(d), cudaMemcpyHostToDevice, stream_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_static_, &st, sizeof(st), cudaMemcpyHostToDevice, stream_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_input, &in, sizeof(in), cudaMemcpyHostToDevice, stream_);
@@ -279,6 +287,7 @@ int SphEngine::allocate(SphRecord& r) {
         r.non_pressure = r.arena.alloc<float4>(n, e);
         r.predicted = r.arena.alloc<float4>(n, e);
         r.predicted_density = r.arena.alloc<float>(n, e);
+        r.displacement = r.arena.alloc<unsigned int>(kDisplacementSlots, e);
         if (config_.method == SPH_METHOD_DFSPH) {
             r.divergence_acceleration = r.arena.alloc<float4>(n, e);
             r.pressure[1] = r.arena.alloc<float>(n, e);
@@ -402,6 +411,7 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
                r.aux,
                r.non_pressure,
                r.predicted,
+               r.displacement,
                r.sorted_index,
                {control->external_accelerations.x, control->external_accelerations.y, control->external_accelerations.z}};
     const unsigned block = shape.block;
@@ -418,12 +428,16 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
                                          r.viscosity_acceleration, r.surface_acceleration, block),
                      "WCSPH forces");
     }
+    // Prediction p of the step records its largest displacement in slot p; the predicted density
+    // that evaluates it reads that slot.
+    if (int rc = check(cudaMemsetAsync(r.displacement, 0, kDisplacementSlots * sizeof(unsigned int), s), "clear")) return rc;
     if (method == SPH_METHOD_PCISPH || method == SPH_METHOD_IISPH) {
         const uint32_t K = config_.pressure_iterations;
         r.final_pressure = 0;
-        if (int rc = check(launch_non_pressure(s, st, K > 0 ? 1 : 2, out_x, out_v, block), "non-pressure acceleration")) return rc;
-        const PressureUpdate update{method, 0u, 0u};
+        if (int rc = check(launch_non_pressure(s, st, K > 0 ? 1 : 2, out_x, out_v, 0u, block), "non-pressure acceleration"))
+            return rc;
         for (uint32_t it = 1; it <= K; ++it) {
+            const PressureUpdate update{method, 0u, 0u, it - 1u};
             if (int rc = check(launch_predicted_density(s, st, update, r.pressure[0], r.pressure_term[0], r.predicted_density, block),
                                "predicted density"))
                 return rc;
@@ -434,17 +448,18 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
             a.out_positions = out_x;
             a.out_velocities = out_v;
             a.store_acceleration = it == K ? r.pressure_acceleration : nullptr;
+            a.displacement_slot = it;
             if (int rc = check(launch_pressure(s, st, a, block), "pressure acceleration")) return rc;
         }
         return PBF_SUCCESS;
     }
     // DFSPH::forward (sph/sph.cpp:572-610): divergence phase on pressure buffer 0, density phase on
     // buffer 1; the divergence phase's last pressure pass also loads the density phase's warm start.
-    if (int rc = check(launch_non_pressure(s, st, 0, out_x, out_v, block), "non-pressure acceleration")) return rc;
+    if (int rc = check(launch_non_pressure(s, st, 0, out_x, out_v, 0u, block), "non-pressure acceleration")) return rc;
     const uint32_t Kd = config_.divergence_iterations, Kr = config_.density_iterations;
     for (uint32_t it = 0; it <= Kd; ++it) {
         if (it > 0) {
-            if (int rc = check(launch_predicted_density(s, st, PressureUpdate{SPH_METHOD_DFSPH, 0u, 1u}, r.pressure[0],
+            if (int rc = check(launch_predicted_density(s, st, PressureUpdate{SPH_METHOD_DFSPH, 0u, 1u, it - 1u}, r.pressure[0],
                                                         r.pressure_term[0], r.predicted_density, block),
                                "predicted density"))
                 return rc;
@@ -454,6 +469,7 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
         a.pressure = r.pressure[0];
         a.out_positions = out_x;
         a.out_velocities = out_v;
+        a.displacement_slot = it;
         if (it == Kd) {
             a.store_acceleration = r.divergence_acceleration;
             a.warm_out = next_method_state->warm_divergence_pressure;
@@ -463,10 +479,11 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
         }
         if (int rc = check(launch_pressure(s, st, a, block), "pressure acceleration")) return rc;
     }
+    const uint32_t density_slots = Kd + 1u;
     for (uint32_t it = 0; it <= Kr; ++it) {
         if (it > 0) {
-            if (int rc = check(launch_predicted_density(s, st, PressureUpdate{SPH_METHOD_DFSPH, 1u, 0u}, r.pressure[1],
-                                                        r.pressure_term[1], r.predicted_density, block),
+            if (int rc = check(launch_predicted_density(s, st, PressureUpdate{SPH_METHOD_DFSPH, 1u, 0u, density_slots + it - 1u},
+                                                        r.pressure[1], r.pressure_term[1], r.predicted_density, block),
                                "predicted density"))
                 return rc;
         }
@@ -476,6 +493,7 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
         a.base = r.divergence_acceleration;
         a.out_positions = out_x;
         a.out_velocities = out_v;
+        a.displacement_slot = density_slots + it;
         if (it == Kr) {
             a.last = 1;
             a.warm_out = next_method_state->warm_density_pressure;

@@ -29,6 +29,7 @@ struct SphConstants {
     float reference_gradient_norm;  // host value of sph/sph.cpp:36-58
     float box_vx, box_vy, box_vz;   // box velocity, written on collision    (sph/common.cu:313-319)
     uint32_t no_slip;
+    float skin_bound;               // the predicted density replays the lists while 2 max|x* - x| <= this
 };
 
 // Sorted per-particle parameters of an SPH step, packed by the grid build:
@@ -48,6 +49,7 @@ struct SphStep {
     float4* aux;                     // (density, viscosity, speed of sound, 0)
     float4* non_pressure;            // non-pressure acceleration (iterative methods)
     float4* predicted;               // (predicted position, mass)
+    unsigned int* displacement;      // per prediction: max |x* - x| (float bits), zeroed every step
     const uint32_t* sorted_index;
     Field3 controls;                 // external accelerations, original order
 };
@@ -70,7 +72,7 @@ cudaError_t launch_wcsph_forces(cudaStream_t stream, const SphStep& st, const fl
 //   mode: 0 acceleration only (DFSPH), 1 also the first predicted positions, 2 the prediction is the
 //   next state (no pressure iteration), written in original order.
 cudaError_t launch_non_pressure(cudaStream_t stream, const SphStep& st, int mode, MutField3 out_positions,
-                                MutField3 out_velocities, unsigned block);
+                                MutField3 out_velocities, uint32_t displacement_slot, unsigned block);
 
 // Predicted density at the predicted positions over the full stencil of the input positions
 // (density::sph_forward(topology = x, positions = x*)), then the method's pressure update.
@@ -79,6 +81,7 @@ struct PressureUpdate {
     uint32_t method;       // kPcisph, kIisph, kDfsph
     uint32_t relaxation;   // 0: params_a.w, 1: params_b.x
     uint32_t target;       // 0 rest density, 1 density
+    uint32_t displacement_slot;   // the prediction this pass evaluates
 };
 cudaError_t launch_predicted_density(cudaStream_t stream, const SphStep& st, PressureUpdate update, float* pressure,
                                      float* pressure_term, float* predicted_density_record, unsigned block);
@@ -102,6 +105,7 @@ struct PressurePassArgs {
     float* next_pressure;
     float* next_pressure_term;
     const float* next_warm;
+    uint32_t displacement_slot;   // where the prediction's max displacement goes (when not last)
 };
 cudaError_t launch_pressure(cudaStream_t stream, const SphStep& st, const PressurePassArgs& a, unsigned block);
 
@@ -111,6 +115,7 @@ struct SphSceneInput {
     float h, particle_radius, reference_gradient_norm;
     float box_vx, box_vy, box_vz;
     uint32_t no_slip;
+    float skin;   // list skin as a fraction of h (0: the lists hold the cubic support only)
 };
 cudaError_t launch_sph_constants(cudaStream_t stream, const SphSceneInput* inputs, uint32_t n, SphConstants* out,
                                  KernelConstants* list_constants);
