@@ -486,13 +486,13 @@ SPH_WORKLOAD = ("sph_dam_break_1m: 1,048,576 particles (128x64x128 lattice, spac
                 "reference's defaults), DFSPH warm start from zero")
 
 
-def bench_sph(args, world, rank):
+def bench_sph(args, world, rank, methods=SPH_METHODS):
     """The SPH family's forward substep (SPH<Method>::forward_step) at 1M particles, one solver per method."""
     from physica_b200 import sph, scenes
     out = {"unit": UNIT, "config": {"workload": SPH_WORKLOAD, "l2": "flushed between timed steps (256 MiB write)"}}
     flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     steps = max(3, min(args.steps, 8))
-    for name in SPH_METHODS:
+    for name in methods:
         sc = scenes.sph_large(seed=6 + rank, method=name)
         solver, state, control, params = sph.solver_for_scene(sc, sph.Method[name])
         cache = solver.allocate_step_cache()
@@ -510,14 +510,14 @@ def bench_sph(args, world, rank):
     return out
 
 
-def bench_reference_sph(args, world, rank):
+def bench_reference_sph(args, world, rank, methods=SPH_METHODS):
     """The same SPH workloads through the reference's SPH kernels replayed by the harness."""
     from oracle import reference
     from physica_b200 import sph, scenes
     out = {"unit": UNIT, "config": {"workload": SPH_WORKLOAD, "l2": "flushed between timed steps (256 MiB write)"}}
     flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     steps = max(3, min(args.steps, 8))
-    for name in SPH_METHODS:
+    for name in methods:
         sc = scenes.sph_large(seed=6 + rank, method=name)
         ref = reference.ReferenceSPH(sc, int(sph.Method[name]))
         x = torch.from_numpy(sc.positions).cuda().contiguous()
@@ -723,13 +723,19 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-sph", action="store_true", help="skip the SPH family's substeps")
+    ap.add_argument("--sph-only", default="", help="time only these SPH methods (comma list, e.g. pcisph) and print "
+                                                   "their line (profiling)")
     ap.add_argument("--launch-shape", default="", help="fixed list-scan variant and its block size, e.g. "
                                                         "per_lane:128, gather passes at 128 (default: autotuned)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = setup_dist()
-    if args.impl == "reference":
+    if args.sph_only:
+        methods = tuple(m for m in args.sph_only.split(",") if m)
+        run = bench_reference_sph if args.impl == "reference" else bench_sph
+        out = {"impl": args.impl, "sph_family": run(args, world, rank, methods)}
+    elif args.impl == "reference":
         out = bench_reference(args, world, rank)
     else:
         out = bench_b200(args, world, rank)
