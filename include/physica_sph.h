@@ -11,8 +11,8 @@
  * The domain description is the PBF one (pbf_domain_configuration: the reference's
  * DomainConfiguration is shared by both families, domain/domain.ixx:12-165).
  *
- * Forward mode only: SPH<Method>::jvp_step and ::vjp_step (sph/sph.ixx:356-365) are not provided
- * by this library; sph_create rejects PBF_EXECUTION_DIFFERENTIABLE with PBF_ERROR_UNSUPPORTED.
+ * Differentiable mode (PBF_EXECUTION_DIFFERENTIABLE) adds SPH<Method>::vjp_step
+ * (sph/sph.ixx:361-365): FP64 adjoints, accumulated like the PBF ones.
  */
 #ifndef PHYSICA_SPH_H
 #define PHYSICA_SPH_H
@@ -69,6 +69,28 @@ typedef struct {
     float* warm_density_pressure;
 } sph_method_state;
 
+/* SPH<Method>::ParameterAdjoint (sph/sph.ixx:295-298): FP64, one array per parameter, ACCUMULATED.
+ * Arrays of the other methods may be NULL. */
+typedef struct {
+    double* masses;
+    double* rest_densities;
+    double* viscosities;
+    double* surface_tensions;
+    double* speed_of_sound;             /* WCSPH */
+    double* tait_exponent;              /* WCSPH */
+    double* boundary_surface_tension;   /* WCSPH */
+    double* pressure_relaxation;        /* PCISPH */
+    double* jacobi_relaxation;          /* IISPH */
+    double* divergence_relaxation;      /* DFSPH */
+    double* density_relaxation;         /* DFSPH */
+} sph_parameter_adjoint;
+
+/* Method::StateAdjoint (sph/sph.ixx:210-213): DFSPH's warm-start pressure adjoints (FP64). */
+typedef struct {
+    double* warm_divergence_pressure;
+    double* warm_density_pressure;
+} sph_method_state_adjoint;
+
 typedef struct sph_solver sph_solver;           /* SPH<Method> (sph/sph.ixx:273-372) */
 typedef struct sph_step_cache sph_step_cache;   /* SPH<Method>::StepCache (sph/sph.ixx:299-303) */
 
@@ -98,6 +120,19 @@ int sph_free_step_cache(sph_solver* solver, sph_step_cache* cache);
 int sph_forward_step(sph_solver* solver, const pbf_particle_state* state, const sph_method_state* method_state,
                      const pbf_control* control, const sph_parameters* parameters, pbf_particle_state* next_state,
                      sph_method_state* next_method_state, sph_step_cache* cache);
+
+/* SPH<Method>::vjp_step (sph/sph.ixx:361-365): the adjoint of the step recorded in `cache` (the
+ * forward_step of `state`), solver in PBF_EXECUTION_DIFFERENTIABLE mode.  previous_adjoint,
+ * control_adjoint and parameter_adjoint are ACCUMULATED.  DFSPH: next_method_adjoint holds the
+ * adjoints of the next warm-start pressures (NULL = zero); previous_method_adjoint receives those of
+ * the input warm starts, overwritten when the configuration warm-starts (sph/sph.cpp:714).
+ * next_state is accepted for the reference's signature and not read. */
+int sph_vjp_step(sph_solver* solver, const pbf_particle_state* state, const sph_method_state* method_state,
+                 const pbf_control* control, const sph_parameters* parameters, const pbf_particle_state* next_state,
+                 const sph_step_cache* cache, const pbf_particle_state_adjoint* next_adjoint,
+                 const sph_method_state_adjoint* next_method_adjoint, pbf_particle_state_adjoint* previous_adjoint,
+                 sph_method_state_adjoint* previous_method_adjoint, pbf_control_adjoint* control_adjoint,
+                 sph_parameter_adjoint* parameter_adjoint);
 
 /* A field of the step held by `cache`, written to device memory in original particle order
  * (x only for scalar fields). */

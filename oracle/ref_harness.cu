@@ -634,48 +634,116 @@ float sph_reference_gradient_norm(const float support_radius, const float partic
     return gx * gx + gy * gy + gz * gz + squared;
 }
 
+// PressureIterationCache / Tangent / Adjoint (sph/sph.ixx:14-37)
+struct IterCache {
+    uint32_t iteration = 0;
+    float* pressures = nullptr;
+    float* predicted_densities = nullptr;
+    Vec pressure_acc, predicted_positions, predicted_velocities;
+};
+struct IterTangent {
+    float* pressures = nullptr;
+    float* predicted_densities = nullptr;
+    Vec pressure_acc, predicted_positions, predicted_velocities;
+};
+struct IterAdjoint {
+    double* pressures = nullptr;
+    double* predicted_densities = nullptr;
+    DVec pressure_acc, predicted_positions, predicted_velocities;
+};
+
 struct SphReplay {
     Harness* h = nullptr;
     int method = 0;   // 0 WCSPH, 1 PCISPH, 2 IISPH, 3 DFSPH
-    uint32_t pressure_iterations = 6, divergence_iterations = 4, density_iterations = 6;
+    uint32_t pressure_iterations = 6, divergence_iterations = 4, density_iterations = 6, checkpoint_interval = 2;
     int warm_start = 1;
+    bool differentiable = false;
     float reference_gradient_norm = 0.0F;
     std::vector<void*> allocations;
     float* densities = nullptr;
     // WCSPH::Cache (sph/sph.ixx:63-70)
     float* pressures = nullptr;
     Vec pressure_acc, viscosity_acc, surface_acc, external_acc, total_acc;
-    // PressureIterationCache `primal` and the iterative methods' caches (sph/sph.ixx:14-21, 114-117, 160-163, 226-232)
-    Vec non_pressure_acc, primal_pressure_acc, predicted_positions, predicted_velocities, divergence_pressure_acc,
-        total_pressure_acc, total_pressure_acceleration;
-    float *primal_pressures = nullptr, *predicted_densities = nullptr;
+    // the iterative methods' caches (sph/sph.ixx:114-117, 160-163, 226-232) and members
+    Vec non_pressure_acc, divergence_pressure_acc, total_pressure_acc, total_pressure_acceleration;
+    IterCache primal;
+    std::vector<IterCache> checkpoints, divergence_checkpoints, density_checkpoints, recomputed;
+    // differentiation workspaces (sph/sph.ixx:71-79, 119-125, 235-246, 306-308)
+    float* density_tangent = nullptr;
+    double* density_adjoint = nullptr;
+    float* pressure_tangent = nullptr;
+    Vec pressure_acc_tangent, viscosity_acc_tangent, surface_acc_tangent, total_acc_tangent;
+    double* pressure_adjoint = nullptr;
+    DVec total_acc_adjoint;
+    IterTangent tangent;
+    IterAdjoint adjoint, previous_adjoint;
+    Vec non_pressure_acc_tangent, divergence_pressure_acc_tangent, total_pressure_acc_tangent;
+    DVec non_pressure_acc_adjoint, divergence_pressure_acc_adjoint, total_pressure_acc_adjoint;
+    double* target_density_adjoint = nullptr;
 
     template <class T>
     T* alloc(size_t n) {
         void* p = nullptr;
-        if (cudaMalloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        if (cudaMalloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) {
+            allocations.push_back(nullptr);
+            return nullptr;
+        }
         allocations.push_back(p);
         return static_cast<T*>(p);
     }
-    Vec vec() { const size_t n = h->cfg.particle_count; return {alloc<float>(n), alloc<float>(n), alloc<float>(n)}; }
+    size_t n() const { return h->cfg.particle_count; }
+    Vec vec() { return {alloc<float>(n()), alloc<float>(n()), alloc<float>(n())}; }
+    DVec dvec() { return {alloc<double>(n()), alloc<double>(n()), alloc<double>(n())}; }
+    IterCache iter() { return {0u, alloc<float>(n()), alloc<float>(n()), vec(), vec(), vec()}; }
+    IterTangent iter_tangent() { return {alloc<float>(n()), alloc<float>(n()), vec(), vec(), vec()}; }
+    IterAdjoint iter_adjoint() { return {alloc<double>(n()), alloc<double>(n()), dvec(), dvec(), dvec()}; }
     ~SphReplay() {
         if (h) cudaStreamSynchronize(h->stream);
-        for (void* p : allocations) cudaFree(p);
+        for (void* p : allocations)
+            if (p) cudaFree(p);
     }
-    void clear(float* p) const { cudaMemsetAsync(p, 0, h->cfg.particle_count * sizeof(float), h->stream); }
+    void clear(float* p) const { cudaMemsetAsync(p, 0, n() * sizeof(float), h->stream); }
+    void clear(double* p) const { cudaMemsetAsync(p, 0, n() * sizeof(double), h->stream); }
     void clear(const Vec& v) const { clear(v.x); clear(v.y); clear(v.z); }
+    void clear(const DVec& v) const { clear(v.x); clear(v.y); clear(v.z); }
     void copy(const float* src, float* dst) const {
-        cudaMemcpyAsync(dst, src, h->cfg.particle_count * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(dst, src, n() * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
     }
-    // clear_iteration (sph/sph.cpp:91-97)
-    void clear_primal() const {
-        clear(primal_pressures);
-        clear(predicted_densities);
-        clear(primal_pressure_acc);
-        clear(predicted_positions);
-        clear(predicted_velocities);
+    void copy(const double* src, double* dst) const {
+        cudaMemcpyAsync(dst, src, n() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
+    }
+    void copy(const Vec& a, const Vec& b) const { copy(a.x, b.x); copy(a.y, b.y); copy(a.z, b.z); }
+    void copy(const DVec& a, const DVec& b) const { copy(a.x, b.x); copy(a.y, b.y); copy(a.z, b.z); }
+    // clear_iteration / copy_iteration (sph/sph.cpp:91-126)
+    void clear(IterCache& c) const {
+        clear(c.pressures); clear(c.predicted_densities); clear(c.pressure_acc); clear(c.predicted_positions);
+        clear(c.predicted_velocities);
+    }
+    void clear(IterTangent& c) const {
+        clear(c.pressures); clear(c.predicted_densities); clear(c.pressure_acc); clear(c.predicted_positions);
+        clear(c.predicted_velocities);
+    }
+    void clear(IterAdjoint& c) const {
+        clear(c.pressures); clear(c.predicted_densities); clear(c.pressure_acc); clear(c.predicted_positions);
+        clear(c.predicted_velocities);
+    }
+    void copy(const IterCache& a, IterCache& b) const {
+        b.iteration = a.iteration;
+        copy(a.pressures, b.pressures); copy(a.predicted_densities, b.predicted_densities); copy(a.pressure_acc, b.pressure_acc);
+        copy(a.predicted_positions, b.predicted_positions); copy(a.predicted_velocities, b.predicted_velocities);
+    }
+    // Method::allocate_cache: checkpoints at 0, every interval and the last iteration (sph/sph.cpp:282-288)
+    std::vector<IterCache> checkpoint_set(const uint32_t iterations) {
+        const uint32_t ci = checkpoint_interval;
+        const uint32_t count = 1u + iterations / ci + (iterations % ci == 0u ? 0u : 1u);
+        std::vector<IterCache> out;
+        for (uint32_t k = 0; k < count; ++k) out.push_back(iter());
+        return out;
     }
 };
+
+cd::ParticleParameterTangentView tangent_view(const float* const* p) { return {p[0], p[1], p[2], p[3]}; }
+cd::ParticleParameterAdjointView adjoint_view(double* const* p) { return {p[0], p[1], p[2], p[3]}; }
 
 }  // namespace
 
@@ -687,6 +755,8 @@ typedef struct {
     uint32_t divergence_iterations;   // DFSPH
     uint32_t density_iterations;      // DFSPH
     int pressure_warm_start;          // DFSPH
+    uint32_t checkpoint_interval;     // differentiable mode
+    int differentiable;
 } ref_sph_config;
 
 // ParticleParameters (masses, rest densities, viscosities, surface tensions) and the method's
@@ -706,8 +776,10 @@ int ref_sph_create(void* harness, const ref_sph_config* c, void** out) {
     r->divergence_iterations = c->divergence_iterations;
     r->density_iterations = c->density_iterations;
     r->warm_start = c->pressure_warm_start;
+    r->checkpoint_interval = c->checkpoint_interval ? c->checkpoint_interval : 2u;
+    r->differentiable = c->differentiable != 0;
     r->reference_gradient_norm = sph_reference_gradient_norm(r->h->cfg.support_radius, r->h->cfg.particle_radius);
-    const size_t n = r->h->cfg.particle_count;
+    const size_t n = r->n();
     r->densities = r->alloc<float>(n);
     if (r->method == 0) {
         r->pressures = r->alloc<float>(n);
@@ -718,15 +790,42 @@ int ref_sph_create(void* harness, const ref_sph_config* c, void** out) {
         r->total_acc = r->vec();
     } else {
         r->non_pressure_acc = r->vec();
-        r->primal_pressures = r->alloc<float>(n);
-        r->predicted_densities = r->alloc<float>(n);
-        r->primal_pressure_acc = r->vec();
-        r->predicted_positions = r->vec();
-        r->predicted_velocities = r->vec();
+        r->primal = r->iter();
         if (r->method == 3) {
             r->divergence_pressure_acc = r->vec();
             r->total_pressure_acc = r->vec();
             r->total_pressure_acceleration = r->vec();
+            r->divergence_checkpoints = r->checkpoint_set(r->divergence_iterations);
+            r->density_checkpoints = r->checkpoint_set(r->density_iterations);
+        } else {
+            r->checkpoints = r->checkpoint_set(r->pressure_iterations);
+        }
+    }
+    if (r->differentiable) {
+        r->density_tangent = r->alloc<float>(n);
+        r->density_adjoint = r->alloc<double>(n);
+        if (r->method == 0) {
+            r->pressure_tangent = r->alloc<float>(n);
+            r->pressure_acc_tangent = r->vec();
+            r->viscosity_acc_tangent = r->vec();
+            r->surface_acc_tangent = r->vec();
+            r->total_acc_tangent = r->vec();
+            r->pressure_adjoint = r->alloc<double>(n);
+            r->total_acc_adjoint = r->dvec();
+        } else {
+            for (uint32_t k = 0; k <= r->checkpoint_interval; ++k) r->recomputed.push_back(r->iter());
+            r->tangent = r->iter_tangent();
+            r->adjoint = r->iter_adjoint();
+            r->previous_adjoint = r->iter_adjoint();
+            r->non_pressure_acc_tangent = r->vec();
+            r->non_pressure_acc_adjoint = r->dvec();
+            if (r->method == 3) {
+                r->divergence_pressure_acc_tangent = r->vec();
+                r->total_pressure_acc_tangent = r->vec();
+                r->target_density_adjoint = r->alloc<double>(n);
+                r->divergence_pressure_acc_adjoint = r->dvec();
+                r->total_pressure_acc_adjoint = r->dvec();
+            }
         }
     }
     for (void* p : r->allocations)
@@ -780,6 +879,7 @@ int ref_sph_forward_step(void* sph, const ref_state_in* state, const float* cons
     cd::sph::non_pressure_forward(s, n, hr, h->cfg.gravity[0], h->cfg.gravity[1], h->cfg.gravity[2], x, v, a, pv,
                                   h->neighborhood(), h->boundary(), r->densities, h->mv(r->non_pressure_acc));
     const float rgn = r->reference_gradient_norm;
+    IterCache& pr = r->primal;
     auto predict = [&](const Vec& pressure_acc, const cd::VectorView<float> px, const cd::VectorView<float> pvv) {
         if (r->method == 1)
             cd::pcisph::launch_predict_forward(s, n, dt, box, x, v, h->cv(r->non_pressure_acc), h->cv(pressure_acc), px, pvv);
@@ -789,60 +889,416 @@ int ref_sph_forward_step(void* sph, const ref_state_in* state, const float* cons
             cd::dfsph::launch_predict_forward(s, n, dt, box, x, v, h->cv(r->non_pressure_acc), h->cv(pressure_acc), px, pvv);
     };
     auto pressure = [&]() {
-        cd::sph::pressure_forward(s, n, hr, x, pv, h->neighborhood(), h->boundary(), r->densities, r->primal_pressures,
-                                  h->mv(r->primal_pressure_acc));
+        cd::sph::pressure_forward(s, n, hr, x, pv, h->neighborhood(), h->boundary(), r->densities, pr.pressures,
+                                  h->mv(pr.pressure_acc));
     };
     auto predicted_density = [&]() {
-        cd::density_forward(s, n, hr, false, x, h->cv(r->predicted_positions), pv, h->neighborhood(), h->boundary(),
-                            r->predicted_densities);
+        cd::density_forward(s, n, hr, false, x, h->cv(pr.predicted_positions), pv, h->neighborhood(), h->boundary(),
+                            pr.predicted_densities);
+    };
+    auto checkpoint = [&](std::vector<IterCache>& set, size_t& next_checkpoint, const uint32_t it, const uint32_t last) {
+        if (it == 0u || it % r->checkpoint_interval == 0u || it == last) r->copy(pr, set[next_checkpoint++]);
     };
     if (r->method == 1 || r->method == 2) {   // PCISPH::forward / IISPH::forward (sph/sph.cpp:296-312, 409-425)
-        r->clear_primal();
+        r->clear(pr);
+        pr.iteration = 0u;
+        size_t c = 0;
+        checkpoint(r->checkpoints, c, 0u, r->pressure_iterations);
         for (uint32_t it = 1; it <= r->pressure_iterations; ++it) {
-            predict(r->primal_pressure_acc, h->mv(r->predicted_positions), h->mv(r->predicted_velocities));
+            predict(pr.pressure_acc, h->mv(pr.predicted_positions), h->mv(pr.predicted_velocities));
             predicted_density();
             if (r->method == 1)
-                cd::pcisph::launch_pressure_update_forward(s, n, dt, rgn, pv, r->primal_pressures, r->predicted_densities,
-                                                           p->method0, r->primal_pressures);
+                cd::pcisph::launch_pressure_update_forward(s, n, dt, rgn, pv, pr.pressures, pr.predicted_densities, p->method0,
+                                                           pr.pressures);
             else
-                cd::iisph::launch_jacobi_update_forward(s, n, dt, rgn, pv, r->densities, r->primal_pressures,
-                                                        r->predicted_densities, p->method0, r->primal_pressures);
+                cd::iisph::launch_jacobi_update_forward(s, n, dt, rgn, pv, r->densities, pr.pressures, pr.predicted_densities,
+                                                        p->method0, pr.pressures);
             pressure();
+            pr.iteration = it;
+            checkpoint(r->checkpoints, c, it, r->pressure_iterations);
         }
-        predict(r->primal_pressure_acc, xo, vo);
+        predict(pr.pressure_acc, xo, vo);
         return cudaGetLastError() == cudaSuccess ? 0 : 3;
     }
     // DFSPH::forward (sph/sph.cpp:572-610)
-    r->clear_primal();
-    if (r->warm_start) r->copy(warm_divergence, r->primal_pressures);
+    r->clear(pr);
+    if (r->warm_start) r->copy(warm_divergence, pr.pressures);
     pressure();
+    pr.iteration = 0u;
+    size_t c = 0;
+    checkpoint(r->divergence_checkpoints, c, 0u, r->divergence_iterations);
     for (uint32_t it = 1; it <= r->divergence_iterations; ++it) {
-        predict(r->primal_pressure_acc, h->mv(r->predicted_positions), h->mv(r->predicted_velocities));
+        predict(pr.pressure_acc, h->mv(pr.predicted_positions), h->mv(pr.predicted_velocities));
         predicted_density();
-        cd::dfsph::launch_projection_update_forward(s, n, dt, rgn, pv, r->densities, r->densities, r->primal_pressures,
-                                                    r->predicted_densities, p->method0, r->primal_pressures);
+        cd::dfsph::launch_projection_update_forward(s, n, dt, rgn, pv, r->densities, r->densities, pr.pressures,
+                                                    pr.predicted_densities, p->method0, pr.pressures);
         pressure();
+        pr.iteration = it;
+        checkpoint(r->divergence_checkpoints, c, it, r->divergence_iterations);
     }
-    for (int c = 0; c < 3; ++c) {
-        const float* src[3] = {r->primal_pressure_acc.x, r->primal_pressure_acc.y, r->primal_pressure_acc.z};
-        float* dst[3] = {r->divergence_pressure_acc.x, r->divergence_pressure_acc.y, r->divergence_pressure_acc.z};
-        r->copy(src[c], dst[c]);
-    }
-    r->copy(r->primal_pressures, next_warm_divergence);
-    r->clear_primal();
-    if (r->warm_start) r->copy(warm_density, r->primal_pressures);
+    r->copy(pr.pressure_acc, r->divergence_pressure_acc);
+    r->copy(pr.pressures, next_warm_divergence);
+    r->clear(pr);
+    if (r->warm_start) r->copy(warm_density, pr.pressures);
     pressure();
+    pr.iteration = 0u;
+    c = 0;
+    checkpoint(r->density_checkpoints, c, 0u, r->density_iterations);
     for (uint32_t it = 1; it <= r->density_iterations; ++it) {
-        cd::sph::add(s, n, h->cv(r->divergence_pressure_acc), h->cv(r->primal_pressure_acc), h->mv(r->total_pressure_acceleration));
-        predict(r->total_pressure_acceleration, h->mv(r->predicted_positions), h->mv(r->predicted_velocities));
+        cd::sph::add(s, n, h->cv(r->divergence_pressure_acc), h->cv(pr.pressure_acc), h->mv(r->total_pressure_acceleration));
+        predict(r->total_pressure_acceleration, h->mv(pr.predicted_positions), h->mv(pr.predicted_velocities));
         predicted_density();
-        cd::dfsph::launch_projection_update_forward(s, n, dt, rgn, pv, r->densities, p->rest_densities, r->primal_pressures,
-                                                    r->predicted_densities, p->method1, r->primal_pressures);
+        cd::dfsph::launch_projection_update_forward(s, n, dt, rgn, pv, r->densities, p->rest_densities, pr.pressures,
+                                                    pr.predicted_densities, p->method1, pr.pressures);
+        pressure();
+        pr.iteration = it;
+        checkpoint(r->density_checkpoints, c, it, r->density_iterations);
+    }
+    cd::sph::add(s, n, h->cv(r->divergence_pressure_acc), h->cv(pr.pressure_acc), h->mv(r->total_pressure_acc));
+    r->copy(pr.pressures, next_warm_density);
+    predict(r->total_pressure_acc, xo, vo);
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+// SPH<Method>::jvp_step (sph/sph.ixx:356-359) after ref_sph_forward_step of the same state.
+//   tangent: state tangent (SoA); control_tangent[3]; particle_tangent[4] (masses, rest densities,
+//   viscosities, surface tensions); method_tangent[3] (the method's parameters, as in ref_sph_params);
+//   warm_tangent[2] / next_warm_tangent[2]: DFSPH's method-state tangents.
+int ref_sph_jvp_step(void* sph, const ref_state_in* state, const ref_sph_params* p, const ref_state_in* tangent,
+                     const float* const* control_tangent, const float* const* particle_tangent,
+                     const float* const* method_tangent, const float* const* warm_tangent, const ref_state_out* next_tangent,
+                     float* const* next_warm_tangent, const uint64_t step_index, const float* warm_divergence,
+                     const float* warm_density) {
+    auto* r = static_cast<SphReplay*>(sph);
+    if (!r->differentiable) return 1;
+    Harness* h = r->h;
+    const ::cuda::stream_ref s{h->stream};
+    const uint32_t n = h->cfg.particle_count;
+    const float hr = h->cfg.support_radius;
+    const float dt = h->cfg.time_step;
+    const cd::ConstVectorView<float> x{state->px, state->py, state->pz}, v{state->vx, state->vy, state->vz};
+    const cd::ConstVectorView<float> xt{tangent->px, tangent->py, tangent->pz}, vt{tangent->vx, tangent->vy, tangent->vz};
+    const cd::ConstVectorView<float> at{control_tangent[0], control_tangent[1], control_tangent[2]};
+    const cd::VectorView<float> xo{next_tangent->px, next_tangent->py, next_tangent->pz},
+        vo{next_tangent->vx, next_tangent->vy, next_tangent->vz};
+    const cd::ParticleParameterView pv{p->masses, p->rest_densities, p->viscosities, p->surface_tensions};
+    const cd::ParticleParameterTangentView pt = tangent_view(particle_tangent);
+    const cd::Box box = h->collision_box(step_index);
+    const auto nb = h->neighborhood();
+    const auto bd = h->boundary();
+    cd::density_jvp(s, n, hr, false, x, x, xt, pv, pt, nb, bd, r->density_tangent);
+    const float* rho = r->densities;
+    const float* rho_t = r->density_tangent;
+    if (r->method == 0) {   // WCSPH::jvp (sph/sph.cpp:227-237)
+        namespace w = cd::wcsph;
+        w::launch_eos_jvp(s, n, rho, rho_t, pv, pt, p->method0, method_tangent[0], p->method1, method_tangent[1], r->pressure_tangent);
+        cd::sph::pressure_jvp(s, n, hr, x, xt, pv, pt, nb, bd, rho, rho_t, r->pressures, r->pressure_tangent,
+                              h->mv(r->pressure_acc_tangent));
+        w::launch_artificial_viscosity_jvp(s, n, hr, x, v, xt, vt, pv, pt, p->method0, method_tangent[0], nb, bd, rho, rho_t,
+                                           h->mv(r->viscosity_acc_tangent));
+        w::launch_surface_jvp(s, n, hr, h->cfg.particle_radius, x, xt, pv, pt, p->method2, method_tangent[2], nb, bd,
+                              h->mv(r->surface_acc_tangent));
+        cd::sph::add(s, n, h->cv(r->pressure_acc_tangent), h->cv(r->viscosity_acc_tangent), h->mv(r->total_acc_tangent));
+        cd::sph::add(s, n, h->cv(r->total_acc_tangent), h->cv(r->surface_acc_tangent), h->mv(r->total_acc_tangent));
+        cd::sph::add(s, n, h->cv(r->total_acc_tangent), at, h->mv(r->total_acc_tangent));
+        cd::sph::integrate_jvp(s, n, dt, box, x, v, h->cv(r->total_acc), xt, vt, h->cv(r->total_acc_tangent), xo, vo);
+        return cudaGetLastError() == cudaSuccess ? 0 : 3;
+    }
+    const float rgn = r->reference_gradient_norm;
+    IterCache& pr = r->primal;
+    IterTangent& tg = r->tangent;
+    cd::sph::non_pressure_jvp(s, n, hr, x, v, at, xt, vt, pv, pt, nb, bd, rho, rho_t, h->mv(r->non_pressure_acc_tangent));
+    auto predict = [&](const Vec& pressure_acc, const cd::VectorView<float> px, const cd::VectorView<float> pvv) {
+        if (r->method == 1)
+            cd::pcisph::launch_predict_forward(s, n, dt, box, x, v, h->cv(r->non_pressure_acc), h->cv(pressure_acc), px, pvv);
+        else if (r->method == 2)
+            cd::iisph::launch_predict_forward(s, n, dt, box, x, v, h->cv(r->non_pressure_acc), h->cv(pressure_acc), px, pvv);
+        else
+            cd::dfsph::launch_predict_forward(s, n, dt, box, x, v, h->cv(r->non_pressure_acc), h->cv(pressure_acc), px, pvv);
+    };
+    auto predict_jvp = [&](const Vec& pressure_acc, const Vec& pressure_acc_tangent, const cd::VectorView<float> px,
+                           const cd::VectorView<float> pvv) {
+        const auto anp = h->cv(r->non_pressure_acc);
+        const auto anpt = h->cv(r->non_pressure_acc_tangent);
+        if (r->method == 1)
+            cd::pcisph::launch_predict_jvp(s, n, dt, box, x, v, anp, h->cv(pressure_acc), xt, vt, anpt, h->cv(pressure_acc_tangent), px, pvv);
+        else if (r->method == 2)
+            cd::iisph::launch_predict_jvp(s, n, dt, box, x, v, anp, h->cv(pressure_acc), xt, vt, anpt, h->cv(pressure_acc_tangent), px, pvv);
+        else
+            cd::dfsph::launch_predict_jvp(s, n, dt, box, x, v, anp, h->cv(pressure_acc), xt, vt, anpt, h->cv(pressure_acc_tangent), px, pvv);
+    };
+    auto pressure = [&]() {
+        cd::sph::pressure_forward(s, n, hr, x, pv, nb, bd, rho, pr.pressures, h->mv(pr.pressure_acc));
+    };
+    auto pressure_jvp = [&]() {
+        cd::sph::pressure_jvp(s, n, hr, x, xt, pv, pt, nb, bd, rho, rho_t, pr.pressures, tg.pressures, h->mv(tg.pressure_acc));
+    };
+    auto densities_at_prediction = [&]() {
+        cd::density_forward(s, n, hr, false, x, h->cv(pr.predicted_positions), pv, nb, bd, pr.predicted_densities);
+        cd::density_jvp(s, n, hr, false, x, h->cv(pr.predicted_positions), h->cv(tg.predicted_positions), pv, pt, nb, bd,
+                        tg.predicted_densities);
+    };
+    if (r->method == 1 || r->method == 2) {   // PCISPH::jvp / IISPH::jvp (sph/sph.cpp:314-330, 427-443)
+        r->clear(pr);
+        r->clear(tg);
+        for (uint32_t it = 1; it <= r->pressure_iterations; ++it) {
+            predict(pr.pressure_acc, h->mv(pr.predicted_positions), h->mv(pr.predicted_velocities));
+            predict_jvp(pr.pressure_acc, tg.pressure_acc, h->mv(tg.predicted_positions), h->mv(tg.predicted_velocities));
+            densities_at_prediction();
+            if (r->method == 1) {
+                cd::pcisph::launch_pressure_update_jvp(s, n, dt, rgn, pv, pt, pr.pressures, pr.predicted_densities, p->method0,
+                                                       tg.pressures, tg.predicted_densities, method_tangent[0], tg.pressures);
+                cd::pcisph::launch_pressure_update_forward(s, n, dt, rgn, pv, pr.pressures, pr.predicted_densities, p->method0,
+                                                           pr.pressures);
+            } else {
+                cd::iisph::launch_jacobi_update_jvp(s, n, dt, rgn, pv, pt, rho, rho_t, pr.pressures, pr.predicted_densities,
+                                                    p->method0, tg.pressures, tg.predicted_densities, method_tangent[0],
+                                                    tg.pressures);
+                cd::iisph::launch_jacobi_update_forward(s, n, dt, rgn, pv, rho, pr.pressures, pr.predicted_densities, p->method0,
+                                                        pr.pressures);
+            }
+            pressure_jvp();
+            pressure();
+        }
+        predict_jvp(pr.pressure_acc, tg.pressure_acc, xo, vo);
+        return cudaGetLastError() == cudaSuccess ? 0 : 3;
+    }
+    // DFSPH::jvp (sph/sph.cpp:612-659)
+    r->clear(pr);
+    r->clear(tg);
+    if (r->warm_start) {
+        r->copy(warm_divergence, pr.pressures);
+        r->copy(warm_tangent[0], tg.pressures);
+    }
+    pressure();
+    pressure_jvp();
+    for (uint32_t it = 1; it <= r->divergence_iterations; ++it) {
+        predict(pr.pressure_acc, h->mv(pr.predicted_positions), h->mv(pr.predicted_velocities));
+        predict_jvp(pr.pressure_acc, tg.pressure_acc, h->mv(tg.predicted_positions), h->mv(tg.predicted_velocities));
+        densities_at_prediction();
+        cd::dfsph::launch_projection_update_jvp(s, n, dt, rgn, pv, pt, rho, rho_t, rho, rho_t, pr.pressures, pr.predicted_densities,
+                                                p->method0, tg.pressures, tg.predicted_densities, method_tangent[0], tg.pressures);
+        cd::dfsph::launch_projection_update_forward(s, n, dt, rgn, pv, rho, rho, pr.pressures, pr.predicted_densities, p->method0,
+                                                    pr.pressures);
+        pressure_jvp();
         pressure();
     }
-    cd::sph::add(s, n, h->cv(r->divergence_pressure_acc), h->cv(r->primal_pressure_acc), h->mv(r->total_pressure_acc));
-    r->copy(r->primal_pressures, next_warm_density);
-    predict(r->total_pressure_acc, xo, vo);
+    r->copy(tg.pressure_acc, r->divergence_pressure_acc_tangent);
+    r->copy(tg.pressures, next_warm_tangent[0]);
+    r->clear(pr);
+    r->clear(tg);
+    if (r->warm_start) {
+        r->copy(warm_density, pr.pressures);
+        r->copy(warm_tangent[1], tg.pressures);
+    }
+    pressure();
+    pressure_jvp();
+    for (uint32_t it = 1; it <= r->density_iterations; ++it) {
+        cd::sph::add(s, n, h->cv(r->divergence_pressure_acc), h->cv(pr.pressure_acc), h->mv(r->total_pressure_acceleration));
+        cd::sph::add(s, n, h->cv(r->divergence_pressure_acc_tangent), h->cv(tg.pressure_acc), h->mv(r->total_pressure_acc_tangent));
+        predict(r->total_pressure_acceleration, h->mv(pr.predicted_positions), h->mv(pr.predicted_velocities));
+        predict_jvp(r->total_pressure_acceleration, r->total_pressure_acc_tangent, h->mv(tg.predicted_positions),
+                    h->mv(tg.predicted_velocities));
+        densities_at_prediction();
+        cd::dfsph::launch_projection_update_jvp(s, n, dt, rgn, pv, pt, rho, rho_t, p->rest_densities, pt.rest_densities,
+                                                pr.pressures, pr.predicted_densities, p->method1, tg.pressures,
+                                                tg.predicted_densities, method_tangent[1], tg.pressures);
+        cd::dfsph::launch_projection_update_forward(s, n, dt, rgn, pv, rho, p->rest_densities, pr.pressures, pr.predicted_densities,
+                                                    p->method1, pr.pressures);
+        pressure_jvp();
+        pressure();
+    }
+    cd::sph::add(s, n, h->cv(r->divergence_pressure_acc_tangent), h->cv(tg.pressure_acc), h->mv(r->total_pressure_acc_tangent));
+    r->copy(tg.pressures, next_warm_tangent[1]);
+    predict_jvp(r->total_pressure_acc, r->total_pressure_acc_tangent, xo, vo);
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+// SPH<Method>::vjp_step (sph/sph.ixx:361-365) after ref_sph_forward_step of the same state.  All
+// outputs are accumulated (FP64, SoA): previous[6] (positions, velocities), control[3], particle[4]
+// (masses, rest densities, viscosities, surface tensions), method[3] (the method's parameters);
+// next_warm[2] / previous_warm[2]: DFSPH's method-state adjoints (the reference copies into
+// previous_warm, sph/sph.cpp:714).
+int ref_sph_vjp_step(void* sph, const ref_state_in* state, const ref_sph_params* p, const double* const* next_adjoint,
+                     const double* const* next_warm, double* const* previous, double* const* control, double* const* particle,
+                     double* const* method_adjoint, double* const* previous_warm, const uint64_t step_index) {
+    auto* r = static_cast<SphReplay*>(sph);
+    if (!r->differentiable) return 1;
+    Harness* h = r->h;
+    const ::cuda::stream_ref s{h->stream};
+    const uint32_t n = h->cfg.particle_count;
+    const float hr = h->cfg.support_radius;
+    const float dt = h->cfg.time_step;
+    const cd::ConstVectorView<float> x{state->px, state->py, state->pz}, v{state->vx, state->vy, state->vz};
+    const cd::ConstVectorView<double> nx{next_adjoint[0], next_adjoint[1], next_adjoint[2]},
+        nv{next_adjoint[3], next_adjoint[4], next_adjoint[5]};
+    const cd::VectorView<double> px{previous[0], previous[1], previous[2]}, pvv{previous[3], previous[4], previous[5]};
+    const DVec control_adjoint{control[0], control[1], control[2]};
+    const cd::ParticleParameterView pv{p->masses, p->rest_densities, p->viscosities, p->surface_tensions};
+    const cd::ParticleParameterAdjointView pa = adjoint_view(particle);
+    const cd::Box box = h->collision_box(step_index);
+    const auto nb = h->neighborhood();
+    const auto bd = h->boundary();
+    const float* rho = r->densities;
+    double* rho_a = r->density_adjoint;
+    r->clear(rho_a);
+    auto accumulate = [&](const DVec& from, const DVec& to) {   // domain.accumulate (domain/domain.cu)
+        cd::accumulate(s, h->cdv(from), h->mdv(to), n);
+    };
+    if (r->method == 0) {   // WCSPH::vjp (sph/sph.cpp:239-250)
+        namespace w = cd::wcsph;
+        r->clear(r->pressure_adjoint);
+        r->clear(r->total_acc_adjoint);
+        cd::sph::integrate_vjp(s, n, dt, box, x, v, h->cv(r->total_acc), nx, nv, px, pvv, h->mdv(r->total_acc_adjoint));
+        accumulate(r->total_acc_adjoint, control_adjoint);
+        w::launch_surface_vjp(s, n, hr, h->cfg.particle_radius, x, pv, p->method2, nb, bd, h->cdv(r->total_acc_adjoint), px, pa,
+                              method_adjoint[2]);
+        w::launch_artificial_viscosity_vjp(s, n, hr, x, v, pv, p->method0, nb, bd, rho, h->cdv(r->total_acc_adjoint), px, pvv,
+                                           rho_a, pa, method_adjoint[0]);
+        cd::sph::pressure_vjp(s, n, hr, x, pv, nb, bd, rho, r->pressures, h->cdv(r->total_acc_adjoint), px, rho_a,
+                              r->pressure_adjoint, pa);
+        w::launch_eos_vjp(s, n, rho, pv, p->method0, p->method1, r->pressure_adjoint, rho_a, pa, method_adjoint[0],
+                          method_adjoint[1]);
+        cd::density_vjp(s, n, hr, false, x, x, pv, nb, bd, rho_a, px, pa);
+        return cudaGetLastError() == cudaSuccess ? 0 : 3;
+    }
+    const float rgn = r->reference_gradient_norm;
+    const auto anp = h->cv(r->non_pressure_acc);
+    auto predict_forward = [&](const Vec& pressure_acc, const Vec& pos, const Vec& vel) {
+        if (r->method == 1) cd::pcisph::launch_predict_forward(s, n, dt, box, x, v, anp, h->cv(pressure_acc), h->mv(pos), h->mv(vel));
+        else if (r->method == 2) cd::iisph::launch_predict_forward(s, n, dt, box, x, v, anp, h->cv(pressure_acc), h->mv(pos), h->mv(vel));
+        else cd::dfsph::launch_predict_forward(s, n, dt, box, x, v, anp, h->cv(pressure_acc), h->mv(pos), h->mv(vel));
+    };
+    auto predict_vjp = [&](const Vec& pressure_acc, const cd::ConstVectorView<double> pos_a, const cd::ConstVectorView<double> vel_a,
+                           const DVec& pressure_acc_adjoint) {
+        const auto npa = h->mdv(r->non_pressure_acc_adjoint);
+        if (r->method == 1)
+            cd::pcisph::launch_predict_vjp(s, n, dt, box, x, v, anp, h->cv(pressure_acc), pos_a, vel_a, px, pvv, npa, h->mdv(pressure_acc_adjoint));
+        else if (r->method == 2)
+            cd::iisph::launch_predict_vjp(s, n, dt, box, x, v, anp, h->cv(pressure_acc), pos_a, vel_a, px, pvv, npa, h->mdv(pressure_acc_adjoint));
+        else
+            cd::dfsph::launch_predict_vjp(s, n, dt, box, x, v, anp, h->cv(pressure_acc), pos_a, vel_a, px, pvv, npa, h->mdv(pressure_acc_adjoint));
+    };
+    auto pressure_forward = [&](IterCache& c) {
+        cd::sph::pressure_forward(s, n, hr, x, pv, nb, bd, rho, c.pressures, h->mv(c.pressure_acc));
+    };
+    auto pressure_vjp = [&](const float* pressures) {
+        cd::sph::pressure_vjp(s, n, hr, x, pv, nb, bd, rho, pressures, h->cdv(r->adjoint.pressure_acc), px, rho_a,
+                              r->adjoint.pressures, pa);
+    };
+    r->clear(r->non_pressure_acc_adjoint);
+    r->clear(r->adjoint);
+    r->clear(r->previous_adjoint);
+    if (r->method == 1 || r->method == 2) {   // PCISPH::vjp / IISPH::vjp (sph/sph.cpp:332-373, 445-486)
+        predict_vjp(r->checkpoints.back().pressure_acc, nx, nv, r->adjoint.pressure_acc);
+        for (size_t c = r->checkpoints.size() - 1; c > 0; --c) {
+            const IterCache& first = r->checkpoints[c - 1];
+            const IterCache& last = r->checkpoints[c];
+            r->copy(first, r->recomputed[0]);
+            for (uint32_t it = first.iteration + 1u; it <= last.iteration; ++it) {
+                IterCache& prev = r->recomputed[it - first.iteration - 1u];
+                IterCache& cur = r->recomputed[it - first.iteration];
+                cur.iteration = it;
+                predict_forward(prev.pressure_acc, cur.predicted_positions, cur.predicted_velocities);
+                cd::density_forward(s, n, hr, false, x, h->cv(cur.predicted_positions), pv, nb, bd, cur.predicted_densities);
+                if (r->method == 1)
+                    cd::pcisph::launch_pressure_update_forward(s, n, dt, rgn, pv, prev.pressures, cur.predicted_densities,
+                                                               p->method0, cur.pressures);
+                else
+                    cd::iisph::launch_jacobi_update_forward(s, n, dt, rgn, pv, rho, prev.pressures, cur.predicted_densities,
+                                                            p->method0, cur.pressures);
+                pressure_forward(cur);
+            }
+            for (uint32_t it = last.iteration; it > first.iteration; --it) {
+                IterCache& prev = r->recomputed[it - first.iteration - 1u];
+                IterCache& cur = r->recomputed[it - first.iteration];
+                r->clear(r->previous_adjoint);
+                pressure_vjp(cur.pressures);
+                if (r->method == 1)
+                    cd::pcisph::launch_pressure_update_vjp(s, n, dt, rgn, pv, prev.pressures, cur.predicted_densities, p->method0,
+                                                           r->adjoint.pressures, pa, r->previous_adjoint.pressures,
+                                                           r->adjoint.predicted_densities, method_adjoint[0]);
+                else
+                    cd::iisph::launch_jacobi_update_vjp(s, n, dt, rgn, pv, rho, prev.pressures, cur.predicted_densities,
+                                                        p->method0, r->adjoint.pressures, pa, rho_a, r->previous_adjoint.pressures,
+                                                        r->adjoint.predicted_densities, method_adjoint[0]);
+                cd::density_vjp(s, n, hr, false, x, h->cv(cur.predicted_positions), pv, nb, bd, r->adjoint.predicted_densities,
+                                h->mdv(r->adjoint.predicted_positions), pa);
+                predict_vjp(prev.pressure_acc, h->cdv(r->adjoint.predicted_positions), h->cdv(r->adjoint.predicted_velocities),
+                            r->previous_adjoint.pressure_acc);
+                std::swap(r->adjoint, r->previous_adjoint);
+            }
+        }
+    } else {   // DFSPH::vjp (sph/sph.cpp:661-722)
+        r->clear(r->target_density_adjoint);
+        r->clear(r->divergence_pressure_acc_adjoint);
+        r->clear(r->total_pressure_acc_adjoint);
+        predict_vjp(r->total_pressure_acc, nx, nv, r->total_pressure_acc_adjoint);
+        r->copy(r->total_pressure_acc_adjoint, r->divergence_pressure_acc_adjoint);
+        r->copy(r->total_pressure_acc_adjoint, r->adjoint.pressure_acc);
+        r->copy(next_warm[1], r->adjoint.pressures);
+        auto reverse_phase = [&](std::vector<IterCache>& checkpoints, const float* relaxation, double* relaxation_adjoint,
+                                 const float* target, double* target_adjoint, const Vec* base, const DVec* base_adjoint,
+                                 double* warm_adjoint) {
+            for (size_t c = checkpoints.size(); c-- > 1;) {
+                const IterCache& first = checkpoints[c - 1];
+                const IterCache& last = checkpoints[c];
+                r->copy(first, r->recomputed[0]);
+                for (uint32_t it = first.iteration + 1u; it <= last.iteration; ++it) {
+                    IterCache& prev = r->recomputed[it - first.iteration - 1u];
+                    IterCache& cur = r->recomputed[it - first.iteration];
+                    cur.iteration = it;
+                    const Vec* prediction = &prev.pressure_acc;
+                    if (base) {
+                        cd::sph::add(s, n, h->cv(*base), h->cv(prev.pressure_acc), h->mv(r->total_pressure_acceleration));
+                        prediction = &r->total_pressure_acceleration;
+                    }
+                    predict_forward(*prediction, cur.predicted_positions, cur.predicted_velocities);
+                    cd::density_forward(s, n, hr, false, x, h->cv(cur.predicted_positions), pv, nb, bd, cur.predicted_densities);
+                    cd::dfsph::launch_projection_update_forward(s, n, dt, rgn, pv, rho, target, prev.pressures,
+                                                                cur.predicted_densities, relaxation, cur.pressures);
+                    pressure_forward(cur);
+                }
+                for (uint32_t it = last.iteration; it > first.iteration; --it) {
+                    IterCache& prev = r->recomputed[it - first.iteration - 1u];
+                    IterCache& cur = r->recomputed[it - first.iteration];
+                    r->clear(r->previous_adjoint);
+                    pressure_vjp(cur.pressures);
+                    cd::dfsph::launch_projection_update_vjp(s, n, dt, rgn, pv, rho, target, prev.pressures, cur.predicted_densities,
+                                                            relaxation, r->adjoint.pressures, pa, rho_a, target_adjoint,
+                                                            r->previous_adjoint.pressures, r->adjoint.predicted_densities,
+                                                            relaxation_adjoint);
+                    cd::density_vjp(s, n, hr, false, x, h->cv(cur.predicted_positions), pv, nb, bd,
+                                    r->adjoint.predicted_densities, h->mdv(r->adjoint.predicted_positions), pa);
+                    if (!base) {
+                        predict_vjp(prev.pressure_acc, h->cdv(r->adjoint.predicted_positions),
+                                    h->cdv(r->adjoint.predicted_velocities), r->previous_adjoint.pressure_acc);
+                    } else {
+                        r->clear(r->total_pressure_acc_adjoint);
+                        cd::sph::add(s, n, h->cv(*base), h->cv(prev.pressure_acc), h->mv(r->total_pressure_acceleration));
+                        predict_vjp(r->total_pressure_acceleration, h->cdv(r->adjoint.predicted_positions),
+                                    h->cdv(r->adjoint.predicted_velocities), r->total_pressure_acc_adjoint);
+                        cd::sph::add_adjoint(s, n, h->cdv(r->total_pressure_acc_adjoint), h->mdv(*base_adjoint),
+                                             h->mdv(r->previous_adjoint.pressure_acc));
+                    }
+                    std::swap(r->adjoint, r->previous_adjoint);
+                }
+            }
+            pressure_vjp(checkpoints.front().pressures);
+            if (r->warm_start) r->copy(r->adjoint.pressures, warm_adjoint);
+        };
+        reverse_phase(r->density_checkpoints, p->method1, method_adjoint[1], p->rest_densities, pa.rest_densities,
+                      &r->divergence_pressure_acc, &r->divergence_pressure_acc_adjoint, previous_warm[1]);
+        r->clear(r->adjoint);
+        r->copy(r->divergence_pressure_acc_adjoint, r->adjoint.pressure_acc);
+        r->copy(next_warm[0], r->adjoint.pressures);
+        reverse_phase(r->divergence_checkpoints, p->method0, method_adjoint[0], rho, r->target_density_adjoint, nullptr, nullptr,
+                      previous_warm[0]);
+        cd::accumulate(s, r->target_density_adjoint, rho_a, n);
+    }
+    cd::sph::non_pressure_vjp(s, n, hr, x, v, pv, nb, bd, rho, h->cdv(r->non_pressure_acc_adjoint), px, pvv,
+                              h->mdv(control_adjoint), rho_a, pa);
+    cd::density_vjp(s, n, hr, false, x, x, pv, nb, bd, rho_a, px, pa);
     return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }
 
@@ -868,11 +1324,11 @@ int ref_sph_read(void* sph, const int field, float* x, float* y, float* z) {
     int rc = 1;
     switch (field) {
         case 0: rc = scalar(r->densities); break;
-        case 1: rc = scalar(w ? r->pressures : r->primal_pressures); break;
-        case 2: rc = vec3(w ? r->pressure_acc : r->primal_pressure_acc); break;
+        case 1: rc = scalar(w ? r->pressures : r->primal.pressures); break;
+        case 2: rc = vec3(w ? r->pressure_acc : r->primal.pressure_acc); break;
         case 3: rc = vec3(w ? r->viscosity_acc : r->non_pressure_acc); break;
         case 4: rc = w ? vec3(r->surface_acc) : 1; break;
-        case 5: rc = scalar(r->predicted_densities); break;
+        case 5: rc = scalar(r->primal.predicted_densities); break;
         case 6: rc = vec3(w ? r->total_acc : r->total_pressure_acc); break;
         default: break;
     }

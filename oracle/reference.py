@@ -217,7 +217,8 @@ class ReferencePBF:
 
 class RefSphConfig(ctypes.Structure):
     _fields_ = [("method", ctypes.c_int), ("pressure_iterations", ctypes.c_uint32), ("divergence_iterations", ctypes.c_uint32),
-                ("density_iterations", ctypes.c_uint32), ("pressure_warm_start", ctypes.c_int)]
+                ("density_iterations", ctypes.c_uint32), ("pressure_warm_start", ctypes.c_int),
+                ("checkpoint_interval", ctypes.c_uint32), ("differentiable", ctypes.c_int)]
 
 
 class RefSphParams(ctypes.Structure):
@@ -241,6 +242,10 @@ def _load_sph():
         lib.ref_sph_forward_step.argtypes = [vp, P(RefStateIn), P(vp), P(RefSphParams), vp, vp, P(RefStateOut), vp, vp,
                                              ctypes.c_uint64]
         lib.ref_sph_read.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+        lib.ref_sph_jvp_step.argtypes = [vp, P(RefStateIn), P(RefSphParams), P(RefStateIn), P(vp), P(vp), P(vp), P(vp),
+                                         P(RefStateOut), P(vp), ctypes.c_uint64, vp, vp]
+        lib.ref_sph_vjp_step.argtypes = [vp, P(RefStateIn), P(RefSphParams), P(vp), P(vp), P(vp), P(vp), P(vp), P(vp), P(vp),
+                                         ctypes.c_uint64]
         lib.ref_sph_reference_gradient_norm.argtypes = [vp]
         lib.ref_sph_reference_gradient_norm.restype = ctypes.c_float
         lib._sph_bound = True
@@ -253,12 +258,12 @@ class ReferenceSPH:
     method: 0 WCSPH, 1 PCISPH, 2 IISPH, 3 DFSPH; scene.sph holds the parameter arrays."""
 
     def __init__(self, scene, method, pressure_iterations=6, divergence_iterations=4, density_iterations=6,
-                 pressure_warm_start=True, device="cuda"):
+                 pressure_warm_start=True, checkpoint_interval=2, differentiable=False, device="cuda"):
         self.base = ReferencePBF(scene, device=device)
         lib = _load_sph()
         self.method = int(method)
         c = RefSphConfig(self.method, pressure_iterations, divergence_iterations, density_iterations,
-                         1 if pressure_warm_start else 0)
+                         1 if pressure_warm_start else 0, checkpoint_interval, 1 if differentiable else 0)
         h = ctypes.c_void_p()
         rc = lib.ref_sph_create(self.base.handle, ctypes.byref(c), ctypes.byref(h))
         if rc:
@@ -313,6 +318,77 @@ class ReferenceSPH:
             raise RuntimeError(f"ref_sph_forward_step failed: {rc}")
         if synchronize:
             load().ref_synchronize(self.base.handle)
+
+    def _method_names(self):
+        names = list(SPH_METHOD_PARAMETERS[self.method])
+        return names + [names[0]] * (3 - len(names))
+
+    def jvp_step(self, x, v, tangent, control_tangent, param_tangent, next_tangent, step_index, warm=None, warm_tangent=None,
+                 next_warm_tangent=None):
+        """SPH<Method>::jvp_step after forward_step of (x, v).  tangent / next_tangent: dicts of (3, N)
+        float32 tensors "positions" / "velocities"; param_tangent: dict of (N,) float32 tensors keyed
+        like scene.sph; warm / warm_tangent / next_warm_tangent: DFSPH pairs of (N,) float32."""
+        lib = _load_sph()
+        z = torch.zeros(self.n, dtype=torch.float32, device=self.device)
+        sin = RefStateIn(_p(x[0]), _p(x[1]), _p(x[2]), _p(v[0]), _p(v[1]), _p(v[2]))
+        tin = RefStateIn(*[_p(tangent[k][a]) for k in ("positions", "velocities") for a in range(3)])
+        tout = RefStateOut(*[_p(next_tangent[k][a]) for k in ("positions", "velocities") for a in range(3)])
+        vp = ctypes.c_void_p
+        ct = (vp * 3)(*[control_tangent[a].data_ptr() for a in range(3)])
+        get = lambda k: param_tangent.get(k, z)
+        pt = (vp * 4)(*[get(k).data_ptr() for k in ("masses", "rest_densities", "viscosities", "surface_tensions")])
+        mt = (vp * 3)(*[get(k).data_ptr() for k in self._method_names()])
+        wt = (vp * 2)(*[(warm_tangent[a] if warm_tangent is not None else z).data_ptr() for a in range(2)])
+        nwt = (vp * 2)(*[(next_warm_tangent[a] if next_warm_tangent is not None else z).data_ptr() for a in range(2)])
+        w = [vp(t.data_ptr()) if t is not None else None for t in (warm if warm is not None else (None, None))]
+        params = self._pstruct()
+        torch.cuda.synchronize(self.device)
+        rc = lib.ref_sph_jvp_step(self.handle, ctypes.byref(sin), ctypes.byref(params), ctypes.byref(tin), ct, pt, mt, wt,
+                                  ctypes.byref(tout), nwt, step_index, w[0], w[1])
+        if rc:
+            raise RuntimeError(f"ref_sph_jvp_step failed: {rc}")
+        load().ref_synchronize(self.base.handle)
+
+    def vjp_step(self, x, v, next_adjoint, previous_adjoint, control_adjoint, param_adjoint, step_index, next_warm=None,
+                 previous_warm=None):
+        """SPH<Method>::vjp_step after forward_step of (x, v).  Adjoints are float64 CUDA tensors:
+        next_adjoint / previous_adjoint dicts of (3, N) "positions" / "velocities"; control_adjoint
+        (3, N); param_adjoint dict of (N,) keyed like scene.sph; next_warm / previous_warm: DFSPH
+        pairs of (N,).  Outputs are accumulated (previous_warm is overwritten, as the reference does)."""
+        lib = _load_sph()
+        zd = lambda: torch.zeros(self.n, dtype=torch.float64, device=self.device)
+        vp = ctypes.c_void_p
+        sin = RefStateIn(_p(x[0]), _p(x[1]), _p(x[2]), _p(v[0]), _p(v[1]), _p(v[2]))
+        na = (vp * 6)(*[next_adjoint[k][a].data_ptr() for k in ("positions", "velocities") for a in range(3)])
+        pa = (vp * 6)(*[previous_adjoint[k][a].data_ptr() for k in ("positions", "velocities") for a in range(3)])
+        ca = (vp * 3)(*[control_adjoint[a].data_ptr() for a in range(3)])
+        keep = []
+
+        def slot(d, k):
+            if k in d:
+                return d[k].data_ptr()
+            t = zd()
+            keep.append(t)
+            return t.data_ptr()
+        qa = (vp * 4)(*[slot(param_adjoint, k) for k in ("masses", "rest_densities", "viscosities", "surface_tensions")])
+        names = list(SPH_METHOD_PARAMETERS[self.method])
+        ma_ptrs = [slot(param_adjoint, k) for k in names]
+        while len(ma_ptrs) < 3:
+            t = zd()
+            keep.append(t)
+            ma_ptrs.append(t.data_ptr())
+        ma = (vp * 3)(*ma_ptrs)
+        nw = next_warm if next_warm is not None else (zd(), zd())
+        pw = previous_warm if previous_warm is not None else (zd(), zd())
+        keep.extend([nw, pw])
+        nwp = (vp * 2)(nw[0].data_ptr(), nw[1].data_ptr())
+        pwp = (vp * 2)(pw[0].data_ptr(), pw[1].data_ptr())
+        params = self._pstruct()
+        torch.cuda.synchronize(self.device)
+        rc = lib.ref_sph_vjp_step(self.handle, ctypes.byref(sin), ctypes.byref(params), na, nwp, pa, ca, qa, ma, pwp, step_index)
+        if rc:
+            raise RuntimeError(f"ref_sph_vjp_step failed: {rc}")
+        load().ref_synchronize(self.base.handle)
 
     def read(self, field: str) -> torch.Tensor:
         code = SPH_FIELDS[field]

@@ -21,8 +21,7 @@
 // so that pass walks the full stencil of the input positions, as the reference does.
 #include <cmath>
 
-#include "gather.cuh"
-#include "sph_launch.h"
+#include "sph_math.cuh"
 
 namespace pbf {
 namespace sph {
@@ -30,95 +29,7 @@ namespace sph {
 namespace {
 
 using namespace gather_detail;
-
-// x*y + ... as the reference's dot(a, b) compiles (density/device.cuh, domain/device.cuh:56-58):
-// fma(a.z, b.z, fma(a.x, b.x, a.y * b.y)).
-__device__ __forceinline__ float dot_xfirst(const f3 a, const f3 b) {
-    return __fmaf_rn(a.z, b.z, __fmaf_rn(a.x, b.x, __fmul_rn(a.y, b.y)));
-}
-
-// Cubic spline weight at distance `distance` < h (density/device.cuh:26-34).
-__device__ __forceinline__ float cubic_inside(const float distance, const SphConstants& k) {
-    const float q = __fdiv_rn(distance, k.h);
-    if (q <= 0.5F) {
-        // 6 q q q - 6 q q + 1 with the shared product t = 6 q q: fma(t, q, -t) + 1
-        const float t = __fmul_rn(__fmul_rn(6.0F, q), q);
-        return __fmul_rn(k.cubic_coefficient, __fadd_rn(__fmaf_rn(t, q, -t), 1.0F));
-    }
-    const float difference = __fsub_rn(1.0F, q);
-    return __fmul_rn(__fmul_rn(__fmul_rn(k.cubic_coefficient_2, difference), difference), difference);
-}
-
-// Scale of the cubic gradient, grad W = d * s, at 0 < distance < h (density/device.cuh:36-42).
-__device__ __forceinline__ float cubic_gradient_scale(const float distance, const SphConstants& k) {
-    const float q = __fdiv_rn(distance, k.h);
-    float derivative;
-    if (q <= 0.5F) {
-        derivative = __fmaf_rn(__fmul_rn(18.0F, q), q, -__fmul_rn(12.0F, q));
-    } else {
-        const float difference = __fsub_rn(1.0F, q);
-        derivative = __fmul_rn(__fmul_rn(-6.0F, difference), difference);
-    }
-    return __fdiv_rn(__fmul_rn(k.cubic_coefficient, derivative), __fmul_rn(k.h, distance));
-}
-
-// Viscosity Laplacian at distance < h (density/device.cuh:76-79).
-__device__ __forceinline__ float laplacian_inside(const float distance, const SphConstants& k) {
-    return __fdiv_rn(__fmul_rn(45.0F, __fsub_rn(k.h, distance)), k.laplacian_denominator);
-}
-
-// predict (sph/pcisph.cu:26-45, the same body as integrate, sph/common.cu:302-320):
-// v* = v + dt a, x* = x + dt v*, then the collision box of the step.
-__device__ __forceinline__ void predict(const f3 x, const f3 v, const f3 a, const float dt, const Box& box,
-                                        const SphConstants& k, f3& xo, f3& vo) {
-    f3 vel = fma3(dt, a, v);
-    f3 pos = fma3(dt, vel, x);
-    const bool cx = pos.x < box.min_x || pos.x > box.max_x;
-    const bool cy = pos.y < box.min_y || pos.y > box.max_y;
-    const bool cz = pos.z < box.min_z || pos.z > box.max_z;
-    pos.x = fminf(box.max_x, fmaxf(box.min_x, pos.x));
-    pos.y = fminf(box.max_y, fmaxf(box.min_y, pos.y));
-    pos.z = fminf(box.max_z, fmaxf(box.min_z, pos.z));
-    if (k.no_slip != 0u && (cx || cy || cz)) {
-        vel = mk(k.box_vx, k.box_vy, k.box_vz);
-    } else {
-        if (cx) vel.x = k.box_vx;
-        if (cy) vel.y = k.box_vy;
-        if (cz) vel.z = k.box_vz;
-    }
-    xo = pos;
-    vo = vel;
-}
-
-// Largest |x* - x| of the particles predicted by one pass, as the bits of a non-negative float
-// (their unsigned order is the float order): a warp maximum, then one atomic per warp.
-__device__ __forceinline__ void record_displacement(unsigned int* word, const f3 predicted, const f3 x) {
-    const float d = __fsqrt_rn(sq_xfirst(sub(predicted, x)));
-    const unsigned int bits = __float_as_uint(d);   // d >= 0 or NaN (NaN bits exceed every finite bound)
-    const unsigned int mask = __activemask();
-    const unsigned int m = __reduce_max_sync(mask, bits);
-    if ((threadIdx.x & 31u) == static_cast<unsigned int>(__ffs(mask) - 1)) atomicMax(word, m);
-}
-
-struct Own {
-    Particle p;
-    f3 x;
-    float mass;
-    float4 pa;   // (rest density, viscosity, surface tension, method parameter 0)
-    const SphConstants* k;
-};
-
-__device__ __forceinline__ Own own(const SphStep& st) {
-    Own o;
-    o.p = locate(st.g);
-    if (!o.p.active) return o;
-    const float4 xi = st.topology[o.p.s];
-    o.x = xyz(xi);
-    o.mass = xi.w;
-    o.pa = st.g.params_a[o.p.s];
-    o.k = st.constants + o.p.scene->constants;
-    return o;
-}
+using namespace detail;
 
 // ------------------------------------------------------------------ density (+ Tait EOS)
 template <bool WithBoundary>
@@ -167,7 +78,7 @@ __global__ void __launch_bounds__(kBlock) sph_density_kernel(const SphStep st, c
         const float rest = o.pa.x, speed = o.pa.w, exponent = pb.x;
         const float ratio = __fdiv_rn(rho, rest);
         p = __fdiv_rn(__fmul_rn(__fmul_rn(__fmul_rn(rest, speed), speed), __fsub_rn(powf(ratio, exponent), 1.0F)), exponent);
-        st.aux[o.p.s] = make_float4(rho, o.pa.y, speed, 0.0F);
+        st.aux[o.p.s] = make_float4(rho, o.pa.y, speed, o.pa.z);
     } else {
         st.aux[o.p.s] = make_float4(rho, o.pa.y, 0.0F, 0.0F);
         if (warm) p = warm[st.sorted_index[o.p.s]];
@@ -275,6 +186,7 @@ struct WcsphForceArgs {
     float4* record_pressure;
     float4* record_viscosity;
     float4* record_surface;
+    float4* record_total;   // the total acceleration (differentiable mode), or null
 };
 
 template <bool WithBoundary>
@@ -323,6 +235,7 @@ __global__ void __launch_bounds__(kBlock, 4) wcsph_force_kernel(const WcsphForce
     if (a.record_pressure) a.record_pressure[s] = make_float4(op.pressure.x, op.pressure.y, op.pressure.z, 0.0F);
     if (a.record_viscosity) a.record_viscosity[s] = make_float4(op.artificial.x, op.artificial.y, op.artificial.z, 0.0F);
     if (a.record_surface) a.record_surface[s] = make_float4(op.surface.x, op.surface.y, op.surface.z, 0.0F);
+    if (a.record_total) a.record_total[s] = make_float4(total.x, total.y, total.z, 0.0F);
 }
 
 // ------------------------------------------------------------------ non-pressure acceleration
@@ -646,10 +559,11 @@ cudaError_t launch_density(cudaStream_t stream, const SphStep& st, const uint32_
 
 cudaError_t launch_wcsph_forces(cudaStream_t stream, const SphStep& st, const float* pressure_term, const MutField3 out_positions,
                                 const MutField3 out_velocities, float4* record_pressure, float4* record_viscosity,
-                                float4* record_surface, const unsigned block) {
+                                float4* record_surface, float4* record_total, const unsigned block) {
     if (st.g.count == 0) return cudaSuccess;
     const unsigned b = block_of(block);
-    const WcsphForceArgs a{st, pressure_term, out_positions, out_velocities, record_pressure, record_viscosity, record_surface};
+    const WcsphForceArgs a{st, pressure_term, out_positions, out_velocities, record_pressure, record_viscosity, record_surface,
+                           record_total};
     if (st.g.boundary) wcsph_force_kernel<true><<<grid_of(st.g.count, b), b, 0, stream>>>(a);
     else wcsph_force_kernel<false><<<grid_of(st.g.count, b), b, 0, stream>>>(a);
     count_launch();

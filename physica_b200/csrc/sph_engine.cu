@@ -39,16 +39,34 @@ struct SphRecord {
     float* density = nullptr;
     float4* aux = nullptr;
     float4* non_pressure = nullptr;
-    float4* predicted = nullptr;
-    float4* divergence_acceleration = nullptr;   // DFSPH
+    float4* divergence_acceleration = nullptr;   // DFSPH, forward mode
     float4* pressure_acceleration = nullptr;     // the last pressure pass (WCSPH: pressure term)
     float4* viscosity_acceleration = nullptr;    // WCSPH
     float4* surface_acceleration = nullptr;      // WCSPH
-    float* pressure[2] = {nullptr, nullptr};
-    float* pressure_term[2] = {nullptr, nullptr};
-    float* predicted_density = nullptr;
     unsigned int* displacement = nullptr;   // max |x* - x| of every prediction of the step
-    uint32_t final_pressure = 0;   // which pressure buffer holds the last iterate
+    // The pressure-iteration phases of the iterative methods (PCISPH / IISPH: one; DFSPH: the
+    // divergence and the density phase).  Differentiable mode keeps every iterate k = 0..K
+    // (pressures, predictions, predicted densities, pressure accelerations) for the tangent and
+    // the reverse passes; forward mode reuses one buffer of each.
+    struct Phase {
+        uint32_t iterations = 0;
+        uint32_t first_slot = 0;                // displacement slot of the phase's first prediction
+        std::vector<float*> pressure;           // p_k
+        std::vector<float4*> predicted;         // x*_k (index k; K + 1 is scratch)
+        std::vector<float*> predicted_density;  // rho*_k
+        std::vector<float4*> acceleration;      // pressure acceleration of iterate k
+        float* pressure_term = nullptr;         // p / rho^2 of the current iterate
+        float* P(uint32_t k) const { return pressure[pressure.size() > 1 ? k : 0]; }
+        float4* X(uint32_t k) const { return predicted[predicted.size() > 1 ? k : 0]; }
+        float* R(uint32_t k) const { return predicted_density[predicted_density.size() > 1 ? k : 0]; }
+        float4* A(uint32_t k) const { return acceleration.empty() ? nullptr : acceleration[k]; }
+    };
+    Phase phase[2];
+    float4* total_acceleration = nullptr;   // WCSPH, differentiable mode
+    const float* final_pressure = nullptr;
+    const float* final_predicted_density = nullptr;
+    float4* final_acceleration = nullptr;
+    bool differentiable = false;
 };
 
 // List skin of the iterative methods, as a fraction of h: their predicted densities replay the
@@ -56,6 +74,8 @@ struct SphRecord {
 // stays inside it (always exact: otherwise they walk).
 constexpr float kIterativeSkin = 0.1F;
 constexpr uint32_t kDisplacementSlots = 2u * kMaxIterations + 4u;
+
+using Phase = SphRecord::Phase;
 
 class SphEngine {
 public:
@@ -73,6 +93,12 @@ public:
                 const sph_parameters* parameters, pbf_particle_state* next_state, sph_method_state* next_method_state,
                 SphRecord& r);
     int read(const SphRecord& r, sph_cache_field field, float* x, float* y, float* z);
+    int reverse(const pbf_particle_state* state, const sph_method_state* method_state, const sph_parameters* parameters,
+                const SphRecord& r, const pbf_particle_state_adjoint* next_adjoint,
+                const sph_method_state_adjoint* next_method_adjoint, pbf_particle_state_adjoint* previous_adjoint,
+                sph_method_state_adjoint* previous_method_adjoint, pbf_control_adjoint* control_adjoint,
+                sph_parameter_adjoint* parameter_adjoint);
+    bool differentiable() const { return differentiable_; }
     int check(cudaError_t e, const char* what) {
         if (e == cudaSuccess) return PBF_SUCCESS;
         cudaGetLastError();
@@ -89,6 +115,7 @@ private:
                SphRecord& r);
 
     sph_configuration config_{};
+    bool differentiable_ = false;
     pbf_domain_configuration domain_{};
     std::vector<pbf_boundary_particle> boundary_host_;
     uint32_t count_ = 0;
@@ -113,6 +140,16 @@ private:
     uint32_t* boundary_keys_ = nullptr;
     uint32_t* boundary_arrival_ = nullptr;
     uint32_t* boundary_unordered_ = nullptr;
+    // reverse-pass workspace (sorted order), allocated on first use
+    int reverse_workspace();
+    SphStep step_of(const SphRecord& r) const;
+    DeviceArena reverse_arena_;
+    double4* acceleration_adjoint_[2] = {nullptr, nullptr};
+    double4* non_pressure_adjoint_ = nullptr;
+    double4* divergence_adjoint_ = nullptr;
+    double* density_adjoint_ = nullptr;
+    double* pressure_adjoint_[2] = {nullptr, nullptr};
+    double* predicted_density_adjoint_ = nullptr;
 };
 
 namespace {
@@ -122,11 +159,7 @@ bool has3(const pbf_vector_field& f) { return f.x && f.y && f.z; }
 
 int SphEngine::init(const pbf_domain_configuration* domain, const sph_configuration* configuration, const pbf_execution_mode mode,
                     cudaStream_t stream) {
-    if (mode == PBF_EXECUTION_DIFFERENTIABLE) {
-        set_error("the SPH solvers are forward-mode only (SPH jvp_step / vjp_step are not provided)");
-        return PBF_ERROR_UNSUPPORTED;
-    }
-    if (mode != PBF_EXECUTION_FORWARD) {
+    if (mode != PBF_EXECUTION_FORWARD && mode != PBF_EXECUTION_DIFFERENTIABLE) {
         set_error("unknown execution mode");
         return PBF_ERROR_INVALID_ARGUMENT;
     }
@@ -153,6 +186,7 @@ int SphEngine::init(const pbf_domain_configuration* domain, const sph_configurat
         return PBF_ERROR_INVALID_ARGUMENT;
     }
     config_ = *configuration;
+    differentiable_ = mode == PBF_EXECUTION_DIFFERENTIABLE;
     domain_ = c;
     domain_.boundary_particles = nullptr;
     if (c.boundary_particle_count > 0) boundary_host_.assign(c.boundary_particles, c.boundary_particles + c.boundary_particle_count);
@@ -278,27 +312,41 @@ int SphEngine::allocate(SphRecord& r) {
     r.density = r.arena.alloc<float>(n, e);
     r.aux = r.arena.alloc<float4>(n, e);
     r.pressure_acceleration = r.arena.alloc<float4>(n, e);
-    r.pressure[0] = r.arena.alloc<float>(n, e);
-    r.pressure_term[0] = r.arena.alloc<float>(n, e);
+    r.differentiable = differentiable_;
     if (config_.method == SPH_METHOD_WCSPH) {
+        Phase& ph = r.phase[0];
+        ph.pressure.push_back(r.arena.alloc<float>(n, e));
+        ph.pressure_term = r.arena.alloc<float>(n, e);
         r.viscosity_acceleration = r.arena.alloc<float4>(n, e);
         r.surface_acceleration = r.arena.alloc<float4>(n, e);
+        if (differentiable_) r.total_acceleration = r.arena.alloc<float4>(n, e);
     } else {
         r.non_pressure = r.arena.alloc<float4>(n, e);
-        r.predicted = r.arena.alloc<float4>(n, e);
-        r.predicted_density = r.arena.alloc<float>(n, e);
         r.displacement = r.arena.alloc<unsigned int>(kDisplacementSlots, e);
-        if (config_.method == SPH_METHOD_DFSPH) {
-            r.divergence_acceleration = r.arena.alloc<float4>(n, e);
-            r.pressure[1] = r.arena.alloc<float>(n, e);
-            r.pressure_term[1] = r.arena.alloc<float>(n, e);
+        const bool dfsph = config_.method == SPH_METHOD_DFSPH;
+        const uint32_t phases = dfsph ? 2u : 1u;
+        for (uint32_t q = 0; q < phases; ++q) {
+            Phase& ph = r.phase[q];
+            ph.iterations = dfsph ? (q == 0 ? config_.divergence_iterations : config_.density_iterations) : config_.pressure_iterations;
+            ph.first_slot = q == 0 ? 0u : config_.divergence_iterations + 1u;
+            const uint32_t K = ph.iterations;
+            const uint32_t copies = differentiable_ ? K + 1u : 1u;
+            for (uint32_t k = 0; k < copies; ++k) ph.pressure.push_back(r.arena.alloc<float>(n, e));
+            for (uint32_t k = 0; k < (differentiable_ ? K + 2u : 1u); ++k) ph.predicted.push_back(r.arena.alloc<float4>(n, e));
+            for (uint32_t k = 0; k < copies; ++k) ph.predicted_density.push_back(r.arena.alloc<float>(n, e));
+            if (differentiable_)
+                for (uint32_t k = 0; k <= K; ++k) ph.acceleration.push_back(r.arena.alloc<float4>(n, e));
+            ph.pressure_term = r.arena.alloc<float>(n, e);
         }
+        if (dfsph && !differentiable_) r.divergence_acceleration = r.arena.alloc<float4>(n, e);
     }
     r.valid = false;
     if (int rc = check(e, "step cache allocation")) return rc;
-    if (r.predicted_density) {
-        if (int rc = check(cudaMemsetAsync(r.predicted_density, 0, static_cast<size_t>(n) * sizeof(float), stream_), "clear"))
-            return rc;
+    for (uint32_t q = 0; q < 2; ++q) {
+        for (float* d : r.phase[q].predicted_density)
+            if (int rc = check(cudaMemsetAsync(d, 0, static_cast<size_t>(n) * sizeof(float), stream_), "clear")) return rc;
+        for (float4* a : r.phase[q].acceleration)
+            if (int rc = check(cudaMemsetAsync(a, 0, static_cast<size_t>(n) * sizeof(float4), stream_), "clear")) return rc;
     }
     return check(cudaStreamSynchronize(stream_), "step cache allocation");
 }
@@ -410,7 +458,7 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
                r.boundary_velocity,
                r.aux,
                r.non_pressure,
-               r.predicted,
+               nullptr,
                r.displacement,
                r.sorted_index,
                {control->external_accelerations.x, control->external_accelerations.y, control->external_accelerations.z}};
@@ -418,91 +466,317 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
     const MutField3 out_x{next_state->positions.x, next_state->positions.y, next_state->positions.z};
     const MutField3 out_v{next_state->velocities.x, next_state->velocities.y, next_state->velocities.z};
     const bool warm = method == SPH_METHOD_DFSPH && config_.pressure_warm_start != 0;
-    if (int rc = check(launch_density(s, st, method, r.density, r.pressure[0], r.pressure_term[0],
+    const bool diff = differentiable_;
+    Phase& p0 = r.phase[0];
+    if (int rc = check(launch_density(s, st, method, r.density, p0.P(0), p0.pressure_term,
                                       warm ? method_state->warm_divergence_pressure : nullptr, block),
                        "density"))
         return rc;
     if (method == SPH_METHOD_WCSPH) {
-        r.final_pressure = 0;
-        return check(launch_wcsph_forces(s, st, r.pressure_term[0], out_x, out_v, r.pressure_acceleration,
-                                         r.viscosity_acceleration, r.surface_acceleration, block),
+        r.final_pressure = p0.P(0);
+        r.final_acceleration = r.pressure_acceleration;
+        return check(launch_wcsph_forces(s, st, p0.pressure_term, out_x, out_v, r.pressure_acceleration,
+                                         r.viscosity_acceleration, r.surface_acceleration, r.total_acceleration, block),
                      "WCSPH forces");
     }
     // Prediction p of the step records its largest displacement in slot p; the predicted density
     // that evaluates it reads that slot.
     if (int rc = check(cudaMemsetAsync(r.displacement, 0, kDisplacementSlots * sizeof(unsigned int), s), "clear")) return rc;
+    const size_t scalar_bytes = static_cast<size_t>(count_) * sizeof(float);
+    // One pressure iteration k of a phase: predicted density at x*_k with the pressure update, then
+    // the pressure acceleration with the next prediction (sph/sph.cpp:301-306).
+    auto iterate = [&](Phase& ph, const uint32_t k, const PressureUpdate update) -> int {
+        if (diff && count_ > 0) {   // p_k starts from p_(k-1); the update runs in place
+            if (int rc = check(cudaMemcpyAsync(ph.P(k), ph.P(k - 1), scalar_bytes, cudaMemcpyDeviceToDevice, s), "copy")) return rc;
+        }
+        SphStep sk = st;
+        sk.predicted = ph.X(k);
+        return check(launch_predicted_density(s, sk, update, ph.P(k), ph.pressure_term, ph.R(k), block), "predicted density");
+    };
+    auto pressure_pass = [&](Phase& ph, const uint32_t k, PressurePassArgs a) -> int {
+        SphStep sk = st;
+        sk.predicted = ph.X(k + 1);   // the next prediction (index K + 1: scratch)
+        a.pressure_term = ph.pressure_term;
+        a.pressure = ph.P(k);
+        a.out_positions = out_x;
+        a.out_velocities = out_v;
+        a.displacement_slot = ph.first_slot + k;
+        if (diff) a.store_acceleration = ph.A(k);
+        return check(launch_pressure(s, sk, a, block), "pressure acceleration");
+    };
     if (method == SPH_METHOD_PCISPH || method == SPH_METHOD_IISPH) {
-        const uint32_t K = config_.pressure_iterations;
-        r.final_pressure = 0;
-        if (int rc = check(launch_non_pressure(s, st, K > 0 ? 1 : 2, out_x, out_v, 0u, block), "non-pressure acceleration"))
+        const uint32_t K = p0.iterations;
+        SphStep s1 = st;
+        s1.predicted = p0.X(1 <= K ? 1 : 0);
+        if (int rc = check(launch_non_pressure(s, s1, K > 0 ? 1 : 2, out_x, out_v, 0u, block), "non-pressure acceleration"))
             return rc;
         for (uint32_t it = 1; it <= K; ++it) {
-            const PressureUpdate update{method, 0u, 0u, it - 1u};
-            if (int rc = check(launch_predicted_density(s, st, update, r.pressure[0], r.pressure_term[0], r.predicted_density, block),
-                               "predicted density"))
-                return rc;
+            if (int rc = iterate(p0, it, PressureUpdate{method, 0u, 0u, it - 1u})) return rc;
             PressurePassArgs a{};
-            a.pressure_term = r.pressure_term[0];
-            a.pressure = r.pressure[0];
             a.last = it == K ? 1 : 0;
-            a.out_positions = out_x;
-            a.out_velocities = out_v;
             a.store_acceleration = it == K ? r.pressure_acceleration : nullptr;
-            a.displacement_slot = it;
-            if (int rc = check(launch_pressure(s, st, a, block), "pressure acceleration")) return rc;
+            if (int rc = pressure_pass(p0, it, a)) return rc;
         }
+        r.final_pressure = p0.P(K);
+        r.final_predicted_density = p0.R(K);
+        r.final_acceleration = diff ? p0.A(K) : r.pressure_acceleration;
         return PBF_SUCCESS;
     }
-    // DFSPH::forward (sph/sph.cpp:572-610): divergence phase on pressure buffer 0, density phase on
-    // buffer 1; the divergence phase's last pressure pass also loads the density phase's warm start.
+    // DFSPH::forward (sph/sph.cpp:572-610): the divergence phase, then the density phase, whose
+    // warm start the divergence phase's last pressure pass loads (its neighbours still read the
+    // divergence pressures, so the phases use separate buffers).
     if (int rc = check(launch_non_pressure(s, st, 0, out_x, out_v, 0u, block), "non-pressure acceleration")) return rc;
-    const uint32_t Kd = config_.divergence_iterations, Kr = config_.density_iterations;
+    Phase& p1 = r.phase[1];
+    const uint32_t Kd = p0.iterations, Kr = p1.iterations;
+    float4* divergence_acceleration = diff ? p0.A(Kd) : r.divergence_acceleration;
     for (uint32_t it = 0; it <= Kd; ++it) {
         if (it > 0) {
-            if (int rc = check(launch_predicted_density(s, st, PressureUpdate{SPH_METHOD_DFSPH, 0u, 1u, it - 1u}, r.pressure[0],
-                                                        r.pressure_term[0], r.predicted_density, block),
-                               "predicted density"))
-                return rc;
+            if (int rc = iterate(p0, it, PressureUpdate{SPH_METHOD_DFSPH, 0u, 1u, it - 1u})) return rc;
         }
         PressurePassArgs a{};
-        a.pressure_term = r.pressure_term[0];
-        a.pressure = r.pressure[0];
-        a.out_positions = out_x;
-        a.out_velocities = out_v;
-        a.displacement_slot = it;
         if (it == Kd) {
-            a.store_acceleration = r.divergence_acceleration;
+            a.store_acceleration = divergence_acceleration;
             a.warm_out = next_method_state->warm_divergence_pressure;
-            a.next_pressure = r.pressure[1];
-            a.next_pressure_term = r.pressure_term[1];
+            a.next_pressure = p1.P(0);
+            a.next_pressure_term = p1.pressure_term;
             a.next_warm = warm ? method_state->warm_density_pressure : nullptr;
         }
-        if (int rc = check(launch_pressure(s, st, a, block), "pressure acceleration")) return rc;
+        if (int rc = pressure_pass(p0, it, a)) return rc;
     }
-    const uint32_t density_slots = Kd + 1u;
     for (uint32_t it = 0; it <= Kr; ++it) {
         if (it > 0) {
-            if (int rc = check(launch_predicted_density(s, st, PressureUpdate{SPH_METHOD_DFSPH, 1u, 0u, density_slots + it - 1u},
-                                                        r.pressure[1], r.pressure_term[1], r.predicted_density, block),
-                               "predicted density"))
-                return rc;
+            if (int rc = iterate(p1, it, PressureUpdate{SPH_METHOD_DFSPH, 1u, 0u, p1.first_slot + it - 1u})) return rc;
         }
         PressurePassArgs a{};
-        a.pressure_term = r.pressure_term[1];
-        a.pressure = r.pressure[1];
-        a.base = r.divergence_acceleration;
-        a.out_positions = out_x;
-        a.out_velocities = out_v;
-        a.displacement_slot = density_slots + it;
+        a.base = divergence_acceleration;
         if (it == Kr) {
             a.last = 1;
             a.warm_out = next_method_state->warm_density_pressure;
             a.store_acceleration = r.pressure_acceleration;
         }
-        if (int rc = check(launch_pressure(s, st, a, block), "pressure acceleration")) return rc;
+        if (int rc = pressure_pass(p1, it, a)) return rc;
     }
-    r.final_pressure = 1;
+    r.final_pressure = p1.P(Kr);
+    r.final_predicted_density = Kr > 0 ? p1.R(Kr) : (Kd > 0 ? p0.R(Kd) : p1.R(0));
+    r.final_acceleration = diff ? p1.A(Kr) : r.pressure_acceleration;
     return PBF_SUCCESS;
+}
+
+SphStep SphEngine::step_of(const SphRecord& r) const {
+    GatherCommon gc{count_, d_scenes_, d_list_constants_, r.cell_offsets, r.cell, r.params_a, r.params_b};
+    if (boundary_count_ > 0) {
+        gc.boundary_offsets = r.boundary_offsets;
+        gc.boundary = r.boundary;
+    }
+    return SphStep{gc,
+                   d_constants_,
+                   r.topology,
+                   r.velocity,
+                   StoredList{r.list_entries, r.list_counts, r.list_capacity},
+                   r.boundary_velocity,
+                   r.aux,
+                   r.non_pressure,
+                   nullptr,
+                   r.displacement,
+                   r.sorted_index,
+                   {nullptr, nullptr, nullptr}};
+}
+
+int SphEngine::reverse_workspace() {
+    if (density_adjoint_) return PBF_SUCCESS;
+    reverse_arena_.set_stream(stream_);
+    cudaError_t e = cudaSuccess;
+    const size_t n = count_;
+    for (auto& a : acceleration_adjoint_) a = reverse_arena_.alloc<double4>(n, e);
+    non_pressure_adjoint_ = reverse_arena_.alloc<double4>(n, e);
+    divergence_adjoint_ = reverse_arena_.alloc<double4>(n, e);
+    for (auto& p : pressure_adjoint_) p = reverse_arena_.alloc<double>(n, e);
+    predicted_density_adjoint_ = reverse_arena_.alloc<double>(n, e);
+    density_adjoint_ = reverse_arena_.alloc<double>(n, e);
+    if (int rc = check(e, "reverse workspace")) {
+        reverse_arena_.release();
+        density_adjoint_ = nullptr;
+        return rc;
+    }
+    return PBF_SUCCESS;
+}
+
+// SPH<Method>::vjp_step (sph/sph.ixx:361-365): Method::vjp (sph/sph.cpp:239-250, 332-373,
+// 445-486, 661-722) from the iterates the forward kept, newest first, then the density's reverse.
+int SphEngine::reverse(const pbf_particle_state* state, const sph_method_state* method_state, const sph_parameters* parameters,
+                       const SphRecord& r, const pbf_particle_state_adjoint* next_adjoint,
+                       const sph_method_state_adjoint* next_method_adjoint, pbf_particle_state_adjoint* previous_adjoint,
+                       sph_method_state_adjoint* previous_method_adjoint, pbf_control_adjoint* control_adjoint,
+                       sph_parameter_adjoint* parameter_adjoint) {
+    if (!differentiable_) {
+        set_error("vjp_step needs a solver created in PBF_EXECUTION_DIFFERENTIABLE mode");
+        return PBF_ERROR_NOT_DIFFERENTIABLE;
+    }
+    if (!state || !parameters || !next_adjoint || !previous_adjoint || !control_adjoint || !parameter_adjoint) {
+        set_error("null argument");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    (void)method_state;
+    if (!r.valid || !r.differentiable || r.step_index != state->step_index) {
+        set_error("the step cache does not hold the forward step of this state");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (count_ == 0) return PBF_SUCCESS;
+    auto has = [](const pbf_vector_adjoint_field& f) { return f.x && f.y && f.z; };
+    if (!has(next_adjoint->positions) || !has(next_adjoint->velocities) || !has(previous_adjoint->positions) ||
+        !has(previous_adjoint->velocities) || !has(control_adjoint->external_accelerations)) {
+        set_error("null adjoint field pointer");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (int rc = reverse_workspace()) return rc;
+    const uint32_t method = config_.method;
+    const sph_parameter_adjoint& q = *parameter_adjoint;
+    SphParameterAdjoints pa{q.masses, q.rest_densities, q.viscosities, q.surface_tensions, nullptr, nullptr, nullptr};
+    if (method == SPH_METHOD_WCSPH) {
+        pa.method0 = q.speed_of_sound;
+        pa.method1 = q.tait_exponent;
+        pa.method2 = q.boundary_surface_tension;
+    } else if (method == SPH_METHOD_PCISPH) {
+        pa.method0 = q.pressure_relaxation;
+    } else if (method == SPH_METHOD_IISPH) {
+        pa.method0 = q.jacobi_relaxation;
+    } else {
+        pa.method0 = q.divergence_relaxation;
+        pa.method1 = q.density_relaxation;
+    }
+    const SphStep st = step_of(r);
+    const cudaStream_t s = stream_;
+    const unsigned block = shape.block;
+    const ConstAdjField3 nx{next_adjoint->positions.x, next_adjoint->positions.y, next_adjoint->positions.z};
+    const ConstAdjField3 nv{next_adjoint->velocities.x, next_adjoint->velocities.y, next_adjoint->velocities.z};
+    const AdjField3 X{previous_adjoint->positions.x, previous_adjoint->positions.y, previous_adjoint->positions.z};
+    const AdjField3 V{previous_adjoint->velocities.x, previous_adjoint->velocities.y, previous_adjoint->velocities.z};
+    const AdjField3 C{control_adjoint->external_accelerations.x, control_adjoint->external_accelerations.y,
+                      control_adjoint->external_accelerations.z};
+    const size_t n = count_;
+    auto zero = [&](void* p, const size_t bytes) { return check(cudaMemsetAsync(p, 0, bytes, s), "clear"); };
+    if (int rc = zero(density_adjoint_, n * sizeof(double))) return rc;
+    auto density_step = [&]() {   // density_vjp at the step's positions (sph/sph.ixx:364)
+        DensityVjpLaunch d{};
+        d.st = st;
+        d.positions = r.topology;
+        d.density_adjoint = density_adjoint_;
+        d.x = X;
+        d.v = V;
+        d.pa = pa;
+        return check(launch_density_vjp(s, d, block), "density reverse");
+    };
+    if (method == SPH_METHOD_WCSPH) {
+        if (int rc = check(launch_integrate_vjp(s, st, r.total_acceleration, nx, nv, X, V, C, acceleration_adjoint_[0]),
+                           "integrate reverse"))
+            return rc;
+        if (int rc = check(launch_wcsph_force_vjp(s, st, r.phase[0].P(0), acceleration_adjoint_[0], X, V, pa, density_adjoint_, block),
+                           "force reverse"))
+            return rc;
+        return density_step();
+    }
+    for (double4* a : {acceleration_adjoint_[0], acceleration_adjoint_[1], non_pressure_adjoint_, divergence_adjoint_})
+        if (int rc = zero(a, n * sizeof(double4))) return rc;
+    for (double* a : {pressure_adjoint_[0], pressure_adjoint_[1]})
+        if (int rc = zero(a, n * sizeof(double))) return rc;
+    uint32_t cur = 0;
+    // One reverse iteration k of a phase: the pressure pass with the update that produced p_k, then
+    // the predicted density of x*_k with the prediction that produced it.
+    auto reverse_iteration = [&](const Phase& ph, const uint32_t k, const uint32_t relaxation, const uint32_t target,
+                                 double* relaxation_adjoint, const float4* base, double4* base_adjoint) -> int {
+        const uint32_t prev = cur ^ 1u;
+        if (int rc = zero(acceleration_adjoint_[prev], n * sizeof(double4))) return rc;
+        if (int rc = zero(pressure_adjoint_[prev], n * sizeof(double))) return rc;
+        PressureVjpLaunch p{};
+        p.st = st;
+        p.pressure = ph.P(k);
+        p.acceleration_adjoint = acceleration_adjoint_[cur];
+        p.pressure_adjoint = pressure_adjoint_[cur];
+        p.density_adjoint = density_adjoint_;
+        p.x = X;
+        p.pa = pa;
+        p.method = method;
+        p.relaxation = relaxation;
+        p.target = target;
+        p.previous_pressure = ph.P(k - 1);
+        p.predicted_density = ph.R(k);
+        p.previous_pressure_adjoint = pressure_adjoint_[prev];
+        p.predicted_density_adjoint = predicted_density_adjoint_;
+        p.relaxation_adjoint = relaxation_adjoint;
+        if (int rc = check(launch_pressure_vjp(s, p, block), "pressure reverse")) return rc;
+        DensityVjpLaunch d{};
+        d.st = st;
+        d.positions = ph.X(k);
+        d.density_adjoint = predicted_density_adjoint_;
+        d.walk = 2;
+        d.displacement_slot = ph.first_slot + k - 1u;
+        d.x = X;
+        d.v = V;
+        d.pa = pa;
+        d.predicted = 1;
+        d.acceleration = ph.A(k - 1);
+        d.base = base;
+        d.non_pressure_adjoint = non_pressure_adjoint_;
+        d.acceleration_adjoint = acceleration_adjoint_[prev];
+        d.base_adjoint = base_adjoint;
+        if (int rc = check(launch_density_vjp(s, d, block), "predicted density reverse")) return rc;
+        cur = prev;
+        return PBF_SUCCESS;
+    };
+    // The pressure pass of an iteration-0 pressure (DFSPH's warm starts): no update before it.
+    auto reverse_warm_pressure = [&](const Phase& ph, double* warm_adjoint) -> int {
+        PressureVjpLaunch p{};
+        p.st = st;
+        p.pressure = ph.P(0);
+        p.acceleration_adjoint = acceleration_adjoint_[cur];
+        p.pressure_adjoint = pressure_adjoint_[cur];
+        p.density_adjoint = density_adjoint_;
+        p.x = X;
+        p.pa = pa;
+        p.method = 0u;
+        p.warm_adjoint = warm_adjoint;
+        return check(launch_pressure_vjp(s, p, block), "pressure reverse");
+    };
+    const Phase& p0 = r.phase[0];
+    if (method == SPH_METHOD_PCISPH || method == SPH_METHOD_IISPH) {
+        const uint32_t K = p0.iterations;
+        if (int rc = check(launch_predict_vjp(s, st, p0.A(K), nullptr, nx, nv, X, V, non_pressure_adjoint_, acceleration_adjoint_[cur],
+                                              nullptr, nullptr, pressure_adjoint_[cur]),
+                           "prediction reverse"))
+            return rc;
+        for (uint32_t k = K; k >= 1u; --k)
+            if (int rc = reverse_iteration(p0, k, 0u, 0u, pa.method0, nullptr, nullptr)) return rc;
+    } else {
+        const Phase& p1 = r.phase[1];
+        const uint32_t Kd = p0.iterations, Kr = p1.iterations;
+        const bool warm = config_.pressure_warm_start != 0;
+        const float4* divergence = p0.A(Kd);
+        const double* next_warm_density = next_method_adjoint ? next_method_adjoint->warm_density_pressure : nullptr;
+        const double* next_warm_divergence = next_method_adjoint ? next_method_adjoint->warm_divergence_pressure : nullptr;
+        if (warm && (!previous_method_adjoint || !previous_method_adjoint->warm_divergence_pressure ||
+                     !previous_method_adjoint->warm_density_pressure)) {
+            set_error("DFSPH with warm starts needs previous_method_adjoint");
+            return PBF_ERROR_INVALID_ARGUMENT;
+        }
+        if (int rc = check(launch_predict_vjp(s, st, p1.A(Kr), divergence, nx, nv, X, V, non_pressure_adjoint_, acceleration_adjoint_[cur],
+                                              divergence_adjoint_, next_warm_density, pressure_adjoint_[cur]),
+                           "prediction reverse"))
+            return rc;
+        for (uint32_t k = Kr; k >= 1u; --k)
+            if (int rc = reverse_iteration(p1, k, 1u, 0u, pa.method1, divergence, divergence_adjoint_)) return rc;
+        if (int rc = reverse_warm_pressure(p1, warm ? previous_method_adjoint->warm_density_pressure : nullptr)) return rc;
+        if (int rc = check(launch_phase_seed(s, count_, r.sorted_index, divergence_adjoint_, acceleration_adjoint_[cur],
+                                             next_warm_divergence, pressure_adjoint_[cur]),
+                           "phase switch"))
+            return rc;
+        for (uint32_t k = Kd; k >= 1u; --k)
+            if (int rc = reverse_iteration(p0, k, 0u, 1u, pa.method0, nullptr, nullptr)) return rc;
+        if (int rc = reverse_warm_pressure(p0, warm ? previous_method_adjoint->warm_divergence_pressure : nullptr)) return rc;
+    }
+    if (int rc = check(launch_non_pressure_vjp(s, st, non_pressure_adjoint_, X, V, C, density_adjoint_, pa, block),
+                       "non-pressure reverse"))
+        return rc;
+    return density_step();
 }
 
 int SphEngine::read(const SphRecord& r, const sph_cache_field field, float* x, float* y, float* z) {
@@ -535,11 +809,11 @@ int SphEngine::read(const SphRecord& r, const sph_cache_field field, float* x, f
     const bool w = config_.method == SPH_METHOD_WCSPH;
     switch (field) {
         case SPH_CACHE_DENSITIES: return scalar(r.density);
-        case SPH_CACHE_PRESSURES: return scalar(r.pressure[r.final_pressure]);
-        case SPH_CACHE_PRESSURE_ACCELERATIONS: return vec(r.pressure_acceleration);
+        case SPH_CACHE_PRESSURES: return scalar(r.final_pressure);
+        case SPH_CACHE_PRESSURE_ACCELERATIONS: return vec(r.final_acceleration);
         case SPH_CACHE_VISCOSITY_ACCELERATIONS: return vec(w ? r.viscosity_acceleration : r.non_pressure);
         case SPH_CACHE_SURFACE_ACCELERATIONS: return vec(r.surface_acceleration);
-        case SPH_CACHE_PREDICTED_DENSITIES: return scalar(r.predicted_density);
+        case SPH_CACHE_PREDICTED_DENSITIES: return scalar(r.final_predicted_density);
         default: break;
     }
     set_error("unknown cache field");
@@ -646,6 +920,26 @@ int sph_forward_step(sph_solver* solver, const pbf_particle_state* state, const 
     }
     return guarded([&] {
         return solver->engine.forward(state, method_state, control, parameters, next_state, next_method_state, cache->record);
+    });
+}
+
+int sph_vjp_step(sph_solver* solver, const pbf_particle_state* state, const sph_method_state* method_state,
+                 const pbf_control* control, const sph_parameters* parameters, const pbf_particle_state* next_state,
+                 const sph_step_cache* cache, const pbf_particle_state_adjoint* next_adjoint,
+                 const sph_method_state_adjoint* next_method_adjoint, pbf_particle_state_adjoint* previous_adjoint,
+                 sph_method_state_adjoint* previous_method_adjoint, pbf_control_adjoint* control_adjoint,
+                 sph_parameter_adjoint* parameter_adjoint) {
+    if (!solver) return null_arg("solver");
+    if (!cache) return null_arg("cache");
+    (void)control;
+    (void)next_state;
+    if (cache->solver != solver) {
+        pbf::set_error("the step cache belongs to another solver");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    return guarded([&] {
+        return solver->engine.reverse(state, method_state, parameters, cache->record, next_adjoint, next_method_adjoint,
+                                      previous_adjoint, previous_method_adjoint, control_adjoint, parameter_adjoint);
     });
 }
 

@@ -3,7 +3,7 @@
 // The SPH family of the reference (sph/sph.ixx:39-372: WCSPH, PCISPH, IISPH, DFSPH) runs on the
 // same cell-sorted particles, stencil order and stored neighbour lists as the PBF substep.  The
 // grid is built from the input positions at the input step's time (sph/sph.ixx:351) and every
-// gather uses the cubic spline kernel (density/device.cuh:26-42, 76-79).
+// gather uses the cubic spline kernel (density/device.cuh:26-43, 72-76).
 #pragma once
 
 #include <cstdint>
@@ -22,7 +22,7 @@ struct SphConstants {
     float cubic_coefficient;        // 8 / (pi h h h)                        (density/device.cuh:29)
     float cubic_coefficient_2;      // 2 * cubic_coefficient (exact)         (density/device.cuh:32)
     float support_threshold;        // smallest r2 with sqrtf(r2) >= h: the cubic kernels vanish at r2 >= this
-    float laplacian_denominator;    // pi h h h h h h                        (density/device.cuh:78)
+    float laplacian_denominator;    // pi h h h h h h                        (density/device.cuh:75)
     float epsilon_factor;           // 0.01 h: the viscosity denominator is r2 + 0.01 h h (sph/wcsph.cu:157, 169)
     float diameter;                 // 2 r                                   (sph/wcsph.cu:467)
     float contact_weight;           // cubic((2 r, 0, 0))                    (sph/wcsph.cu:326)
@@ -46,7 +46,7 @@ struct SphStep {
     const float4* velocity;          // (v, 0)
     StoredList list;                 // in-support neighbours of every particle (fluid and boundary)
     const float4* boundary_velocity; // (velocity, 0) of the cell-sorted boundary particles, or null
-    float4* aux;                     // (density, viscosity, speed of sound, 0)
+    float4* aux;                     // (density, viscosity, speed of sound, surface tension)
     float4* non_pressure;            // non-pressure acceleration (iterative methods)
     float4* predicted;               // (predicted position, mass)
     unsigned int* displacement;      // per prediction: max |x* - x| (float bits), zeroed every step
@@ -65,7 +65,7 @@ cudaError_t launch_density(cudaStream_t stream, const SphStep& st, uint32_t meth
 // (sph/sph.cpp:214-225) in one pass; writes the next state in original order.
 cudaError_t launch_wcsph_forces(cudaStream_t stream, const SphStep& st, const float* pressure_term, MutField3 out_positions,
                                 MutField3 out_velocities, float4* record_pressure, float4* record_viscosity,
-                                float4* record_surface, unsigned block);
+                                float4* record_surface, float4* record_total, unsigned block);
 
 // Non-pressure acceleration (sph/common.cu:14-47) and, for PCISPH / IISPH, the first prediction
 // with the cleared pressure acceleration (sph/sph.cpp:300-303).
@@ -119,6 +119,82 @@ struct SphSceneInput {
 };
 cudaError_t launch_sph_constants(cudaStream_t stream, const SphSceneInput* inputs, uint32_t n, SphConstants* out,
                                  KernelConstants* list_constants);
+
+// ------------------------------------------------------------------ reverse passes (sph_grad.cu)
+// Caller-side parameter adjoints, original order (accumulated).  method0..2 follow the packing of
+// params_a.w / params_b.x / params_b.y.
+struct SphParameterAdjoints {
+    double* masses;
+    double* rest_densities;
+    double* viscosities;
+    double* surface_tensions;
+    double* method0;
+    double* method1;
+    double* method2;
+};
+
+// integrate_vjp (sph/common.cu:344-366) of WCSPH; also adds the acceleration adjoint to the control's.
+cudaError_t launch_integrate_vjp(cudaStream_t stream, const SphStep& st, const float4* total, ConstAdjField3 next_x,
+                                 ConstAdjField3 next_v, AdjField3 x, AdjField3 v, AdjField3 control, double4* acceleration);
+// surface, viscosity and pressure VJPs of WCSPH with the equation of state's (sph/sph.cpp:245-248);
+// writes the density adjoint (sorted).
+cudaError_t launch_wcsph_force_vjp(cudaStream_t stream, const SphStep& st, const float* pressure, const double4* acceleration,
+                                   AdjField3 x, AdjField3 v, const SphParameterAdjoints& pa, double* density_adjoint, unsigned block);
+
+// density_vjp (density/density.cu:68-99) at the step's positions or at a prediction; for a
+// prediction also the reverse of the prediction (predict_vjp, sph/pcisph.cu:67-103).
+struct DensityVjpLaunch {
+    SphStep st;
+    const float4* positions;
+    const double* density_adjoint;
+    int walk;                       // 0 list, 1 stencil walk, 2 as the forward decided from the displacement slot
+    uint32_t displacement_slot;
+    AdjField3 x, v;
+    SphParameterAdjoints pa;
+    int predicted;
+    const float4* acceleration;     // the pressure acceleration of the prediction
+    const float4* base;             // DFSPH's divergence acceleration, or null
+    double4* non_pressure_adjoint;
+    double4* acceleration_adjoint;
+    double4* base_adjoint;
+};
+cudaError_t launch_density_vjp(cudaStream_t stream, const DensityVjpLaunch& d, unsigned block);
+
+// The reverse of the last prediction (the next state) of an iterative method.
+cudaError_t launch_predict_vjp(cudaStream_t stream, const SphStep& st, const float4* acceleration, const float4* base,
+                               ConstAdjField3 next_x, ConstAdjField3 next_v, AdjField3 x, AdjField3 v, double4* non_pressure_adjoint,
+                               double4* acceleration_adjoint, double4* base_adjoint, const double* next_warm,
+                               double* pressure_adjoint);
+
+// pressure_vjp (sph/common.cu:239-300) of iterate k and, when it has one, the reverse of the
+// pressure update that produced it.
+struct PressureVjpLaunch {
+    SphStep st;
+    const float* pressure;
+    const double4* acceleration_adjoint;
+    double* pressure_adjoint;
+    double* density_adjoint;
+    AdjField3 x;
+    SphParameterAdjoints pa;
+    uint32_t method;                // 0: no update (an iteration-0 pressure)
+    uint32_t relaxation;
+    uint32_t target;
+    const float* previous_pressure;
+    const float* predicted_density;
+    double* previous_pressure_adjoint;
+    double* predicted_density_adjoint;
+    double* relaxation_adjoint;
+    double* warm_adjoint;
+};
+cudaError_t launch_pressure_vjp(cudaStream_t stream, const PressureVjpLaunch& d, unsigned block);
+
+// non_pressure_vjp (sph/common.cu:98-163).
+cudaError_t launch_non_pressure_vjp(cudaStream_t stream, const SphStep& st, const double4* adjoint, AdjField3 x, AdjField3 v,
+                                    AdjField3 control, double* density_adjoint, const SphParameterAdjoints& pa, unsigned block);
+
+// DFSPH's switch from the density to the divergence phase in the reverse sweep.
+cudaError_t launch_phase_seed(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const double4* from,
+                              double4* acceleration_adjoint, const double* next_warm, double* pressure_adjoint);
 
 // compute_reference_gradient_norm (sph/sph.cpp:36-58) on the host.
 float reference_gradient_norm(float support_radius, float particle_radius);

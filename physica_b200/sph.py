@@ -62,6 +62,10 @@ class MethodStateC(ctypes.Structure):
     _fields_ = [("warm_divergence_pressure", ctypes.c_void_p), ("warm_density_pressure", ctypes.c_void_p)]
 
 
+class ParameterAdjointC(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in PARAMETER_NAMES]
+
+
 _bound = False
 
 
@@ -79,6 +83,9 @@ def library() -> ctypes.CDLL:
         lib.sph_forward_step.argtypes = [vp, P(ParticleStateC), P(MethodStateC), P(ControlC), P(ParametersC),
                                          P(ParticleStateC), P(MethodStateC), vp]
         lib.sph_read_cache.argtypes = [vp, vp, ctypes.c_int, vp, vp, vp]
+        lib.sph_vjp_step.argtypes = [vp, P(ParticleStateC), P(MethodStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
+                                     P(pbf.StateAdjointC), P(MethodStateC), P(pbf.StateAdjointC), P(MethodStateC), P(ControlC),
+                                     P(ParameterAdjointC)]
         lib.sph_reference_gradient_norm.argtypes = [vp, P(ctypes.c_float)]
         lib.sph_set_launch_shape.argtypes = [vp, P(LaunchShapeC)]
         lib.sph_get_launch_shape.argtypes = [vp, P(LaunchShapeC)]
@@ -116,6 +123,23 @@ class State:
 
     def c(self) -> ParticleStateC:
         return ParticleStateC(_vf(self.positions), _vf(self.velocities), self.step_index)
+
+    def method_c(self) -> MethodStateC:
+        a, b = self.warm_divergence_pressure, self.warm_density_pressure
+        return MethodStateC(_ptr(a) if a is not None and a.numel() else None, _ptr(b) if b is not None and b.numel() else None)
+
+
+@dataclasses.dataclass
+class StateAdjoint:
+    """SPH<Method>::StateAdjoint (sph/sph.ixx:283-286): (3, N) float64 position / velocity adjoints
+    and, for DFSPH, the (N,) float64 adjoints of the warm-start pressures."""
+    positions: torch.Tensor
+    velocities: torch.Tensor
+    warm_divergence_pressure: torch.Tensor | None = None
+    warm_density_pressure: torch.Tensor | None = None
+
+    def c(self) -> pbf.StateAdjointC:
+        return pbf.StateAdjointC(_vf(self.positions), _vf(self.velocities))
 
     def method_c(self) -> MethodStateC:
         a, b = self.warm_divergence_pressure, self.warm_density_pressure
@@ -225,6 +249,18 @@ class SPH:
     def allocate_step_cache(self) -> StepCache:
         return StepCache(self)
 
+    def allocate_state_adjoint(self) -> StateAdjoint:
+        z3 = lambda: torch.zeros((3, self.count), dtype=torch.float64, device=self.device)
+        dfsph = self.method == Method.dfsph
+        z = (lambda: torch.zeros(self.count, dtype=torch.float64, device=self.device)) if dfsph else (lambda: None)
+        return StateAdjoint(z3(), z3(), z(), z())
+
+    def allocate_control_adjoint(self) -> pbf.Control:
+        return pbf.Control(torch.zeros((3, self.count), dtype=torch.float64, device=self.device))
+
+    def allocate_parameter_adjoint(self) -> Parameters:
+        return Parameters({n: torch.zeros(self.count, dtype=torch.float64, device=self.device) for n in PARAMETER_NAMES})
+
     def state_from_arrays(self, positions, velocities, step_index=0) -> State:
         s = self.allocate_state()
         s.positions.copy_(torch.as_tensor(np.ascontiguousarray(positions)))
@@ -256,6 +292,20 @@ class SPH:
                                           ctypes.byref(parameters.c()), ctypes.byref(ns), ctypes.byref(nms), cache.handle))
         next_state.step_index = ns.step_index
 
+    def vjp_step(self, state: State, control: pbf.Control, parameters: Parameters, next_state: State, cache: StepCache,
+                 next_state_adjoint: StateAdjoint, previous_state_adjoint: StateAdjoint, control_adjoint: pbf.Control,
+                 parameter_adjoint: Parameters):
+        """SPH<Method>::vjp_step (sph/sph.ixx:361-365); accumulates into the previous-state, control
+        and parameter adjoints (DFSPH's previous warm-pressure adjoints are overwritten)."""
+        pa = ParameterAdjointC(*[_ptr(parameter_adjoint.tensors[n]) if parameter_adjoint.tensors.get(n) is not None else None
+                                 for n in PARAMETER_NAMES])
+        check(library().sph_vjp_step(self.handle, ctypes.byref(state.c()), ctypes.byref(state.method_c()),
+                                     ctypes.byref(control.c()), ctypes.byref(parameters.c()), ctypes.byref(next_state.c()),
+                                     cache.handle, ctypes.byref(next_state_adjoint.c()),
+                                     ctypes.byref(next_state_adjoint.method_c()), ctypes.byref(previous_state_adjoint.c()),
+                                     ctypes.byref(previous_state_adjoint.method_c()), ctypes.byref(control_adjoint.c()),
+                                     ctypes.byref(pa)))
+
     @property
     def reference_gradient_norm(self) -> float:
         v = ctypes.c_float()
@@ -276,11 +326,12 @@ class SPH:
         check(library().sph_synchronize(self.handle))
 
 
-def solver_for_scene(scene, method: Method, *, configuration: Configuration | None = None, device="cuda"):
+def solver_for_scene(scene, method: Method, *, configuration: Configuration | None = None,
+                     mode: pbf.ExecutionMode = pbf.ExecutionMode.forward, device="cuda"):
     """A solver, state, control and parameters for a synthetic SPH scene (scenes.sph_dam_break)."""
     dc = pbf.DomainConfiguration.from_scene(scene)
     cfg = configuration or Configuration(method=Method(method))
-    solver = SPH(dc, cfg, device=device)
+    solver = SPH(dc, cfg, mode, device=device)
     state = solver.state_from_arrays(scene.positions, scene.velocities)
     control = solver.allocate_control()
     control.external_accelerations.copy_(torch.from_numpy(scene.controls))

@@ -162,12 +162,16 @@ def test_launch_shapes_give_identical_results(shape):
     assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
 
 
-def test_differentiable_mode_is_rejected():
+def test_vjp_needs_a_differentiable_solver():
     sc = _scene("wcsph")
-    dc = pbf.DomainConfiguration.from_scene(sc)
+    solver, state, control, params = sph.solver_for_scene(sc, sph.Method.wcsph)
+    cache = solver.allocate_step_cache()
+    nxt = solver.allocate_state()
+    solver.forward_step(state, control, params, nxt, cache)
     with pytest.raises(pbf.PBFError) as err:
-        sph.SPH(dc, sph.Configuration(), pbf.ExecutionMode.differentiable)
-    assert err.value.status == 5   # PBF_ERROR_UNSUPPORTED
+        solver.vjp_step(state, control, params, nxt, cache, solver.allocate_state_adjoint(), solver.allocate_state_adjoint(),
+                        solver.allocate_control_adjoint(), solver.allocate_parameter_adjoint())
+    assert err.value.status == 4   # PBF_ERROR_NOT_DIFFERENTIABLE
 
 
 def test_empty_scene_steps():

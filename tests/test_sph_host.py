@@ -20,10 +20,9 @@ def _create(cuda_lib, configuration, mode=0, **domain):
     return rc, h
 
 
-def test_create_rejects_differentiable_mode(cuda_lib):
-    rc, h = _create(cuda_lib, sph.Configuration(), mode=1)
-    assert rc == 5 and not h.value
-    assert b"forward-mode" in pbf.library().pbf_last_error()
+def test_create_rejects_unknown_mode(cuda_lib):
+    rc, h = _create(cuda_lib, sph.Configuration(), mode=7)
+    assert rc == 1 and not h.value
 
 
 @pytest.mark.parametrize("field,value", [("time_step", 0.0), ("support_radius", float("nan"))])
