@@ -11,8 +11,8 @@
  * The domain description is the PBF one (pbf_domain_configuration: the reference's
  * DomainConfiguration is shared by both families, domain/domain.ixx:12-165).
  *
- * Differentiable mode (PBF_EXECUTION_DIFFERENTIABLE) adds SPH<Method>::vjp_step
- * (sph/sph.ixx:361-365): FP64 adjoints, accumulated like the PBF ones.
+ * Differentiable mode (PBF_EXECUTION_DIFFERENTIABLE) adds SPH<Method>::jvp_step and ::vjp_step
+ * (sph/sph.ixx:356-365): FP32 tangents, and FP64 adjoints accumulated like the PBF ones.
  */
 #ifndef PHYSICA_SPH_H
 #define PHYSICA_SPH_H
@@ -120,6 +120,21 @@ int sph_free_step_cache(sph_solver* solver, sph_step_cache* cache);
 int sph_forward_step(sph_solver* solver, const pbf_particle_state* state, const sph_method_state* method_state,
                      const pbf_control* control, const sph_parameters* parameters, pbf_particle_state* next_state,
                      sph_method_state* next_method_state, sph_step_cache* cache);
+
+/* SPH<Method>::ParameterTangent (sph/sph.ixx:291-294): the layout of sph_parameters, FP32
+ * tangents; NULL arrays are zero. */
+typedef sph_parameters sph_parameter_tangent;
+
+/* SPH<Method>::jvp_step (sph/sph.ixx:356-359): the tangent of the step recorded in `cache`, FP32,
+ * solver in PBF_EXECUTION_DIFFERENTIABLE mode.  method_tangent / next_method_tangent: DFSPH's
+ * warm-start pressure tangents (NULL = zero in; the next ones are written when not NULL).
+ * next_state is accepted for the reference's signature and not read. */
+int sph_jvp_step(sph_solver* solver, const pbf_particle_state* state, const sph_method_state* method_state,
+                 const pbf_control* control, const sph_parameters* parameters, const pbf_particle_state* next_state,
+                 const sph_step_cache* cache, const pbf_particle_state_tangent* state_tangent,
+                 const sph_method_state* method_tangent, const pbf_control* control_tangent,
+                 const sph_parameter_tangent* parameter_tangent, pbf_particle_state_tangent* next_tangent,
+                 sph_method_state* next_method_tangent);
 
 /* SPH<Method>::vjp_step (sph/sph.ixx:361-365): the adjoint of the step recorded in `cache` (the
  * forward_step of `state`), solver in PBF_EXECUTION_DIFFERENTIABLE mode.  previous_adjoint,

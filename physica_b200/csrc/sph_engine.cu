@@ -99,6 +99,10 @@ public:
                 sph_method_state_adjoint* previous_method_adjoint, pbf_control_adjoint* control_adjoint,
                 sph_parameter_adjoint* parameter_adjoint);
     bool differentiable() const { return differentiable_; }
+    int tangent(const pbf_particle_state* state, const SphRecord& r, const pbf_particle_state_tangent* state_tangent,
+                const sph_method_state* method_tangent, const pbf_control* control_tangent,
+                const sph_parameter_tangent* parameter_tangent, pbf_particle_state_tangent* next_tangent,
+                sph_method_state* next_method_tangent);
     int check(cudaError_t e, const char* what) {
         if (e == cudaSuccess) return PBF_SUCCESS;
         cudaGetLastError();
@@ -150,6 +154,17 @@ private:
     double* density_adjoint_ = nullptr;
     double* pressure_adjoint_[2] = {nullptr, nullptr};
     double* predicted_density_adjoint_ = nullptr;
+    // tangent workspace (sorted order), allocated on first use
+    DeviceArena tangent_arena_;
+    float4* tangent_x_ = nullptr;
+    float4* tangent_v_ = nullptr;
+    float4* tangent_a_ = nullptr;
+    float4* tangent_b_ = nullptr;
+    float* tangent_density_ = nullptr;
+    float* tangent_pressure_[2] = {nullptr, nullptr};
+    float4* tangent_non_pressure_ = nullptr;
+    float4* tangent_predicted_ = nullptr;
+    float4* tangent_divergence_ = nullptr;
 };
 
 namespace {
@@ -779,6 +794,148 @@ int SphEngine::reverse(const pbf_particle_state* state, const sph_method_state* 
     return density_step();
 }
 
+// SPH<Method>::jvp_step (sph/sph.ixx:356-359): the density's tangent, then Method::jvp
+// (sph/sph.cpp:227-237, 314-330, 427-443, 612-659) over the iterates the forward kept.
+int SphEngine::tangent(const pbf_particle_state* state, const SphRecord& r, const pbf_particle_state_tangent* state_tangent,
+                       const sph_method_state* method_tangent, const pbf_control* control_tangent,
+                       const sph_parameter_tangent* parameter_tangent, pbf_particle_state_tangent* next_tangent,
+                       sph_method_state* next_method_tangent) {
+    if (!differentiable_) {
+        set_error("jvp_step needs a solver created in PBF_EXECUTION_DIFFERENTIABLE mode");
+        return PBF_ERROR_NOT_DIFFERENTIABLE;
+    }
+    if (!state || !state_tangent || !control_tangent || !next_tangent) {
+        set_error("null argument");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (!r.valid || !r.differentiable || r.step_index != state->step_index) {
+        set_error("the step cache does not hold the forward step of this state");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (count_ == 0) return PBF_SUCCESS;
+    auto has = [](const pbf_vector_field& f) { return f.x && f.y && f.z; };
+    if (!has(state_tangent->positions) || !has(state_tangent->velocities) || !has(control_tangent->external_accelerations) ||
+        !has(next_tangent->positions) || !has(next_tangent->velocities)) {
+        set_error("null tangent field pointer");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    if (!tangent_x_) {
+        tangent_arena_.set_stream(stream_);
+        cudaError_t e = cudaSuccess;
+        const size_t n = count_;
+        tangent_x_ = tangent_arena_.alloc<float4>(n, e);
+        tangent_v_ = tangent_arena_.alloc<float4>(n, e);
+        tangent_a_ = tangent_arena_.alloc<float4>(n, e);
+        tangent_b_ = tangent_arena_.alloc<float4>(n, e);
+        tangent_density_ = tangent_arena_.alloc<float>(n, e);
+        for (auto& p : tangent_pressure_) p = tangent_arena_.alloc<float>(n, e);
+        tangent_non_pressure_ = tangent_arena_.alloc<float4>(n, e);
+        tangent_predicted_ = tangent_arena_.alloc<float4>(n, e);
+        tangent_divergence_ = tangent_arena_.alloc<float4>(n, e);
+        if (int rc = check(e, "tangent workspace")) {
+            tangent_arena_.release();
+            tangent_x_ = nullptr;
+            return rc;
+        }
+    }
+    const uint32_t method = config_.method;
+    SphParameterTangents pt{};
+    if (parameter_tangent) {
+        const sph_parameter_tangent& q = *parameter_tangent;
+        pt = {q.masses, q.rest_densities, q.viscosities, q.surface_tensions, nullptr, nullptr, nullptr};
+        if (method == SPH_METHOD_WCSPH) {
+            pt.method0 = q.speed_of_sound;
+            pt.method1 = q.tait_exponent;
+            pt.method2 = q.boundary_surface_tension;
+        } else if (method == SPH_METHOD_PCISPH) {
+            pt.method0 = q.pressure_relaxation;
+        } else if (method == SPH_METHOD_IISPH) {
+            pt.method0 = q.jacobi_relaxation;
+        } else {
+            pt.method0 = q.divergence_relaxation;
+            pt.method1 = q.density_relaxation;
+        }
+    }
+    const cudaStream_t s = stream_;
+    const unsigned block = shape.block;
+    SphTangentStep t{step_of(r), tangent_x_, tangent_v_, tangent_a_, tangent_b_, tangent_density_, tangent_pressure_[0],
+                     tangent_non_pressure_, tangent_predicted_};
+    const Field3 tx{state_tangent->positions.x, state_tangent->positions.y, state_tangent->positions.z};
+    const Field3 tv{state_tangent->velocities.x, state_tangent->velocities.y, state_tangent->velocities.z};
+    const Field3 tc{control_tangent->external_accelerations.x, control_tangent->external_accelerations.y,
+                    control_tangent->external_accelerations.z};
+    const MutField3 out_x{next_tangent->positions.x, next_tangent->positions.y, next_tangent->positions.z};
+    const MutField3 out_v{next_tangent->velocities.x, next_tangent->velocities.y, next_tangent->velocities.z};
+    if (int rc = check(launch_tangent_seed(s, t, tx, tv, pt), "tangent seed")) return rc;
+    const bool warm = method == SPH_METHOD_DFSPH && config_.pressure_warm_start != 0;
+    const float* warm_divergence = warm && method_tangent ? method_tangent->warm_divergence_pressure : nullptr;
+    const float* warm_density = warm && method_tangent ? method_tangent->warm_density_pressure : nullptr;
+    if (int rc = check(launch_density_jvp(s, t, method, warm_divergence, block), "density tangent")) return rc;
+    const Phase& p0 = r.phase[0];
+    if (method == SPH_METHOD_WCSPH)
+        return check(launch_wcsph_force_jvp(s, t, p0.P(0), r.total_acceleration, tc, out_x, out_v, block), "force tangent");
+    auto iterate = [&](const SphTangentStep& tp, const Phase& ph, const uint32_t k, const uint32_t relaxation,
+                       const uint32_t target) {
+        const PredictedJvp u{method, relaxation, target, ph.first_slot + k - 1u, ph.X(k), ph.R(k), ph.P(k - 1u)};
+        return check(launch_predicted_density_jvp(s, tp, u, block), "predicted density tangent");
+    };
+    if (method == SPH_METHOD_PCISPH || method == SPH_METHOD_IISPH) {
+        const uint32_t K = p0.iterations;
+        if (int rc = check(launch_non_pressure_jvp(s, t, tc, K > 0 ? 1 : 2, out_x, out_v, block), "non-pressure tangent"))
+            return rc;
+        for (uint32_t k = 1; k <= K; ++k) {
+            if (int rc = iterate(t, p0, k, 0u, 0u)) return rc;
+            PressureJvp u{};
+            u.pressure = p0.P(k);
+            u.acceleration = p0.A(k);
+            u.last = k == K ? 1 : 0;
+            u.out_x = out_x;
+            u.out_v = out_v;
+            if (int rc = check(launch_pressure_jvp(s, t, u, block), "pressure tangent")) return rc;
+        }
+        return PBF_SUCCESS;
+    }
+    // DFSPH: the divergence phase on tangent buffer 0, the density phase on buffer 1
+    if (int rc = check(launch_non_pressure_jvp(s, t, tc, 0, out_x, out_v, block), "non-pressure tangent")) return rc;
+    const Phase& p1 = r.phase[1];
+    const uint32_t Kd = p0.iterations, Kr = p1.iterations;
+    SphTangentStep t1 = t;
+    t1.pressure = tangent_pressure_[1];
+    for (uint32_t k = 0; k <= Kd; ++k) {
+        if (k > 0) {
+            if (int rc = iterate(t, p0, k, 0u, 1u)) return rc;
+        }
+        PressureJvp u{};
+        u.pressure = p0.P(k);
+        u.acceleration = p0.A(k);
+        if (k == Kd) {
+            u.store = tangent_divergence_;
+            u.warm_out = next_method_tangent ? next_method_tangent->warm_divergence_pressure : nullptr;
+            u.next_pressure = tangent_pressure_[1];
+            u.next_warm = warm_density;
+        }
+        if (int rc = check(launch_pressure_jvp(s, t, u, block), "pressure tangent")) return rc;
+    }
+    for (uint32_t k = 0; k <= Kr; ++k) {
+        if (k > 0) {
+            if (int rc = iterate(t1, p1, k, 1u, 0u)) return rc;
+        }
+        PressureJvp u{};
+        u.pressure = p1.P(k);
+        u.acceleration = p1.A(k);
+        u.base = p0.A(Kd);
+        u.base_tangent = tangent_divergence_;
+        if (k == Kr) {
+            u.last = 1;
+            u.out_x = out_x;
+            u.out_v = out_v;
+            u.warm_out = next_method_tangent ? next_method_tangent->warm_density_pressure : nullptr;
+        }
+        if (int rc = check(launch_pressure_jvp(s, t1, u, block), "pressure tangent")) return rc;
+    }
+    return PBF_SUCCESS;
+}
+
 int SphEngine::read(const SphRecord& r, const sph_cache_field field, float* x, float* y, float* z) {
     if (!r.valid) {
         set_error("the step cache holds no forward step");
@@ -920,6 +1077,28 @@ int sph_forward_step(sph_solver* solver, const pbf_particle_state* state, const 
     }
     return guarded([&] {
         return solver->engine.forward(state, method_state, control, parameters, next_state, next_method_state, cache->record);
+    });
+}
+
+int sph_jvp_step(sph_solver* solver, const pbf_particle_state* state, const sph_method_state* method_state,
+                 const pbf_control* control, const sph_parameters* parameters, const pbf_particle_state* next_state,
+                 const sph_step_cache* cache, const pbf_particle_state_tangent* state_tangent,
+                 const sph_method_state* method_tangent, const pbf_control* control_tangent,
+                 const sph_parameter_tangent* parameter_tangent, pbf_particle_state_tangent* next_tangent,
+                 sph_method_state* next_method_tangent) {
+    if (!solver) return null_arg("solver");
+    if (!cache) return null_arg("cache");
+    (void)method_state;
+    (void)control;
+    (void)parameters;
+    (void)next_state;
+    if (cache->solver != solver) {
+        pbf::set_error("the step cache belongs to another solver");
+        return PBF_ERROR_INVALID_ARGUMENT;
+    }
+    return guarded([&] {
+        return solver->engine.tangent(state, cache->record, state_tangent, method_tangent, control_tangent, parameter_tangent,
+                                      next_tangent, next_method_tangent);
     });
 }
 

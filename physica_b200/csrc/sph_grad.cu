@@ -848,3 +848,592 @@ cudaError_t launch_phase_seed(cudaStream_t stream, const uint32_t count, const u
 
 }  // namespace sph
 }  // namespace pbf
+
+// ================================================================== tangent passes (FP32)
+namespace pbf {
+namespace sph {
+
+namespace {
+
+using namespace gather_detail;
+using namespace detail;
+
+// Sorted tangents of the inputs: positions and masses, velocities, and the parameters packed as
+// params_a / params_b.
+__global__ void tangent_seed_kernel(const SphTangentStep t, const Field3 x, const Field3 v, const SphParameterTangents pt) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= t.st.g.count) return;
+    const uint32_t i = t.st.sorted_index[s];
+    auto get = [i](const float* p) { return p ? p[i] : 0.0F; };
+    t.x[s] = make_float4(x.x[i], x.y[i], x.z[i], get(pt.masses));
+    t.v[s] = make_float4(v.x[i], v.y[i], v.z[i], 0.0F);
+    t.params_a[s] = make_float4(get(pt.rest_densities), get(pt.viscosities), get(pt.surface_tensions), get(pt.method0));
+    t.params_b[s] = make_float4(get(pt.method1), get(pt.method2), 0.0F, 0.0F);
+}
+
+// density_jvp (density/density.cu:42-66): sum of dm_j W + m_j grad W . (dx_i - dx_j), boundary
+// V_b (drho0_i W + rho0_i grad W . dx_i).
+struct DensityJvpOp {
+    static constexpr bool kBoundary = true;
+    const float4* __restrict__ pos;
+    const float4* __restrict__ tangent;
+    const float4* __restrict__ boundary;
+    f3 x, dx;
+    float rest, drest;
+    SphConstants k;
+    float result;
+
+    __device__ __forceinline__ void process(const uint32_t t) {
+        if (t & kBoundaryBit) {
+            const float4 q = boundary[t & ~kBoundaryBit];
+            const f3 d = x - xyz(q);
+            const float w = cubic_value(d, k);
+            if (w == 0.0F) return;
+            result += q.w * (drest * w + rest * dot(cubic_gradient_value(d, k), dx));
+            return;
+        }
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        const float w = cubic_value(d, k);
+        if (w == 0.0F) return;
+        const float4 tq = tangent[t];
+        result += tq.w * w + q.w * dot(cubic_gradient_value(d, k), dx - xyz(tq));
+    }
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
+};
+
+// The density tangent at the step's positions (+ WCSPH's equation of state, sph/wcsph.cu:102-117;
+// DFSPH: the divergence phase's warm-start pressure tangent).
+__global__ void __launch_bounds__(kBlock) density_jvp_kernel(const SphTangentStep t, const uint32_t method, const float* warm) {
+    const SphStep& st = t.st;
+    const Own o = own(st);
+    if (!o.p.active) return;
+    const uint32_t s = o.p.s;
+    DensityJvpOp op{};
+    op.pos = st.topology;
+    op.tangent = t.x;
+    op.boundary = st.g.boundary;
+    op.x = o.x;
+    op.dx = xyz(t.x[s]);
+    op.rest = o.pa.x;
+    op.drest = t.params_a[s].x;
+    op.k = *o.k;
+    replay(op, o.p, st.g, st.list);
+    const float drho = op.result;
+    t.density[s] = drho;
+    float dp = 0.0F;
+    if (method == kWcsph) {
+        const float rho = st.aux[s].x, rest = o.pa.x, speed = o.pa.w, exponent = st.g.params_b[s].x;
+        const float4 ta = t.params_a[s], tb = t.params_b[s];
+        const float ratio = rho / rest;
+        const float powered = powf(ratio, exponent);
+        const float difference = powered - 1.0F;
+        const float d_density = speed * speed * powf(ratio, exponent - 1.0F);
+        const float d_rest = speed * speed * difference / exponent - speed * speed * powered;
+        const float d_speed = 2.0F * rest * speed * difference / exponent;
+        const float d_exponent = rest * speed * speed * (exponent * powered * logf(ratio) - difference) / (exponent * exponent);
+        dp = d_density * drho + d_rest * ta.x + d_speed * ta.w + d_exponent * tb.x;
+    } else if (warm) {
+        dp = warm[st.sorted_index[s]];
+    }
+    t.pressure[s] = dp;
+}
+
+// pressure_jvp (sph/common.cu:196-237) of one pair, FP32.
+__device__ __forceinline__ f3 pressure_pair_jvp(const f3 d, const f3 dd, const float factor, const float dfactor,
+                                                const SphConstants& k) {
+    return times(cubic_gradient_value(d, k), dfactor) + times(cubic_gradient_tangent(d, dd, k), factor);
+}
+
+struct ForceJvpOp {
+    static constexpr bool kBoundary = true;
+    const float4* __restrict__ pos;
+    const float4* __restrict__ vel;
+    const float4* __restrict__ aux;
+    const float* __restrict__ pressure;
+    const float4* __restrict__ tx;
+    const float4* __restrict__ tv;
+    const float4* __restrict__ tpa;
+    const float* __restrict__ tdensity;
+    const float* __restrict__ tpressure;
+    const float4* __restrict__ boundary;
+    const float4* __restrict__ boundary_velocity;
+    uint32_t self;
+    f3 x, v, dx, dv;
+    float mass, dmass, rest, drest, density, ddensity, viscosity, dviscosity, speed, dspeed, tension, dtension;
+    float boundary_tension, dboundary_tension, first, dfirst;
+    SphConstants k;
+    f3 rp, rv, rs;   // pressure, viscosity and surface tangents
+
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
+    __device__ __forceinline__ void process(const uint32_t t) {
+        const float h = k.h;
+        if (t & kBoundaryBit) {
+            const uint32_t b = t & ~kBoundaryBit;
+            const float4 q = boundary[b];
+            const f3 d = x - xyz(q);
+            const float distance = sqrtf(dot(d, d));
+            if (distance >= h) return;
+            const float volume = q.w;
+            // pressure (sph/common.cu:225-232)
+            rp = rp + pressure_pair_jvp(d, dx, -rest * volume * first, -volume * (drest * first + rest * dfirst), k);
+            // viscosity (sph/wcsph.cu:222-238)
+            const f3 vd = v - xyz(boundary_velocity[b]);
+            const float compression = dot(vd, d);
+            if (compression < 0.0F) {
+                const float dcompression = dot(dv, d) + dot(vd, dx);
+                const float denominator = dot(d, d) + 0.01F * h * h;
+                const float ddenominator = 2.0F * dot(d, dx);
+                const float nu = viscosity * h * speed / density;
+                const float dnu = h * (dviscosity * speed + viscosity * dspeed) / density - nu * ddensity / density;
+                const float pi = -nu * compression / denominator;
+                const float dpi = -(dnu * compression + nu * dcompression) / denominator +
+                                  nu * compression * ddenominator / (denominator * denominator);
+                const float m = rest * volume, dm = drest * volume;
+                rv = rv + times(cubic_gradient_value(d, k), -(dm * pi + m * dpi)) + times(cubic_gradient_tangent(d, dx, k), -m * pi);
+            }
+            // adhesion (sph/wcsph.cu:371-384)
+            const float weight = distance > k.diameter ? cubic_inside(distance, k) : k.contact_weight;
+            const float dweight = distance > k.diameter ? dot(cubic_gradient_value(d, k), dx) : 0.0F;
+            const float m = rest * volume, dm = drest * volume;
+            const float factor = -boundary_tension * m * weight / mass;
+            const float dfactor = -dboundary_tension * m * weight / mass - boundary_tension * dm * weight / mass -
+                                  boundary_tension * m * dweight / mass + boundary_tension * m * weight * dmass / (mass * mass);
+            rs = rs + times(d, dfactor) + times(dx, factor);
+            return;
+        }
+        if (t == self) return;
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        const float distance = sqrtf(dot(d, d));
+        if (distance >= h) return;
+        const float4 tq = tx[t];
+        const f3 dd = dx - xyz(tq);
+        const float mj = q.w, dmj = tq.w;
+        const float4 au = aux[t];
+        const float rho_j = au.x, drho_j = tdensity[t];
+        // pressure (sph/common.cu:214-222)
+        const float pj = pressure[t];
+        const float second = pj / (rho_j * rho_j);
+        const float dsecond = tpressure[t] / (rho_j * rho_j) - 2.0F * pj * drho_j / (rho_j * rho_j * rho_j);
+        rp = rp + pressure_pair_jvp(d, dd, -mj * (first + second), -dmj * (first + second) - mj * (dfirst + dsecond), k);
+        // viscosity (sph/wcsph.cu:196-220)
+        const f3 vd = v - xyz(vel[t]);
+        const float compression = dot(vd, d);
+        if (compression < 0.0F) {
+            const float4 tpj = tpa[t];
+            const f3 dvd = dv - xyz(tv[t]);
+            const float dcompression = dot(dvd, d) + dot(vd, dd);
+            const float denominator = dot(d, d) + 0.01F * h * h;
+            const float ddenominator = 2.0F * dot(d, dd);
+            const float alpha = 0.5F * (viscosity + au.y), dalpha = 0.5F * (dviscosity + tpj.y);
+            const float c = 0.5F * (speed + au.z), dc = 0.5F * (dspeed + tpj.w);
+            const float density_sum = density + rho_j, ddensity_sum = ddensity + drho_j;
+            const float nu = 2.0F * alpha * h * c / density_sum;
+            const float dnu = 2.0F * h * (dalpha * c + alpha * dc) / density_sum - nu * ddensity_sum / density_sum;
+            const float pi = -nu * compression / denominator;
+            const float dpi = -(dnu * compression + nu * dcompression) / denominator +
+                              nu * compression * ddenominator / (denominator * denominator);
+            rv = rv + times(cubic_gradient_value(d, k), -(dmj * pi + mj * dpi)) + times(cubic_gradient_tangent(d, dd, k), -mj * pi);
+        }
+        // cohesion (sph/wcsph.cu:355-368)
+        const float weight = distance > k.diameter ? cubic_inside(distance, k) : k.contact_weight;
+        const float dweight = distance > k.diameter ? dot(cubic_gradient_value(d, k), dd) : 0.0F;
+        const float factor = -tension * mj * weight / mass;
+        const float dfactor = -dtension * mj * weight / mass - tension * dmj * weight / mass - tension * mj * dweight / mass +
+                              tension * mj * weight * dmass / (mass * mass);
+        rs = rs + times(d, dfactor) + times(dd, factor);
+    }
+};
+
+// The prediction's tangent (sph/pcisph.cu:46-66; integrate_jvp, sph/common.cu:322-342).
+__device__ __forceinline__ void predict_tangent(const f3 x, const f3 v, const f3 a, const f3 dx, const f3 dv, const f3 da,
+                                                const float dt, const Box& box, const SphConstants& k, f3& out_x, f3& out_v) {
+    bool cx, cy, cz;
+    collision_mask(x, v, a, dt, box, cx, cy, cz);
+    f3 tv = dv + times(da, dt);
+    f3 tx = dx + times(tv, dt);
+    if (cx) tx.x = 0.0F;
+    if (cy) tx.y = 0.0F;
+    if (cz) tx.z = 0.0F;
+    if (k.no_slip != 0u && (cx || cy || cz)) {
+        tv = mk(0.0F, 0.0F, 0.0F);
+    } else {
+        if (cx) tv.x = 0.0F;
+        if (cy) tv.y = 0.0F;
+        if (cz) tv.z = 0.0F;
+    }
+    out_x = tx;
+    out_v = tv;
+}
+
+__global__ void __launch_bounds__(kBlock) wcsph_force_jvp_kernel(const SphTangentStep t, const float* pressure,
+                                                                 const float4* total, const Field3 control_tangent,
+                                                                 const MutField3 out_x, const MutField3 out_v) {
+    const SphStep& st = t.st;
+    const Own o = own(st);
+    if (!o.p.active) return;
+    const uint32_t s = o.p.s;
+    ForceJvpOp op{};
+    op.pos = st.topology;
+    op.vel = st.velocity;
+    op.aux = st.aux;
+    op.pressure = pressure;
+    op.tx = t.x;
+    op.tv = t.v;
+    op.tpa = t.params_a;
+    op.tdensity = t.density;
+    op.tpressure = t.pressure;
+    op.boundary = st.g.boundary;
+    op.boundary_velocity = st.boundary_velocity;
+    op.self = s;
+    op.x = o.x;
+    op.v = xyz(st.velocity[s]);
+    const float4 txs = t.x[s], ta = t.params_a[s], tb = t.params_b[s];
+    op.dx = xyz(txs);
+    op.dv = xyz(t.v[s]);
+    op.mass = o.mass;
+    op.dmass = txs.w;
+    op.rest = o.pa.x;
+    op.drest = ta.x;
+    const float4 au = st.aux[s];
+    op.density = au.x;
+    op.ddensity = t.density[s];
+    op.viscosity = o.pa.y;
+    op.dviscosity = ta.y;
+    op.speed = o.pa.w;
+    op.dspeed = ta.w;
+    op.tension = o.pa.z;
+    op.dtension = ta.z;
+    op.boundary_tension = st.g.params_b[s].y;
+    op.dboundary_tension = tb.y;
+    const float p = pressure[s];
+    op.first = p / (au.x * au.x);
+    op.dfirst = t.pressure[s] / (au.x * au.x) - 2.0F * p * op.ddensity / (au.x * au.x * au.x);
+    op.k = *o.k;
+    op.rp = op.rv = op.rs = mk(0.0F, 0.0F, 0.0F);
+    replay(op, o.p, st.g, st.list);
+    const uint32_t i = st.sorted_index[s];
+    const f3 da = op.rp + op.rv + op.rs + mk(control_tangent.x[i], control_tangent.y[i], control_tangent.z[i]);
+    const SceneDesc& sc = *o.p.scene;
+    f3 tx, tv;
+    predict_tangent(o.x, op.v, xyz(total[s]), op.dx, op.dv, da, sc.time_step, sc.box, op.k, tx, tv);
+    out_x.x[i] = tx.x;
+    out_x.y[i] = tx.y;
+    out_x.z[i] = tx.z;
+    out_v.x[i] = tv.x;
+    out_v.y[i] = tv.y;
+    out_v.z[i] = tv.z;
+}
+
+// non_pressure_jvp (sph/common.cu:49-96) and, for PCISPH / IISPH, the first prediction's tangent.
+struct NonPressureJvpOp {
+    static constexpr bool kBoundary = true;
+    const float4* __restrict__ pos;
+    const float4* __restrict__ vel;
+    const float4* __restrict__ aux;
+    const float4* __restrict__ tx;
+    const float4* __restrict__ tv;
+    const float4* __restrict__ tpa;
+    const float* __restrict__ tdensity;
+    const float4* __restrict__ boundary;
+    const float4* __restrict__ boundary_velocity;
+    uint32_t self;
+    f3 x, v, dx, dv;
+    float viscosity, dviscosity;
+    SphConstants k;
+    f3 result;
+
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
+    __device__ __forceinline__ void process(const uint32_t t) {
+        if (t & kBoundaryBit) {
+            const uint32_t b = t & ~kBoundaryBit;
+            const float4 q = boundary[b];
+            const f3 d = x - xyz(q);
+            const float laplacian = laplacian_value(d, k);
+            const float dlaplacian = laplacian_tangent(d, dx, k);
+            if (laplacian == 0.0F && dlaplacian == 0.0F) return;
+            const float weight = viscosity * q.w * laplacian;
+            const float dweight = q.w * (dviscosity * laplacian + viscosity * dlaplacian);
+            const f3 difference = xyz(boundary_velocity[b]) - v;
+            result = result + times(difference, dweight) + times(dv, -weight);
+            return;
+        }
+        if (t == self) return;
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        const float laplacian = laplacian_value(d, k);
+        if (laplacian == 0.0F) return;
+        const float4 tq = tx[t];
+        const f3 dd = dx - xyz(tq);
+        const float dlaplacian = laplacian_tangent(d, dd, k);
+        const float4 au = aux[t];
+        const float mu = 0.5F * (viscosity + au.y), dmu = 0.5F * (dviscosity + tpa[t].y);
+        const float mass = q.w, dmass = tq.w, density = au.x, ddensity = tdensity[t];
+        const float weight = mu * mass * laplacian / density;
+        const float dweight = dmu * mass * laplacian / density + mu * dmass * laplacian / density + mu * mass * dlaplacian / density -
+                              mu * mass * laplacian * ddensity / (density * density);
+        const f3 difference = xyz(vel[t]) - v;
+        const f3 ddifference = xyz(tv[t]) - dv;
+        result = result + times(difference, dweight) + times(ddifference, weight);
+    }
+};
+
+__global__ void __launch_bounds__(kBlock) non_pressure_jvp_kernel(const SphTangentStep t, const Field3 control_tangent,
+                                                                  const int mode, const MutField3 out_x, const MutField3 out_v) {
+    const SphStep& st = t.st;
+    const Own o = own(st);
+    if (!o.p.active) return;
+    const uint32_t s = o.p.s;
+    const uint32_t i = st.sorted_index[s];
+    NonPressureJvpOp op{};
+    op.pos = st.topology;
+    op.vel = st.velocity;
+    op.aux = st.aux;
+    op.tx = t.x;
+    op.tv = t.v;
+    op.tpa = t.params_a;
+    op.tdensity = t.density;
+    op.boundary = st.g.boundary;
+    op.boundary_velocity = st.boundary_velocity;
+    op.self = s;
+    op.x = o.x;
+    op.v = xyz(st.velocity[s]);
+    op.dx = xyz(t.x[s]);
+    op.dv = xyz(t.v[s]);
+    op.viscosity = o.pa.y;
+    op.dviscosity = t.params_a[s].y;
+    op.k = *o.k;
+    op.result = mk(control_tangent.x[i], control_tangent.y[i], control_tangent.z[i]);
+    replay(op, o.p, st.g, st.list);
+    t.non_pressure[s] = make_float4(op.result.x, op.result.y, op.result.z, 0.0F);
+    if (mode == 0) return;
+    const SceneDesc& sc = *o.p.scene;
+    f3 tx, tv;
+    predict_tangent(o.x, op.v, xyz(st.non_pressure[s]), op.dx, op.dv, op.result, sc.time_step, sc.box, op.k, tx, tv);
+    if (mode == 1) {
+        t.predicted[s] = make_float4(tx.x, tx.y, tx.z, 0.0F);
+        return;
+    }
+    out_x.x[i] = tx.x;
+    out_x.y[i] = tx.y;
+    out_x.z[i] = tx.z;
+    out_v.x[i] = tv.x;
+    out_v.y[i] = tv.y;
+    out_v.z[i] = tv.z;
+}
+
+// density_jvp at a prediction (x*, its tangent) and the pressure update's tangent
+// (sph/pcisph.cu:113-122, sph/iisph.cu:113-123, sph/dfsph.cu:113-123).
+struct PredictedDensityJvpOp {
+    static constexpr bool kBoundary = true;
+    const float4* __restrict__ predicted;
+    const float4* __restrict__ tpredicted;
+    const float4* __restrict__ tx;
+    const float4* __restrict__ boundary;
+    f3 x, dx;
+    float rest, drest;
+    SphConstants k;
+    float result;
+
+    __device__ __forceinline__ float4 prefetch(const uint32_t t) const {
+        return (t & kBoundaryBit) ? boundary[t & ~kBoundaryBit] : predicted[t];
+    }
+    __device__ __forceinline__ void apply(const uint32_t t, const float4 q) {
+        const f3 d = x - xyz(q);
+        const float w = cubic_value(d, k);
+        if (w == 0.0F) return;
+        if (t & kBoundaryBit) {
+            result += q.w * (drest * w + rest * dot(cubic_gradient_value(d, k), dx));
+            return;
+        }
+        result += tx[t].w * w + q.w * dot(cubic_gradient_value(d, k), dx - xyz(tpredicted[t]));
+    }
+    __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
+};
+
+__global__ void __launch_bounds__(kBlock) predicted_density_jvp_kernel(const SphTangentStep t, const PredictedJvp u) {
+    const SphStep& st = t.st;
+    const Own o = own(st);
+    if (!o.p.active) return;
+    const uint32_t s = o.p.s;
+    PredictedDensityJvpOp op{};
+    op.predicted = u.predicted;
+    op.tpredicted = t.predicted;
+    op.tx = t.x;
+    op.boundary = st.g.boundary;
+    op.x = xyz(u.predicted[s]);
+    op.dx = xyz(t.predicted[s]);
+    op.rest = o.pa.x;
+    op.drest = t.params_a[s].x;
+    op.k = *o.k;
+    const float displacement = __uint_as_float(st.displacement[u.displacement_slot]);
+    if (__fmul_rn(2.0F, displacement) <= o.k->skin_bound) replay(op, o.p, st.g, st.list);
+    else walk(op, o.p, st.g);
+    const float dpredicted = op.result;
+    const float rho = st.aux[s].x, drho = t.density[s];
+    const float4 ta = t.params_a[s], tb = t.params_b[s];
+    const float relaxation = u.relaxation == 0u ? o.pa.w : st.g.params_b[s].x;
+    const float drelaxation = u.relaxation == 0u ? ta.w : tb.x;
+    const float rest = o.pa.x, drest = ta.x;
+    const float target = u.target == 1u ? rho : rest, dtarget = u.target == 1u ? drho : drest;
+    const float error = u.predicted_density[s] - target;
+    const bool pcisph = u.method == kPcisph;
+    const float volume = o.mass / (pcisph ? rest : rho);
+    const float dt = o.p.scene->time_step;
+    const float delta = 1.0F / (2.0F * dt * dt * volume * volume * o.k->reference_gradient_norm);
+    const float ddelta = -2.0F * delta * (t.x[s].w / o.mass - (pcisph ? drest / rest : drho / rho));
+    const float candidate = u.previous_pressure[s] + relaxation * delta * error;
+    const float previous = t.pressure[s];
+    t.pressure[s] = candidate > 0.0F ? previous + drelaxation * delta * error + relaxation * ddelta * error +
+                                           relaxation * delta * (dpredicted - dtarget)
+                                     : 0.0F;
+}
+
+// pressure_jvp (sph/common.cu:196-237) of iterate k and the next prediction's tangent.
+struct PressureJvpOp {
+    static constexpr bool kBoundary = true;
+    const float4* __restrict__ pos;
+    const float4* __restrict__ aux;
+    const float* __restrict__ pressure;
+    const float4* __restrict__ tx;
+    const float* __restrict__ tdensity;
+    const float* __restrict__ tpressure;
+    const float4* __restrict__ boundary;
+    uint32_t self;
+    f3 x, dx;
+    float rest, drest, first, dfirst;
+    SphConstants k;
+    f3 result;
+
+    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
+    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
+    __device__ __forceinline__ void process(const uint32_t t) {
+        if (t & kBoundaryBit) {
+            const float4 q = boundary[t & ~kBoundaryBit];
+            const f3 d = x - xyz(q);
+            if (dot(d, d) >= k.h * k.h * 1.0001F) return;
+            result = result + pressure_pair_jvp(d, dx, -rest * q.w * first, -q.w * (drest * first + rest * dfirst), k);
+            return;
+        }
+        if (t == self) return;
+        const float4 q = pos[t];
+        const f3 d = x - xyz(q);
+        if (dot(d, d) >= k.h * k.h * 1.0001F) return;
+        const float4 tq = tx[t];
+        const float rho_j = aux[t].x, pj = pressure[t];
+        const float second = pj / (rho_j * rho_j);
+        const float dsecond = tpressure[t] / (rho_j * rho_j) - 2.0F * pj * tdensity[t] / (rho_j * rho_j * rho_j);
+        result = result + pressure_pair_jvp(d, dx - xyz(tq), -q.w * (first + second),
+                                            -tq.w * (first + second) - q.w * (dfirst + dsecond), k);
+    }
+};
+
+__global__ void __launch_bounds__(kBlock) pressure_jvp_kernel(const SphTangentStep t, const PressureJvp u) {
+    const SphStep& st = t.st;
+    const Own o = own(st);
+    if (!o.p.active) return;
+    const uint32_t s = o.p.s;
+    PressureJvpOp op{};
+    op.pos = st.topology;
+    op.aux = st.aux;
+    op.pressure = u.pressure;
+    op.tx = t.x;
+    op.tdensity = t.density;
+    op.tpressure = t.pressure;
+    op.boundary = st.g.boundary;
+    op.self = s;
+    op.x = o.x;
+    op.dx = xyz(t.x[s]);
+    op.rest = o.pa.x;
+    op.drest = t.params_a[s].x;
+    const float rho = st.aux[s].x, drho = t.density[s], p = u.pressure[s];
+    op.first = p / (rho * rho);
+    op.dfirst = t.pressure[s] / (rho * rho) - 2.0F * p * drho / (rho * rho * rho);
+    op.k = *o.k;
+    op.result = mk(0.0F, 0.0F, 0.0F);
+    replay(op, o.p, st.g, st.list);
+    const uint32_t i = st.sorted_index[s];
+    f3 dacceleration = op.result;
+    if (u.store) u.store[s] = make_float4(dacceleration.x, dacceleration.y, dacceleration.z, 0.0F);
+    f3 acceleration = xyz(u.acceleration[s]);
+    if (u.base) {
+        acceleration = add(xyz(u.base[s]), acceleration);
+        dacceleration = xyz(u.base_tangent[s]) + dacceleration;
+    }
+    if (u.warm_out) u.warm_out[i] = t.pressure[s];
+    if (u.next_pressure) u.next_pressure[s] = u.next_warm ? u.next_warm[i] : 0.0F;
+    const SceneDesc& sc = *o.p.scene;
+    f3 tx, tv;
+    predict_tangent(o.x, xyz(st.velocity[s]), add(xyz(st.non_pressure[s]), acceleration), op.dx, xyz(t.v[s]),
+                    xyz(t.non_pressure[s]) + dacceleration, sc.time_step, sc.box, op.k, tx, tv);
+    if (!u.last) {
+        t.predicted[s] = make_float4(tx.x, tx.y, tx.z, 0.0F);
+        return;
+    }
+    u.out_x.x[i] = tx.x;
+    u.out_x.y[i] = tx.y;
+    u.out_x.z[i] = tx.z;
+    u.out_v.x[i] = tv.x;
+    u.out_v.y[i] = tv.y;
+    u.out_v.z[i] = tv.z;
+}
+
+}  // namespace
+
+cudaError_t launch_tangent_seed(cudaStream_t stream, const SphTangentStep& t, const Field3 x, const Field3 v,
+                                const SphParameterTangents& pt) {
+    if (t.st.g.count == 0) return cudaSuccess;
+    tangent_seed_kernel<<<grid_of(t.st.g.count, 256), 256, 0, stream>>>(t, x, v, pt);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_density_jvp(cudaStream_t stream, const SphTangentStep& t, const uint32_t method, const float* warm,
+                               const unsigned block) {
+    if (t.st.g.count == 0) return cudaSuccess;
+    const unsigned b = block_of(block);
+    density_jvp_kernel<<<grid_of(t.st.g.count, b), b, 0, stream>>>(t, method, warm);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wcsph_force_jvp(cudaStream_t stream, const SphTangentStep& t, const float* pressure, const float4* total,
+                                   const Field3 control_tangent, const MutField3 out_x, const MutField3 out_v, const unsigned block) {
+    if (t.st.g.count == 0) return cudaSuccess;
+    const unsigned b = block_of(block);
+    wcsph_force_jvp_kernel<<<grid_of(t.st.g.count, b), b, 0, stream>>>(t, pressure, total, control_tangent, out_x, out_v);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_non_pressure_jvp(cudaStream_t stream, const SphTangentStep& t, const Field3 control_tangent, const int mode,
+                                    const MutField3 out_x, const MutField3 out_v, const unsigned block) {
+    if (t.st.g.count == 0) return cudaSuccess;
+    const unsigned b = block_of(block);
+    non_pressure_jvp_kernel<<<grid_of(t.st.g.count, b), b, 0, stream>>>(t, control_tangent, mode, out_x, out_v);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_predicted_density_jvp(cudaStream_t stream, const SphTangentStep& t, const PredictedJvp& u, const unsigned block) {
+    if (t.st.g.count == 0) return cudaSuccess;
+    const unsigned b = block_of(block);
+    predicted_density_jvp_kernel<<<grid_of(t.st.g.count, b), b, 0, stream>>>(t, u);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pressure_jvp(cudaStream_t stream, const SphTangentStep& t, const PressureJvp& u, const unsigned block) {
+    if (t.st.g.count == 0) return cudaSuccess;
+    const unsigned b = block_of(block);
+    pressure_jvp_kernel<<<grid_of(t.st.g.count, b), b, 0, stream>>>(t, u);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace sph
+}  // namespace pbf

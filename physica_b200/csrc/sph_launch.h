@@ -196,6 +196,63 @@ cudaError_t launch_non_pressure_vjp(cudaStream_t stream, const SphStep& st, cons
 cudaError_t launch_phase_seed(cudaStream_t stream, uint32_t count, const uint32_t* sorted_index, const double4* from,
                               double4* acceleration_adjoint, const double* next_warm, double* pressure_adjoint);
 
+// ------------------------------------------------------------------ tangent passes (sph_grad.cu)
+// Caller-side parameter tangents, original order (null: zero), packed like the adjoints.
+struct SphParameterTangents {
+    const float* masses;
+    const float* rest_densities;
+    const float* viscosities;
+    const float* surface_tensions;
+    const float* method0;
+    const float* method1;
+    const float* method2;
+};
+
+// Sorted tangent workspace of one jvp_step.
+struct SphTangentStep {
+    SphStep st;
+    float4* x;            // (dx, dm)
+    float4* v;            // (dv, 0)
+    float4* params_a;     // tangents of params_a
+    float4* params_b;     // tangents of params_b
+    float* density;       // d rho
+    float* pressure;      // d p of the current phase
+    float4* non_pressure; // d a_np
+    float4* predicted;    // d x* of the current iterate
+};
+
+cudaError_t launch_tangent_seed(cudaStream_t stream, const SphTangentStep& t, Field3 x, Field3 v, const SphParameterTangents& pt);
+// density_jvp at the step's positions (density/density.cu:42-66) with WCSPH's EOS tangent
+// (sph/wcsph.cu:102-117); warm: DFSPH's divergence warm-start tangent (original order) or null.
+cudaError_t launch_density_jvp(cudaStream_t stream, const SphTangentStep& t, uint32_t method, const float* warm, unsigned block);
+// WCSPH force tangents (sph/common.cu:196-237, sph/wcsph.cu:176-240, 341-387) and integrate_jvp
+// (sph/common.cu:322-342) into the next tangent (original order).
+cudaError_t launch_wcsph_force_jvp(cudaStream_t stream, const SphTangentStep& t, const float* pressure, const float4* total,
+                                   Field3 control_tangent, MutField3 out_x, MutField3 out_v, unsigned block);
+// non_pressure_jvp (sph/common.cu:49-96); mode as launch_non_pressure.
+cudaError_t launch_non_pressure_jvp(cudaStream_t stream, const SphTangentStep& t, Field3 control_tangent, int mode,
+                                    MutField3 out_x, MutField3 out_v, unsigned block);
+struct PredictedJvp {
+    uint32_t method, relaxation, target, displacement_slot;
+    const float4* predicted;          // x*_k
+    const float* predicted_density;   // rho*_k
+    const float* previous_pressure;   // p_(k-1)
+};
+cudaError_t launch_predicted_density_jvp(cudaStream_t stream, const SphTangentStep& t, const PredictedJvp& u, unsigned block);
+struct PressureJvp {
+    const float* pressure;            // p_k
+    const float4* acceleration;       // a_k
+    const float4* base;               // DFSPH density phase: the divergence acceleration, or null
+    const float4* base_tangent;
+    float4* store;                    // keep d a_k (DFSPH divergence phase), or null
+    int last;
+    MutField3 out_x, out_v;
+    float* warm_out;                  // d p_k to the caller (original order), or null
+    float* next_pressure;             // DFSPH: the density phase's tangent buffer, loaded with next_warm
+    const float* next_warm;
+};
+cudaError_t launch_pressure_jvp(cudaStream_t stream, const SphTangentStep& t, const PressureJvp& u, unsigned block);
+
 // compute_reference_gradient_norm (sph/sph.cpp:36-58) on the host.
 float reference_gradient_norm(float support_radius, float particle_radius);
 

@@ -2,8 +2,8 @@
 
 Mirrors the reference's SPH<Method> (fluids/liquid/particle/sph/sph.ixx:273-372) with Method one
 of WCSPH, PCISPH, IISPH and DFSPH: `SPH(domain_configuration, method_configuration, mode, stream)`,
-`allocate_state` / `allocate_control` / `allocate_parameters` / `allocate_step_cache`,
-`copy_state` and `forward_step`.  SPH<Method>::State is a particle state plus the method's state
+`allocate_state` / `allocate_control` / `allocate_parameters` / `allocate_step_cache` and their
+tangent / adjoint forms, `copy_state`, `forward_step`, `jvp_step` and `vjp_step`.  SPH<Method>::State is a particle state plus the method's state
 (DFSPH's warm-start pressures); SPH<Method>::Parameters the particle parameters plus the method's.
 Every call goes to libphysica_pbf.so; there is no CPU fallback.
 """
@@ -83,6 +83,9 @@ def library() -> ctypes.CDLL:
         lib.sph_forward_step.argtypes = [vp, P(ParticleStateC), P(MethodStateC), P(ControlC), P(ParametersC),
                                          P(ParticleStateC), P(MethodStateC), vp]
         lib.sph_read_cache.argtypes = [vp, vp, ctypes.c_int, vp, vp, vp]
+        lib.sph_jvp_step.argtypes = [vp, P(ParticleStateC), P(MethodStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
+                                     P(pbf.StateAdjointC), P(MethodStateC), P(ControlC), P(ParametersC), P(pbf.StateAdjointC),
+                                     P(MethodStateC)]
         lib.sph_vjp_step.argtypes = [vp, P(ParticleStateC), P(MethodStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
                                      P(pbf.StateAdjointC), P(MethodStateC), P(pbf.StateAdjointC), P(MethodStateC), P(ControlC),
                                      P(ParameterAdjointC)]
@@ -123,6 +126,23 @@ class State:
 
     def c(self) -> ParticleStateC:
         return ParticleStateC(_vf(self.positions), _vf(self.velocities), self.step_index)
+
+    def method_c(self) -> MethodStateC:
+        a, b = self.warm_divergence_pressure, self.warm_density_pressure
+        return MethodStateC(_ptr(a) if a is not None and a.numel() else None, _ptr(b) if b is not None and b.numel() else None)
+
+
+@dataclasses.dataclass
+class StateTangent:
+    """SPH<Method>::StateTangent (sph/sph.ixx:279-282): (3, N) float32 position / velocity tangents
+    and, for DFSPH, the (N,) float32 tangents of the warm-start pressures."""
+    positions: torch.Tensor
+    velocities: torch.Tensor
+    warm_divergence_pressure: torch.Tensor | None = None
+    warm_density_pressure: torch.Tensor | None = None
+
+    def c(self) -> pbf.StateAdjointC:
+        return pbf.StateAdjointC(_vf(self.positions), _vf(self.velocities))
 
     def method_c(self) -> MethodStateC:
         a, b = self.warm_divergence_pressure, self.warm_density_pressure
@@ -249,6 +269,13 @@ class SPH:
     def allocate_step_cache(self) -> StepCache:
         return StepCache(self)
 
+    def allocate_state_tangent(self) -> StateTangent:
+        s = self.allocate_state()
+        return StateTangent(s.positions, s.velocities, s.warm_divergence_pressure, s.warm_density_pressure)
+
+    def allocate_parameter_tangent(self) -> Parameters:
+        return self.allocate_parameters()
+
     def allocate_state_adjoint(self) -> StateAdjoint:
         z3 = lambda: torch.zeros((3, self.count), dtype=torch.float64, device=self.device)
         dfsph = self.method == Method.dfsph
@@ -291,6 +318,17 @@ class SPH:
         check(library().sph_forward_step(self.handle, ctypes.byref(sc), ctypes.byref(ms), ctypes.byref(control.c()),
                                           ctypes.byref(parameters.c()), ctypes.byref(ns), ctypes.byref(nms), cache.handle))
         next_state.step_index = ns.step_index
+
+    def jvp_step(self, state: State, control: pbf.Control, parameters: Parameters, next_state: State, cache: StepCache,
+                 state_tangent: StateTangent, control_tangent: pbf.Control, parameter_tangent: Parameters | None,
+                 next_state_tangent: StateTangent):
+        """SPH<Method>::jvp_step (sph/sph.ixx:356-359), FP32 tangents of the step held by `cache`."""
+        pt = ctypes.byref(parameter_tangent.c()) if parameter_tangent is not None else None
+        check(library().sph_jvp_step(self.handle, ctypes.byref(state.c()), ctypes.byref(state.method_c()),
+                                     ctypes.byref(control.c()), ctypes.byref(parameters.c()), ctypes.byref(next_state.c()),
+                                     cache.handle, ctypes.byref(state_tangent.c()), ctypes.byref(state_tangent.method_c()),
+                                     ctypes.byref(control_tangent.c()), pt, ctypes.byref(next_state_tangent.c()),
+                                     ctypes.byref(next_state_tangent.method_c())))
 
     def vjp_step(self, state: State, control: pbf.Control, parameters: Parameters, next_state: State, cache: StepCache,
                  next_state_adjoint: StateAdjoint, previous_state_adjoint: StateAdjoint, control_adjoint: pbf.Control,

@@ -103,3 +103,61 @@ def test_vjp_matches_reference(method):
 @pytest.mark.parametrize("method", METHODS)
 def test_vjp_with_boundary_particles_matches_reference(method):
     _compare_vjp(method, _scene(method, 103, boundary=True, box_velocity=(0.1, 0.0, 0.0)), steps_before=2)
+
+
+def _compare_jvp(method, sc, tolerance=1e-4):
+    reference = reference_or_skip()
+    cfg = sph.Configuration(method=sph.Method[method], pressure_iterations=3, divergence_iterations=2, density_iterations=3)
+    solver, state, control, params = sph.solver_for_scene(sc, sph.Method[method], configuration=cfg,
+                                                          mode=pbf.ExecutionMode.differentiable)
+    ref = reference.ReferenceSPH(sc, int(sph.Method[method]), cfg.pressure_iterations, cfg.divergence_iterations,
+                                 cfg.density_iterations, checkpoint_interval=2, differentiable=True)
+    dfsph = method == "dfsph"
+    n = sc.count
+    rng = np.random.default_rng(23)
+    if dfsph:
+        for t in (state.warm_divergence_pressure, state.warm_density_pressure):
+            t.copy_(torch.from_numpy(rng.uniform(0, 50, n).astype(np.float32)))
+    cache = solver.allocate_step_cache()
+    nxt = solver.allocate_state()
+    x, v = state.positions.clone(), state.velocities.clone()
+    warm = (state.warm_divergence_pressure.clone(), state.warm_density_pressure.clone()) if dfsph else None
+    solver.forward_step(state, control, params, nxt, cache)
+    ref.forward_step(x, v, torch.zeros_like(x), torch.zeros_like(v), 0, warm=warm,
+                     warm_out=(torch.zeros(n, device="cuda"), torch.zeros(n, device="cuda")) if dfsph else None)
+    f32 = lambda a: torch.from_numpy(np.asarray(a, dtype=np.float32)).cuda()
+    st = sph.StateTangent(f32(rng.normal(size=(3, n)) * 1e-3), f32(rng.normal(size=(3, n)) * 1e-2),
+                          f32(rng.normal(size=n)) if dfsph else None, f32(rng.normal(size=n)) if dfsph else None)
+    ct = pbf.Control(f32(rng.normal(size=(3, n))))
+    pt = solver.allocate_parameter_tangent()
+    pt.tensors["rest_densities"].copy_(f32(rng.normal(size=n)))
+    pt.tensors["masses"].copy_(f32(rng.normal(size=n) * 1e-7))
+    pt.tensors["viscosities"].copy_(f32(rng.normal(size=n) * 1e-3))
+    pt.tensors["surface_tensions"].copy_(f32(rng.normal(size=n) * 1e-3))
+    for name in sph.METHOD_PARAMETERS[method]:
+        pt.tensors[name].copy_(f32(rng.normal(size=n) * 1e-2))
+    out = solver.allocate_state_tangent()
+    solver.jvp_step(state, control, params, nxt, cache, st, ct, pt, out)
+    tout = {"positions": torch.zeros_like(x), "velocities": torch.zeros_like(v)}
+    nwt = (torch.zeros(n, device="cuda"), torch.zeros(n, device="cuda"))
+    ref.jvp_step(x, v, {"positions": st.positions, "velocities": st.velocities}, ct.external_accelerations, pt.tensors, tout, 0,
+                 warm=warm, warm_tangent=(st.warm_divergence_pressure, st.warm_density_pressure) if dfsph else None,
+                 next_warm_tangent=nwt)
+    torch.cuda.synchronize()
+    errors = {"positions": rel(out.positions, tout["positions"]), "velocities": rel(out.velocities, tout["velocities"])}
+    if dfsph:
+        errors["warm_divergence"] = rel(out.warm_divergence_pressure, nwt[0])
+        errors["warm_density"] = rel(out.warm_density_pressure, nwt[1])
+    bad = {key: value for key, value in errors.items() if not value < tolerance}
+    assert not bad, (method, bad, errors)
+    assert float(out.velocities.abs().max()) > 0
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_jvp_matches_reference(method):
+    _compare_jvp(method, _scene(method, 105))
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_jvp_with_boundary_particles_matches_reference(method):
+    _compare_jvp(method, _scene(method, 107, boundary=True))
