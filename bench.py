@@ -507,7 +507,32 @@ def bench_sph(args, world, rank, methods=SPH_METHODS):
         out[name] = {"value": round(world * sc.count / (ms_per_step * 1e-3), 1), "ms_per_step": round(ms_per_step, 4)}
         del cache, solver
         torch.cuda.synchronize()
+        if not args.no_grad:
+            out[name]["gradient_ms_per_step"] = round(sph_gradient_ms(args, world, sc, name), 4)
     return out
+
+
+def sph_gradient_ms(args, world, sc, name):
+    """One differentiable SPH substep and its vjp_step (a unit next-state adjoint), per step in ms."""
+    from physica_b200 import pbf, sph
+    solver, state, control, params = sph.solver_for_scene(sc, sph.Method[name], mode=pbf.ExecutionMode.differentiable)
+    cache = solver.allocate_step_cache()
+    nxt = solver.allocate_state()
+    n = sc.count
+    na = solver.allocate_state_adjoint()
+    na.positions.fill_(1.0)
+    pa, ca, qa = solver.allocate_state_adjoint(), solver.allocate_control_adjoint(), solver.allocate_parameter_adjoint()
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        solver.forward_step(state, control, params, nxt, cache)
+        solver.vjp_step(state, control, params, nxt, cache, na, pa, ca, qa)
+
+    steps = max(3, min(args.steps, 5))
+    ms, _ = timed(step, steps, 3, world, solver.stream, flush)
+    del cache, solver
+    torch.cuda.synchronize()
+    return max_over_ranks(ms, world) / steps
 
 
 def bench_reference_sph(args, world, rank, methods=SPH_METHODS):
@@ -537,7 +562,39 @@ def bench_reference_sph(args, world, rank, methods=SPH_METHODS):
         out[name] = {"value": round(world * sc.count / (ms_per_step * 1e-3), 1), "ms_per_step": round(ms_per_step, 4)}
         ref.close()
         torch.cuda.synchronize()
+        if not args.no_grad:
+            out[name]["gradient_ms_per_step"] = round(reference_sph_gradient_ms(args, world, sc, name), 4)
     return out
+
+
+def reference_sph_gradient_ms(args, world, sc, name):
+    """The reference's differentiable SPH substep and its vjp_step (checkpoint recomputation
+    included), per step in ms."""
+    from oracle import reference
+    from physica_b200 import sph
+    n = sc.count
+    ref = reference.ReferenceSPH(sc, int(sph.Method[name]), differentiable=True)
+    x = torch.from_numpy(sc.positions).cuda().contiguous()
+    v = torch.from_numpy(sc.velocities).cuda().contiguous()
+    xo, vo = torch.zeros_like(x), torch.zeros_like(v)
+    z = lambda: torch.zeros(n, device="cuda")
+    warm, warm_out = (z(), z()), (z(), z())
+    z3 = lambda: torch.zeros((3, n), dtype=torch.float64, device="cuda")
+    na = {"positions": torch.ones((3, n), dtype=torch.float64, device="cuda"), "velocities": z3()}
+    prev = {"positions": z3(), "velocities": z3()}
+    ctrl = z3()
+    q = {k: torch.zeros(n, dtype=torch.float64, device="cuda") for k in sph.PARAMETER_NAMES}
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        ref.forward_step(x, v, xo, vo, 0, warm=warm, warm_out=warm_out, synchronize=False)
+        ref.vjp_step(x, v, na, prev, ctrl, q, 0)
+
+    steps = max(3, min(args.steps, 5))
+    ms, _ = timed(step, steps, 3, world, torch.cuda.ExternalStream(ref.stream), flush)
+    ref.close()
+    torch.cuda.synchronize()
+    return max_over_ranks(ms, world) / steps
 
 
 def cpu_baseline(sc):
