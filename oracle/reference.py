@@ -95,7 +95,7 @@ class ReferencePBF:
         c.box_min = (ctypes.c_float * 3)(*scene.box_min)
         c.box_max = (ctypes.c_float * 3)(*scene.box_max)
         c.box_velocity = (ctypes.c_float * 3)(*scene.box_velocity)
-        c.no_slip = 1
+        c.no_slip = 1 if getattr(scene, "no_slip", True) else 0
         c.pressure_iterations = scene.pressure_iterations
         c.checkpoint_interval = checkpoint_interval
         c.differentiable = 1 if differentiable else 0

@@ -521,6 +521,11 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
     };
     if (method == SPH_METHOD_PCISPH || method == SPH_METHOD_IISPH) {
         const uint32_t K = p0.iterations;
+        if (K == 0 && !diff) {   // the cleared primal iterate's acceleration (sph/sph.cpp:298)
+            if (int rc = check(cudaMemsetAsync(r.pressure_acceleration, 0, static_cast<size_t>(count_) * sizeof(float4), s),
+                               "clear"))
+                return rc;
+        }
         SphStep s1 = st;
         s1.predicted = p0.X(1 <= K ? 1 : 0);
         if (int rc = check(launch_non_pressure(s, s1, K > 0 ? 1 : 2, out_x, out_v, 0u, block), "non-pressure acceleration"))
@@ -572,7 +577,7 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
         if (int rc = pressure_pass(p1, it, a)) return rc;
     }
     r.final_pressure = p1.P(Kr);
-    r.final_predicted_density = Kr > 0 ? p1.R(Kr) : (Kd > 0 ? p0.R(Kd) : p1.R(0));
+    r.final_predicted_density = p1.R(Kr);   // the density phase's primal (cleared when it has no iteration)
     r.final_acceleration = diff ? p1.A(Kr) : r.pressure_acceleration;
     return PBF_SUCCESS;
 }

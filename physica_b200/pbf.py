@@ -279,7 +279,8 @@ class DomainConfiguration:
         return DomainConfiguration(
             particle_count=scene.count, time_step=scene.time_step, support_radius=scene.support_radius,
             particle_radius=scene.particle_radius, gravity=tuple(scene.gravity),
-            boundary=BoxBoundary(tuple(scene.box_min), tuple(scene.box_max), tuple(scene.box_velocity), True),
+            boundary=BoxBoundary(tuple(scene.box_min), tuple(scene.box_max), tuple(scene.box_velocity),
+                                 bool(getattr(scene, "no_slip", True))),
             boundary_particles=particles)
 
 

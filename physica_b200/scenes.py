@@ -75,6 +75,8 @@ class Scene:
     boundary: dict | None = None
     # SPH parameters (sph_dam_break): one (N,) float32 array per SPH<Method>::Parameters field
     sph: dict | None = None
+    # BoxBoundary::no_slip: a colliding particle takes the box velocity on every axis (SPH reads it)
+    no_slip: bool = True
 
     @property
     def count(self) -> int:

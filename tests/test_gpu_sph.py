@@ -40,17 +40,19 @@ def _scene(method, seed=91, lattice=(10, 10, 10), boundary=False, box_velocity=(
     return sc
 
 
-def _configuration(method):
-    return sph.Configuration(method=sph.Method[method], pressure_iterations=4, divergence_iterations=3, density_iterations=4)
+def _configuration(method, **overrides):
+    values = dict(method=sph.Method[method], pressure_iterations=4, divergence_iterations=3, density_iterations=4)
+    values.update(overrides)
+    return sph.Configuration(**values)
 
 
-def _run_pair(sc, method, steps, check_fields=False):
+def _run_pair(sc, method, steps, check_fields=False, **overrides):
     reference = reference_or_skip()
-    cfg = _configuration(method)
+    cfg = _configuration(method, **overrides)
     solver, state, control, params = sph.solver_for_scene(sc, sph.Method[method], configuration=cfg)
     cache = solver.allocate_step_cache()
     ref = reference.ReferenceSPH(sc, int(sph.Method[method]), cfg.pressure_iterations, cfg.divergence_iterations,
-                                 cfg.density_iterations)
+                                 cfg.density_iterations, pressure_warm_start=cfg.pressure_warm_start)
     dfsph = method == "dfsph"
     rng = np.random.default_rng(5)
     if dfsph:   # non-zero warm starts
@@ -126,6 +128,24 @@ def test_large_displacements_walk_the_stencil(method):
     densities walk the full stencil instead of replaying the lists, with the same results."""
     sc = _scene(method, seed=96, boundary=True, velocity_sigma=20.0)
     _run_pair(sc, method, 4, check_fields=True)
+
+
+@pytest.mark.parametrize("method,overrides", [("pcisph", {"pressure_iterations": 0}), ("iisph", {"pressure_iterations": 1}),
+                                              ("dfsph", {"divergence_iterations": 0, "density_iterations": 2}),
+                                              ("dfsph", {"divergence_iterations": 2, "density_iterations": 0}),
+                                              ("dfsph", {"pressure_warm_start": False})])
+def test_iteration_counts_and_warm_start(method, overrides):
+    """Zero and one pressure iterations, empty DFSPH phases and DFSPH without warm starts."""
+    _run_pair(_scene(method, seed=97, boundary=True), method, 4, check_fields=True, **overrides)
+
+
+@pytest.mark.parametrize("method", ("wcsph", "pcisph"))
+def test_slip_box_matches_reference(method):
+    """A box without no-slip: colliding particles keep their tangential velocities (sph/common.cu:313-319);
+    a fast scene drives many of them into the walls."""
+    sc = _scene(method, seed=98, velocity_sigma=3.0)
+    sc.no_slip = False
+    _run_pair(sc, method, 6)
 
 
 def test_crowded_cells_overflow_the_lists():

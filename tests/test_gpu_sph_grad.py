@@ -43,13 +43,16 @@ def _scene(method, seed, boundary=False, box_velocity=(0.0, 0.0, 0.0)):
     return sc
 
 
-def _compare_vjp(method, sc, tolerance=1e-9, steps_before=1):
+def _compare_vjp(method, sc, tolerance=1e-9, steps_before=1, **overrides):
     reference = reference_or_skip()
-    cfg = sph.Configuration(method=sph.Method[method], pressure_iterations=3, divergence_iterations=2, density_iterations=3)
+    values = dict(method=sph.Method[method], pressure_iterations=3, divergence_iterations=2, density_iterations=3)
+    values.update(overrides)
+    cfg = sph.Configuration(**values)
     solver, state, control, params = sph.solver_for_scene(sc, sph.Method[method], configuration=cfg,
                                                           mode=pbf.ExecutionMode.differentiable)
     ref = reference.ReferenceSPH(sc, int(sph.Method[method]), cfg.pressure_iterations, cfg.divergence_iterations,
-                                 cfg.density_iterations, checkpoint_interval=2, differentiable=True)
+                                 cfg.density_iterations, pressure_warm_start=cfg.pressure_warm_start, checkpoint_interval=2,
+                                 differentiable=True)
     dfsph = method == "dfsph"
     n = sc.count
     rng = np.random.default_rng(17)
@@ -87,7 +90,7 @@ def _compare_vjp(method, sc, tolerance=1e-9, steps_before=1):
               "control": rel(ca.external_accelerations, rctrl)}
     for name in PARTICLE + sph.METHOD_PARAMETERS[method]:
         errors[name] = rel(qa.tensors[name], rq[name])
-    if dfsph:
+    if dfsph and cfg.pressure_warm_start:
         errors["warm_divergence"] = rel(pa.warm_divergence_pressure, rwarm[0])
         errors["warm_density"] = rel(pa.warm_density_pressure, rwarm[1])
     bad = {key: value for key, value in errors.items() if not value < tolerance}
@@ -98,6 +101,14 @@ def _compare_vjp(method, sc, tolerance=1e-9, steps_before=1):
 @pytest.mark.parametrize("method", METHODS)
 def test_vjp_matches_reference(method):
     _compare_vjp(method, _scene(method, 101))
+
+
+@pytest.mark.parametrize("method,overrides", [("pcisph", {"pressure_iterations": 0}), ("iisph", {"pressure_iterations": 5}),
+                                              ("dfsph", {"divergence_iterations": 0, "density_iterations": 1}),
+                                              ("dfsph", {"pressure_warm_start": False})])
+def test_vjp_iteration_counts_and_warm_start(method, overrides):
+    """Zero iterations, odd counts across the reference's checkpoint interval, DFSPH without warm starts."""
+    _compare_vjp(method, _scene(method, 109, boundary=True), **overrides)
 
 
 @pytest.mark.parametrize("method", METHODS)
