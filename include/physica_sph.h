@@ -149,6 +149,20 @@ int sph_vjp_step(sph_solver* solver, const pbf_particle_state* state, const sph_
                  sph_method_state_adjoint* previous_method_adjoint, pbf_control_adjoint* control_adjoint,
                  sph_parameter_adjoint* parameter_adjoint);
 
+/* SPH<Method>::copy_state / copy_state_tangent / copy_state_adjoint / accumulate_state_adjoint
+ * (sph/sph.ixx:326-345): the particle fields plus DFSPH's warm-start pressures (the method fields
+ * are ignored for the other methods and may be NULL there). */
+int sph_copy_state(sph_solver* solver, const pbf_particle_state* source, const sph_method_state* source_method,
+                   pbf_particle_state* destination, sph_method_state* destination_method);
+int sph_copy_state_tangent(sph_solver* solver, const pbf_particle_state_tangent* source, const sph_method_state* source_method,
+                           pbf_particle_state_tangent* destination, sph_method_state* destination_method);
+int sph_copy_state_adjoint(sph_solver* solver, const pbf_particle_state_adjoint* source,
+                           const sph_method_state_adjoint* source_method, pbf_particle_state_adjoint* destination,
+                           sph_method_state_adjoint* destination_method);
+int sph_accumulate_state_adjoint(sph_solver* solver, const pbf_particle_state_adjoint* source,
+                                 const sph_method_state_adjoint* source_method, pbf_particle_state_adjoint* destination,
+                                 sph_method_state_adjoint* destination_method);
+
 /* A field of the step held by `cache`, written to device memory in original particle order
  * (x only for scalar fields). */
 int sph_read_cache(sph_solver* solver, const sph_step_cache* cache, sph_cache_field field, float* x, float* y, float* z);

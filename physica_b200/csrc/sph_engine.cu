@@ -6,6 +6,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/physica_sph.h"
@@ -110,6 +111,8 @@ public:
         return e == cudaErrorMemoryAllocation ? PBF_ERROR_OUT_OF_MEMORY : PBF_ERROR_CUDA;
     }
     cudaStream_t stream() const { return stream_; }
+    uint32_t count() const { return count_; }
+    bool dfsph() const { return config_.method == SPH_METHOD_DFSPH; }
     float reference_gradient_norm() const { return reference_gradient_norm_; }
     LaunchShape shape{};
 
@@ -1125,6 +1128,83 @@ int sph_vjp_step(sph_solver* solver, const pbf_particle_state* state, const sph_
         return solver->engine.reverse(state, method_state, parameters, cache->record, next_adjoint, next_method_adjoint,
                                       previous_adjoint, previous_method_adjoint, control_adjoint, parameter_adjoint);
     });
+}
+
+}  // extern "C"
+
+namespace {
+
+// Copies (or FP64 accumulations) of the six particle fields and, for DFSPH, the two warm-start
+// pressure fields.
+template <class T>
+int copy_fields(sph_solver* solver, const T* const* src, T* const* dst, const int fields, const bool accumulate) {
+    pbf::sph::SphEngine& en = solver->engine;
+    const size_t n = en.count();
+    if (n == 0) return PBF_SUCCESS;
+    for (int k = 0; k < fields; ++k)
+        if (!src[k] || !dst[k]) return null_arg("field");
+    if (!accumulate) {
+        for (int k = 0; k < fields; ++k)
+            if (int rc = en.check(cudaMemcpyAsync(dst[k], src[k], n * sizeof(T), cudaMemcpyDeviceToDevice, en.stream()), "copy"))
+                return rc;
+        return PBF_SUCCESS;
+    }
+    if constexpr (std::is_same_v<T, double>) {
+        for (int k = 0; k < fields; k += 6) {
+            const int count = fields - k < 6 ? fields - k : 6;
+            if (int rc = en.check(pbf::launch_accumulate(en.stream(), n, src + k, dst + k, count), "accumulate")) return rc;
+        }
+    }
+    return PBF_SUCCESS;
+}
+
+template <class State, class Method, class T>
+int copy_state_like(sph_solver* solver, const State* source, const Method* source_method, State* destination,
+                    Method* destination_method, const bool accumulate) {
+    if (!solver || !source || !destination) return null_arg("solver/source/destination");
+    const bool dfsph = solver->engine.dfsph();
+    if (dfsph && (!source_method || !destination_method)) return null_arg("DFSPH method state");
+    const T* src[8] = {source->positions.x, source->positions.y, source->positions.z,
+                       source->velocities.x, source->velocities.y, source->velocities.z,
+                       dfsph ? source_method->warm_divergence_pressure : nullptr,
+                       dfsph ? source_method->warm_density_pressure : nullptr};
+    T* dst[8] = {destination->positions.x, destination->positions.y, destination->positions.z,
+                 destination->velocities.x, destination->velocities.y, destination->velocities.z,
+                 dfsph ? destination_method->warm_divergence_pressure : nullptr,
+                 dfsph ? destination_method->warm_density_pressure : nullptr};
+    return guarded([&] { return copy_fields<T>(solver, src, dst, dfsph ? 8 : 6, accumulate); });
+}
+
+}  // namespace
+
+extern "C" {
+
+int sph_copy_state(sph_solver* solver, const pbf_particle_state* source, const sph_method_state* source_method,
+                   pbf_particle_state* destination, sph_method_state* destination_method) {
+    const int rc = copy_state_like<pbf_particle_state, sph_method_state, float>(solver, source, source_method, destination,
+                                                                               destination_method, false);
+    if (rc == PBF_SUCCESS) destination->step_index = source->step_index;
+    return rc;
+}
+
+int sph_copy_state_tangent(sph_solver* solver, const pbf_particle_state_tangent* source, const sph_method_state* source_method,
+                           pbf_particle_state_tangent* destination, sph_method_state* destination_method) {
+    return copy_state_like<pbf_particle_state_tangent, sph_method_state, float>(solver, source, source_method, destination,
+                                                                               destination_method, false);
+}
+
+int sph_copy_state_adjoint(sph_solver* solver, const pbf_particle_state_adjoint* source,
+                           const sph_method_state_adjoint* source_method, pbf_particle_state_adjoint* destination,
+                           sph_method_state_adjoint* destination_method) {
+    return copy_state_like<pbf_particle_state_adjoint, sph_method_state_adjoint, double>(solver, source, source_method,
+                                                                                        destination, destination_method, false);
+}
+
+int sph_accumulate_state_adjoint(sph_solver* solver, const pbf_particle_state_adjoint* source,
+                                 const sph_method_state_adjoint* source_method, pbf_particle_state_adjoint* destination,
+                                 sph_method_state_adjoint* destination_method) {
+    return copy_state_like<pbf_particle_state_adjoint, sph_method_state_adjoint, double>(solver, source, source_method,
+                                                                                        destination, destination_method, true);
 }
 
 int sph_read_cache(sph_solver* solver, const sph_step_cache* cache, const sph_cache_field field, float* x, float* y, float* z) {

@@ -89,6 +89,11 @@ def library() -> ctypes.CDLL:
         lib.sph_vjp_step.argtypes = [vp, P(ParticleStateC), P(MethodStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
                                      P(pbf.StateAdjointC), P(MethodStateC), P(pbf.StateAdjointC), P(MethodStateC), P(ControlC),
                                      P(ParameterAdjointC)]
+        lib.sph_copy_state.argtypes = [vp, P(ParticleStateC), P(MethodStateC), P(ParticleStateC), P(MethodStateC)]
+        lib.sph_copy_state_tangent.argtypes = [vp, P(pbf.StateAdjointC), P(MethodStateC), P(pbf.StateAdjointC), P(MethodStateC)]
+        lib.sph_copy_state_adjoint.argtypes = [vp, P(pbf.StateAdjointC), P(MethodStateC), P(pbf.StateAdjointC), P(MethodStateC)]
+        lib.sph_accumulate_state_adjoint.argtypes = [vp, P(pbf.StateAdjointC), P(MethodStateC), P(pbf.StateAdjointC),
+                                                     P(MethodStateC)]
         lib.sph_reference_gradient_norm.argtypes = [vp, P(ctypes.c_float)]
         lib.sph_set_launch_shape.argtypes = [vp, P(LaunchShapeC)]
         lib.sph_get_launch_shape.argtypes = [vp, P(LaunchShapeC)]
@@ -301,15 +306,27 @@ class SPH:
             p.tensors[k].copy_(torch.as_tensor(np.ascontiguousarray(v)))
         return p
 
+    def _copy(self, entry, source, destination):
+        sc, dc = source.c(), destination.c()
+        check(entry(self.handle, ctypes.byref(sc), ctypes.byref(source.method_c()), ctypes.byref(dc),
+                    ctypes.byref(destination.method_c())))
+        return dc
+
     def copy_state(self, source: State, destination: State):
-        """SPH<Method>::copy_state (sph/sph.ixx:326-329)."""
-        destination.positions.copy_(source.positions)
-        destination.velocities.copy_(source.velocities)
-        destination.step_index = source.step_index
-        for name in ("warm_divergence_pressure", "warm_density_pressure"):
-            a, b = getattr(source, name), getattr(destination, name)
-            if a is not None and b is not None:
-                b.copy_(a)
+        """SPH<Method>::copy_state (sph/sph.ixx:326-329): particles and DFSPH's warm starts."""
+        destination.step_index = self._copy(library().sph_copy_state, source, destination).step_index
+
+    def copy_state_tangent(self, source: StateTangent, destination: StateTangent):
+        """SPH<Method>::copy_state_tangent (sph/sph.ixx:331-334)."""
+        self._copy(library().sph_copy_state_tangent, source, destination)
+
+    def copy_state_adjoint(self, source: StateAdjoint, destination: StateAdjoint):
+        """SPH<Method>::copy_state_adjoint (sph/sph.ixx:336-339)."""
+        self._copy(library().sph_copy_state_adjoint, source, destination)
+
+    def accumulate_state_adjoint(self, source: StateAdjoint, destination: StateAdjoint):
+        """SPH<Method>::accumulate_state_adjoint (sph/sph.ixx:341-344): destination += source."""
+        self._copy(library().sph_accumulate_state_adjoint, source, destination)
 
     def forward_step(self, state: State, control: pbf.Control, parameters: Parameters, next_state: State, cache: StepCache):
         """SPH<Method>::forward_step (sph/sph.ixx:350-354)."""

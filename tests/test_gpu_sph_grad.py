@@ -172,3 +172,48 @@ def test_jvp_matches_reference(method):
 @pytest.mark.parametrize("method", METHODS)
 def test_jvp_with_boundary_particles_matches_reference(method):
     _compare_jvp(method, _scene(method, 107, boundary=True))
+
+
+@pytest.mark.parametrize("method", ("wcsph", "dfsph"))
+def test_state_copies_and_adjoint_accumulation(method):
+    """copy_state / copy_state_tangent / copy_state_adjoint / accumulate_state_adjoint
+    (sph/sph.ixx:326-345), DFSPH's warm-start fields included."""
+    sc = _scene(method, 111)
+    solver, state, _, _ = sph.solver_for_scene(sc, sph.Method[method], mode=pbf.ExecutionMode.differentiable)
+    dfsph = method == "dfsph"
+    if dfsph:
+        state.warm_divergence_pressure.uniform_(0, 5)
+        state.warm_density_pressure.uniform_(0, 5)
+    state.step_index = 7
+    copy = solver.allocate_state()
+    solver.copy_state(state, copy)
+    assert copy.step_index == 7 and torch.equal(copy.positions, state.positions) and torch.equal(copy.velocities, state.velocities)
+    if dfsph:
+        assert torch.equal(copy.warm_density_pressure, state.warm_density_pressure)
+    t = solver.allocate_state_tangent()
+    t.positions.normal_()
+    if dfsph:
+        t.warm_divergence_pressure.normal_()
+    t2 = solver.allocate_state_tangent()
+    solver.copy_state_tangent(t, t2)
+    assert torch.equal(t2.positions, t.positions)
+    if dfsph:
+        assert torch.equal(t2.warm_divergence_pressure, t.warm_divergence_pressure)
+    a, b = solver.allocate_state_adjoint(), solver.allocate_state_adjoint()
+    a.positions.normal_()
+    a.velocities.normal_()
+    b.positions.normal_()
+    if dfsph:
+        a.warm_density_pressure.normal_()
+        b.warm_density_pressure.normal_()
+    expected = b.positions + a.positions
+    expected_warm = (b.warm_density_pressure + a.warm_density_pressure) if dfsph else None
+    solver.accumulate_state_adjoint(a, b)
+    torch.cuda.synchronize()
+    assert torch.equal(b.positions, expected)
+    if dfsph:
+        assert torch.equal(b.warm_density_pressure, expected_warm)
+    c = solver.allocate_state_adjoint()
+    solver.copy_state_adjoint(a, c)
+    torch.cuda.synchronize()
+    assert torch.equal(c.velocities, a.velocities)
