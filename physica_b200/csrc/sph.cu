@@ -503,6 +503,7 @@ __global__ void sph_constants_kernel(const SphSceneInput* __restrict__ inputs, c
     }
     k.support_threshold = __uint_as_float(hi);
     k.laplacian_denominator = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(kPi, h), h), h), h), h), h);
+    k.laplacian_denominator_d = static_cast<double>(kPi) * pow(static_cast<double>(h), 6.0);
     k.epsilon_factor = __fmul_rn(0.01F, h);
     k.diameter = __fmul_rn(2.0F, in.particle_radius);
     // cubic({diameter, 0, 0}): its length is sqrtf(fma(0, 0, fma(d, d, 0 * 0)))

@@ -49,7 +49,7 @@ __device__ __forceinline__ ViscosityTerms viscosity_reverse(const f3 d, const f3
                                                           const float second_density, const float first_viscosity,
                                                           const float second_viscosity, const float first_speed,
                                                           const float second_speed, const float neighbor_mass,
-                                                          const SphConstants& k, const d3 adjoint) {
+                                                          const SphConstants& k, const d3 adjoint, const CubicHessian& H) {
     ViscosityTerms r{};
     const double compression = dot_xfirst(vd, d);
     if (compression >= 0.0) return r;
@@ -64,7 +64,7 @@ __device__ __forceinline__ ViscosityTerms viscosity_reverse(const f3 d, const f3
     r.neighbor_mass = -pi * dot(adjoint, gradient);
     const double pi_adjoint = -neighbor_mass * dot(adjoint, gradient);
     const d3 gradient_adjoint = times(adjoint, -neighbor_mass * pi);
-    r.displacement = cubic_hessian_product(d, gradient_adjoint, k);
+    r.displacement = hessian_times(H, d, gradient_adjoint);
     const double nu_adjoint = -compression * pi_adjoint / denominator;
     const double compression_adjoint = -nu * pi_adjoint / denominator;
     const double denominator_adjoint = nu * compression * pi_adjoint / (denominator * denominator);
@@ -213,7 +213,8 @@ struct ForceVjpOp {
     __device__ __forceinline__ void apply(const uint32_t t, const ForceVjpData& d) {
         const f3 disp = sub(x, xyz(d.q));
         // every term vanishes once sqrt((double) r2) >= h (the FP64 Hessian's support, the widest)
-        if (sqrt(static_cast<double>(sq_xfirst(disp))) >= k.h) return;
+        const CubicHessian H = cubic_hessian(disp, k);
+        if (H.kind == 0) return;
         const f3 dv = sub(v, xyz(d.v));
         if (t & kBoundaryBit) {
             const float volume = d.q.w;
@@ -224,7 +225,7 @@ struct ForceVjpOp {
             s_rest += sl.second_mass * volume;
             s_boundary_tension += sl.tension;
             const ViscosityTerms vl =
-                viscosity_reverse(disp, dv, density, density, viscosity, viscosity, speed, speed, boundary_mass, k, adjoint);
+                viscosity_reverse(disp, dv, density, density, viscosity, viscosity, speed, speed, boundary_mass, k, adjoint, H);
             v_position = v_position + vl.displacement;
             v_velocity = v_velocity + vl.velocity_difference;
             v_rest += vl.neighbor_mass * volume;
@@ -236,7 +237,7 @@ struct ForceVjpOp {
             const double factor_adjoint = dot(adjoint, gradient);
             p_rest -= factor_adjoint * volume * first_term;
             first_term_adjoint -= factor_adjoint * rest * volume;
-            p_position = p_position + cubic_hessian_product(disp, times(adjoint, factor), k);
+            p_position = p_position + hessian_times(H, disp, times(adjoint, factor));
             return;
         }
         if (t == self) return;
@@ -252,14 +253,14 @@ struct ForceVjpOp {
         s_mass += sc.second_mass;
         // viscosity (sph/wcsph.cu:266-281)
         const ViscosityTerms vl =
-            viscosity_reverse(disp, dv, density, d.aux.x, viscosity, d.aux.y, speed, d.aux.z, mj, k, adjoint);
+            viscosity_reverse(disp, dv, density, d.aux.x, viscosity, d.aux.y, speed, d.aux.z, mj, k, adjoint, H);
         v_position = v_position + vl.displacement;
         v_velocity = v_velocity + vl.velocity_difference;
         v_density += vl.first_density;
         v_viscosity += vl.first_viscosity;
         v_speed += vl.first_speed;
         const ViscosityTerms vc =
-            viscosity_reverse(negf(disp), negf(dv), d.aux.x, density, d.aux.y, viscosity, d.aux.z, speed, mass, k, cross);
+            viscosity_reverse(negf(disp), negf(dv), d.aux.x, density, d.aux.y, viscosity, d.aux.z, speed, mass, k, cross, H);
         v_position = v_position + neg(vc.displacement);
         v_velocity = v_velocity + neg(vc.velocity_difference);
         v_mass += vc.neighbor_mass;
@@ -273,11 +274,11 @@ struct ForceVjpOp {
         const double local_factor = -mj * sum;
         const double local_factor_adjoint = dot(adjoint, gradient);
         first_term_adjoint -= mj * local_factor_adjoint;
-        p_position = p_position + cubic_hessian_product(disp, times(adjoint, local_factor), k);
+        p_position = p_position + hessian_times(H, disp, times(adjoint, local_factor));
         const double cross_projection = dot(cross, gradient);
         p_mass += sum * cross_projection;
         first_term_adjoint += mass * cross_projection;
-        p_position = p_position + cubic_hessian_product(disp, times(cross, mass * sum), k);
+        p_position = p_position + hessian_times(H, disp, times(cross, mass * sum));
     }
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
@@ -539,7 +540,8 @@ struct PressureVjpOp {
     }
     __device__ __forceinline__ void apply(const uint32_t t, const PressureVjpData& d) {
         const f3 disp = sub(x, xyz(d.q));
-        if (sqrt(static_cast<double>(sq_xfirst(disp))) >= k.h) return;
+        const CubicHessian H = cubic_hessian(disp, k);
+        if (H.kind == 0) return;
         const f3 gradient = cubic_gradient_value(disp, k);
         if (t & kBoundaryBit) {   // sph/common.cu:279-290
             const float volume = d.q.w;
@@ -547,7 +549,7 @@ struct PressureVjpOp {
             const double factor_adjoint = dot(adjoint, gradient);
             rest_sum -= factor_adjoint * volume * first_term;
             first_term_adjoint -= factor_adjoint * rest * volume;
-            position = position + cubic_hessian_product(disp, times(adjoint, factor), k);
+            position = position + hessian_times(H, disp, times(adjoint, factor));
             return;
         }
         if (t == self) return;
@@ -557,12 +559,12 @@ struct PressureVjpOp {
         const double local_factor = -mj * sum;
         const double local_factor_adjoint = dot(adjoint, gradient);
         first_term_adjoint -= mj * local_factor_adjoint;
-        position = position + cubic_hessian_product(disp, times(adjoint, local_factor), k);
+        position = position + hessian_times(H, disp, times(adjoint, local_factor));
         const d3 cross = ld(d.adjoint);
         const double cross_projection = dot(cross, gradient);
         mass_sum += sum * cross_projection;
         first_term_adjoint += mass * cross_projection;
-        position = position + cubic_hessian_product(disp, times(cross, mass * sum), k);
+        position = position + hessian_times(H, disp, times(cross, mass * sum));
     }
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };

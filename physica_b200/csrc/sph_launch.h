@@ -30,6 +30,7 @@ struct SphConstants {
     float box_vx, box_vy, box_vz;   // box velocity, written on collision    (sph/common.cu:313-319)
     uint32_t no_slip;
     float skin_bound;               // the predicted density replays the lists while 2 max|x* - x| <= this
+    double laplacian_denominator_d; // pi pow(h, 6) in FP64                  (density/device.cuh:87)
 };
 
 // Sorted per-particle parameters of an SPH step, packed by the grid build:

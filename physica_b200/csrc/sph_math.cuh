@@ -158,11 +158,46 @@ __device__ __forceinline__ d3 cubic_hessian_product(const f3 d, const d3 v, cons
     return times(v, radial) + times(d, radial_derivative * dot(v, d) / r);
 }
 
-// Gradient of the viscosity Laplacian times `scalar`, in FP64 (density/device.cuh:84-88).
+// The scalar part of cubic_hessian_product for one displacement, shared by every vector the
+// Hessian is applied to: applying it gives the same bits as cubic_hessian_product.
+struct CubicHessian {
+    double r, radial, radial_derivative, center;
+    int kind;   // 0 outside the support, 1 at zero distance, 2 inside
+};
+
+__device__ __forceinline__ CubicHessian cubic_hessian(const f3 d, const SphConstants& k) {
+    CubicHessian H{};
+    const float h = k.h;
+    const double r = sqrt(static_cast<double>(sq_xfirst(d)));
+    const double c = 8.0 / (static_cast<double>(kPi) * h * h * h);
+    H.r = r;
+    if (r == 0.0) {
+        H.kind = 1;
+        H.center = -12.0 * c / (h * h);
+        return H;
+    }
+    if (r >= h) return H;
+    const double q = r / h;
+    const double first = q <= 0.5 ? 18.0 * q * q - 12.0 * q : -6.0 * (1.0 - q) * (1.0 - q);
+    const double second = q <= 0.5 ? 36.0 * q - 12.0 : 12.0 * (1.0 - q);
+    H.radial = c * first / (h * r);
+    H.radial_derivative = c * (second / (h * h * r) - first / (h * r * r));
+    H.kind = 2;
+    return H;
+}
+
+__device__ __forceinline__ d3 hessian_times(const CubicHessian& H, const f3 d, const d3 v) {
+    if (H.kind == 1) return times(v, H.center);
+    if (H.kind == 0) return {0.0, 0.0, 0.0};
+    return times(v, H.radial) + times(d, H.radial_derivative * dot(v, d) / H.r);
+}
+
+// Gradient of the viscosity Laplacian times `scalar`, in FP64 (density/device.cuh:84-88); pi h^6
+// is the per-scene constant SphConstants::laplacian_denominator_d.
 __device__ __forceinline__ d3 laplacian_gradient(const f3 d, const SphConstants& k, const double scalar) {
     const double r = sqrt(static_cast<double>(sq_xfirst(d)));
     if (r == 0.0 || r >= k.h) return {0.0, 0.0, 0.0};
-    return times(d, -45.0 * scalar / (static_cast<double>(kPi) * pow(static_cast<double>(k.h), 6.0) * r));
+    return times(d, -45.0 * scalar / (k.laplacian_denominator_d * r));
 }
 
 // The unclamped prediction's collision mask (sph/pcisph.cu:20-24, 69-71).
