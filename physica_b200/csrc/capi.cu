@@ -19,6 +19,14 @@ struct pbf_solver {
     pbf::DeviceArena staging;
     float* in = nullptr;
     float* out = nullptr;
+    // download stream of the *_host entry points: the positions are read back on it while the
+    // post-loop passes still run on the engine's stream
+    cudaStream_t download = nullptr;
+    cudaEvent_t positions_ready = nullptr;
+    ~pbf_solver() {
+        if (positions_ready) cudaEventDestroy(positions_ready);
+        if (download) cudaStreamDestroy(download);
+    }
 };
 
 struct pbf_step_cache {
@@ -239,6 +247,12 @@ int pbf_forward_step_host(pbf_solver* solver, const pbf_host_state* state, const
             solver->out = solver->staging.alloc<float>(6 * n, e);
             if (int rc = en.check(e, "staging allocation")) return rc;
         }
+        if (!solver->download) {
+            if (int rc = en.check(cudaStreamCreateWithFlags(&solver->download, cudaStreamNonBlocking), "download stream"))
+                return rc;
+            if (int rc = en.check(cudaEventCreateWithFlags(&solver->positions_ready, cudaEventDisableTiming), "download event"))
+                return rc;
+        }
         for (int k = 0; k < 3; ++k) {
             if (n && (!state->positions[k] || !state->velocities[k] || !next_state->positions[k] || !next_state->velocities[k]))
                 return null_arg("host field");
@@ -255,17 +269,29 @@ int pbf_forward_step_host(pbf_solver* solver, const pbf_host_state* state, const
                               {solver->in + 3 * n, solver->in + 4 * n, solver->in + 5 * n}, state->step_index};
         pbf_particle_state out{{solver->out, solver->out + n, solver->out + 2 * n},
                                {solver->out + 3 * n, solver->out + 4 * n, solver->out + 5 * n}, 0};
-        if (int rc = en.forward(&in, control, parameters, &out, cache->record)) return rc;
-        for (int k = 0; k < 3; ++k) {
-            if (int rc = en.check(cudaMemcpyAsync(next_state->positions[k], solver->out + k * n, n * sizeof(float),
-                                                  cudaMemcpyDeviceToHost, st), "download"))
-                return rc;
-            if (int rc = en.check(cudaMemcpyAsync(next_state->velocities[k], solver->out + (3 + k) * n, n * sizeof(float),
-                                                  cudaMemcpyDeviceToHost, st), "download"))
-                return rc;
-        }
+        // The positions are final after the last correction: their download on the second stream
+        // overlaps the post-loop passes; the velocities follow XSPH on the engine's stream.
+        en.set_positions_ready_event(solver->positions_ready);
+        const int frc = en.forward(&in, control, parameters, &out, cache->record);
+        en.set_positions_ready_event(nullptr);
+        if (frc) return frc;
+        cudaStream_t dl = solver->download;
+        if (int rc = en.check(cudaStreamWaitEvent(dl, solver->positions_ready, 0), "download wait")) return rc;
+        int rc = PBF_SUCCESS;
+        for (int k = 0; k < 3 && !rc; ++k)
+            rc = en.check(cudaMemcpyAsync(next_state->positions[k], solver->out + k * n, n * sizeof(float),
+                                          cudaMemcpyDeviceToHost, dl), "download");
+        for (int k = 0; k < 3 && !rc; ++k)
+            rc = en.check(cudaMemcpyAsync(next_state->velocities[k], solver->out + (3 + k) * n, n * sizeof(float),
+                                          cudaMemcpyDeviceToHost, st), "download");
+        // both streams drain before returning, so the next call may reuse the staging buffers
+        const int src = en.check(cudaStreamSynchronize(st), "forward_step_host");
+        const int drc = en.check(cudaStreamSynchronize(dl), "forward_step_host download");
+        if (rc) return rc;
+        if (src) return src;
+        if (drc) return drc;
         next_state->step_index = out.step_index;
-        return en.check(cudaStreamSynchronize(st), "forward_step_host");
+        return static_cast<int>(PBF_SUCCESS);
     });
 }
 

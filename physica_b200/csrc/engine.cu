@@ -306,7 +306,7 @@ int Engine::init(const pbf_domain_configuration* scenes, const uint32_t scene_co
 }
 
 bool Engine::GraphKey::operator==(const GraphKey& o) const {
-    if (record != o.record) return false;
+    if (record != o.record || positions_ready != o.positions_ready) return false;
     for (int k = 0; k < 16; ++k)
         if (p[k] != o.p[k]) return false;
     return true;
@@ -418,6 +418,7 @@ int Engine::forward(const pbf_particle_state* state, const pbf_control* control,
                                 next_state->positions.x, next_state->velocities.x, parameters->vorticity_confinement};
         for (int k = 0; k < 16; ++k) key.p[k] = ptrs[k];
         key.record = &r;
+        key.positions_ready = positions_ready_;
         cudaGraphExec_t exec = nullptr;
         unsigned captured_launches = 0;
         for (size_t k = 0; k < graph_cache_.size(); ++k) {
@@ -562,6 +563,14 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
                                               out_positions, r.velocity),
                            "reconstruct"))
             return rc;
+    }
+    // next_state.positions are final here.  Under capture the record must be external to become an
+    // event node of the graph; outside a capture it is a plain record.
+    if (positions_ready_) {
+        cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+        if (int rc = check(cudaStreamIsCapturing(stream, &capture), "capture status")) return rc;
+        const unsigned flags = capture == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+        if (int rc = check(cudaEventRecordWithFlags(positions_ready_, stream, flags), "positions event")) return rc;
     }
     const uint32_t lp = diff ? K : 0u;
     const StoredList post{r.list_entries[lp], r.list_counts[lp], r.list_capacity};

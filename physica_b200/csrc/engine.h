@@ -197,12 +197,17 @@ public:
     // Replay the forward launch sequence as a CUDA graph, captured once per buffer set.
     void set_graphs(bool on) { graphs_ = on; }
     bool graphs() const { return graphs_; }
+    // Optional event recorded on the step's stream as soon as next_state.positions are final (after
+    // the last correction, before the post-loop passes), so that a caller can start reading them
+    // while vorticity, confinement and XSPH run.  Null: no event.  Part of the graph key.
+    void set_positions_ready_event(cudaEvent_t event) { positions_ready_ = event; }
     void forget(const StepRecord* record);
 
 private:
     struct GraphKey {
         const void* p[16];
         const StepRecord* record;
+        cudaEvent_t positions_ready;
         bool operator==(const GraphKey& o) const;
     };
     struct GraphEntry {
@@ -219,6 +224,7 @@ private:
 
     PassTimer timer_;
     bool graphs_ = false;
+    cudaEvent_t positions_ready_ = nullptr;
     cudaStream_t capture_stream_ = nullptr;
     std::vector<GraphEntry> graph_cache_;
     SceneStatic* d_static_ = nullptr;

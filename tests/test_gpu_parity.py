@@ -280,6 +280,33 @@ def test_host_buffer_entry_matches_device_entry():
     assert np.array_equal(ov.numpy(), nxt.velocities.cpu().numpy())
 
 
+@pytest.mark.parametrize("graphs", [False, True])
+def test_host_buffer_rollout_matches_device_rollout(graphs):
+    """Four host-buffer steps, alternating buffers as a rollout does (the positions are read back on
+    a second stream while the post-loop passes run), against four device steps."""
+    sc = scenes.plain_small(lattice=(12, 12, 12))
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    cur, nxt = state, solver.allocate_state()
+    for _ in range(4):
+        solver.forward_step(cur, control, params, nxt, cache)
+        cur, nxt = nxt, cur
+    torch.cuda.synchronize()
+    hsolver, _, _, _ = pbf.solver_for_scene(sc)
+    hsolver.set_graph_mode(graphs)
+    hcache = hsolver.allocate_step_cache()
+    hx = torch.from_numpy(sc.positions.copy()).pin_memory()
+    hv = torch.from_numpy(sc.velocities.copy()).pin_memory()
+    ox, ov = torch.empty_like(hx).pin_memory(), torch.empty_like(hv).pin_memory()
+    step_index = 0
+    for _ in range(4):
+        step_index = hsolver.forward_step_host(hx, hv, control, params, ox, ov, hcache, step_index)
+        hx, ox, hv, ov = ox, hx, ov, hv
+    assert step_index == 4
+    assert np.array_equal(hx.numpy(), cur.positions.cpu().numpy())
+    assert np.array_equal(hv.numpy(), cur.velocities.cpu().numpy())
+
+
 def test_vjp_requires_differentiable_mode():
     sc = scenes.plain_small(lattice=(4, 4, 4))
     solver, state, control, params = pbf.solver_for_scene(sc)
