@@ -265,7 +265,7 @@ def bench_b200(args, world, rank):
         achieved = bytes_per_particle[top["name"]] * n / (avg * 1e-3) / 1e9
         roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                     "frac": round(achieved / hbm, 5), "traffic": traffic_from_profiles(top["name"]),
-                    "kernel": top["name"], "peak_source": hbm_src,
+                    "kernel": top["name"], "peak_source": hbm_src, "issue": issue_roofline(top["name"], avg),
                     "note": "gather passes are FP32/issue bound; fp32 fraction in per_pass and step_roofline"}
     b_alg = (192 + 44 * K) * n + 12 * cells
     f_alg = neighbors * (69 * K + 81) * n
@@ -348,16 +348,38 @@ def read_profile(lib, handle):
             for k in range(cnt.value)]
 
 
-def traffic_from_profiles(kernel: str):
-    """DRAM bytes per launch of `kernel` recorded from an ncu capture under profiles/ (or None)."""
+def profile_figure(name: str, kernel: str):
+    """A per-launch figure `name [kernel] = value` recorded from an ncu capture under profiles/ (or None)."""
     for p in sorted((ROOT / "profiles").glob("*.md")):
         for line in p.read_text().splitlines():
-            if line.startswith("traffic_bytes_per_launch") and f"[{kernel}]" in line:
+            if line.startswith(name) and f"[{kernel}]" in line:
                 try:
                     return int(line.split("=")[-1].strip())
                 except ValueError:
                     pass
     return None
+
+
+def traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` recorded from an ncu capture under profiles/ (or None)."""
+    return profile_figure("traffic_bytes_per_launch", kernel)
+
+
+def issue_roofline(kernel: str, launch_ms: float):
+    """The bound the gather passes actually meet: instruction issue.  The warp instructions of one
+    launch (ncu, profiles/) over its live CUDA-event duration, against the SM's issue limit of one
+    warp instruction per scheduler per cycle (4 per SM) at the maximum SM clock."""
+    instructions = profile_figure("warp_instructions_per_launch", kernel)
+    if instructions is None or launch_ms <= 0:
+        return None
+    try:
+        mhz = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["sm_max_mhz"])
+    except Exception:
+        mhz = 1965.0
+    peak = 148 * 4 * mhz * 1e6 / 1e9
+    achieved = instructions / (launch_ms * 1e-3) / 1e9
+    return {"achieved": round(achieved, 1), "peak": round(peak, 1), "unit": "G warp-instructions/s",
+            "frac": round(achieved / peak, 4), "warp_instructions": instructions}
 
 
 def bench_grad(args, world, rank):
