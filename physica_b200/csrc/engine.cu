@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <string>
 
@@ -208,6 +209,15 @@ int Engine::init(const pbf_domain_configuration* scenes, const uint32_t scene_co
     d_constants_ = arena_.alloc<KernelConstants>(scene_count, e);
     float* d_radii = arena_.alloc<float>(scene_count, e);
     predicted_ = arena_.alloc<float4>(count_, e);
+    {
+        // three arrays of `stride` floats, each 16-byte aligned with readable slack past the end
+        const size_t stride = (static_cast<size_t>(count_) + 4u + 31u) / 32u * 32u;
+        float* base = arena_.alloc<float>(3 * stride + 4, e);
+        if (base) {
+            base = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(base) + 15u) & ~uintptr_t{15});
+            packed_ = PackedPositions{base, base + stride, base + 2 * stride};
+        }
+    }
     arrival_ = arena_.alloc<uint32_t>(count_, e);
     unordered_ = arena_.alloc<uint32_t>(count_, e);
     tile_sums_ = arena_.alloc<uint32_t>(scan_tile_count(cells_ + 1), e);
@@ -525,6 +535,7 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
     g.params_a = r.params_a;
     g.params_b = r.params_b;
     g.input_flags = input_checks_ ? d_input_flags_ : nullptr;
+    g.packed = packed_;
     timer_.begin(stream, kPassGrid);
     if (int rc = check(launch_grid_build(stream, g), "grid build")) return rc;
     if (boundary_count_ > 0) {
@@ -544,7 +555,9 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
         const uint32_t l = diff ? k : 0u;
         const StoredList list{r.list_entries[l], r.list_counts[l], r.list_capacity};
         timer_.begin(stream, kPassListScan);
-        if (int rc = check(launch_list_scan(stream, ListScanArgs{gc, xk, list, 1}, shape_), "neighbour list scan")) return rc;
+        ListScanArgs scan{gc, xk, list, 1};
+        scan.packed = packed_;
+        if (int rc = check(launch_list_scan(stream, scan, shape_), "neighbour list scan")) return rc;
         timer_.end(stream, kPassListScan);
         DensityLambdaArgs d{gc, xk, lam, diff ? r.density[k] : (k == 0 ? r.first_density : nullptr),
                             diff ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr, list};
@@ -553,6 +566,7 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
         timer_.end(stream, kPassDensityLambda);
         CorrectionArgs c{gc, xk, lam, xk1, diff ? r.mask[k] : nullptr, k + 1 == K ? 1 : 0, previous, r.sorted_index,
                          out_positions, r.velocity, list};
+        c.packed = packed_;
         timer_.begin(stream, kPassCorrection);
         if (int rc = check(launch_correction(stream, c, shape_.block), "correction/project")) return rc;
         timer_.end(stream, kPassCorrection);
@@ -575,7 +589,9 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
     const uint32_t lp = diff ? K : 0u;
     const StoredList post{r.list_entries[lp], r.list_counts[lp], r.list_capacity};
     timer_.begin(stream, kPassListScan);
-    if (int rc = check(launch_list_scan(stream, ListScanArgs{gc, xK, post}, shape_), "neighbour list scan")) return rc;
+    ListScanArgs post_scan{gc, xK, post};
+    post_scan.packed = packed_;
+    if (int rc = check(launch_list_scan(stream, post_scan, shape_), "neighbour list scan")) return rc;
     timer_.end(stream, kPassListScan);
     VorticityArgs v{gc, xK, r.velocity, r.vorticity, post};
     timer_.begin(stream, kPassVorticity);

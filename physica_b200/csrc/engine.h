@@ -259,6 +259,9 @@ private:
     uint32_t* d_scene_of_ = nullptr;
     // grid-build scratch
     float4* predicted_ = nullptr;
+    // The current iterate as three arrays in sorted order (x, y, z), written by the grid build and
+    // every correction, read by the per-lane list scan.
+    PackedPositions packed_{};
     uint32_t* arrival_ = nullptr;
     uint32_t* unordered_ = nullptr;
     uint32_t* tile_sums_ = nullptr;

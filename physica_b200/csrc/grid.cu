@@ -163,7 +163,8 @@ __global__ void reorder_kernel(const uint32_t count, const SceneDesc* __restrict
                                const float4* __restrict__ predicted, const ParamPointers params,
                                uint32_t* __restrict__ sorted_index, uint32_t* __restrict__ slot_of,
                                int4* __restrict__ cell, float4* __restrict__ topology, float4* __restrict__ params_a,
-                               float4* __restrict__ params_b, const Field3 velocities, float4* __restrict__ sorted_velocity) {
+                               float4* __restrict__ params_b, const Field3 velocities, float4* __restrict__ sorted_velocity,
+                               const PackedPositions packed) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const uint32_t i = unordered[t];
@@ -176,6 +177,11 @@ __global__ void reorder_kernel(const uint32_t count, const SceneDesc* __restrict
     slot_of[i] = s;
     const float4 xs = predicted[i];
     topology[s] = xs;
+    if (packed.x) {
+        packed.x[s] = xs.x;
+        packed.y[s] = xs.y;
+        packed.z[s] = xs.z;
+    }
     const uint32_t scene = scene_of ? scene_of[i] : 0u;
     const Grid& g = scenes[scene].grid;
     // gather-side cell of x* (neighborhood/device.cuh:44-48)
@@ -332,7 +338,7 @@ cudaError_t launch_grid_build(cudaStream_t stream, const GridBuildArgs& a) {
         scatter_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(a.count, a.keys, a.arrival, a.cell_offsets, a.unordered);
         reorder_kernel<<<blocks_for(a.count, tpb), tpb, 0, stream>>>(
             a.count, a.scenes, a.scene_of, a.keys, a.cell_offsets, a.unordered, a.predicted, a.params, a.sorted_index,
-            a.slot_of, a.cell, a.topology, a.params_a, a.params_b, a.velocities, a.sorted_velocity);
+            a.slot_of, a.cell, a.topology, a.params_a, a.params_b, a.velocities, a.sorted_velocity, a.packed);
         count_launch(2);
     }
     return cudaGetLastError();

@@ -11,6 +11,14 @@ namespace pbf {
 void count_launch(unsigned n = 1);
 uint64_t launch_count();
 
+// Iterate positions in sorted order as three arrays (x, y, z) for the packed list scan.  Each
+// array starts 16-byte aligned and has at least three readable floats past its last slot.
+struct PackedPositions {
+    float* x = nullptr;
+    float* y = nullptr;
+    float* z = nullptr;
+};
+
 struct GridBuildArgs {
     uint32_t count;
     uint64_t cells;
@@ -33,6 +41,7 @@ struct GridBuildArgs {
     uint32_t* input_flags = nullptr;   // optional input checks (PBF_INPUT_* bits), null when off
     int key_current = 0;               // key the input positions instead of the predicted ones (SPH)
     float4* sorted_velocity = nullptr; // optional (v, 0) in sorted order
+    PackedPositions packed{};          // optional x* as three arrays in sorted order
 };
 
 size_t scan_tile_count(uint64_t n);
@@ -109,6 +118,7 @@ struct CorrectionArgs {
     MutField3 out_positions;   // original order (next_state.positions)
     float4* velocity;          // reconstructed velocity (sorted)
     StoredList list;
+    PackedPositions packed{};  // optional copy of pos_next as three arrays
 };
 
 struct VorticityArgs {
@@ -143,6 +153,9 @@ struct ListScanArgs {
     const float4* pos;
     StoredList list;
     int boundary = 0;   // also list boundary particles (density, lambda and correction lists)
+    // optional: the same positions as three arrays; the per-lane scan then tests candidates in
+    // pairs with packed FP32 arithmetic (ignored for lists with boundary particles)
+    PackedPositions packed{};
 };
 
 // Launch shape of the neighbour-list and gather kernels.  Every shape gives bit-identical results
