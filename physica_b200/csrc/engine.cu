@@ -209,15 +209,7 @@ int Engine::init(const pbf_domain_configuration* scenes, const uint32_t scene_co
     d_constants_ = arena_.alloc<KernelConstants>(scene_count, e);
     float* d_radii = arena_.alloc<float>(scene_count, e);
     predicted_ = arena_.alloc<float4>(count_, e);
-    {
-        // three arrays of `stride` floats, each 16-byte aligned with readable slack past the end
-        const size_t stride = (static_cast<size_t>(count_) + 4u + 31u) / 32u * 32u;
-        float* base = arena_.alloc<float>(3 * stride + 4, e);
-        if (base) {
-            base = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(base) + 15u) & ~uintptr_t{15});
-            packed_ = PackedPositions{base, base + stride, base + 2 * stride};
-        }
-    }
+    packed_ = alloc_packed(arena_, count_, e);
     arrival_ = arena_.alloc<uint32_t>(count_, e);
     unordered_ = arena_.alloc<uint32_t>(count_, e);
     tile_sums_ = arena_.alloc<uint32_t>(scan_tile_count(cells_ + 1), e);

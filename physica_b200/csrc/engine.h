@@ -46,6 +46,15 @@ private:
     std::vector<void*> ptrs_;
 };
 
+// Three arrays of count + 4 floats or more, each 16-byte aligned, for the packed list scan.
+inline PackedPositions alloc_packed(DeviceArena& arena, const uint32_t count, cudaError_t& err) {
+    const size_t stride = (static_cast<size_t>(count) + 4u + 31u) / 32u * 32u;
+    float* base = arena.alloc<float>(3 * stride + 4, err);
+    if (!base) return PackedPositions{};
+    base = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(base) + 15u) & ~uintptr_t{15});
+    return PackedPositions{base, base + stride, base + 2 * stride};
+}
+
 struct SceneHost {
     pbf_domain_configuration config;     // boundary pointer cleared
     std::vector<pbf_boundary_particle> boundary;

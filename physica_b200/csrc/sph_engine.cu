@@ -138,6 +138,7 @@ private:
     unsigned long long* d_step_ = nullptr;
     uint64_t host_step_ = ~0ull;
     float4* scratch_ = nullptr;      // grid build: (x, m) in original order
+    PackedPositions packed_{};       // the sorted positions again as x, y, z arrays (packed list scan)
     uint32_t* arrival_ = nullptr;
     uint32_t* unordered_ = nullptr;
     uint32_t* tile_sums_ = nullptr;
@@ -240,6 +241,7 @@ int SphEngine::init(const pbf_domain_configuration* domain, const sph_configurat
     float* d_radius = arena_.alloc<float>(1, e);
     SphSceneInput* d_input = arena_.alloc<SphSceneInput>(1, e);
     scratch_ = arena_.alloc<float4>(count_, e);
+    packed_ = alloc_packed(arena_, count_, e);
     arrival_ = arena_.alloc<uint32_t>(count_, e);
     unordered_ = arena_.alloc<uint32_t>(count_, e);
     tile_sums_ = arena_.alloc<uint32_t>(scan_tile_count(cells_ + 1), e);
@@ -454,6 +456,7 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
     g.params_b = r.params_b;
     g.key_current = 1;
     g.sorted_velocity = r.velocity;
+    g.packed = packed_;
     if (int rc = check(launch_grid_build(s, g), "grid build")) return rc;
     if (boundary_count_ > 0) {
         BoundaryBuildArgs b{boundary_count_, cells_, d_scenes_, nullptr, boundary_rest_, boundary_velocity_, boundary_keys_,
@@ -467,7 +470,9 @@ int SphEngine::launch(cudaStream_t s, const pbf_particle_state* state, const sph
         gc.boundary = r.boundary;
     }
     const StoredList list{r.list_entries, r.list_counts, r.list_capacity};
-    if (int rc = check(launch_list_scan(s, ListScanArgs{gc, r.topology, list, 1}, shape), "neighbour list scan")) return rc;
+    ListScanArgs scan{gc, r.topology, list, 1};
+    scan.packed = packed_;
+    if (int rc = check(launch_list_scan(s, scan, shape), "neighbour list scan")) return rc;
     SphStep st{gc,
                d_constants_,
                r.topology,
