@@ -301,8 +301,10 @@ def bench_b200(args, world, rank):
 
     # differentiable rollout: grad-steps/s at 64k
     grad = None
+    tangent = None
     if not args.no_grad:
         grad = bench_grad(args, world, rank)
+        tangent = tangent_ms(args, world, sc)
 
     batched = None
     if not args.no_batch:
@@ -328,7 +330,7 @@ def bench_b200(args, world, rank):
                                     "autotune_ms_per_step": None if math.isnan(tuned_ms) else round(tuned_ms, 4)}},
         "roofline": roofline, "step_roofline": step_roofline, "per_pass": per_pass,
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(round(per_step_launches * args.steps)),
-        "clocks": clk.summary(), "grad_steps_per_s": grad, "batched_scenes": batched,
+        "clocks": clk.summary(), "grad_steps_per_s": grad, "tangent_ms_per_step": tangent, "batched_scenes": batched,
         "batched_grad_steps_per_s": batched_grad, "sph_family": sph_family,
     }
 
@@ -408,6 +410,31 @@ def bench_grad(args, world, rank):
                        "launch_shape": {"list_scan": ["per_lane", "cooperative", "staged"][shape.list_scan],
                                         "scan_block": shape.scan_block_size, "block": shape.block_size}},
             "loss": g.loss}
+
+
+def tangent_ms(args, world, sc):
+    """One differentiable substep and its jvp_step (unit position tangent, zero control and
+    parameter tangents) on the 1M dam break, per step in ms."""
+    from physica_b200 import pbf
+    solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable)
+    cache = solver.allocate_step_cache()
+    nxt = solver.allocate_state()
+    st, nt = solver.allocate_state_tangent(), solver.allocate_state_tangent()
+    st.positions.fill_(1.0)
+    ct, pt = solver.allocate_control(), solver.allocate_parameter_tangent()
+    for t in pt.tensors.values():
+        t.zero_()
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        solver.forward_step(state, control, params, nxt, cache)
+        solver.jvp_step(state, control, params, nxt, cache, st, ct, pt, nt)
+
+    steps = max(3, min(args.steps, 5))
+    ms, _ = timed(step, steps, 3, world, solver.stream, flush)
+    del cache, solver
+    torch.cuda.synchronize()
+    return round(max_over_ranks(ms, world) / steps, 4)
 
 
 def bench_batch(args, world, rank):
@@ -663,6 +690,7 @@ def bench_reference(args, world, rank):
     ms_per_step = ms_max / args.steps
     value = world * n / (ms_per_step * 1e-3)
     grad = None if args.no_grad else bench_reference_grad(world, rank)
+    tangent = None if args.no_grad else reference_tangent_ms(args, world, sc)
     batched = None if args.no_batch else bench_reference_batch(args, world, rank)
     sph_family = None if args.no_sph else bench_reference_sph(args, world, rank)
     return {
@@ -678,7 +706,8 @@ def bench_reference(args, world, rank):
                                    "compiled from its sources) replaying PBF::forward_step on the same B200; the reference "
                                    "has no CPU implementation of this path"},
         "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "clocks": clk.summary(), "grad_steps_per_s": grad, "batched_scenes": batched, "sph_family": sph_family,
+        "clocks": clk.summary(), "grad_steps_per_s": grad, "tangent_ms_per_step": tangent, "batched_scenes": batched,
+        "sph_family": sph_family,
     }
 
 
@@ -736,6 +765,36 @@ def bench_reference_batch(args, world, rank):
     return {"unit": UNIT, "per_scene_solvers": round(world * total / (ms * 1e-3), 1), "per_scene_ms_per_step": round(ms, 4),
             "config": {"workload": "batched_forward_256: 256 dam-break scenes, counts log-uniform in [2048, 65536], "
                                    "4 iterations", "particles_per_gpu": total, "scenes_per_gpu": len(scs)}}
+
+
+def reference_tangent_ms(args, world, sc):
+    """The same differentiable substep and jvp_step through the reference's kernels, per step in ms."""
+    from oracle import reference
+    ref = reference.ReferencePBF(sc, differentiable=True)
+    n = sc.count
+    x = torch.from_numpy(sc.positions).cuda().contiguous()
+    v = torch.from_numpy(sc.velocities).cuda().contiguous()
+    xo, vo = torch.zeros_like(x), torch.zeros_like(v)
+    tangent = {"positions": torch.ones((3, n), dtype=torch.float32, device="cuda"),
+               "velocities": torch.zeros((3, n), dtype=torch.float32, device="cuda")}
+    next_tangent = {k: torch.zeros_like(t) for k, t in tangent.items()}
+    control_tangent = torch.zeros((3, n), dtype=torch.float32, device="cuda")
+    names = ("masses", "rest_densities", "relaxation", "artificial_pressure_strength", "artificial_pressure_exponent",
+             "artificial_pressure_radius", "xsph_viscosity", "vorticity_confinement")
+    param_tangent = {k: torch.zeros(n, dtype=torch.float32, device="cuda") for k in names}
+    stream = torch.cuda.ExternalStream(ref.stream)
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+
+    def step():
+        ref.forward_step(x, v, xo, vo, 0, synchronize=False)
+        ref.jvp_step(x, v, tangent, control_tangent, param_tangent, next_tangent, synchronize=False)
+
+    steps = max(3, min(args.steps, 5))
+    ms, _ = timed(step, steps, 3, world, stream, flush)
+    ref.close()
+    torch.cuda.synchronize()
+    return round(max_over_ranks(ms, world) / steps, 4)
 
 
 def bench_reference_grad(world, rank):

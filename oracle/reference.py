@@ -176,9 +176,10 @@ class ReferencePBF:
             raise RuntimeError(f"ref_vjp_step failed: {rc}")
         lib.ref_synchronize(self.handle)
 
-    def jvp_step(self, x, v, tangent, control_tangent, param_tangent, next_tangent):
+    def jvp_step(self, x, v, tangent, control_tangent, param_tangent, next_tangent, synchronize=True):
         """PBF::jvp_step after forward_step of (x, v).  tangent / next_tangent: dicts with (3, N)
-        float32 CUDA tensors "positions" and "velocities"; param_tangent: dict of float32 (N,) tensors."""
+        float32 CUDA tensors "positions" and "velocities"; param_tangent: dict of float32 (N,) tensors.
+        synchronize=False leaves the launches queued on the harness's stream (inputs must be ready)."""
         lib = load()
         sin = RefStateIn(_p(x[0]), _p(x[1]), _p(x[2]), _p(v[0]), _p(v[1]), _p(v[2]))
         tin = RefStateIn(*[_p(tangent[k][a]) for k in ("positions", "velocities") for a in range(3)])
@@ -188,12 +189,15 @@ class ReferencePBF:
         pt = RefParams(_p(g["masses"]), _p(g["rest_densities"]), _p(g["relaxation"]),
                        _p(g["artificial_pressure_strength"]), _p(g["artificial_pressure_exponent"]),
                        _p(g["artificial_pressure_radius"]), _p(g["xsph_viscosity"]), _p(g["vorticity_confinement"]))
-        torch.cuda.synchronize(self.device)
+        if synchronize:
+            torch.cuda.synchronize(self.device)
+        self._keep_tangent = (sin, tin, tout, ct, pt)
         rc = lib.ref_jvp_step(self.handle, ctypes.byref(sin), ctypes.byref(self._pstruct()), ctypes.byref(tin), ct,
                               ctypes.byref(pt), ctypes.byref(tout))
         if rc:
             raise RuntimeError(f"ref_jvp_step failed: {rc}")
-        lib.ref_synchronize(self.handle)
+        if synchronize:
+            lib.ref_synchronize(self.handle)
 
     def read(self, field: str) -> torch.Tensor:
         n = self.n
