@@ -558,6 +558,7 @@ def bench_sph(args, world, rank, methods=SPH_METHODS):
         torch.cuda.synchronize()
         if not args.no_grad:
             out[name]["gradient_ms_per_step"] = round(sph_gradient_ms(args, world, sc, name), 4)
+            out[name]["tangent_ms_per_step"] = round(sph_tangent_ms(args, world, sc, name), 4)
     return out
 
 
@@ -580,6 +581,59 @@ def sph_gradient_ms(args, world, sc, name):
     steps = max(3, min(args.steps, 5))
     ms, _ = timed(step, steps, 3, world, solver.stream, flush)
     del cache, solver
+    torch.cuda.synchronize()
+    return max_over_ranks(ms, world) / steps
+
+
+def sph_tangent_ms(args, world, sc, name):
+    """One differentiable SPH substep and its jvp_step (unit position tangent), per step in ms."""
+    from physica_b200 import pbf, sph
+    solver, state, control, params = sph.solver_for_scene(sc, sph.Method[name], mode=pbf.ExecutionMode.differentiable)
+    cache = solver.allocate_step_cache()
+    nxt = solver.allocate_state()
+    st, nt = solver.allocate_state_tangent(), solver.allocate_state_tangent()
+    st.positions.fill_(1.0)
+    ct, pt = solver.allocate_control(), solver.allocate_parameter_tangent()
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        solver.forward_step(state, control, params, nxt, cache)
+        solver.jvp_step(state, control, params, nxt, cache, st, ct, pt, nt)
+
+    steps = max(3, min(args.steps, 5))
+    ms, _ = timed(step, steps, 3, world, solver.stream, flush)
+    del cache, solver
+    torch.cuda.synchronize()
+    return max_over_ranks(ms, world) / steps
+
+
+def reference_sph_tangent_ms(args, world, sc, name):
+    """The reference's differentiable SPH substep and its jvp_step, per step in ms."""
+    from oracle import reference
+    from physica_b200 import sph
+    n = sc.count
+    ref = reference.ReferenceSPH(sc, int(sph.Method[name]), differentiable=True)
+    x = torch.from_numpy(sc.positions).cuda().contiguous()
+    v = torch.from_numpy(sc.velocities).cuda().contiguous()
+    xo, vo = torch.zeros_like(x), torch.zeros_like(v)
+    z = lambda: torch.zeros(n, device="cuda")
+    warm, warm_out = (z(), z()), (z(), z())
+    tangent = {"positions": torch.ones((3, n), dtype=torch.float32, device="cuda"),
+               "velocities": torch.zeros((3, n), dtype=torch.float32, device="cuda")}
+    next_tangent = {k: torch.zeros_like(t) for k, t in tangent.items()}
+    control_tangent = torch.zeros((3, n), dtype=torch.float32, device="cuda")
+    warm_tangent, next_warm_tangent = (z(), z()), (z(), z())
+    flush = torch.zeros(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+
+    def step():
+        ref.forward_step(x, v, xo, vo, 0, warm=warm, warm_out=warm_out, synchronize=False)
+        ref.jvp_step(x, v, tangent, control_tangent, {}, next_tangent, 0, warm=warm, warm_tangent=warm_tangent,
+                     next_warm_tangent=next_warm_tangent, synchronize=False)
+
+    steps = max(3, min(args.steps, 5))
+    ms, _ = timed(step, steps, 3, world, torch.cuda.ExternalStream(ref.stream), flush)
+    ref.close()
     torch.cuda.synchronize()
     return max_over_ranks(ms, world) / steps
 
@@ -613,6 +667,7 @@ def bench_reference_sph(args, world, rank, methods=SPH_METHODS):
         torch.cuda.synchronize()
         if not args.no_grad:
             out[name]["gradient_ms_per_step"] = round(reference_sph_gradient_ms(args, world, sc, name), 4)
+            out[name]["tangent_ms_per_step"] = round(reference_sph_tangent_ms(args, world, sc, name), 4)
     return out
 
 

@@ -328,12 +328,15 @@ class ReferenceSPH:
         return names + [names[0]] * (3 - len(names))
 
     def jvp_step(self, x, v, tangent, control_tangent, param_tangent, next_tangent, step_index, warm=None, warm_tangent=None,
-                 next_warm_tangent=None):
+                 next_warm_tangent=None, synchronize=True):
         """SPH<Method>::jvp_step after forward_step of (x, v).  tangent / next_tangent: dicts of (3, N)
         float32 tensors "positions" / "velocities"; param_tangent: dict of (N,) float32 tensors keyed
-        like scene.sph; warm / warm_tangent / next_warm_tangent: DFSPH pairs of (N,) float32."""
+        like scene.sph; warm / warm_tangent / next_warm_tangent: DFSPH pairs of (N,) float32.
+        synchronize=False leaves the launches queued on the harness's stream (inputs must be ready)."""
         lib = _load_sph()
-        z = torch.zeros(self.n, dtype=torch.float32, device=self.device)
+        if getattr(self, "_zero_tangent", None) is None or self._zero_tangent.numel() != self.n:
+            self._zero_tangent = torch.zeros(self.n, dtype=torch.float32, device=self.device)
+        z = self._zero_tangent
         sin = RefStateIn(_p(x[0]), _p(x[1]), _p(x[2]), _p(v[0]), _p(v[1]), _p(v[2]))
         tin = RefStateIn(*[_p(tangent[k][a]) for k in ("positions", "velocities") for a in range(3)])
         tout = RefStateOut(*[_p(next_tangent[k][a]) for k in ("positions", "velocities") for a in range(3)])
@@ -346,12 +349,15 @@ class ReferenceSPH:
         nwt = (vp * 2)(*[(next_warm_tangent[a] if next_warm_tangent is not None else z).data_ptr() for a in range(2)])
         w = [vp(t.data_ptr()) if t is not None else None for t in (warm if warm is not None else (None, None))]
         params = self._pstruct()
-        torch.cuda.synchronize(self.device)
+        if synchronize:
+            torch.cuda.synchronize(self.device)
+        self._keep_tangent = (sin, tin, tout, ct, pt, mt, wt, nwt, w, params)
         rc = lib.ref_sph_jvp_step(self.handle, ctypes.byref(sin), ctypes.byref(params), ctypes.byref(tin), ct, pt, mt, wt,
                                   ctypes.byref(tout), nwt, step_index, w[0], w[1])
         if rc:
             raise RuntimeError(f"ref_sph_jvp_step failed: {rc}")
-        load().ref_synchronize(self.base.handle)
+        if synchronize:
+            load().ref_synchronize(self.base.handle)
 
     def vjp_step(self, x, v, next_adjoint, previous_adjoint, control_adjoint, param_adjoint, step_index, next_warm=None,
                  previous_warm=None):
