@@ -219,6 +219,9 @@ int pbf_vjp_step(pbf_solver* solver, const pbf_particle_state* state, const pbf_
 /* ---- PBF::copy_state / copy_state_adjoint / accumulate_state_adjoint (pbf/pbf.cpp:162-165,
  *      domain/domain.cpp:129-199) ---- */
 int pbf_copy_state(pbf_solver* solver, const pbf_particle_state* source, pbf_particle_state* destination);
+/* PBF::copy_state_tangent (pbf/pbf.cpp:163) */
+int pbf_copy_state_tangent(pbf_solver* solver, const pbf_particle_state_tangent* source,
+                           pbf_particle_state_tangent* destination);
 int pbf_copy_state_adjoint(pbf_solver* solver, const pbf_particle_state_adjoint* source,
                            pbf_particle_state_adjoint* destination);
 int pbf_accumulate_state_adjoint(pbf_solver* solver, const pbf_particle_state_adjoint* source,

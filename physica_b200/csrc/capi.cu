@@ -199,6 +199,26 @@ int pbf_copy_state(pbf_solver* solver, const pbf_particle_state* source, pbf_par
     });
 }
 
+int pbf_copy_state_tangent(pbf_solver* solver, const pbf_particle_state_tangent* source,
+                           pbf_particle_state_tangent* destination) {
+    if (!solver || !source || !destination) return null_arg("solver/source/destination");
+    return guarded([&] {
+        const size_t bytes = static_cast<size_t>(solver->engine.count()) * sizeof(float);
+        cudaStream_t st = solver->engine.stream();
+        const float* src[6] = {source->positions.x, source->positions.y, source->positions.z,
+                               source->velocities.x, source->velocities.y, source->velocities.z};
+        float* dst[6] = {destination->positions.x, destination->positions.y, destination->positions.z,
+                         destination->velocities.x, destination->velocities.y, destination->velocities.z};
+        for (int k = 0; k < 6; ++k) {
+            if (bytes && (!src[k] || !dst[k])) return null_arg("field");
+            if (int rc = solver->engine.check(cudaMemcpyAsync(dst[k], src[k], bytes, cudaMemcpyDeviceToDevice, st),
+                                              "copy_state_tangent"))
+                return rc;
+        }
+        return static_cast<int>(PBF_SUCCESS);
+    });
+}
+
 int pbf_copy_state_adjoint(pbf_solver* solver, const pbf_particle_state_adjoint* source, pbf_particle_state_adjoint* destination) {
     if (!solver || !source || !destination) return null_arg("solver/source/destination");
     return guarded([&] {

@@ -3,7 +3,7 @@
 Mirrors the reference's solver interface (fluids/liquid/particle/pbf/pbf.ixx:14-141 and
 domain/domain.ixx:12-165): `PBF(domain_configuration, configuration, mode, stream)`,
 the `allocate_*` family, `forward_step`, `jvp_step`, `vjp_step`, `copy_state`,
-`copy_state_adjoint`, `accumulate_state_adjoint`.  Device memory comes from torch
+`copy_state_tangent`, `copy_state_adjoint`, `accumulate_state_adjoint`.  Device memory comes from torch
 (tensors are the `VectorField` x/y/z buffers); every call goes to the CUDA library
 libphysica_pbf.so.  There is no CPU fallback: importing works without a GPU, but
 creating a solver without the built library or a CUDA device raises.
@@ -177,6 +177,7 @@ def library() -> ctypes.CDLL:
                                      P(StateAdjointC), P(ControlC), P(ParametersC), P(StateAdjointC)]
         lib.pbf_copy_state.argtypes = [vp, P(ParticleStateC), P(ParticleStateC)]
         lib.pbf_copy_state_adjoint.argtypes = [vp, P(StateAdjointC), P(StateAdjointC)]
+        lib.pbf_copy_state_tangent.argtypes = [vp, P(StateAdjointC), P(StateAdjointC)]   # same six-pointer layout
         lib.pbf_accumulate_state_adjoint.argtypes = [vp, P(StateAdjointC), P(StateAdjointC)]
         lib.pbf_forward_step_host.argtypes = [vp, P(HostStateC), P(ControlC), P(ParametersC), P(HostStateC), vp]
         lib.pbf_step_cache_read.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_size_t]
@@ -541,6 +542,10 @@ class PBF:
         dc = destination.c()
         check(library().pbf_copy_state(self.handle, ctypes.byref(source.c()), ctypes.byref(dc)))
         destination.step_index = source.step_index
+
+    def copy_state_tangent(self, source: StateTangent, destination: StateTangent):
+        """PBF::copy_state_tangent (pbf/pbf.cpp:163)."""
+        check(library().pbf_copy_state_tangent(self.handle, ctypes.byref(source.c()), ctypes.byref(destination.c())))
 
     def copy_state_adjoint(self, source: StateAdjoint, destination: StateAdjoint):
         check(library().pbf_copy_state_adjoint(self.handle, ctypes.byref(source.c()), ctypes.byref(destination.c())))

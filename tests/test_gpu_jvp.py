@@ -161,3 +161,16 @@ def test_jvp_needs_a_differentiable_solver():
     with pytest.raises(pbf.PBFError):
         solver.jvp_step(state, control, params, nxt, cache, st, solver.allocate_control(),
                         solver.allocate_parameter_tangent(), solver.allocate_state_tangent())
+
+
+def test_copy_state_tangent_copies_all_six_fields():
+    """PBF::copy_state_tangent (pbf/pbf.cpp:163): positions and velocities, bit for bit."""
+    sc = _scene((5, 5, 5), 45)
+    solver, _, _, _ = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable)
+    src, dst = solver.allocate_state_tangent(), solver.allocate_state_tangent()
+    g = torch.Generator(device="cuda").manual_seed(7)
+    src.positions.copy_(torch.randn(src.positions.shape, generator=g, device="cuda"))
+    src.velocities.copy_(torch.randn(src.velocities.shape, generator=g, device="cuda"))
+    solver.copy_state_tangent(src, dst)
+    torch.cuda.synchronize()
+    assert torch.equal(dst.positions, src.positions) and torch.equal(dst.velocities, src.velocities)
