@@ -187,6 +187,24 @@ inline pbf_vector_adjoint_field view(const VectorAdjointField& f) {
 }
 inline VectorField vector_field(const std::size_t n, cudaStream_t s) { return {{n, s}, {n, s}, {n, s}}; }
 inline VectorAdjointField vector_adjoint_field(const std::size_t n, cudaStream_t s) { return {{n, s}, {n, s}, {n, s}}; }
+// The C description of a domain; `storage` holds the boundary particles it points to.
+inline pbf_domain_configuration domain_view(const DomainConfiguration& d, std::vector<pbf_boundary_particle>& storage) {
+    storage.clear();
+    storage.reserve(d.boundary_particles.size());
+    for (const BoundaryParticle& b : d.boundary_particles)
+        storage.push_back({{b.position.x, b.position.y, b.position.z}, {b.velocity.x, b.velocity.y, b.velocity.z}, b.volume});
+    return {d.particle_count,
+            d.time_step,
+            d.support_radius,
+            d.particle_radius,
+            {d.gravity.x, d.gravity.y, d.gravity.z},
+            {{d.boundary.minimum.x, d.boundary.minimum.y, d.boundary.minimum.z},
+             {d.boundary.maximum.x, d.boundary.maximum.y, d.boundary.maximum.z},
+             {d.boundary.velocity.x, d.boundary.velocity.y, d.boundary.velocity.z},
+             d.boundary.no_slip ? 1u : 0u},
+            storage.empty() ? nullptr : storage.data(),
+            static_cast<std::uint32_t>(storage.size())};
+}
 }  // namespace detail
 
 // ---------------------------------------------------------------- pbf/pbf.ixx:14-141
@@ -261,21 +279,7 @@ struct PBF final {
     PBF(DomainConfiguration domain_configuration, Configuration configuration, ExecutionMode mode, cudaStream_t stream)
         : configuration_(configuration), count_(domain_configuration.particle_count), stream_(stream) {
         std::vector<pbf_boundary_particle> boundary;
-        boundary.reserve(domain_configuration.boundary_particles.size());
-        for (const BoundaryParticle& b : domain_configuration.boundary_particles)
-            boundary.push_back({{b.position.x, b.position.y, b.position.z}, {b.velocity.x, b.velocity.y, b.velocity.z}, b.volume});
-        const DomainConfiguration& d = domain_configuration;
-        const pbf_domain_configuration dc{d.particle_count,
-                                          d.time_step,
-                                          d.support_radius,
-                                          d.particle_radius,
-                                          {d.gravity.x, d.gravity.y, d.gravity.z},
-                                          {{d.boundary.minimum.x, d.boundary.minimum.y, d.boundary.minimum.z},
-                                           {d.boundary.maximum.x, d.boundary.maximum.y, d.boundary.maximum.z},
-                                           {d.boundary.velocity.x, d.boundary.velocity.y, d.boundary.velocity.z},
-                                           d.boundary.no_slip ? 1u : 0u},
-                                          boundary.empty() ? nullptr : boundary.data(),
-                                          static_cast<std::uint32_t>(boundary.size())};
+        const pbf_domain_configuration dc = detail::domain_view(domain_configuration, boundary);
         const pbf_configuration cc{configuration.pressure_iterations, configuration.checkpoint_interval};
         detail::check(pbf_create(&dc, &cc,
                                  mode == ExecutionMode::differentiable ? PBF_EXECUTION_DIFFERENTIABLE : PBF_EXECUTION_FORWARD,
