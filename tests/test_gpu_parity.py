@@ -317,3 +317,35 @@ def test_vjp_requires_differentiable_mode():
                         solver.allocate_state_adjoint(), solver.allocate_control_adjoint(),
                         solver.allocate_parameter_adjoint())
     assert e.value.status == 4
+
+
+def test_benchmark_workload_matches_reference_bit_for_bit():
+    """The 1,048,576-particle benchmark dam break (8 iterations, 4,096,000 cells): five substeps
+    through the graph-replayed, autotuned solver equal the reference kernels' bit for bit."""
+    reference = reference_or_skip()
+    sc = scenes.plain_large()
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    solver.autotune(state, control, params, repeats=1)
+    solver.set_graph_mode(True)
+    errs = _trajectory_with(solver, state, control, params, cache, sc, 5, reference)
+    assert errs[5][2] == 0, errs
+
+
+def _trajectory_with(solver, state, control, params, cache, sc, steps, reference):
+    ref = reference.ReferencePBF(sc)
+    cur, nxt = pbf.State(state.positions.clone(), state.velocities.clone(), state.step_index), solver.allocate_state()
+    xr, vr = state.positions.clone(), state.velocities.clone()
+    xr2, vr2 = torch.zeros_like(xr), torch.zeros_like(vr)
+    errs = {}
+    for k in range(steps):
+        solver.forward_step(cur, control, params, nxt, cache)
+        torch.cuda.synchronize()
+        ref.forward_step(xr, vr, xr2, vr2, k)
+        cur, nxt = nxt, cur
+        xr, xr2, vr, vr2 = xr2, xr, vr2, vr
+        torch.cuda.synchronize()
+        errs[k + 1] = (float((cur.positions - xr).abs().max()), float((cur.velocities - vr).abs().max()),
+                       bits_equal(cur.positions, xr) + bits_equal(cur.velocities, vr))
+    ref.close()
+    return errs

@@ -203,3 +203,33 @@ def test_empty_scene_steps():
         solver.forward_step(state, solver.allocate_control(), solver.allocate_parameters(), nxt, solver.allocate_step_cache())
         solver.synchronize()
         assert nxt.step_index == 1
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_benchmark_workload_matches_reference_bit_for_bit(method):
+    """The 1,048,576-particle SPH benchmark dam break with the reference's default iteration counts:
+    two substeps equal the reference kernels' bit for bit."""
+    reference = reference_or_skip()
+    sc = scenes.sph_large(method=method)
+    solver, state, control, params = sph.solver_for_scene(sc, sph.Method[method])
+    cache = solver.allocate_step_cache()
+    ref = reference.ReferenceSPH(sc, int(sph.Method[method]))
+    n = sc.count
+    cur, nxt = state, solver.allocate_state()
+    xr, vr = state.positions.clone(), state.velocities.clone()
+    xr2, vr2 = torch.zeros_like(xr), torch.zeros_like(vr)
+    dfsph = method == "dfsph"
+    wr = (torch.zeros(n, device="cuda"), torch.zeros(n, device="cuda")) if dfsph else None
+    wr2 = (torch.zeros(n, device="cuda"), torch.zeros(n, device="cuda")) if dfsph else None
+    for k in range(2):
+        solver.forward_step(cur, control, params, nxt, cache)
+        ref.forward_step(xr, vr, xr2, vr2, k, warm=wr, warm_out=wr2)
+        torch.cuda.synchronize()
+        cur, nxt = nxt, cur
+        xr, xr2, vr, vr2 = xr2, xr, vr2, vr
+        if dfsph:
+            wr, wr2 = wr2, wr
+        assert bits(cur.positions, xr) == 0 and bits(cur.velocities, vr) == 0, (method, k)
+        if dfsph:
+            assert bits(cur.warm_density_pressure, wr[1]) == 0, (method, k)
+    ref.close()
