@@ -197,3 +197,57 @@ def test_rollout_reuse_and_graph_mode_give_identical_gradients():
         assert np.array_equal(other[1], results[0][1])
         assert np.array_equal(other[2], results[0][2])
         assert other[3] == results[0][3]
+
+
+def test_benchmark_rollout_gradient_matches_reference_rollout():
+    """The 65,536-particle gradient benchmark (20 steps, 4 iterations, trajectory checkpoints every
+    10): the checkpointed rollout gradient equals the one chained through the reference's own
+    forward_step / vjp_step to FP64 rounding."""
+    from oracle import reference
+    if not reference.available():
+        pytest.skip("reference kernels (oracle/_ref) not built")
+    sc = scenes.differentiable()
+    steps, every = 20, 10
+    n = sc.count
+    targets = torch.from_numpy(sc.targets).cuda()
+    solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
+    mine = trajectory.loss_and_gradients(solver, state, control, params, targets, steps, every)
+    torch.cuda.synchronize()
+
+    refs = [reference.ReferencePBF(sc, checkpoint_interval=2, differentiable=True) for _ in range(every)]
+    x = torch.from_numpy(sc.positions).cuda().contiguous()
+    v = torch.from_numpy(sc.velocities).cuda().contiguous()
+    checkpoints = []
+    for k in range(steps):
+        if k % every == 0:
+            checkpoints.append((x.clone(), v.clone()))
+        xo, vo = torch.empty_like(x), torch.empty_like(v)
+        refs[k % every].forward_step(x, v, xo, vo, k)
+        x, v = xo, vo
+    diff = x.double() - targets.double()
+    assert abs(float((diff * diff).sum() / n) - mine.loss) <= 1e-12 * abs(mine.loss)   # bit-identical trajectory
+    adj = {"positions": diff * (2.0 / n), "velocities": torch.zeros((3, n), dtype=torch.float64, device="cuda")}
+    pa = {k: torch.zeros(n, dtype=torch.float64, device="cuda") for k in NAMES}
+    ctrl = torch.zeros((3, n), dtype=torch.float64, device="cuda")
+    for seg in reversed(range(len(checkpoints))):
+        xs, vs = [checkpoints[seg][0]], [checkpoints[seg][1]]
+        begin = seg * every
+        for k in range(begin, min(begin + every, steps)):
+            xo, vo = torch.empty_like(xs[-1]), torch.empty_like(vs[-1])
+            refs[k - begin].forward_step(xs[-1], vs[-1], xo, vo, k)
+            xs.append(xo)
+            vs.append(vo)
+        for k in reversed(range(begin, min(begin + every, steps))):
+            j = k - begin
+            prev = {"positions": torch.zeros((3, n), dtype=torch.float64, device="cuda"),
+                    "velocities": torch.zeros((3, n), dtype=torch.float64, device="cuda")}
+            refs[j].vjp_step(xs[j], vs[j], adj, prev, ctrl, pa)
+            adj = prev
+    torch.cuda.synchronize()
+    assert rel(mine.initial_positions.cpu().numpy(), adj["positions"].cpu().numpy()) < 1e-7
+    assert rel(mine.initial_velocities.cpu().numpy(), adj["velocities"].cpu().numpy()) < 1e-7
+    assert rel(mine.controls.cpu().numpy(), ctrl.cpu().numpy()) < 1e-7
+    for k in ("masses", "rest_densities", "relaxation", "xsph_viscosity", "vorticity_confinement"):
+        assert rel(mine.parameters.tensors[k].cpu().numpy(), pa[k].cpu().numpy()) < 1e-7, k
+    for r in refs:
+        r.close()
