@@ -103,3 +103,28 @@ def test_batched_rollout_gradients_equal_per_scene_rollouts():
         assert g.loss[s] == gs.loss
         assert torch.equal(g.initial_velocities[:, sl], gs.initial_velocities), s
         assert g.scalar["xsph_viscosity"][s] == gs.scalar["xsph_viscosity"], s
+
+
+def test_benchmark_batch_equals_per_scene_solvers():
+    """The 256-scene batched benchmark (2,048-65,536 particles per scene, 4 iterations), autotuned
+    and graph-replayed as bench.py runs it: three substeps equal each scene's own solver bit for bit."""
+    scs = scenes.batched_forward()
+    batch, state, control, params = pbf.batch_for_scenes(scs)
+    batch.autotune(state, control, params, repeats=1)
+    batch.set_graph_mode(True)
+    cur, nxt = pbf.State(state.positions.clone(), state.velocities.clone(), 0), batch.allocate_state()
+    for _ in range(3):
+        batch.forward_step(cur, control, params, nxt)
+        cur, nxt = nxt, cur
+    torch.cuda.synchronize()
+    for s, sc in enumerate(scs):
+        solver, st, ctl, prm = pbf.solver_for_scene(sc)
+        cache = solver.allocate_step_cache()
+        a, b = st, solver.allocate_state()
+        for _ in range(3):
+            solver.forward_step(a, ctl, prm, b, cache)
+            a, b = b, a
+        sl = batch.particle_range(s)
+        assert torch.equal(cur.positions[:, sl], a.positions), s
+        assert torch.equal(cur.velocities[:, sl], a.velocities), s
+        del solver, cache
