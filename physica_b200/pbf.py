@@ -65,8 +65,14 @@ class ControlC(ctypes.Structure):
     _fields_ = [("external_accelerations", VectorFieldC)]
 
 
-class StateAdjointC(ctypes.Structure):
+class StateFieldsC(ctypes.Structure):
+    """pbf_particle_state_tangent and pbf_particle_state_adjoint: positions and velocities as three
+    device pointers each (float arrays for a tangent, double arrays for an adjoint)."""
     _fields_ = [("positions", VectorFieldC), ("velocities", VectorFieldC)]
+
+
+StateTangentC = StateFieldsC
+StateAdjointC = StateFieldsC
 
 
 PARAMETER_NAMES = ("masses", "rest_densities", "viscosities", "surface_tensions", "relaxation",
@@ -174,10 +180,10 @@ def library() -> ctypes.CDLL:
         lib.pbf_vjp_step.argtypes = [vp, P(ParticleStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
                                      P(StateAdjointC), P(StateAdjointC), P(ControlC), P(ParametersC)]
         lib.pbf_jvp_step.argtypes = [vp, P(ParticleStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
-                                     P(StateAdjointC), P(ControlC), P(ParametersC), P(StateAdjointC)]
+                                     P(StateTangentC), P(ControlC), P(ParametersC), P(StateTangentC)]
         lib.pbf_copy_state.argtypes = [vp, P(ParticleStateC), P(ParticleStateC)]
         lib.pbf_copy_state_adjoint.argtypes = [vp, P(StateAdjointC), P(StateAdjointC)]
-        lib.pbf_copy_state_tangent.argtypes = [vp, P(StateAdjointC), P(StateAdjointC)]   # same six-pointer layout
+        lib.pbf_copy_state_tangent.argtypes = [vp, P(StateTangentC), P(StateTangentC)]
         lib.pbf_accumulate_state_adjoint.argtypes = [vp, P(StateAdjointC), P(StateAdjointC)]
         lib.pbf_forward_step_host.argtypes = [vp, P(HostStateC), P(ControlC), P(ParametersC), P(HostStateC), vp]
         lib.pbf_step_cache_read.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_size_t]
@@ -196,7 +202,7 @@ def library() -> ctypes.CDLL:
                                            ctypes.c_uint32, P(StateAdjointC), P(StateAdjointC), P(ControlC),
                                            P(ParametersC)]
         lib.pbf_batch_jvp_step.argtypes = [vp, P(ParticleStateC), P(ControlC), P(ParametersC), P(ParticleStateC),
-                                           ctypes.c_uint32, P(StateAdjointC), P(ControlC), P(ParametersC), P(StateAdjointC)]
+                                           ctypes.c_uint32, P(StateTangentC), P(ControlC), P(ParametersC), P(StateTangentC)]
         lib.pbf_batch_reserve_caches.argtypes = [vp, ctypes.c_uint32]
         lib.pbf_set_launch_shape.argtypes = [vp, P(LaunchShapeC)]
         lib.pbf_get_launch_shape.argtypes = [vp, P(LaunchShapeC)]
@@ -336,8 +342,8 @@ class StateTangent:
     positions: torch.Tensor
     velocities: torch.Tensor
 
-    def c(self) -> StateAdjointC:
-        return StateAdjointC(_vf(self.positions), _vf(self.velocities))
+    def c(self) -> StateTangentC:
+        return StateTangentC(_vf(self.positions), _vf(self.velocities))
 
 
 class Parameters:

@@ -59,6 +59,8 @@ class ParametersC(ctypes.Structure):
 
 
 class MethodStateC(ctypes.Structure):
+    """sph_method_state and sph_method_state_adjoint: DFSPH's two warm-start pressure arrays as device
+    pointers (float for a state or tangent, double for an adjoint)."""
     _fields_ = [("warm_divergence_pressure", ctypes.c_void_p), ("warm_density_pressure", ctypes.c_void_p)]
 
 
@@ -84,13 +86,13 @@ def library() -> ctypes.CDLL:
                                          P(ParticleStateC), P(MethodStateC), vp]
         lib.sph_read_cache.argtypes = [vp, vp, ctypes.c_int, vp, vp, vp]
         lib.sph_jvp_step.argtypes = [vp, P(ParticleStateC), P(MethodStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
-                                     P(pbf.StateAdjointC), P(MethodStateC), P(ControlC), P(ParametersC), P(pbf.StateAdjointC),
+                                     P(pbf.StateTangentC), P(MethodStateC), P(ControlC), P(ParametersC), P(pbf.StateTangentC),
                                      P(MethodStateC)]
         lib.sph_vjp_step.argtypes = [vp, P(ParticleStateC), P(MethodStateC), P(ControlC), P(ParametersC), P(ParticleStateC), vp,
                                      P(pbf.StateAdjointC), P(MethodStateC), P(pbf.StateAdjointC), P(MethodStateC), P(ControlC),
                                      P(ParameterAdjointC)]
         lib.sph_copy_state.argtypes = [vp, P(ParticleStateC), P(MethodStateC), P(ParticleStateC), P(MethodStateC)]
-        lib.sph_copy_state_tangent.argtypes = [vp, P(pbf.StateAdjointC), P(MethodStateC), P(pbf.StateAdjointC), P(MethodStateC)]
+        lib.sph_copy_state_tangent.argtypes = [vp, P(pbf.StateTangentC), P(MethodStateC), P(pbf.StateTangentC), P(MethodStateC)]
         lib.sph_copy_state_adjoint.argtypes = [vp, P(pbf.StateAdjointC), P(MethodStateC), P(pbf.StateAdjointC), P(MethodStateC)]
         lib.sph_accumulate_state_adjoint.argtypes = [vp, P(pbf.StateAdjointC), P(MethodStateC), P(pbf.StateAdjointC),
                                                      P(MethodStateC)]
@@ -146,8 +148,8 @@ class StateTangent:
     warm_divergence_pressure: torch.Tensor | None = None
     warm_density_pressure: torch.Tensor | None = None
 
-    def c(self) -> pbf.StateAdjointC:
-        return pbf.StateAdjointC(_vf(self.positions), _vf(self.velocities))
+    def c(self) -> pbf.StateTangentC:
+        return pbf.StateTangentC(_vf(self.positions), _vf(self.velocities))
 
     def method_c(self) -> MethodStateC:
         a, b = self.warm_divergence_pressure, self.warm_density_pressure
