@@ -292,7 +292,6 @@ __global__ void __launch_bounds__(kBlock) list_scan_kernel(const ListScanArgs a)
     const bool active = s < a.g.count;
     const int4 c = active ? a.g.cell[s] : make_int4(0, 0, 0, 0);
     const float threshold = active ? a.g.constants[a.g.scenes[c.w].constants].list_threshold : 0.0F;
-    const uint32_t warp_first = s - lane;
     const int nact = __popc(__ballot_sync(kFull, active));
     home_s[w][lane] = active ? a.pos[s] : make_float4(0.0F, 0.0F, 0.0F, 0.0F);
     const int px = __shfl_up_sync(kFull, c.x, 1), py = __shfl_up_sync(kFull, c.y, 1);
