@@ -45,7 +45,8 @@ typedef enum {
     PBF_ERROR_CUDA = 3,
     PBF_ERROR_NOT_DIFFERENTIABLE = 4,   /* adjoint/tangent call on a forward-mode solver */
     PBF_ERROR_UNSUPPORTED = 5,
-    PBF_ERROR_DEVICE_TIMEOUT = 6,       /* a bounded device-side wait gave up */
+    PBF_ERROR_DEVICE_TIMEOUT = 6,       /* reserved for a bounded device-side wait that gives up; no kernel
+                                           of this library waits on another today */
     PBF_ERROR_CAPACITY = 7              /* a size exceeds a documented maximum */
 } pbf_status;
 
