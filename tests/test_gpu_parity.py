@@ -320,16 +320,17 @@ def test_vjp_requires_differentiable_mode():
 
 
 def test_benchmark_workload_matches_reference_bit_for_bit():
-    """The 1,048,576-particle benchmark dam break (8 iterations, 4,096,000 cells): five substeps
-    through the graph-replayed, autotuned solver equal the reference kernels' bit for bit."""
+    """The 1,048,576-particle benchmark dam break (8 iterations, 4,096,000 cells): thirty substeps
+    through the graph-replayed, autotuned solver equal the reference kernels' bit for bit, past
+    substep 27, from where single particles jump by up to 220 h in one iteration."""
     reference = reference_or_skip()
     sc = scenes.plain_large()
     solver, state, control, params = pbf.solver_for_scene(sc)
     cache = solver.allocate_step_cache()
     solver.autotune(state, control, params, repeats=1)
     solver.set_graph_mode(True)
-    errs = _trajectory_with(solver, state, control, params, cache, sc, 5, reference)
-    assert errs[5][2] == 0, errs
+    errs = _trajectory_with(solver, state, control, params, cache, sc, 30, reference)
+    assert all(e[2] == 0 for e in errs.values()), {k: e for k, e in errs.items() if e[2]}
 
 
 def _trajectory_with(solver, state, control, params, cache, sc, steps, reference):
