@@ -295,9 +295,8 @@ int pbf_batch_set_graph_mode(pbf_batch* batch, int enable);
 /* ---- forward substep without any device allocation.  No counterpart in the reference.
  *
  *  For callers that cannot call cudaMalloc where they advance the fluid: hosts with a fixed
- *  device-memory budget that hand out no memory after start-up, plugins running while their host
- *  captures a CUDA graph (an allocation inside a global-mode capture is an error), code whose
- *  device memory belongs to another allocator.  The caller passes the scene, its inputs and its
+ *  device-memory budget that hand out no memory after start-up, and code whose device memory
+ *  belongs to another allocator that must not be fragmented.  The caller passes the scene, its inputs and its
  *  outputs (device pointers, as for pbf_forward_step); every intermediate buffer lives in one
  *  library-owned device array of at most PBF_PREALLOCATED_SCRATCH_BYTES that every GPU loading
  *  this library holds until the process exits.  Scenes above PBF_PREALLOCATED_MAX_PARTICLES

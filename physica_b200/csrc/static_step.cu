@@ -2,9 +2,8 @@
 //
 // Some callers cannot call cudaMalloc on the path where they advance the fluid: a host that
 // enforces a fixed device-memory budget and hands out no memory after start-up (game and
-// visual-effects engines, embedded simulators), a plugin that runs while the host application is
-// capturing its own CUDA graph (an allocation during a global-mode capture is an error), or code
-// whose device memory belongs to another allocator that must not be fragmented.  For them this
+// visual-effects engines, embedded simulators), or code whose device memory belongs to another
+// allocator that must not be fragmented.  For them this
 // entry point takes the caller's inputs and outputs only and keeps every intermediate buffer of
 // the substep (scene table, kernel constants, cell-sorted copies, cell offsets, iterates, neighbour
 // lists) in one file-scope device array, `g_scratch`, of kScratchBytes, sized for scenes of at most
