@@ -219,8 +219,7 @@ def bench_b200(args, world, rank):
         holder["cur"], holder["nxt"] = holder["nxt"], holder["cur"]
 
     if args.launch_shape:   # a fixed shape (e.g. to profile one kernel variant); else the autotuner picks it
-        v, b = args.launch_shape.split(":")
-        shape, tuned_ms = pbf.LaunchShape(["per_lane", "cooperative", "staged"].index(v), int(b), 128), float("nan")
+        shape, tuned_ms = fixed_shape(args.launch_shape), float("nan")
         solver.launch_shape = shape
     else:
         shape, tuned_ms = solver.autotune(state, control, params, repeats=2)   # outside the timing
@@ -384,13 +383,27 @@ def issue_roofline(kernel: str, launch_ms: float):
             "frac": round(achieved / peak, 4), "warp_instructions": instructions}
 
 
+def fixed_shape(text: str):
+    """A launch shape from "variant:scan_block[:gather_block]", e.g. per_lane:128 or per_lane:128:32
+    (the gather block defaults to 128): under a profiler the autotuner's timings mean nothing, so a
+    profiled run fixes the shape that the plain run chose."""
+    from physica_b200 import pbf
+    parts = text.split(":")
+    return pbf.LaunchShape(["per_lane", "cooperative", "staged"].index(parts[0]), int(parts[1]),
+                           int(parts[2]) if len(parts) > 2 else 128)
+
+
 def bench_grad(args, world, rank):
     from physica_b200 import pbf, scenes, trajectory
     sc = scenes.differentiable(seed=3 + rank)
     solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
     targets = torch.from_numpy(sc.targets).cuda()
     steps = 20
-    shape, _ = solver.autotune(state, control, params, repeats=2)
+    if args.launch_shape:
+        shape = fixed_shape(args.launch_shape)
+        solver.launch_shape = shape
+    else:
+        shape, _ = solver.autotune(state, control, params, repeats=2)
     solver.set_graph_mode(True)
     rollout = trajectory.Rollout(solver, control, params, steps, 10)   # buffers allocated once, outside the timing
     trajectory.loss_and_gradients(solver, state, control, params, targets, steps, rollout=rollout)   # warm-up
@@ -918,8 +931,11 @@ def main():
     ap.add_argument("--no-sph", action="store_true", help="skip the SPH family's substeps")
     ap.add_argument("--sph-only", default="", help="time only these SPH methods (comma list, e.g. pcisph) and print "
                                                    "their line (profiling)")
-    ap.add_argument("--launch-shape", default="", help="fixed list-scan variant and its block size, e.g. "
-                                                        "per_lane:128, gather passes at 128 (default: autotuned)")
+    ap.add_argument("--grad-only", action="store_true", help="time only the 64k differentiable rollout and print its "
+                                                             "line (profiling)")
+    ap.add_argument("--launch-shape", default="", help="fixed list-scan variant, its block size and optionally the "
+                                                        "gather passes' block size, e.g. per_lane:128 or per_lane:128:32 "
+                                                        "(gather passes at 128 unless given; default: autotuned)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -928,6 +944,9 @@ def main():
         methods = tuple(m for m in args.sph_only.split(",") if m)
         run = bench_reference_sph if args.impl == "reference" else bench_sph
         out = {"impl": args.impl, "sph_family": run(args, world, rank, methods)}
+    elif args.grad_only:
+        out = {"impl": args.impl,
+               "grad_steps_per_s": bench_reference_grad(world, rank) if args.impl == "reference" else bench_grad(args, world, rank)}
     elif args.impl == "reference":
         out = bench_reference(args, world, rank)
     else:
