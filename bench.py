@@ -324,7 +324,7 @@ def bench_b200(args, world, rank):
                                "box [0,4]^3, 8 Jacobi iterations, dt=1/120, XSPH c=0.01, vorticity eps=1e-4",
                    "particles_per_gpu": n, "pressure_iterations": K, "cells": cells, "replicas": world,
                    "l2": "flushed between timed steps (256 MiB write)", "wall_s": round(wall, 3), "graphs": True,
-                   "launch_shape": {"list_scan": ["per_lane", "cooperative", "staged"][shape.list_scan],
+                   "launch_shape": {"list_scan": SCAN_VARIANTS[shape.list_scan],
                                     "scan_block": shape.scan_block_size, "block": shape.block_size,
                                     "autotune_ms_per_step": None if math.isnan(tuned_ms) else round(tuned_ms, 4)}},
         "roofline": roofline, "step_roofline": step_roofline, "per_pass": per_pass,
@@ -383,13 +383,16 @@ def issue_roofline(kernel: str, launch_ms: float):
             "frac": round(achieved / peak, 4), "warp_instructions": instructions}
 
 
+SCAN_VARIANTS = ["per_lane", "cooperative", "staged", "split"]   # pbf_launch_shape.list_scan 0..3
+
+
 def fixed_shape(text: str):
     """A launch shape from "variant:scan_block[:gather_block]", e.g. per_lane:128 or per_lane:128:32
     (the gather block defaults to 128): under a profiler the autotuner's timings mean nothing, so a
     profiled run fixes the shape that the plain run chose."""
     from physica_b200 import pbf
     parts = text.split(":")
-    return pbf.LaunchShape(["per_lane", "cooperative", "staged"].index(parts[0]), int(parts[1]),
+    return pbf.LaunchShape(SCAN_VARIANTS.index(parts[0]), int(parts[1]),
                            int(parts[2]) if len(parts) > 2 else 128)
 
 
@@ -420,7 +423,7 @@ def bench_grad(args, world, rank):
             "config": {"workload": "differentiable_64k: 65,536 particles (32x64x32 lattice), v0 ~ N(0, 0.1), "
                                    "4 iterations, target-cloud loss", "rollout_steps": steps,
                        "trajectory_checkpoint_every": 10, "graphs": True,
-                       "launch_shape": {"list_scan": ["per_lane", "cooperative", "staged"][shape.list_scan],
+                       "launch_shape": {"list_scan": SCAN_VARIANTS[shape.list_scan],
                                         "scan_block": shape.scan_block_size, "block": shape.block_size}},
             "loss": g.loss}
 
@@ -489,7 +492,7 @@ def bench_batch(args, world, rank):
             "batched_ms_per_step": round(ms_b, 4), "per_scene_ms_per_step": round(ms_l, 4),
             "config": {"workload": "batched_forward_256: 256 dam-break scenes, counts log-uniform in [2048, 65536], "
                                    "4 iterations", "particles_per_gpu": total, "scenes_per_gpu": len(scs),
-                       "graphs": True, "launch_shape": {"list_scan": ["per_lane", "cooperative", "staged"][shape.list_scan],
+                       "graphs": True, "launch_shape": {"list_scan": SCAN_VARIANTS[shape.list_scan],
                                                          "scan_block": shape.scan_block_size, "block": shape.block_size}}}
 
 
