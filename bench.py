@@ -383,7 +383,7 @@ def issue_roofline(kernel: str, launch_ms: float):
             "frac": round(achieved / peak, 4), "warp_instructions": instructions}
 
 
-SCAN_VARIANTS = ["per_lane", "cooperative", "staged", "split"]   # pbf_launch_shape.list_scan 0..3
+SCAN_VARIANTS = ["per_lane", "cooperative", "staged"]   # pbf_launch_shape.list_scan 0..2
 
 
 def fixed_shape(text: str):
