@@ -222,7 +222,7 @@ def bench_b200(args, world, rank):
         shape, tuned_ms = fixed_shape(args.launch_shape), float("nan")
         solver.launch_shape = shape
     else:
-        shape, tuned_ms = solver.autotune(state, control, params, repeats=2)   # outside the timing
+        shape, tuned_ms = solver.autotune(state, control, params, repeats=4)   # outside the timing; 4 steps per shape steady the choice
     solver.set_graph_mode(True)   # one CUDA graph launch per substep (captured in the warm-up)
     launches0 = pbf.launch_count()
     clk = Clocks(torch.cuda.current_device())
