@@ -280,6 +280,21 @@ def test_host_buffer_entry_matches_device_entry():
     assert np.array_equal(ov.numpy(), nxt.velocities.cpu().numpy())
 
 
+def test_host_buffer_entry_accepts_pageable_memory():
+    """The host-buffer entry with ordinary (pageable, not pinned) host arrays, as a C caller's
+    malloc'd buffers are: the same substep as the device entry."""
+    sc = scenes.plain_small(lattice=(10, 10, 10))
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    cache = solver.allocate_step_cache()
+    nxt = step(solver, state, control, params, cache)
+    hx, hv = torch.from_numpy(sc.positions.copy()), torch.from_numpy(sc.velocities.copy())
+    assert not hx.is_pinned()
+    ox, ov = torch.empty_like(hx), torch.empty_like(hv)
+    assert solver.forward_step_host(hx, hv, control, params, ox, ov, cache) == 1
+    assert np.array_equal(ox.numpy(), nxt.positions.cpu().numpy())
+    assert np.array_equal(ov.numpy(), nxt.velocities.cpu().numpy())
+
+
 @pytest.mark.parametrize("graphs", [False, True])
 def test_host_buffer_rollout_matches_device_rollout(graphs):
     """Four host-buffer steps, alternating buffers as a rollout does (the positions are read back on
