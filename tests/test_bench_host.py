@@ -46,3 +46,34 @@ def test_issue_roofline_uses_the_recorded_instruction_count():
 def test_profile_figures_name_the_command_that_made_them():
     text = (ROOT / "profiles" / "substep_dam_break_1m.md").read_text()
     assert "ncu --set full --clock-control none" in text and "ncu --metrics gpu__time_duration.sum --clock-control none" in text
+
+
+def _max_rank(rank, world, port, out):
+    import os
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # every rank reports its own time; the job's time is the slowest rank's
+        out[rank] = bench.max_over_ranks(1.5 + rank, world)
+        bench.barrier(world)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_takes_the_slowest_rank():
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_max_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert dict(out) == {0: 2.5, 1: 2.5}
+
