@@ -937,6 +937,8 @@ def main():
                                                    "their line (profiling)")
     ap.add_argument("--grad-only", action="store_true", help="time only the 64k differentiable rollout and print its "
                                                              "line (profiling)")
+    ap.add_argument("--tangent-only", action="store_true", help="time only the 1M differentiable substep + jvp_step "
+                                                                "and print its line (profiling)")
     ap.add_argument("--launch-shape", default="", help="fixed list-scan variant, its block size and optionally the "
                                                         "gather passes' block size, e.g. per_lane:128 or per_lane:128:32 "
                                                         "(gather passes at 128 unless given; default: autotuned)")
@@ -948,6 +950,11 @@ def main():
         methods = tuple(m for m in args.sph_only.split(",") if m)
         run = bench_reference_sph if args.impl == "reference" else bench_sph
         out = {"impl": args.impl, "sph_family": run(args, world, rank, methods)}
+    elif args.tangent_only:
+        from physica_b200 import scenes
+        sc = scenes.plain_large(seed=2 + rank)
+        run = reference_tangent_ms if args.impl == "reference" else tangent_ms
+        out = {"impl": args.impl, "tangent_ms_per_step": run(args, world, sc)}
     elif args.grad_only:
         out = {"impl": args.impl,
                "grad_steps_per_s": bench_reference_grad(world, rank) if args.impl == "reference" else bench_grad(args, world, rank)}
