@@ -257,7 +257,10 @@ struct CorrectionJvpOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-__global__ void __launch_bounds__(kBlock) correction_jvp_kernel(const CorrectionJvpArgs a) {
+// Seven resident blocks per SM (at most 72 registers, a few spilled) against 88 registers and five
+// blocks unbounded: the pass waits on its neighbours' loads, and the extra warps hide more of that
+// (the 1M tangent step fell from 11.54 to 10.64 ms; 80 and 64 registers were slower).
+__global__ void __launch_bounds__(kBlock, 7) correction_jvp_kernel(const CorrectionJvpArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
     CorrectionJvpOp op;
