@@ -115,7 +115,7 @@ struct DensityLambdaJvpOp {
     const float4* __restrict__ params_a_dot;
     f3 x, xd;
     uint32_t self;
-    float rest, rest_dot;
+    float rest, rest_dot, inverse_rest;
     KernelConstants k;
     float density_dot, denominator_dot;
     f3 gsum_dot;
@@ -141,12 +141,22 @@ struct DensityLambdaJvpOp {
         const float mass_dot = in.aux.x;
         if (r2 < k.h2) density_dot += mass_dot * poly6_inside(r2, k) + in.q.w * dot(poly6_gradient(d, k), dd);
         if (t == self) return;
-        const float distance = sqrtf(r2);
-        if (distance == 0.0F || distance >= k.h) return;
-        const f3 gradient = spiky_gradient_at(d, distance, k);
-        const f3 gradient_dot = spiky_gradient_tangent(d, dd, distance, k);
-        const float coefficient = in.q.w / rest;
-        const float coefficient_dot = mass_dot / rest - in.q.w * rest_dot / (rest * rest);
+        // The tangent is compared with the reference to FP32 rounding, not bit for bit, so the spiky
+        // gradient and its derivative share one reciprocal square root, and the divisions by the
+        // particle's rest density become products with its reciprocal (the 1M tangent step: 10.65 ->
+        // 9.65 ms; against the reference 1.6e-7 relative before and after).
+        if (r2 == 0.0F || r2 >= k.spiky_threshold) return;   // sqrtf(r2) == 0 or >= h
+        const float inverse = rsqrtf(r2);
+        const float distance = r2 * inverse;
+        const f3 direction = times(d, inverse);
+        const float difference = k.h - distance;
+        const float radial = dot(direction, dd);
+        const f3 gradient = times(direction, k.spiky_coefficient * difference * difference);
+        const f3 direction_tangent = times(dd + times(direction, -radial), inverse);
+        const f3 gradient_dot = times(times(direction, -2.0F * difference * radial) + times(direction_tangent, difference * difference),
+                                      k.spiky_coefficient);
+        const float coefficient = in.q.w * inverse_rest;
+        const float coefficient_dot = (mass_dot - in.q.w * rest_dot * inverse_rest) * inverse_rest;
         const f3 ng = times(gradient, coefficient);
         const f3 ng_dot = times(gradient, coefficient_dot) + times(gradient_dot, coefficient);
         gsum_dot = gsum_dot + ng_dot;
@@ -171,6 +181,7 @@ __global__ void __launch_bounds__(kBlock) density_lambda_jvp_kernel(const Densit
     const float4 pad = a.params_a_dot[p.s];
     op.rest = pa.x;
     op.rest_dot = pad.y;
+    op.inverse_rest = 1.0F / pa.x;
     op.density_dot = 0.0F;
     op.denominator_dot = pad.z;   // relaxation tangent
     op.gsum_dot = mk(0.0F, 0.0F, 0.0F);
