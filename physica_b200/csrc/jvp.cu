@@ -70,6 +70,23 @@ __device__ __forceinline__ f3 spiky_gradient_tangent(const f3 d, const f3 dd, co
                  k.spiky_coefficient);
 }
 
+// The spiky gradient (pbf.cu:26-32) and its directional derivative (pbf.cu:34-43) of one pair with
+// 0 < r2 < spiky_threshold, sharing one reciprocal square root.  The tangent passes are held to FP32
+// rounding against the reference, not to its bits, so they need not repeat its IEEE square root
+// and divisions pair by pair.
+__device__ __forceinline__ void spiky_pair(const f3 d, const f3 dd, const float r2, const KernelConstants& k, f3& gradient,
+                                           f3& gradient_dot) {
+    const float inverse = rsqrtf(r2);
+    const float distance = r2 * inverse;
+    const f3 direction = times(d, inverse);
+    const float difference = k.h - distance;
+    const float radial = dot(direction, dd);
+    gradient = times(direction, k.spiky_coefficient * difference * difference);
+    const f3 direction_tangent = times(dd + times(direction, -radial), inverse);
+    gradient_dot = times(times(direction, -2.0F * difference * radial) + times(direction_tangent, difference * difference),
+                         k.spiky_coefficient);
+}
+
 // ------------------------------------------------------------------- seed
 __global__ void tangent_seed_kernel(const uint32_t count, const uint32_t* __restrict__ sorted_index, const int4* __restrict__ cell,
                                     const SceneDesc* __restrict__ scenes, const Field3 x_dot, const Field3 v_dot,
@@ -141,20 +158,12 @@ struct DensityLambdaJvpOp {
         const float mass_dot = in.aux.x;
         if (r2 < k.h2) density_dot += mass_dot * poly6_inside(r2, k) + in.q.w * dot(poly6_gradient(d, k), dd);
         if (t == self) return;
-        // The tangent is compared with the reference to FP32 rounding, not bit for bit, so the spiky
-        // gradient and its derivative share one reciprocal square root, and the divisions by the
-        // particle's rest density become products with its reciprocal (the 1M tangent step: 10.65 ->
-        // 9.65 ms; against the reference 1.6e-7 relative before and after).
+        // one reciprocal square root per pair and the reciprocal rest density instead of IEEE
+        // divisions (the 1M tangent step: 10.65 -> 9.65 ms; 1.6e-7 relative to the reference
+        // before and after)
         if (r2 == 0.0F || r2 >= k.spiky_threshold) return;   // sqrtf(r2) == 0 or >= h
-        const float inverse = rsqrtf(r2);
-        const float distance = r2 * inverse;
-        const f3 direction = times(d, inverse);
-        const float difference = k.h - distance;
-        const float radial = dot(direction, dd);
-        const f3 gradient = times(direction, k.spiky_coefficient * difference * difference);
-        const f3 direction_tangent = times(dd + times(direction, -radial), inverse);
-        const f3 gradient_dot = times(times(direction, -2.0F * difference * radial) + times(direction_tangent, difference * difference),
-                                      k.spiky_coefficient);
+        f3 gradient, gradient_dot;
+        spiky_pair(d, dd, r2, k, gradient, gradient_dot);
         const float coefficient = in.q.w * inverse_rest;
         const float coefficient_dot = (mass_dot - in.q.w * rest_dot * inverse_rest) * inverse_rest;
         const f3 ng = times(gradient, coefficient);
@@ -228,7 +237,7 @@ struct CorrectionJvpOp {
     const float4* __restrict__ params_a_dot;
     f3 x, xd;
     uint32_t self;
-    float rest, rest_dot, lambda_i, lambda_dot_i;
+    float rest, rest_dot, inverse_rest, lambda_i, lambda_dot_i;
     float strength, exponent, radius, strength_dot, exponent_dot, radius_dot;
     bool artificial;
     KernelConstants k;
@@ -242,8 +251,9 @@ struct CorrectionJvpOp {
         if (t == self) return;
         const f3 d = x - xyz(in.q);
         const f3 dd = xd - xyz(in.qd);
-        const float distance = sqrtf(squared(d));
-        if (distance == 0.0F || distance >= k.h) return;   // both spiky terms vanish
+        const float r2 = squared(d);
+        if (r2 == 0.0F || r2 >= k.spiky_threshold) return;   // both spiky terms vanish (sqrtf(r2) == 0 or >= h)
+        const float distance = sqrtf(r2);
         float art = 0.0F, art_dot = 0.0F;
         if (artificial) {
             const ArtificialPressure ap = artificial_pressure(d, k, strength, exponent, radius);
@@ -258,12 +268,14 @@ struct CorrectionJvpOp {
                                     in.q.w);
             return;
         }
-        const float coefficient = in.q.w / rest;
-        const float coefficient_dot = in.mass_dot / rest - in.q.w * rest_dot / (rest * rest);
+        f3 gradient, gradient_dot;
+        spiky_pair(d, dd, r2, k, gradient, gradient_dot);
+        const float coefficient = in.q.w * inverse_rest;
+        const float coefficient_dot = (in.mass_dot - in.q.w * rest_dot * inverse_rest) * inverse_rest;
         const float multiplier = lambda_i + in.lambda + art;
         const float multiplier_dot = lambda_dot_i + in.lambda_dot + art_dot;
-        result = result + times(spiky_gradient_at(d, distance, k), coefficient_dot * multiplier + coefficient * multiplier_dot) +
-                 times(spiky_gradient_tangent(d, dd, distance, k), coefficient * multiplier);
+        result = result + times(gradient, coefficient_dot * multiplier + coefficient * multiplier_dot) +
+                 times(gradient_dot, coefficient * multiplier);
     }
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
@@ -288,6 +300,7 @@ __global__ void __launch_bounds__(kBlock, 7) correction_jvp_kernel(const Correct
     const float4 pa = a.g.params_a[p.s], pb = a.g.params_b[p.s];
     const float4 pad = a.params_a_dot[p.s], pbd = a.params_b_dot[p.s];
     op.rest = pa.x;
+    op.inverse_rest = 1.0F / pa.x;
     op.rest_dot = pad.y;
     op.lambda_i = a.lambda[p.s];
     op.lambda_dot_i = a.lambda_dot[p.s];
