@@ -144,12 +144,18 @@ __device__ __forceinline__ d3 ld3(const double4 v) { return {v.x, v.y, v.z}; }
 __device__ __forceinline__ double4 st3(const d3 v) { return make_double4(v.x, v.y, v.z, 0.0); }
 
 // Spiky Hessian applied to a vector, in FP64 (pbf/pbf.cu:45-54 evaluation order).
+// The adjoint is held to FP64 rounding against the reference, so the distance and its reciprocal
+// come from one reciprocal square root rather than a square root and a division; the support test
+// is the exact one on the squared distance.
 __device__ __forceinline__ d3 spiky_hessian_product(const f3 d, const d3 v, const KernelConstants& k) {
-    const double distance = sqrt(static_cast<double>(squared(d)));
-    if (distance == 0.0 || distance >= k.h) return {0.0, 0.0, 0.0};
-    const d3 direction = times(d, 1.0 / distance);
+    const float r2f = squared(d);
+    if (r2f == 0.0F || r2f >= k.hessian_threshold) return {0.0, 0.0, 0.0};   // sqrt((double)r2) == 0 or >= h
+    const double r2 = r2f;
+    const double inverse = rsqrt(r2);
+    const double distance = r2 * inverse;
+    const d3 direction = times(d, inverse);
     const double projection = dot(direction, v);
-    const d3 direction_tangent = times(v - times(direction, projection), 1.0 / distance);
+    const d3 direction_tangent = times(v - times(direction, projection), inverse);
     const double difference = k.h - distance;
     return times(times(direction, -2.0 * difference * projection) + times(direction_tangent, difference * difference),
                  k.spiky_coefficient_d);
@@ -161,13 +167,14 @@ __device__ __forceinline__ d3 spiky_hessian_product(const f3 d, const d3 v, cons
 // H(-d) v equals H(d) v exactly: the reverse term of a pair uses the forward term's setup.
 __device__ __forceinline__ void spiky_hessian_products(const f3 d, const d3 v1, const d3 v2, const KernelConstants& k, d3& out1,
                                                        d3& out2) {
-    const double r2 = static_cast<double>(squared(d));
-    const double distance = sqrt(r2);
-    if (distance == 0.0 || distance >= k.h) {
+    const float r2f = squared(d);
+    if (r2f == 0.0F || r2f >= k.hessian_threshold) {   // sqrt((double)r2) == 0 or >= h
         out1 = out2 = {0.0, 0.0, 0.0};
         return;
     }
-    const double inverse = 1.0 / distance;
+    const double r2 = r2f;
+    const double inverse = rsqrt(r2);
+    const double distance = r2 * inverse;
     const d3 direction = times(d, inverse);
     const double difference = k.h - distance;
     auto product = [&](const d3 v) {
