@@ -371,12 +371,13 @@ struct VorticityJvpOp {
         if (t == self) return;
         const f3 d = x - xyz(in.q);
         const f3 dd = xd - xyz(in.qd);
-        const float distance = sqrtf(squared(d));
-        if (distance == 0.0F || distance >= k.h) return;
+        const float r2 = squared(d);
+        if (r2 == 0.0F || r2 >= k.spiky_threshold) return;   // sqrtf(r2) == 0 or >= h
+        f3 gradient, gradient_dot;
+        spiky_pair(d, dd, r2, k, gradient, gradient_dot);
         const f3 difference = xyz(in.w) - v;
         const f3 difference_dot = xyz(in.wd) - vd;
-        result = result + cross(difference_dot, spiky_gradient_at(d, distance, k)) +
-                 cross(difference, spiky_gradient_tangent(d, dd, distance, k));
+        result = result + cross(difference_dot, gradient) + cross(difference, gradient_dot);
     }
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
@@ -438,10 +439,11 @@ struct NormalJvpOp {
         if (t == self) return;
         const f3 d = x - xyz(in.q);
         const f3 dd = xd - xyz(in.qd);
-        const float distance = sqrtf(squared(d));
-        if (distance == 0.0F || distance >= k.h) return;
-        result = result + times(spiky_gradient_at(d, distance, k), in.md - magnitude_dot) +
-                 times(spiky_gradient_tangent(d, dd, distance, k), in.m - magnitude);
+        const float r2 = squared(d);
+        if (r2 == 0.0F || r2 >= k.spiky_threshold) return;   // sqrtf(r2) == 0 or >= h
+        f3 gradient, gradient_dot;
+        spiky_pair(d, dd, r2, k, gradient, gradient_dot);
+        result = result + times(gradient, in.md - magnitude_dot) + times(gradient_dot, in.m - magnitude);
     }
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
