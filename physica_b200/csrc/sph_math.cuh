@@ -121,25 +121,33 @@ __device__ __forceinline__ float laplacian_value(const f3 d, const SphConstants&
 
 // Directional derivative of the cubic gradient along the displacement tangent t
 // (density/device.cuh:45-57), FP32.
+// The tangents are held to FP32 rounding against the reference, not to its bits, so the distance
+// and its reciprocal come from one reciprocal square root and the divisions by h and r become
+// products with their reciprocals (1/h is loop-invariant in every caller).
 __device__ __forceinline__ f3 cubic_gradient_tangent(const f3 d, const f3 t, const SphConstants& k) {
-    const float r = sqrtf(dot(d, d));
+    const float r2 = dot(d, d);
     const float c = k.cubic_coefficient;
-    if (r == 0.0F) return times(t, -12.0F * c / (k.h * k.h));
+    const float inverse_h = 1.0F / k.h;
+    if (r2 == 0.0F) return times(t, -12.0F * c * inverse_h * inverse_h);
+    const float inverse_r = rsqrtf(r2);
+    const float r = r2 * inverse_r;
     if (r >= k.h) return mk(0.0F, 0.0F, 0.0F);
-    const float q = r / k.h;
+    const float q = r * inverse_h;
     const float first = q <= 0.5F ? 18.0F * q * q - 12.0F * q : -6.0F * (1.0F - q) * (1.0F - q);
     const float second = q <= 0.5F ? 36.0F * q - 12.0F : 12.0F * (1.0F - q);
-    const float radial_tangent = dot(d, t) / r;
-    const float radial = c * first / (k.h * r);
-    const float radial_derivative = c * (second / (k.h * k.h * r) - first / (k.h * r * r));
+    const float radial_tangent = dot(d, t) * inverse_r;
+    const float radial = c * first * inverse_h * inverse_r;
+    const float radial_derivative = c * inverse_h * inverse_r * (second * inverse_h - first * inverse_r);
     return times(t, radial) + times(d, radial_derivative * radial_tangent);
 }
 
 // Directional derivative of the viscosity Laplacian (density/device.cuh:78-82), FP32.
 __device__ __forceinline__ float laplacian_tangent(const f3 d, const f3 t, const SphConstants& k) {
-    const float r = sqrtf(dot(d, d));
-    if (r == 0.0F || r >= k.h) return 0.0F;
-    return -45.0F * dot(d, t) / (k.laplacian_denominator * r);
+    const float r2 = dot(d, d);
+    if (r2 == 0.0F) return 0.0F;
+    const float inverse_r = rsqrtf(r2);
+    if (r2 * inverse_r >= k.h) return 0.0F;
+    return -45.0F * dot(d, t) * inverse_r * (1.0F / k.laplacian_denominator);
 }
 
 // Hessian of the cubic kernel applied to v, in FP64 from the FP32 squared distance
