@@ -504,6 +504,11 @@ __global__ void sph_constants_kernel(const SphSceneInput* __restrict__ inputs, c
     k.support_threshold = __uint_as_float(hi);
     k.laplacian_denominator = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(kPi, h), h), h), h), h), h);
     k.laplacian_denominator_d = static_cast<double>(kPi) * pow(static_cast<double>(h), 6.0);
+    k.support_squared_d = static_cast<double>(h) * static_cast<double>(h);
+    k.inverse_h_d = 1.0 / static_cast<double>(h);
+    k.inverse_hh_d = 1.0 / static_cast<double>(__fmul_rn(h, h));
+    k.cubic_coefficient_d = 8.0 / (static_cast<double>(kPi) * h * h * h);
+    k.laplacian_scale_d = -45.0 / k.laplacian_denominator_d;
     k.epsilon_factor = __fmul_rn(0.01F, h);
     k.diameter = __fmul_rn(2.0F, in.particle_radius);
     // cubic({diameter, 0, 0}): its length is sqrtf(fma(0, 0, fma(d, d, 0 * 0)))

@@ -31,6 +31,11 @@ struct SphConstants {
     uint32_t no_slip;
     float skin_bound;               // the predicted density replays the lists while 2 max|x* - x| <= this
     double laplacian_denominator_d; // pi pow(h, 6) in FP64                  (density/device.cuh:87)
+    double support_squared_d;       // h h in FP64 (exact): sqrt(r2) >= h exactly when r2 >= this
+    double inverse_h_d;             // 1 / h in FP64
+    double inverse_hh_d;            // 1 / (h h), h h rounded to float as in density/device.cuh:59-70
+    double cubic_coefficient_d;     // 8 / (pi h h h) in FP64                (density/device.cuh:59-70)
+    double laplacian_scale_d;       // -45 / (pi pow(h, 6)) in FP64          (density/device.cuh:84-88)
 };
 
 // Sorted per-particle parameters of an SPH step, packed by the grid build:

@@ -150,46 +150,37 @@ __device__ __forceinline__ float laplacian_tangent(const f3 d, const f3 t, const
     return -45.0F * dot(d, t) * inverse_r * (1.0F / k.laplacian_denominator);
 }
 
-// Hessian of the cubic kernel applied to v, in FP64 from the FP32 squared distance
-// (density/device.cuh:59-70; the h h products are float, as there).
-__device__ __forceinline__ d3 cubic_hessian_product(const f3 d, const d3 v, const SphConstants& k) {
-    const float h = k.h;
-    const double r = sqrt(static_cast<double>(sq_xfirst(d)));
-    const double c = 8.0 / (static_cast<double>(kPi) * h * h * h);
-    if (r == 0.0) return times(v, -12.0 * c / (h * h));
-    if (r >= h) return {0.0, 0.0, 0.0};
-    const double q = r / h;
-    const double first = q <= 0.5 ? 18.0 * q * q - 12.0 * q : -6.0 * (1.0 - q) * (1.0 - q);
-    const double second = q <= 0.5 ? 36.0 * q - 12.0 : 12.0 * (1.0 - q);
-    const double radial = c * first / (h * r);
-    const double radial_derivative = c * (second / (h * h * r) - first / (h * r * r));
-    return times(v, radial) + times(d, radial_derivative * dot(v, d) / r);
-}
-
-// The scalar part of cubic_hessian_product for one displacement, shared by every vector the
-// Hessian is applied to: applying it gives the same bits as cubic_hessian_product.
+// Hessian of the cubic kernel, in FP64 from the FP32 squared distance (density/device.cuh:59-70;
+// the h h products are float there, and so in SphConstants::inverse_hh_d).
+// CubicHessian is its scalar part for one displacement, shared by every vector the Hessian is
+// applied to; H(-d) v = H(d) v exactly, because every step is sign-symmetric.
+// The adjoint is held to FP64 rounding against the reference, not to its bits: one double
+// reciprocal square root per pair replaces the square root and the divisions.  The support test
+// stays exact, because for a float r2 and a float h, sqrt(r2) >= h in FP64 exactly when r2 >= h h
+// (h h is exact in FP64, and a float r2 below it keeps sqrt(r2) more than half an FP64 ulp below h).
 struct CubicHessian {
-    double r, radial, radial_derivative, center;
+    double inverse_r, radial, radial_derivative, center;
     int kind;   // 0 outside the support, 1 at zero distance, 2 inside
 };
 
 __device__ __forceinline__ CubicHessian cubic_hessian(const f3 d, const SphConstants& k) {
     CubicHessian H{};
-    const float h = k.h;
-    const double r = sqrt(static_cast<double>(sq_xfirst(d)));
-    const double c = 8.0 / (static_cast<double>(kPi) * h * h * h);
-    H.r = r;
-    if (r == 0.0) {
+    const double r2 = static_cast<double>(sq_xfirst(d));
+    const double c = k.cubic_coefficient_d;
+    if (r2 == 0.0) {
         H.kind = 1;
-        H.center = -12.0 * c / (h * h);
+        H.center = -12.0 * c * k.inverse_hh_d;
         return H;
     }
-    if (r >= h) return H;
-    const double q = r / h;
+    if (r2 >= k.support_squared_d) return H;
+    const double inverse_r = rsqrt(r2);
+    const double q = r2 * inverse_r * k.inverse_h_d;
     const double first = q <= 0.5 ? 18.0 * q * q - 12.0 * q : -6.0 * (1.0 - q) * (1.0 - q);
     const double second = q <= 0.5 ? 36.0 * q - 12.0 : 12.0 * (1.0 - q);
-    H.radial = c * first / (h * r);
-    H.radial_derivative = c * (second / (h * h * r) - first / (h * r * r));
+    const double scale = c * inverse_r;
+    H.inverse_r = inverse_r;
+    H.radial = scale * first * k.inverse_h_d;                                            // c first / (h r)
+    H.radial_derivative = scale * (second * k.inverse_hh_d - first * k.inverse_h_d * inverse_r);  // c (second / (hh r) - first / (h r r))
     H.kind = 2;
     return H;
 }
@@ -197,15 +188,15 @@ __device__ __forceinline__ CubicHessian cubic_hessian(const f3 d, const SphConst
 __device__ __forceinline__ d3 hessian_times(const CubicHessian& H, const f3 d, const d3 v) {
     if (H.kind == 1) return times(v, H.center);
     if (H.kind == 0) return {0.0, 0.0, 0.0};
-    return times(v, H.radial) + times(d, H.radial_derivative * dot(v, d) / H.r);
+    return times(v, H.radial) + times(d, H.radial_derivative * dot(v, d) * H.inverse_r);
 }
 
-// Gradient of the viscosity Laplacian times `scalar`, in FP64 (density/device.cuh:84-88); pi h^6
-// is the per-scene constant SphConstants::laplacian_denominator_d.
+// Gradient of the viscosity Laplacian times `scalar`, in FP64 (density/device.cuh:84-88); -45 / (pi h^6)
+// is the per-scene constant SphConstants::laplacian_scale_d, and the support test is the exact one above.
 __device__ __forceinline__ d3 laplacian_gradient(const f3 d, const SphConstants& k, const double scalar) {
-    const double r = sqrt(static_cast<double>(sq_xfirst(d)));
-    if (r == 0.0 || r >= k.h) return {0.0, 0.0, 0.0};
-    return times(d, -45.0 * scalar / (k.laplacian_denominator_d * r));
+    const double r2 = static_cast<double>(sq_xfirst(d));
+    if (r2 == 0.0 || r2 >= k.support_squared_d) return {0.0, 0.0, 0.0};
+    return times(d, k.laplacian_scale_d * scalar * rsqrt(r2));
 }
 
 // The unclamped prediction's collision mask (sph/pcisph.cu:20-24, 69-71).
