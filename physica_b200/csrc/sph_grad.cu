@@ -666,7 +666,7 @@ struct NonPressureVjpOp {
     }
     __device__ __forceinline__ void apply(const uint32_t t, const NonPressureVjpData& d) {
         const f3 disp = sub(x, xyz(d.q));
-        if (sqrt(static_cast<double>(sq_xfirst(disp))) >= k.h) return;
+        if (static_cast<double>(sq_xfirst(disp)) >= k.support_squared_d) return;   // sqrt(r2) >= h, exactly
         const f3 difference = sub(xyz(d.v), v);
         const float laplacian = laplacian_value(disp, k);
         if (t & kBoundaryBit) {   // sph/common.cu:145-155
