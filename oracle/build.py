@@ -9,7 +9,8 @@
   over the reference's own launch_* functions.  The
   reference's C++23 module host layer (import std) cannot be compiled by this
   toolchain, so the harness stands in for it.  Built only where the reference
-  tree exists; the .so then travels with the repository copy.
+  tree exists ($PHYSICA_REFERENCE, or a checkout named `reference` beside this repository's
+  directory); the .so then travels with the repository copy.
 """
 from __future__ import annotations
 
@@ -20,8 +21,18 @@ import subprocess
 import sys
 
 HERE = pathlib.Path(__file__).resolve().parent
-REFERENCE = pathlib.Path(os.environ.get("PHYSICA_REFERENCE", "/root/reference"))
-PARTICLE = REFERENCE / "fluids" / "liquid" / "particle"
+
+
+def reference_root() -> pathlib.Path:
+    """The reference checkout: $PHYSICA_REFERENCE, else a checkout named `reference` beside this
+    repository's directory."""
+    env = os.environ.get("PHYSICA_REFERENCE")
+    return pathlib.Path(env) if env else HERE.parent.parent / "reference"
+
+
+def particle_root() -> pathlib.Path:
+    return reference_root() / "fluids" / "liquid" / "particle"
+
 REF_SOURCES = ["pbf/pbf.cu", "density/density.cu", "neighborhood/neighborhood.cu", "domain/domain.cu",
                "sph/common.cu", "sph/wcsph.cu", "sph/pcisph.cu", "sph/iisph.cu", "sph/dfsph.cu"]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
@@ -57,7 +68,8 @@ def build_oracle(force: bool = False) -> pathlib.Path:
 
 
 def reference_available() -> bool:
-    return all((PARTICLE / s).exists() for s in REF_SOURCES) and _cccl_root() is not None
+    particle = particle_root()
+    return all((particle / s).exists() for s in REF_SOURCES) and _cccl_root() is not None
 
 
 def build_reference(force: bool = False) -> pathlib.Path | None:
@@ -68,6 +80,7 @@ def build_reference(force: bool = False) -> pathlib.Path | None:
         return out if out.exists() else None
     if not force and out.exists() and out.stat().st_mtime >= harness.stat().st_mtime:
         return out
+    particle = particle_root()
     cccl = _cccl_root()
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     objdir = HERE / "_ref" / "obj"
@@ -79,10 +92,10 @@ def build_reference(force: bool = False) -> pathlib.Path | None:
     procs = []
     for rel in REF_SOURCES:
         obj = objdir / (rel.replace("/", "_") + ".o")
-        procs.append(subprocess.Popen([*common, "-c", str(PARTICLE / rel), "-o", str(obj)]))
+        procs.append(subprocess.Popen([*common, "-c", str(particle / rel), "-o", str(obj)]))
         objs.append(obj)
     hobj = objdir / "ref_harness.o"
-    procs.append(subprocess.Popen([*common, f"-I{PARTICLE}", "-c", str(harness), "-o", str(hobj)]))
+    procs.append(subprocess.Popen([*common, f"-I{particle}", "-c", str(harness), "-o", str(hobj)]))
     objs.append(hobj)
     for p in procs:
         if p.wait() != 0:

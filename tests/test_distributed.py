@@ -43,7 +43,6 @@ def test_two_rank_partition_and_max_reduction():
     manager = mp.Manager()
     out = manager.dict()
     ctx = mp.get_context("spawn")
-    procs = [ctx.Process(target=_worker, args=(r, world, _free_port() if r == 0 else None, out)) for r in range(world)]
     port = _free_port()
     procs = [ctx.Process(target=_worker, args=(r, world, port, out)) for r in range(world)]
     for p in procs:
