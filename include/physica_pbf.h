@@ -303,8 +303,12 @@ int pbf_batch_set_graph_mode(pbf_batch* batch, int enable);
  *  particles or PBF_PREALLOCATED_MAX_CELLS grid cells return PBF_ERROR_CAPACITY; boundary
  *  particles return PBF_ERROR_UNSUPPORTED.  Forward mode only; no step cache is kept.
  *  Results are bit-identical to pbf_forward_step on a forward-mode solver of the same scene.
- *  The first call on a device (that device current) looks up the array's device address; make it
- *  before any stream capture.  All calls on a device share the array and it keeps the last call's
+ *  The array exists once per CUDA context (the device's primary context, or a context the caller
+ *  created and made current).  The first call in a context looks up the array's device address
+ *  there; under lazy module loading (the CUDA default) that call also loads the library's device
+ *  code and commits the PBF_PREALLOCATED_SCRATCH_BYTES array, so make it at start-up, inside the
+ *  memory budget, and before any stream capture.  A context created later, or the new primary
+ *  context after cudaDeviceReset, gets its own first call.  All calls in a context share the array and it keeps the last call's
  *  contents (the call clears what must start at zero): calls whose GPU work overlaps, on different
  *  streams or host threads, race and give undefined results, so order them on one stream.
  *  `cuda_stream` is a cudaStream_t (NULL: the legacy default stream). ---- */

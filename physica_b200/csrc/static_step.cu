@@ -10,9 +10,14 @@
 // kMaxParticles particles and kMaxCells grid cells.  Every GPU that loads this library holds the
 // array until the process exits.
 //
-// Set-up: the first call on a device (with that device current) asks the runtime for the array's
-// device address with cudaGetSymbolAddress and keeps it per device; make that first call before
-// any stream capture.  Every later call reuses the address.
+// Set-up: the array exists once per CUDA context (the device's primary context, or a context the
+// caller created with the driver API and made current).  The first call in a context asks the
+// runtime for the array's device address there with cudaGetSymbolAddress and keeps it, keyed by
+// the context's process-unique ID, so a later context on the same device (one created by the
+// caller, or the new primary context after cudaDeviceReset) gets its own look-up.  Under lazy
+// module loading, the CUDA default, that first call also loads this library's device code into the
+// context and commits the array: make it at start-up, inside the caller's memory budget, and before
+// any stream capture.  Every later call in the context reuses the address.
 //
 // Sharing: every call on a device uses the same array, and the array keeps the last call's
 // contents.  The substep clears what must start at zero (the cell histogram) and writes every
@@ -23,10 +28,13 @@
 // The launch sequence is the one of a forward-mode solver (pbf_forward_step) with these buffers
 // in place of the solver's, so the outputs are bit-identical to pbf_forward_step on the same inputs.
 #include <algorithm>
+#include <exception>
 #include <cmath>
 #include <mutex>
 #include <string>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include "../../include/physica_pbf.h"
@@ -39,7 +47,6 @@ namespace {
 
 constexpr uint32_t kMaxParticles = PBF_PREALLOCATED_MAX_PARTICLES;
 constexpr uint64_t kMaxCells = PBF_PREALLOCATED_MAX_CELLS;
-constexpr int kMaxDevices = 64;
 constexpr size_t kAlign = 256;
 
 constexpr size_t align_up(const size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
@@ -103,32 +110,79 @@ static_assert(kScratchBytes <= PBF_PREALLOCATED_SCRATCH_BYTES, "the documented s
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
+// One set-up per CUDA context, keyed by the context's process-unique ID (cuCtxGetId).
+struct ScratchSlot {
+    unsigned long long context;
+    unsigned char* address;
+};
+constexpr size_t kMaxSlots = 64;
 std::mutex g_setup_mutex;
-unsigned char* g_scratch_address[kMaxDevices] = {};
+ScratchSlot g_slots[kMaxSlots] = {};
+size_t g_slot_count = 0, g_slot_next = 0;
+PFN_cuCtxGetCurrent g_ctx_get_current = nullptr;
+PFN_cuCtxGetId g_ctx_get_id = nullptr;
 
-// The device address of g_scratch on the current device (looked up once per device).
-int scratch_address(unsigned char** out) {
-    int device = -1;
-    cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess) {
-        set_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-        return PBF_ERROR_CUDA;
-    }
-    if (device < 0 || device >= kMaxDevices) {
-        set_error("device ordinal beyond the preallocated-scratch table");
-        return PBF_ERROR_CAPACITY;
-    }
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_address[device]) {
-        void* ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_scratch);
-        if (e != cudaSuccess || !ptr) {
-            set_error(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+// The process-unique ID of the current context, 0 when none is current.  Called with the mutex held.
+int current_context(unsigned long long* id) {
+    *id = 0;
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        cudaDriverEntryPointQueryResult found{};
+        void* fn = nullptr;
+        cudaError_t e = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, &found);
+        if (e != cudaSuccess || found != cudaDriverEntryPointSuccess || !fn) {
+            set_error("driver entry point cuCtxGetCurrent not found");
             return PBF_ERROR_CUDA;
         }
-        g_scratch_address[device] = static_cast<unsigned char*>(ptr);
+        g_ctx_get_current = reinterpret_cast<PFN_cuCtxGetCurrent>(fn);
+        fn = nullptr;
+        e = cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &found);
+        if (e != cudaSuccess || found != cudaDriverEntryPointSuccess || !fn) {
+            set_error("driver entry point cuCtxGetId not found");
+            return PBF_ERROR_CUDA;
+        }
+        g_ctx_get_id = reinterpret_cast<PFN_cuCtxGetId>(fn);
     }
-    *out = g_scratch_address[device];
+    CUcontext context = nullptr;
+    if (g_ctx_get_current(&context) != CUDA_SUCCESS) {
+        set_error("cuCtxGetCurrent failed");
+        return PBF_ERROR_CUDA;
+    }
+    if (context && g_ctx_get_id(context, id) != CUDA_SUCCESS) {
+        set_error("cuCtxGetId failed");
+        return PBF_ERROR_CUDA;
+    }
+    return PBF_SUCCESS;
+}
+
+// The device address of g_scratch in the current context (looked up once per context).
+int scratch_address(unsigned char** out) {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    unsigned long long context = 0;
+    if (int rc = current_context(&context)) return rc;
+    if (context)
+        for (size_t k = 0; k < g_slot_count; ++k)
+            if (g_slots[k].context == context) {
+                *out = g_slots[k].address;
+                return PBF_SUCCESS;
+            }
+    // Set-up.  With no context current, the runtime makes the device's primary context current here.
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_scratch);
+    if (e != cudaSuccess || !ptr) {
+        set_error(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        return PBF_ERROR_CUDA;
+    }
+    if (int rc = current_context(&context)) return rc;
+    if (!context) {
+        set_error("no CUDA context is current after the scratch look-up");
+        return PBF_ERROR_CUDA;
+    }
+    // Slots of contexts that no longer exist (after cudaDeviceReset) are never matched again; the
+    // table overwrites its oldest slot once full.
+    g_slots[g_slot_next] = {context, static_cast<unsigned char*>(ptr)};
+    g_slot_next = (g_slot_next + 1) % kMaxSlots;
+    if (g_slot_count < kMaxSlots) ++g_slot_count;
+    *out = static_cast<unsigned char*>(ptr);
     return PBF_SUCCESS;
 }
 
@@ -320,7 +374,11 @@ int pbf_forward_step_preallocated(const pbf_domain_configuration* domain, const 
     try {
         return pbf::forward_preallocated(domain, configuration, state, control, parameters, next_state,
                                          static_cast<cudaStream_t>(cuda_stream));
+    } catch (const std::exception& e) {
+        pbf::set_error(std::string("internal exception: ") + e.what());
+        return PBF_ERROR_CUDA;
     } catch (...) {
+        pbf::set_error("internal exception");
         return PBF_ERROR_CUDA;
     }
 }
