@@ -246,9 +246,9 @@ def bench_b200(args, world, rank):
     K = sc.pressure_iterations
     cells = solver.cells
     bytes_per_particle = {"list_scan": 16, "density_lambda": 16, "correction_project": 28, "vorticity": 36, "normal_confinement": 48,
-                          "xsph": 48}
+                          "xsph": 48, "list_scan_density_lambda": 20}
     flops_per_pair = {"list_scan": 9, "density_lambda": 14 + 30, "correction_project": 25, "vorticity": 34, "normal_confinement": 26,
-                      "xsph": 21}
+                      "xsph": 21, "list_scan_density_lambda": 9 + 14 + 30}
     hbm, hbm_src = peaks()
     top = max((p for p in passes if p["name"] in bytes_per_particle), key=lambda p: p["ms"], default=None)
     roofline = None
@@ -384,7 +384,7 @@ def issue_roofline(kernel: str, launch_ms: float):
             "frac": round(achieved / peak, 4), "warp_instructions": instructions}
 
 
-SCAN_VARIANTS = ["per_lane", "cooperative", "staged"]   # pbf_launch_shape.list_scan 0..2
+SCAN_VARIANTS = ["per_lane", "cooperative", "staged", "fused_density"]   # pbf_launch_shape.list_scan 0..3
 
 
 def fixed_shape(text: str):

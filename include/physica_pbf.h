@@ -152,7 +152,8 @@ typedef struct pbf_solver pbf_solver;          /* PBF (pbf/pbf.ixx:14-141) */
 typedef struct pbf_step_cache pbf_step_cache;  /* PBF::StepCache (pbf/pbf.ixx:54-70) */
 typedef struct pbf_batch pbf_batch;            /* many independent scenes in one launch sequence (no reference counterpart) */
 typedef struct pbf_launch_shape {
-    uint32_t list_scan;         /* 0: per-lane walk, 1: warp-cooperative scan, 2: shared-memory staged walk */
+    uint32_t list_scan;         /* 0: per-lane walk, 1: warp-cooperative scan, 2: shared-memory staged walk,
+                                   3: per-lane walk with density + lambda in the same kernel */
     uint32_t scan_block_size;   /* threads per block of the list scan: 32, 64, 96 or 128 */
     uint32_t block_size;        /* threads per block of the gather passes: 32, 64, 96 or 128 */
 } pbf_launch_shape;
@@ -323,8 +324,10 @@ int pbf_forward_step_preallocated(const pbf_domain_configuration* domain, const 
  *      counterpart.  Every shape gives bit-identical results; only the speed changes.
  *      list_scan: 0 = each lane walks its own stencil, 1 = a warp walks each home cell's
  *      candidates once, 2 = each lane walks its stencil in a shared-memory copy of its warp's
- *      stencil columns; scan_block_size and block_size: 32, 64, 96 or 128 threads.  pbf_autotune
- *      times the twelve list-scan shapes by their scan time, then the gather block sizes by the
+ *      stencil columns, 3 = as 0, and each Jacobi iteration's scan also computes density and lambda
+ *      in the same kernel, replaying the list from shared memory (scenes with boundary particles run
+ *      3 as 0); scan_block_size and block_size: 32, 64, 96 or 128 threads.  pbf_autotune
+ *      times the sixteen list-scan shapes by their scan and density + lambda time, then the gather block sizes by the
  *      gather passes' time, on `repeats` forward steps from `state` (writing `scratch_state` and
  *      the cache, which then hold that step); it keeps the fastest shape, returns it in `chosen`
  *      (may be NULL) and the substep time with it in `milliseconds_per_step` (may be NULL).  It

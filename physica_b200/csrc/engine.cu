@@ -33,7 +33,8 @@ const char* pass_name(const int pass) {
                                             "normal_confinement", "xsph", "adjoint_seed", "xsph_vjp", "normal_vjp",
                                             "vorticity_vjp", "correction_vjp", "lambda_vjp", "density_vjp",
                                             "tangent_seed", "density_lambda_jvp", "correction_jvp", "vorticity_jvp",
-                                            "normal_jvp", "xsph_jvp"};
+                                            "normal_jvp", "xsph_jvp", "list_scan_density_lambda", "host_upload",
+                                            "host_download"};
     return pass >= 0 && pass < kPassCount ? names[pass] : "unknown";
 }
 
@@ -546,16 +547,23 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
         float* lam = diff ? r.lambda[k] : (k == 0 ? r.first_lambda : r.lambda[0]);
         const uint32_t l = diff ? k : 0u;
         const StoredList list{r.list_entries[l], r.list_counts[l], r.list_capacity};
-        timer_.begin(stream, kPassListScan);
         ListScanArgs scan{gc, xk, list, 1};
         scan.packed = packed_;
-        if (int rc = check(launch_list_scan(stream, scan, shape_), "neighbour list scan")) return rc;
-        timer_.end(stream, kPassListScan);
         DensityLambdaArgs d{gc, xk, lam, diff ? r.density[k] : (k == 0 ? r.first_density : nullptr),
                             diff ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr, list};
-        timer_.begin(stream, kPassDensityLambda);
-        if (int rc = check(launch_density_lambda(stream, d, shape_.block), "density/lambda")) return rc;
-        timer_.end(stream, kPassDensityLambda);
+        if (fuses_density(shape_, scan)) {
+            timer_.begin(stream, kPassScanDensityLambda);
+            if (int rc = check(launch_scan_density_lambda(stream, scan, d, shape_), "neighbour list scan + density/lambda"))
+                return rc;
+            timer_.end(stream, kPassScanDensityLambda);
+        } else {
+            timer_.begin(stream, kPassListScan);
+            if (int rc = check(launch_list_scan(stream, scan, shape_), "neighbour list scan")) return rc;
+            timer_.end(stream, kPassListScan);
+            timer_.begin(stream, kPassDensityLambda);
+            if (int rc = check(launch_density_lambda(stream, d, shape_.block), "density/lambda")) return rc;
+            timer_.end(stream, kPassDensityLambda);
+        }
         CorrectionArgs c{gc, xk, lam, xk1, diff ? r.mask[k] : nullptr, k + 1 == K ? 1 : 0, previous, r.sorted_index,
                          out_positions, r.velocity, list};
         c.packed = packed_;
@@ -638,22 +646,24 @@ int Engine::autotune(const pbf_particle_state* state, const pbf_control* control
         timer_.enable(false);
         return rc;
     };
-    const uint32_t scans[3] = {kScanPerLane, kScanCooperative, kScanStaged};
+    const uint32_t scans[4] = {kScanPerLane, kScanCooperative, kScanStaged, kScanFusedDensity};
     const uint32_t blocks[4] = {32u, 64u, 96u, 128u};
     double ms[kPassCount];
     int rc = PBF_SUCCESS;
-    // 1. the list scan: variant x block size, by the scan's own time
+    // 1. the list scan: variant x block size, by the time of the scans and the density + lambda
+    //    passes (one kernel in the fused variant)
     LaunchShape best = previous;
     best.block = 128u;
     double best_scan = -1.0;
-    for (int v = 0; v < 3 && !rc; ++v)
+    for (int v = 0; v < 4 && !rc; ++v)
         for (int b = 0; b < 4 && !rc; ++b) {
             shape_ = best;
             shape_.scan = scans[v];
             shape_.scan_block = blocks[b];
             if ((rc = measure(ms))) break;
-            if (best_scan < 0.0 || ms[kPassListScan] < best_scan) {
-                best_scan = ms[kPassListScan];
+            const double scan_ms = ms[kPassListScan] + ms[kPassDensityLambda] + ms[kPassScanDensityLambda];
+            if (best_scan < 0.0 || scan_ms < best_scan) {
+                best_scan = scan_ms;
                 best.scan = scans[v];
                 best.scan_block = blocks[b];
             }

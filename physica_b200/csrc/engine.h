@@ -126,6 +126,9 @@ enum PassId : int {
     kPassVorticityJvp,
     kPassNormalJvp,
     kPassXsphJvp,
+    kPassScanDensityLambda,
+    kPassHostUpload,
+    kPassHostDownload,
     kPassCount
 };
 

@@ -452,6 +452,112 @@ __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLam
     if (a.neighbor_count) a.neighbor_count[p.s] = op.neighbors;
 }
 
+// ------------------------------------------- list scan fused with density + lambda
+// One kernel per Jacobi iteration in place of list_walk_kernel + density_lambda_kernel: each lane
+// runs the per-lane packed scan of its particle, writing the stored list (which the correction pass
+// replays) and, for its first kStagedEntries entries, a copy in shared memory; it then replays its
+// own list with the density and lambda arithmetic, reading the staged entries from shared memory
+// (the rest, if any, from the stored list).  The list, its order and every sum are those of the
+// two-kernel path, so the results are bit-identical.  Scenes with boundary particles use the two
+// kernels.
+constexpr uint32_t kStagedEntries = 48;   // 24 KB of shared memory per 128-thread block
+
+__global__ void __launch_bounds__(kBlock, 8) scan_density_lambda_kernel(const ListScanArgs a, const DensityLambdaArgs d) {
+    __shared__ uint32_t staged[kStagedEntries][kBlock];
+    const Particle p = locate(a.g);
+    if (!p.active) return;
+    const uint32_t s = p.s, lane_slot = threadIdx.x;
+    const Grid& grid = p.scene->grid;
+    const int cx = static_cast<int>(grid.cells_x), cy = static_cast<int>(grid.cells_y), cz = static_cast<int>(grid.cells_z);
+    const uint32_t z_lo = static_cast<uint32_t>(p.c.z > 0 ? p.c.z - 1 : 0);
+    const uint32_t z_hi = static_cast<uint32_t>(p.c.z + 1 < cz ? p.c.z + 1 : cz - 1);
+    const float4 xi = a.pos[s];
+    const uint32_t capacity = a.list.capacity;
+    uint32_t* __restrict__ entries = a.list.entries + list_row(s, capacity);
+    const uint32_t* __restrict__ offsets = a.g.cell_offsets;
+    // 1. the per-lane packed scan (PackedScan), appending to the stored list and the stage
+    uint32_t n = 0;
+    {
+        const float threshold = p.k.list_threshold;
+        const float2 nx = make_float2(-xi.x, -xi.x), ny = make_float2(-xi.y, -xi.y), nz = make_float2(-xi.z, -xi.z);
+        auto hits2 = [&](const float2 x, const float2 y, const float2 z) -> uint32_t {
+            const float2 dx = __fadd2_rn(x, nx), dy = __fadd2_rn(y, ny), dz = __fadd2_rn(z, nz);
+            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
+            return (r2.x < threshold ? 1u : 0u) | (r2.y < threshold ? 2u : 0u);
+        };
+        const PackedPositions pk = a.packed;
+#pragma unroll 1
+        for (int o = 0; o < 9; ++o) {
+            const int x = p.c.x + o / 3 - 1, y = p.c.y + o % 3 - 1;
+            if (x < 0 || x >= cx || y < 0 || y >= cy) continue;
+            const uint32_t first = offsets[cell_index(grid, x, y, z_lo)];
+            const uint32_t end = offsets[cell_index(grid, x, y, z_hi) + 1u];
+            if (first >= end) continue;
+            for (uint32_t base = first & ~3u; base < end; base += 32u) {
+                const uint32_t stop = min(end, base + 32u);
+                uint32_t mask = 0u;
+                for (uint32_t k = 0u; base + k < stop; k += 4u) {
+                    const uint32_t t = base + k;
+                    const float4 qx = *reinterpret_cast<const float4*>(pk.x + t);
+                    const float4 qy = *reinterpret_cast<const float4*>(pk.y + t);
+                    const float4 qz = *reinterpret_cast<const float4*>(pk.z + t);
+                    mask |= (hits2(make_float2(qx.x, qx.y), make_float2(qy.x, qy.y), make_float2(qz.x, qz.y)) |
+                             (hits2(make_float2(qx.z, qx.w), make_float2(qy.z, qy.w), make_float2(qz.z, qz.w)) << 2))
+                            << k;
+                }
+                if (base < first) mask &= ~0u << (first - base);
+                if (end - base < 32u) mask &= (1u << (end - base)) - 1u;
+                while (mask) {
+                    const uint32_t k = static_cast<uint32_t>(__ffs(mask)) - 1u;
+                    if (n < capacity) entries[static_cast<size_t>(n) * 32u] = base + k;
+                    if (n < kStagedEntries) staged[n][lane_slot] = base + k;
+                    ++n;
+                    mask &= mask - 1u;
+                }
+            }
+        }
+        a.list.counts[s] = n <= capacity ? n : kOverflow;
+    }
+    // 2. density (density/density.cu:18-40) and lambda (pbf/pbf.cu:95-127) over the same list
+    DensityLambdaOp<false> op;
+    op.pos = a.pos;
+    op.boundary = nullptr;
+    op.self = s;
+    op.k = p.k;
+    const float4 pa = a.g.params_a[s];
+    op.x = xyz(xi);
+    op.rest_density = pa.x;
+    op.density = 0.0F;
+    op.gradient_sum = mk(0.0F, 0.0F, 0.0F);
+    op.denominator = pa.y;  // relaxation
+    op.neighbors = 0;
+    op.ratio.reset(xi.w, op.rest_density);
+    if (n > capacity) {
+        walk(op, p, a.g);
+    } else if (n > 0) {
+        auto entry = [&](const uint32_t k) -> uint32_t {
+            return k < kStagedEntries ? staged[k][lane_slot] : entries[static_cast<size_t>(k) * 32u];
+        };
+        uint32_t t = entry(0);
+        uint32_t tn = n > 1u ? entry(1) : 0u;
+        float4 data = op.prefetch(t);
+        for (uint32_t k = 1; k < n; ++k) {
+            const uint32_t tnn = k + 1u < n ? entry(k + 1u) : 0u;
+            const float4 next = op.prefetch(tn);
+            op.apply(t, data);
+            t = tn;
+            tn = tnn;
+            data = next;
+        }
+        op.apply(t, data);
+    }
+    const float denominator = __fadd_rn(op.denominator, sq_yfirst(op.gradient_sum));
+    d.lambda[s] = __fdiv_rn(-__fsub_rn(__fdiv_rn(op.density, op.rest_density), 1.0F), denominator);
+    if (d.density) d.density[s] = op.density;
+    if (d.gsum_denom) d.gsum_denom[s] = make_float4(op.gradient_sum.x, op.gradient_sum.y, op.gradient_sum.z, denominator);
+    if (d.neighbor_count) d.neighbor_count[s] = op.neighbors;
+}
+
 // ------------------------------------------------------- correction + project
 // correction (pbf/pbf.cu:254-288) and project (pbf/pbf.cu:417-431); on the last iteration
 // also reconstruct (pbf/pbf.cu:456-460) and the write-back of next_state.positions.
@@ -809,8 +915,13 @@ cudaError_t launch_constants(cudaStream_t stream, const float* radii, const uint
 
 bool valid_shape(const LaunchShape& shape) {
     auto ok = [](const uint32_t b) { return b >= 32u && b <= static_cast<uint32_t>(kBlock) && b % 32u == 0u; };
-    return (shape.scan == kScanPerLane || shape.scan == kScanCooperative || shape.scan == kScanStaged) &&
+    return (shape.scan == kScanPerLane || shape.scan == kScanCooperative || shape.scan == kScanStaged ||
+            shape.scan == kScanFusedDensity) &&
            ok(shape.scan_block) && ok(shape.block);
+}
+
+bool fuses_density(const LaunchShape& shape, const ListScanArgs& a) {
+    return shape.scan == kScanFusedDensity && a.packed.x && !a.g.boundary && !a.g.boundary_offsets;
 }
 
 namespace {
@@ -831,6 +942,15 @@ cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a, const L
         list_staged_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     else
         list_walk_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scan_density_lambda(cudaStream_t stream, const ListScanArgs& a, const DensityLambdaArgs& d,
+                                       const LaunchShape& shape) {
+    if (a.g.count == 0) return cudaSuccess;
+    const unsigned block = block_of(shape.scan_block);
+    scan_density_lambda_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a, d);
     count_launch();
     return cudaGetLastError();
 }

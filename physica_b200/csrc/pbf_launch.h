@@ -164,6 +164,8 @@ enum ListScanVariant : uint32_t {
     kScanPerLane = 0,       // every lane walks its own 27 cells (run-mates share each load)
     kScanCooperative = 1,   // a warp walks each home-cell run's candidates once, 32 at a time
     kScanStaged = 2,        // a warp stages its column group's candidates in shared memory
+    kScanFusedDensity = 3,  // per lane, and the Jacobi iterations' scans also run density + lambda
+                            // in the same kernel (scenes without boundary particles)
 };
 struct LaunchShape {
     uint32_t scan = kScanPerLane;
@@ -173,6 +175,12 @@ struct LaunchShape {
 bool valid_shape(const LaunchShape& shape);
 
 cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a, const LaunchShape& shape = LaunchShape{});
+// Whether `shape` runs the scan of `a` fused with density + lambda (launch_scan_density_lambda).
+bool fuses_density(const LaunchShape& shape, const ListScanArgs& a);
+// The list scan of a Jacobi iteration and its density + lambda pass in one kernel (same list and
+// results as launch_list_scan followed by launch_density_lambda).
+cudaError_t launch_scan_density_lambda(cudaStream_t stream, const ListScanArgs& a, const DensityLambdaArgs& d,
+                                       const LaunchShape& shape);
 // Device step counter and the per-step scene fields derived from it (time, grid origin, collision box).
 cudaError_t launch_set_step(cudaStream_t stream, unsigned long long* step, uint64_t value);
 cudaError_t launch_advance_step(cudaStream_t stream, unsigned long long* step);

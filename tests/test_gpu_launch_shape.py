@@ -9,7 +9,7 @@ from physica_b200 import pbf, scenes
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [pbf.LaunchShape(v, b, g) for v, b, g in itertools.product((0, 1, 2), (32, 64, 96, 128), (32, 64, 96, 128))]
+SHAPES = [pbf.LaunchShape(v, b, g) for v, b, g in itertools.product((0, 1, 2, 3), (32, 64, 96, 128), (32, 64, 96, 128))]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -44,7 +44,7 @@ def test_every_shape_gives_identical_substeps():
 
 def test_invalid_shapes_are_rejected():
     solver, _, _, _ = pbf.solver_for_scene(scenes.dam_break((4, 4, 4), (0, 0, 0), (1, 2, 1), 32, 2))
-    for bad in (pbf.LaunchShape(3, 128, 128), pbf.LaunchShape(0, 48, 128), pbf.LaunchShape(0, 128, 256),
+    for bad in (pbf.LaunchShape(4, 128, 128), pbf.LaunchShape(0, 48, 128), pbf.LaunchShape(0, 128, 256),
                 pbf.LaunchShape(1, 0, 64)):
         with pytest.raises(pbf.PBFError):
             solver.launch_shape = bad
@@ -65,7 +65,8 @@ def test_batch_autotune_and_shapes_give_identical_substeps():
     scs = [scenes.batched_scene(c, 200 + k, 3) for k, c in enumerate((1500, 4000, 257))]
     batch, state, control, params = pbf.batch_for_scenes(scs)
     out = []
-    for shape in (pbf.LaunchShape(0, 128, 128), pbf.LaunchShape(1, 64, 96), pbf.LaunchShape(2, 128, 64)):
+    for shape in (pbf.LaunchShape(0, 128, 128), pbf.LaunchShape(1, 64, 96), pbf.LaunchShape(2, 128, 64),
+                  pbf.LaunchShape(3, 96, 128)):
         batch.launch_shape = shape
         cur = pbf.State(state.positions.clone(), state.velocities.clone(), 0)
         nxt = batch.allocate_state()
@@ -78,3 +79,32 @@ def test_batch_autotune_and_shapes_give_identical_substeps():
         assert torch.equal(out[0][0], other[0]) and torch.equal(out[0][1], other[1])
     shape, ms = batch.autotune(state, control, params, repeats=1)
     assert shape in SHAPES and ms > 0.0
+
+
+def test_fused_density_records_the_same_iterates_for_the_adjoint():
+    """Differentiable mode: the fused scan + density/lambda kernel records the same densities,
+    gradient sums and lambdas as the two-kernel path, so the adjoint is bit-identical."""
+    import numpy as np
+    sc = scenes.dam_break((12, 12, 12), (0, 0, 0), (1, 2, 1), 34, 3, velocity_sigma=0.2)
+    rng = np.random.default_rng(7)
+    wx = torch.from_numpy(rng.normal(size=(3, sc.count))).cuda()
+    wv = torch.from_numpy(rng.normal(size=(3, sc.count))).cuda()
+    out = []
+    for shape in (pbf.LaunchShape(0, 128, 128), pbf.LaunchShape(3, 64, 128)):
+        solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable)
+        solver.launch_shape = shape
+        cache = solver.allocate_step_cache()
+        nxt = solver.allocate_state()
+        solver.forward_step(state, control, params, nxt, cache)
+        pa, ca, qa = solver.allocate_state_adjoint(), solver.allocate_control_adjoint(), solver.allocate_parameter_adjoint()
+        solver.vjp_step(state, control, params, nxt, cache, pbf.StateAdjoint(wx, wv), pa, ca, qa)
+        torch.cuda.synchronize()
+        fields = [cache.read_iteration(pbf.IterationField.DENSITIES, k) for k in range(3)]
+        fields += [cache.read_iteration(pbf.IterationField.LAMBDAS, k) for k in range(3)]
+        fields += [cache.read_iteration(pbf.IterationField.GRADIENT_SUMS, k) for k in range(3)]
+        out.append((nxt.positions.clone(), nxt.velocities.clone(), pa.positions.clone(), pa.velocities.clone(), fields))
+    a, b = out
+    for x, y in zip(a[:4], b[:4]):
+        assert torch.equal(x, y)
+    for x, y in zip(a[4], b[4]):
+        assert torch.equal(x, y)

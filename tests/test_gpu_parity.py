@@ -103,13 +103,15 @@ def _ref_pass_fn(reference):
     return run, topology
 
 
-@pytest.mark.parametrize("warm_steps", [0, 15])
-def test_every_pass_bit_exact_against_reference(warm_steps):
-    """Each fused pass, fed the same inputs as the reference kernel it replaces, is bit-identical."""
+@pytest.mark.parametrize("warm_steps,list_scan", [(0, 0), (15, 0), (15, 3)])
+def test_every_pass_bit_exact_against_reference(warm_steps, list_scan):
+    """Each fused pass, fed the same inputs as the reference kernel it replaces, is bit-identical
+    (list_scan 3: the scan and the density + lambda pass in one kernel)."""
     reference = reference_or_skip()
     run, topology = _ref_pass_fn(reference)
     sc = scenes.plain_small(lattice=(20, 20, 20))
     solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
+    solver.launch_shape = pbf.LaunchShape(list_scan, 128, 128)
     cache = solver.allocate_step_cache()
     for _ in range(warm_steps):
         nxt = step(solver, state, control, params, cache)
