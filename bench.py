@@ -243,6 +243,18 @@ def bench_b200(args, world, rank):
     passes = read_profile(lib, solver.handle)
     lib.pbf_profile_enable(solver.handle, 0)
     neighbors = float(cache.read(CacheField.NEIGHBOR_COUNTS).double().mean())
+
+    # throughput past the ejections (they start at substep 27): advance the scene to substep 97,
+    # then time 20 more substeps after 3 warm-up ones, the same way
+    done = args.warmup + args.steps + 3
+    for _ in range(max(0, 97 - done)):
+        step()
+    ms_late, _ = timed(step, 20, 3, world, stream, flush)
+    ms_late = max_over_ranks(ms_late, world) / 20
+    first_late = max(done, 97) + 3
+    late = {"substeps": f"{first_late}-{first_late + 20}", "ms_per_step": round(ms_late, 4),
+            "value": round(world * n / (ms_late * 1e-3), 1), "unit": UNIT,
+            "mean_neighbors": round(float(cache.read(CacheField.NEIGHBOR_COUNTS).double().mean()), 3)}
     K = sc.pressure_iterations
     cells = solver.cells
     bytes_per_particle = {"list_scan": 16, "density_lambda": 16, "correction_project": 28, "vorticity": 36, "normal_confinement": 48,
@@ -293,11 +305,28 @@ def bench_b200(args, world, rank):
             host_step()
         barrier(world)
         ke = max(3, min(args.steps, 10))
-        t0 = time.perf_counter()
+        total = 0.0
         for _ in range(ke):
+            with torch.cuda.stream(stream):   # the same L2 flush as the device-timed loop, outside the timing
+                flush.add_(1.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            host_step()   # returns after its downloads completed
+            total += time.perf_counter() - t0
+        dt = max_over_ranks(total / ke, world)
+        # the copies alone: CUDA events around the uploads and the downloads of three profiled host steps
+        lib.pbf_profile_enable(solver.handle, 1)
+        for _ in range(3):
+            with torch.cuda.stream(stream):
+                flush.add_(1.0)
             host_step()
-        dt = max_over_ranks((time.perf_counter() - t0) / ke, world)
-        e2e = {"value": world * n / dt, "unit": UNIT, "h2d_bytes_per_step": 6 * 4 * n, "d2h_bytes_per_step": 6 * 4 * n}
+        copies = {q["name"]: q["ms"] / 3 for q in read_profile(lib, solver.handle)}
+        lib.pbf_profile_enable(solver.handle, 0)
+        e2e = {"value": world * n / dt, "unit": UNIT, "h2d_bytes_per_step": 6 * 4 * n, "d2h_bytes_per_step": 6 * 4 * n,
+               "ms_per_step": round(dt * 1e3, 4), "h2d_ms_per_step": round(copies.get("host_upload", float("nan")), 4),
+               "d2h_ms_per_step": round(copies.get("host_download", float("nan")), 4),
+               "timing": "host wall clock around each pbf_forward_step_host call (pinned host buffers, L2 flushed "
+                         "before each call); d2h overlaps the post-loop passes (positions on a second stream)"}
 
     # differentiable rollout: grad-steps/s at 64k
     grad = None
@@ -314,9 +343,10 @@ def bench_b200(args, world, rank):
         batched_grad = bench_batch_grad(args, world, rank)
 
     sph_family = None if args.no_sph else bench_sph(args, world, rank)
-    cpu = None
+    cpu, oracle_error = None, None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(sc)
+        cpu, first, small_100 = cpu_baseline(sc)
+        oracle_error = oracle_errors(sc, first, small_100)
     return {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
@@ -328,8 +358,9 @@ def bench_b200(args, world, rank):
                    "launch_shape": {"list_scan": SCAN_VARIANTS[shape.list_scan],
                                     "scan_block": shape.scan_block_size, "block": shape.block_size,
                                     "autotune_ms_per_step": None if math.isnan(tuned_ms) else round(tuned_ms, 4)}},
-        "roofline": roofline, "step_roofline": step_roofline, "per_pass": per_pass,
-        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(round(per_step_launches * args.steps)),
+        "roofline": roofline, "step_roofline": step_roofline, "per_pass": per_pass, "after_ejections": late,
+        "cpu_baseline": cpu, "oracle_error": oracle_error, "e2e": e2e,
+        "gpu_launches": int(round(per_step_launches * args.steps)),
         "clocks": clk.summary(), "grad_steps_per_s": grad, "tangent_ms_per_step": tangent, "batched_scenes": batched,
         "batched_grad_steps_per_s": batched_grad, "sph_family": sph_family,
     }
@@ -719,18 +750,123 @@ def reference_sph_gradient_ms(args, world, sc, name):
 
 
 def cpu_baseline(sc):
-    """FP64 host oracle on all host cores: consecutive substeps of the same 1M workload from its
-    initial state until at least 10 s of CPU work (at most 4 substeps)."""
+    """FP64 host oracle on all host cores (the reference's PBF has no CPU path):
+    - consecutive substeps of the same 1M workload from its initial state until at least 10 s of
+      CPU work (at most 4 substeps): the reported value;
+    - the 32,768-particle dam break (4 iterations) run for its full 100 substeps.
+    Returns the baseline, the oracle's first 1M substep and its 32k state after 100 substeps (for
+    the oracle-error check)."""
     from oracle import oracle
     x, v = sc.positions, sc.velocities
+    first = None
     steps, t0 = 0, time.perf_counter()
     while steps < 4 and (steps == 0 or time.perf_counter() - t0 < 10.0):
         x, v = oracle.forward_step(sc, x, v, step_index=steps)
+        if first is None:
+            first = (x, v)
         steps += 1
     dt = time.perf_counter() - t0
-    return {"value": round(steps * sc.count / dt, 1), "unit": UNIT, "cores": oracle.thread_count(), "kind": "port",
-            "sample": f"{steps} consecutive substeps of the 1,048,576-particle workload from rest "
-                      f"(FP64 OpenMP oracle, {dt:.2f} s)"}
+    from physica_b200 import scenes
+    small = scenes.plain_small()
+    xs, vs = small.positions, small.velocities
+    t1 = time.perf_counter()
+    for k in range(100):
+        xs, vs = oracle.forward_step(small, xs, vs, step_index=k)
+    dt_small = time.perf_counter() - t1
+    out = {"value": round(steps * sc.count / dt, 1), "unit": UNIT, "cores": oracle.thread_count(), "kind": "port",
+           "sample": f"{steps} consecutive substeps of the 1,048,576-particle workload from rest "
+                     f"(FP64 OpenMP oracle, {dt:.2f} s)",
+           "dam_break_32k_100_steps": {"value": round(100 * small.count / dt_small, 1), "unit": UNIT,
+                                       "seconds": round(dt_small, 2),
+                                       "sample": "the 32,768-particle dam break (32x32x32 lattice, 4 iterations) for "
+                                                 "its full 100 substeps (FP64 OpenMP oracle)"}}
+    return out, first, (xs, vs)
+
+
+def _errors(x, v, xo, vo, h, dt):
+    """max |x - x_oracle| / h and max |v - v_oracle| * dt / h of FP32 (3, N) results against FP64 ones."""
+    ex = float(np.abs(x.astype(np.float64) - xo).max()) / h if x.size else 0.0
+    ev = float(np.abs(v.astype(np.float64) - vo).max()) * dt / h if v.size else 0.0
+    return {"max_dx_over_h": float(f"{ex:.3e}"), "max_dv_dt_over_h": float(f"{ev:.3e}")}
+
+
+def oracle_errors(sc_large, first_large, small_100):
+    """Error of this library's FP32 substep against the FP64 host oracle for every configuration.
+
+    One substep from each configuration's initial state (the dam break is chaotic, so longer runs
+    measure the divergence of two roundings, not an error; the 32k run's 100-substep divergence is
+    given beside its one-step error).  Batched configurations check a stated subset of their scenes;
+    the differentiable ones also give the relative max-norm error of the one-step adjoint of the
+    target-cloud loss with respect to the initial velocities."""
+    from oracle import oracle
+    from physica_b200 import pbf, scenes
+    out = {}
+
+    def one(sc, mode=pbf.ExecutionMode.forward):
+        solver, state, control, params = pbf.solver_for_scene(sc, mode=mode)
+        cache = solver.allocate_step_cache()
+        nxt = solver.allocate_state()
+        solver.forward_step(state, control, params, nxt, cache)
+        torch.cuda.synchronize()
+        return solver, state, control, params, cache, nxt
+
+    sc = sc_large
+    *_, nxt = one(sc)
+    out["dam_break_1m"] = {**_errors(nxt.positions.cpu().numpy(), nxt.velocities.cpu().numpy(), *first_large,
+                                     sc.support_radius, sc.time_step), "substeps": 1}
+    small = scenes.plain_small()
+    solver, state, control, params, cache, nxt = one(small)
+    x1, v1 = oracle.forward_step(small, small.positions, small.velocities)
+    e = _errors(nxt.positions.cpu().numpy(), nxt.velocities.cpu().numpy(), x1, v1, small.support_radius, small.time_step)
+    cur, other = nxt, solver.allocate_state()
+    for _ in range(99):
+        solver.forward_step(cur, control, params, other, cache)
+        cur, other = other, cur
+    torch.cuda.synchronize()
+    e["after_100_substeps"] = _errors(cur.positions.cpu().numpy(), cur.velocities.cpu().numpy(), *small_100,
+                                      small.support_radius, small.time_step)
+    out["dam_break_32k"] = {**e, "substeps": 1}
+
+    def with_adjoint(sc):
+        solver, state, control, params, cache, nxt = one(sc, pbf.ExecutionMode.differentiable)
+        n = sc.count
+        x1 = nxt.positions.double()
+        wx = (x1 - torch.from_numpy(sc.targets).cuda().double()) * (2.0 / n)
+        na = pbf.StateAdjoint(wx, torch.zeros_like(wx))
+        pa, ca, qa = solver.allocate_state_adjoint(), solver.allocate_control_adjoint(), solver.allocate_parameter_adjoint()
+        solver.vjp_step(state, control, params, nxt, cache, na, pa, ca, qa)
+        torch.cuda.synchronize()
+        xo, vo = oracle.forward_step(sc, sc.positions, sc.velocities)
+        e = _errors(nxt.positions.cpu().numpy(), nxt.velocities.cpu().numpy(), xo, vo, sc.support_radius, sc.time_step)
+        adj = oracle.vjp_step(sc, sc.positions, sc.velocities, wx.cpu().numpy(), np.zeros((3, n)))
+        got = pa.velocities.cpu().numpy()
+        e["adjoint_velocity_rel"] = float(f"{np.abs(got - adj['velocity']).max() / np.abs(adj['velocity']).max():.3e}")
+        return e
+
+    out["differentiable_64k"] = {**with_adjoint(scenes.differentiable()), "substeps": 1}
+    subset = list(range(0, 256, 32))
+    scs = scenes.batched_forward()
+    batch, state, control, params = pbf.batch_for_scenes(scs)
+    nxt = batch.allocate_state()
+    batch.forward_step(state, control, params, nxt)
+    torch.cuda.synchronize()
+    worst = {"max_dx_over_h": 0.0, "max_dv_dt_over_h": 0.0}
+    for k in subset:
+        r = batch.particle_range(k)
+        xo, vo = oracle.forward_step(scs[k], scs[k].positions, scs[k].velocities)
+        e = _errors(nxt.positions[:, r].cpu().numpy(), nxt.velocities[:, r].cpu().numpy(), xo, vo,
+                    scs[k].support_radius, scs[k].time_step)
+        worst = {q: max(worst[q], e[q]) for q in worst}
+    out["batched_forward_256"] = {**worst, "substeps": 1, "scenes_checked": subset}
+    del batch, state, control, params, nxt
+    adj_subset = [0, 11, 22, 31]
+    scs = scenes.batched_adjoint()
+    worst = {"max_dx_over_h": 0.0, "max_dv_dt_over_h": 0.0, "adjoint_velocity_rel": 0.0}
+    for k in adj_subset:   # each checked scene through a one-scene differentiable solver of the same scene
+        e = with_adjoint(scs[k])
+        worst = {q: max(worst[q], e[q]) for q in worst}
+    out["batched_adjoint_32"] = {**worst, "substeps": 1, "scenes_checked": adj_subset}
+    return out
 
 
 # --------------------------------------------------------------------------- reference arm
@@ -773,10 +909,11 @@ def bench_reference(args, world, rank):
                                "box [0,4]^3, 8 Jacobi iterations, dt=1/120, XSPH c=0.01, vorticity eps=1e-4",
                    "particles_per_gpu": n, "replicas": world, "l2": "flushed between timed steps (256 MiB write)",
                    "wall_s": round(wall, 3)},
-        "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": 0, "kind": "reference",
-                         "sample": "the reference's own CUDA PBF kernels (pbf.cu, density.cu, neighborhood.cu, domain.cu "
-                                   "compiled from its sources) replaying PBF::forward_step on the same B200; the reference "
-                                   "has no CPU implementation of this path"},
+        "cpu_baseline": None,
+        "reference_arm": {"device": "cuda (the same B200)", "kind": "reference",
+                          "sample": "the reference's own CUDA PBF kernels (pbf.cu, density.cu, neighborhood.cu, domain.cu "
+                                    "compiled from its sources) replaying PBF::forward_step; the reference has no CPU "
+                                    "implementation of this path, so this line carries no CPU figure"},
         "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "clocks": clk.summary(), "grad_steps_per_s": grad, "tangent_ms_per_step": tangent, "batched_scenes": batched,
         "sph_family": sph_family,

@@ -277,6 +277,7 @@ int pbf_forward_step_host(pbf_solver* solver, const pbf_host_state* state, const
             if (n && (!state->positions[k] || !state->velocities[k] || !next_state->positions[k] || !next_state->velocities[k]))
                 return null_arg("host field");
         }
+        en.timer().begin(st, pbf::kPassHostUpload);
         for (int k = 0; k < 3; ++k) {
             if (int rc = en.check(cudaMemcpyAsync(solver->in + k * n, state->positions[k], n * sizeof(float),
                                                   cudaMemcpyHostToDevice, st), "upload"))
@@ -285,6 +286,7 @@ int pbf_forward_step_host(pbf_solver* solver, const pbf_host_state* state, const
                                                   cudaMemcpyHostToDevice, st), "upload"))
                 return rc;
         }
+        en.timer().end(st, pbf::kPassHostUpload);
         pbf_particle_state in{{solver->in, solver->in + n, solver->in + 2 * n},
                               {solver->in + 3 * n, solver->in + 4 * n, solver->in + 5 * n}, state->step_index};
         pbf_particle_state out{{solver->out, solver->out + n, solver->out + 2 * n},
@@ -298,12 +300,17 @@ int pbf_forward_step_host(pbf_solver* solver, const pbf_host_state* state, const
         cudaStream_t dl = solver->download;
         if (int rc = en.check(cudaStreamWaitEvent(dl, solver->positions_ready, 0), "download wait")) return rc;
         int rc = PBF_SUCCESS;
+        // profiled: the two downloads are timed on their own streams and summed under host_download
+        en.timer().begin(dl, pbf::kPassHostDownload);
         for (int k = 0; k < 3 && !rc; ++k)
             rc = en.check(cudaMemcpyAsync(next_state->positions[k], solver->out + k * n, n * sizeof(float),
                                           cudaMemcpyDeviceToHost, dl), "download");
+        en.timer().end(dl, pbf::kPassHostDownload);
+        en.timer().begin(st, pbf::kPassHostDownload);
         for (int k = 0; k < 3 && !rc; ++k)
             rc = en.check(cudaMemcpyAsync(next_state->velocities[k], solver->out + (3 + k) * n, n * sizeof(float),
                                           cudaMemcpyDeviceToHost, st), "download");
+        en.timer().end(st, pbf::kPassHostDownload);
         // both streams drain before returning, so the next call may reuse the staging buffers
         const int src = en.check(cudaStreamSynchronize(st), "forward_step_host");
         const int drc = en.check(cudaStreamSynchronize(dl), "forward_step_host download");
