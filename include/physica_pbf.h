@@ -291,6 +291,19 @@ int pbf_batch_profile_read(pbf_batch* batch, pbf_pass_time* passes, uint32_t cap
  *      state / control / parameter / cache buffers and replayed with one graph launch per call
  *      (default off for a solver, on for a batch).  No reference counterpart. ---- */
 int pbf_set_graph_mode(pbf_solver* solver, int enable);
+
+/* ---- checkpoint recomputation of the Jacobi iterations (differentiable mode).  The reference's
+ *      StepCache keeps the iterate of every checkpoint_interval-th Jacobi iteration and the last one
+ *      (pbf/pbf.ixx:54-70, pbf/pbf.cpp:173-182); vjp_step recomputes each segment's lists,
+ *      densities, lambdas and iterates from its first iterate before reversing it
+ *      (pbf/pbf.cpp:232-245) and jvp_step reruns the iterations (pbf/pbf.cpp:198-212).  Off (the
+ *      default): step caches keep every iterate, its fields and its neighbour list, and nothing is
+ *      recomputed.  On: step caches allocated afterwards keep the checkpoints only, plus every
+ *      iteration's collision mask (1 byte per particle); the solver holds one segment of
+ *      recomputed iterations.  Gradients and tangents are bit-identical in both forms.  Returns
+ *      PBF_ERROR_NOT_DIFFERENTIABLE for a forward-mode solver. ---- */
+int pbf_set_checkpoint_recompute(pbf_solver* solver, int enable);
+int pbf_batch_set_checkpoint_recompute(pbf_batch* batch, int enable);
 int pbf_batch_set_graph_mode(pbf_batch* batch, int enable);
 
 /* ---- forward substep without any device allocation.  No counterpart in the reference.

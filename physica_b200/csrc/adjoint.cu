@@ -862,7 +862,9 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
                          control_adjoint->external_accelerations.z};
     const float4* xK = r.iterate(K, K, true);
     const unsigned blocks = grid_of(n, kBlock);
-    const StoredList post_list{r.list_entries[K], r.list_counts[K], r.list_capacity};
+    const bool keep = r.keeps_all(true);
+    // A checkpoint-recompute record keeps one list: the post-loop list.
+    const StoredList post_list{r.list_entries[keep ? K : 0u], r.list_counts[keep ? K : 0u], r.list_capacity};
 
     timer_.begin(stream_, kPassSeed);
     seed_kernel<<<grid_of(n, 256), 256, 0, stream_>>>(
@@ -885,16 +887,40 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
     vorticity_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(va);
     timer_.end(stream_, kPassVorticityVjp);
     count_launch(4);
+    // Checkpoint recomputation (pbf/pbf.cpp:232-245): before the iterations of a segment between two
+    // kept iterates are reversed, its lists and per-iteration fields are recomputed from the first.
+    uint32_t segment_first = 0;
     for (uint32_t k = K; k-- > 0;) {
         double4* acc = ws->x[(K - k) & 1u];
         double4* other = ws->x[(K - k + 1) & 1u];
-        const float4* xk = r.iterate(k, K, true);
-        const StoredList it_list{r.list_entries[k], r.list_counts[k], r.list_capacity};
-        CorrectionVjpArgs ca{gc, it_list, r.sorted_index, xk, ws->s_corr, r.lambda[k], ws->correction, acc, ws->lambda, pa};
+        const float4* xk;
+        StoredList it_list;
+        const float* lambda_k;
+        const float* density_k;
+        const float4* gsum_k;
+        if (keep) {
+            xk = r.iterate(k, K, true);
+            it_list = StoredList{r.list_entries[k], r.list_counts[k], r.list_capacity};
+            lambda_k = r.lambda[k];
+            density_k = r.density[k];
+            gsum_k = r.gsum[k];
+        } else {
+            if (k + 1 == K || r.is_checkpoint(k + 1, K)) {   // the last iteration of a segment: recompute it
+                segment_first = k / r.checkpoint_interval * r.checkpoint_interval;
+                if (int rc = recompute_segment(r, segment_first, k + 1 - segment_first)) return rc;
+            }
+            const uint32_t j = k - segment_first;
+            xk = segment_iterate(r, segment_first, j);
+            it_list = StoredList{segment_->list_entries[j], segment_->list_counts[j], kListCapacity};
+            lambda_k = segment_->lambda[j];
+            density_k = segment_->density[j];
+            gsum_k = segment_->gsum[j];
+        }
+        CorrectionVjpArgs ca{gc, it_list, r.sorted_index, xk, ws->s_corr, lambda_k, ws->correction, acc, ws->lambda, pa};
         timer_.begin(stream_, kPassCorrectionVjp);
         correction_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(ca);
         timer_.end(stream_, kPassCorrectionVjp);
-        LambdaVjpArgs la{gc, it_list, r.sorted_index, xk, r.density[k], r.gsum[k], ws->lambda, acc, ws->density, pa};
+        LambdaVjpArgs la{gc, it_list, r.sorted_index, xk, density_k, gsum_k, ws->lambda, acc, ws->density, pa};
         timer_.begin(stream_, kPassLambdaVjp);
         lambda_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(la);
         timer_.end(stream_, kPassLambdaVjp);

@@ -164,6 +164,16 @@ int pbf_batch_scene_sums(pbf_batch* batch, const double* values, double* result)
                                "batch scene sums");
 }
 
+int pbf_batch_set_checkpoint_recompute(pbf_batch* batch, const int enable) {
+    if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
+    if (!batch->engine.differentiable()) {
+        pbf::set_error("checkpoint recomputation needs PBF_EXECUTION_DIFFERENTIABLE");
+        return PBF_ERROR_NOT_DIFFERENTIABLE;
+    }
+    batch->engine.set_recompute(enable != 0);
+    return PBF_SUCCESS;
+}
+
 int pbf_batch_set_graph_mode(pbf_batch* batch, const int enable) {
     if (!batch) return PBF_ERROR_INVALID_ARGUMENT;
     batch->engine.set_graphs(enable != 0);

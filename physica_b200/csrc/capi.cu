@@ -346,6 +346,16 @@ int pbf_sum_compensated(pbf_solver* solver, const double* values, const uint32_t
                                 "sum_compensated");
 }
 
+int pbf_set_checkpoint_recompute(pbf_solver* solver, const int enable) {
+    if (!solver) return null_arg("solver");
+    if (!solver->engine.differentiable()) {
+        pbf::set_error("checkpoint recomputation needs PBF_EXECUTION_DIFFERENTIABLE");
+        return PBF_ERROR_NOT_DIFFERENTIABLE;
+    }
+    solver->engine.set_recompute(enable != 0);
+    return PBF_SUCCESS;
+}
+
 int pbf_set_graph_mode(pbf_solver* solver, const int enable) {
     if (!solver) return null_arg("solver");
     solver->engine.set_graphs(enable != 0);

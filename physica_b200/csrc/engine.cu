@@ -131,6 +131,8 @@ Engine::~Engine() {
     adjoint_ = nullptr;
     destroy_tangent_workspace(tangent_);
     tangent_ = nullptr;
+    delete segment_;
+    segment_ = nullptr;
     arena_.release();
 }
 
@@ -336,6 +338,9 @@ int Engine::allocate_record(StepRecord& r) {
     cudaError_t e = cudaSuccess;
     const uint32_t n = count_, K = iterations_;
     const bool diff = differentiable();
+    r.recompute = diff && recompute_;
+    r.checkpoint_interval = checkpoint_interval_;
+    const bool keep = r.keeps_all(diff);
     r.cell_offsets = r.arena.alloc<uint32_t>(cells_ + 1, e);
     r.sorted_index = r.arena.alloc<uint32_t>(n, e);
     r.slot_of = r.arena.alloc<uint32_t>(n, e);
@@ -344,20 +349,26 @@ int Engine::allocate_record(StepRecord& r) {
     r.topology = r.arena.alloc<float4>(n, e);
     r.params_a = r.arena.alloc<float4>(n, e);
     r.params_b = r.arena.alloc<float4>(n, e);
-    const uint32_t npos = diff ? K : (K < 2 ? K : 2);
+    const uint32_t npos = keep ? K : (K < 2 ? K : 2);
     r.positions.assign(npos, nullptr);
     for (auto& p : r.positions) p = r.arena.alloc<float4>(n, e);
-    r.lambda.assign(diff ? K : (K ? 1 : 0), nullptr);
+    if (r.recompute) {
+        r.checkpoints.assign(K ? (K + r.checkpoint_interval - 1) / r.checkpoint_interval : 0, nullptr);
+        for (auto& p : r.checkpoints) p = r.arena.alloc<float4>(n, e);
+    }
+    r.lambda.assign(keep ? K : (K ? 1 : 0), nullptr);
     for (auto& p : r.lambda) p = r.arena.alloc<float>(n, e);
-    if (diff) {
+    if (keep) {
         r.density.assign(K, nullptr);
         r.gsum.assign(K, nullptr);
-        r.mask.assign(K, nullptr);
         for (uint32_t k = 0; k < K; ++k) {
             r.density[k] = r.arena.alloc<float>(n, e);
             r.gsum[k] = r.arena.alloc<float4>(n, e);
-            r.mask[k] = r.arena.alloc<uint8_t>(n, e);
         }
+    }
+    if (diff) {
+        r.mask.assign(K, nullptr);
+        for (uint32_t k = 0; k < K; ++k) r.mask[k] = r.arena.alloc<uint8_t>(n, e);
     }
     r.first_density = r.arena.alloc<float>(n, e);
     r.first_lambda = r.arena.alloc<float>(n, e);
@@ -369,7 +380,7 @@ int Engine::allocate_record(StepRecord& r) {
     // Neighbour lists: kListCapacity entries per particle, warp-interleaved.
     r.list_capacity = kListCapacity;
     const size_t padded = (static_cast<size_t>(n) + 31u) / 32u * 32u;
-    const uint32_t lists = diff ? K + 1 : 1;
+    const uint32_t lists = keep ? K + 1 : 1;
     r.list_entries.assign(lists, nullptr);
     r.list_counts.assign(lists, nullptr);
     for (uint32_t l = 0; l < lists; ++l) {
@@ -503,6 +514,7 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
                        "scene table"))
         return rc;
     const bool diff = differentiable();
+    const bool keep = r.keeps_all(diff);
     const uint32_t K = iterations_;
     GridBuildArgs g{};
     g.count = count_;
@@ -544,13 +556,13 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
     for (uint32_t k = 0; k < K; ++k) {
         const float4* xk = r.iterate(k, K, diff);
         float4* xk1 = const_cast<float4*>(r.iterate(k + 1, K, diff));
-        float* lam = diff ? r.lambda[k] : (k == 0 ? r.first_lambda : r.lambda[0]);
-        const uint32_t l = diff ? k : 0u;
+        float* lam = keep ? r.lambda[k] : (k == 0 ? r.first_lambda : r.lambda[0]);
+        const uint32_t l = keep ? k : 0u;
         const StoredList list{r.list_entries[l], r.list_counts[l], r.list_capacity};
         ListScanArgs scan{gc, xk, list, 1};
         scan.packed = packed_;
-        DensityLambdaArgs d{gc, xk, lam, diff ? r.density[k] : (k == 0 ? r.first_density : nullptr),
-                            diff ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr, list};
+        DensityLambdaArgs d{gc, xk, lam, keep ? r.density[k] : (k == 0 ? r.first_density : nullptr),
+                            keep ? r.gsum[k] : nullptr, k == 0 ? r.neighbor_count : nullptr, list};
         if (fuses_density(shape_, scan)) {
             timer_.begin(stream, kPassScanDensityLambda);
             if (int rc = check(launch_scan_density_lambda(stream, scan, d, shape_), "neighbour list scan + density/lambda"))
@@ -586,7 +598,7 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
         const unsigned flags = capture == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
         if (int rc = check(cudaEventRecordWithFlags(positions_ready_, stream, flags), "positions event")) return rc;
     }
-    const uint32_t lp = diff ? K : 0u;
+    const uint32_t lp = keep ? K : 0u;
     const StoredList post{r.list_entries[lp], r.list_counts[lp], r.list_capacity};
     timer_.begin(stream, kPassListScan);
     ListScanArgs post_scan{gc, xK, post};
@@ -607,6 +619,68 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
     if (int rc = check(launch_xsph(stream, x, shape_.block), "xsph")) return rc;
     timer_.end(stream, kPassXsph);
     return check(launch_advance_step(stream, d_step_), "step counter");
+}
+
+int Engine::segment_workspace(Segment** out) {
+    if (!segment_) {
+        auto* sg = new Segment();
+        sg->arena.set_stream(stream_);
+        const uint32_t n = count_;
+        const uint32_t L = std::max(1u, std::min(checkpoint_interval_, iterations_));
+        sg->length = L;
+        cudaError_t e = cudaSuccess;
+        sg->positions.assign(std::max(L - 1u, 2u), nullptr);
+        for (auto& p : sg->positions) p = sg->arena.alloc<float4>(n, e);
+        sg->lambda.assign(L, nullptr);
+        sg->density.assign(L, nullptr);
+        sg->gsum.assign(L, nullptr);
+        sg->list_entries.assign(L, nullptr);
+        sg->list_counts.assign(L, nullptr);
+        const size_t padded = (static_cast<size_t>(n) + 31u) / 32u * 32u;
+        for (uint32_t j = 0; j < L; ++j) {
+            sg->lambda[j] = sg->arena.alloc<float>(n, e);
+            sg->density[j] = sg->arena.alloc<float>(n, e);
+            sg->gsum[j] = sg->arena.alloc<float4>(n, e);
+            sg->list_entries[j] = sg->arena.alloc<uint32_t>(padded * kListCapacity, e);
+            sg->list_counts[j] = sg->arena.alloc<uint32_t>(n, e);
+        }
+        if (e != cudaSuccess) {
+            delete sg;
+            return check(e, "recomputation workspace");
+        }
+        segment_ = sg;
+    }
+    *out = segment_;
+    return PBF_SUCCESS;
+}
+
+int Engine::recompute_segment(const StepRecord& r, const uint32_t first, const uint32_t length) {
+    Segment* sg = nullptr;
+    if (int rc = segment_workspace(&sg)) return rc;
+    const GatherCommon gc = gather_common(r);
+    for (uint32_t j = 0; j < length; ++j) {
+        const float4* xk = segment_iterate(r, first, j);
+        const StoredList list{sg->list_entries[j], sg->list_counts[j], kListCapacity};
+        // The packed copy holds the iterate written by the previous correction; the segment's first
+        // iterate comes from a checkpoint, so its scan tests the float4 positions (same list).
+        ListScanArgs scan{gc, xk, list, 1};
+        if (j > 0) scan.packed = packed_;
+        DensityLambdaArgs d{gc, xk, sg->lambda[j], sg->density[j], sg->gsum[j], nullptr, list};
+        if (fuses_density(shape_, scan)) {
+            if (int rc = check(launch_scan_density_lambda(stream_, scan, d, shape_), "recompute: scan + density/lambda"))
+                return rc;
+        } else {
+            if (int rc = check(launch_list_scan(stream_, scan, shape_), "recompute: neighbour list scan")) return rc;
+            if (int rc = check(launch_density_lambda(stream_, d, shape_.block), "recompute: density/lambda")) return rc;
+        }
+        if (j + 1 < length) {
+            CorrectionArgs c{gc, xk, sg->lambda[j], sg->positions[j], nullptr, 0, Field3{}, r.sorted_index, MutField3{},
+                             nullptr, list};
+            c.packed = packed_;
+            if (int rc = check(launch_correction(stream_, c, shape_.block), "recompute: correction/project")) return rc;
+        }
+    }
+    return PBF_SUCCESS;
 }
 
 int Engine::autotune(const pbf_particle_state* state, const pbf_control* control, const pbf_parameters* parameters,
@@ -764,11 +838,13 @@ int Engine::read(const StepRecord& r, const pbf_cache_field field, void* destina
         case PBF_CACHE_CONFINED_VELOCITIES: e = vec(r.confined); break;
         case PBF_CACHE_FIRST_DENSITIES:
             if (iterations_ == 0) { set_error("no Jacobi iteration ran"); return PBF_ERROR_INVALID_ARGUMENT; }
-            e = launch_unsort_scalar(stream_, n, r.sorted_index, diff ? r.density[0] : r.first_density, 4, destination);
+            e = launch_unsort_scalar(stream_, n, r.sorted_index, r.keeps_all(diff) ? r.density[0] : r.first_density, 4,
+                                     destination);
             break;
         case PBF_CACHE_FIRST_LAMBDAS:
             if (iterations_ == 0) { set_error("no Jacobi iteration ran"); return PBF_ERROR_INVALID_ARGUMENT; }
-            e = launch_unsort_scalar(stream_, n, r.sorted_index, diff ? r.lambda[0] : r.first_lambda, 4, destination);
+            e = launch_unsort_scalar(stream_, n, r.sorted_index, r.keeps_all(diff) ? r.lambda[0] : r.first_lambda, 4,
+                                     destination);
             break;
         case PBF_CACHE_NEIGHBOR_COUNTS:
             if (iterations_ == 0) { set_error("no Jacobi iteration ran"); return PBF_ERROR_INVALID_ARGUMENT; }
@@ -794,12 +870,15 @@ int Engine::read_iteration(const StepRecord& r, const pbf_iteration_field field,
         return PBF_ERROR_INVALID_ARGUMENT;
     }
     if (field == PBF_ITERATION_POSITIONS) {
-        if (k > K || (!diff && k != 0 && k != K)) {
-            set_error("iteration positions exist for 0..K (every k only in differentiable mode)");
+        const bool kept = k == 0 || k == K || r.keeps_all(diff) || (r.recompute && r.is_checkpoint(k, K));
+        if (k > K || !kept) {
+            set_error("iteration positions exist for 0..K (every k only in differentiable mode; checkpoint recomputation "
+                      "keeps 0, the checkpoints and K)");
             return PBF_ERROR_INVALID_ARGUMENT;
         }
-    } else if (!diff || k >= K) {
-        set_error("per-iteration fields need differentiable mode and iteration < K");
+    } else if (field == PBF_ITERATION_COLLISION_MASKS ? (!diff || k >= K) : (!r.keeps_all(diff) || k >= K)) {
+        set_error("per-iteration fields need differentiable mode with every iterate kept (collision masks: either form) "
+                  "and iteration < K");
         return PBF_ERROR_INVALID_ARGUMENT;
     }
     if (n == 0) return PBF_SUCCESS;

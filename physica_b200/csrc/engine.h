@@ -77,11 +77,19 @@ struct StepRecord {
     float4* topology = nullptr;      // x* and mass (iterate 0)
     float4* params_a = nullptr;
     float4* params_b = nullptr;
-    std::vector<float4*> positions;  // iterates 1..K (forward mode: 2 ping-pong buffers)
-    std::vector<float*> lambda;      // per iteration (forward mode: 1)
-    std::vector<float*> density;     // per iteration (differentiable mode)
-    std::vector<float4*> gsum;       // per iteration (differentiable mode)
-    std::vector<uint8_t*> mask;      // per iteration (differentiable mode)
+    // Iterates 1..K.  Differentiable records keep all of them; forward-mode records pass them
+    // through 2 ping-pong buffers.  A checkpoint-recompute record (differentiable, `recompute`)
+    // keeps every checkpoint_interval-th iterate and the last one in `checkpoints`, as the
+    // reference's StepCache::checkpoints (pbf/pbf.ixx:54-70, pbf/pbf.cpp:173-182), and passes the
+    // others through the 2 ping-pong buffers.
+    std::vector<float4*> positions;
+    bool recompute = false;
+    uint32_t checkpoint_interval = 1;
+    std::vector<float4*> checkpoints;   // iterates c, 2c, ... below K, then K
+    std::vector<float*> lambda;      // per iteration (forward mode and checkpoint-recompute: 1)
+    std::vector<float*> density;     // per iteration (differentiable mode, all iterates kept)
+    std::vector<float4*> gsum;       // per iteration (differentiable mode, all iterates kept)
+    std::vector<uint8_t*> mask;      // per iteration (differentiable mode, both storage forms)
     float* first_density = nullptr;
     float* first_lambda = nullptr;
     uint32_t* neighbor_count = nullptr;
@@ -89,7 +97,8 @@ struct StepRecord {
     float4* vorticity = nullptr;
     float4* normal = nullptr;
     float4* confined = nullptr;
-    // Stored neighbour lists: one per iterate in differentiable mode (0..K), else one reused.
+    // Stored neighbour lists: one per iterate when all iterates are kept (0..K), else one reused
+    // (it holds the post-loop list after the step).
     std::vector<uint32_t*> list_entries;
     std::vector<uint32_t*> list_counts;
     uint32_t list_capacity = 0;
@@ -97,10 +106,16 @@ struct StepRecord {
     uint32_t* boundary_offsets = nullptr;   // cells + 1
     float4* boundary = nullptr;             // (position at the step's time, volume), cell-sorted
 
+    // Whether every iterate and its per-iteration fields and list are kept.
+    bool keeps_all(bool differentiable) const { return differentiable && !recompute; }
+    bool is_checkpoint(uint32_t k, uint32_t K) const { return k == K || k % checkpoint_interval == 0; }
     const float4* iterate(uint32_t k, uint32_t K, bool differentiable) const {
         if (k == 0) return topology;
+        if (recompute) {
+            if (is_checkpoint(k, K)) return checkpoints[k == K ? (K - 1) / checkpoint_interval : k / checkpoint_interval - 1];
+            return positions[(k - 1) & 1u];
+        }
         if (differentiable) return positions[k - 1];
-        (void)K;
         return positions[(k - 1) & 1u];
     }
 };
@@ -199,6 +214,10 @@ public:
         drop_graphs();
     }
     int read_input_checks(uint32_t* flags);
+    // Checkpoint recomputation (differentiable mode): step caches allocated while it is on keep only
+    // every checkpoint_interval-th Jacobi iterate, and the adjoint and tangent recompute the rest.
+    void set_recompute(bool on) { recompute_ = on; }
+    bool recompute() const { return recompute_; }
     // Times every candidate shape on `repeats` forward steps from `state` (writing `next_state` and
     // the record) and keeps the fastest; returns its per-step milliseconds in `best_ms`.
     int autotune(const pbf_particle_state* state, const pbf_control* control, const pbf_parameters* parameters,
@@ -280,6 +299,27 @@ private:
     friend struct AdjointWorkspace;
     void* adjoint_ = nullptr;  // AdjointWorkspace*, differentiable mode
     void* tangent_ = nullptr;  // TangentWorkspace*, differentiable mode
+    bool recompute_ = false;
+    // One segment of recomputed Jacobi iterations (checkpoint-recompute records): its iterates, their
+    // per-iteration fields and lists, allocated on first use (pbf/pbf.ixx:107-110).
+    struct Segment {
+        DeviceArena arena;
+        uint32_t length = 0;                 // iterations per segment: min(checkpoint interval, K)
+        std::vector<float4*> positions;      // local iterates 1.. (at least 2, the tangent's ping-pong)
+        std::vector<float*> lambda, density;
+        std::vector<float4*> gsum;
+        std::vector<uint32_t*> list_entries, list_counts;
+    };
+    Segment* segment_ = nullptr;
+    int segment_workspace(Segment** out);
+    // Recomputes iterations first .. first + length - 1 of the step in `r` into the segment
+    // workspace: their lists, densities, gradient sums, denominators and lambdas, and the iterates
+    // first + 1 .. first + length - 1 (the last iterate of a segment is a stored checkpoint).
+    int recompute_segment(const StepRecord& r, uint32_t first, uint32_t length);
+    // Iterate first + j of the segment being recomputed.
+    const float4* segment_iterate(const StepRecord& r, uint32_t first, uint32_t j) const {
+        return j == 0 ? r.iterate(first, iterations_, true) : segment_->positions[j - 1];
+    }
 };
 
 int read_profile(Engine& engine, pbf_pass_time* passes, uint32_t capacity, uint32_t* count);

@@ -616,14 +616,53 @@ int Engine::tangent(const pbf_particle_state* state, const StepRecord& r, const 
         pt, ws->x[0], ws->x_state, ws->params_a, ws->params_b);
     timer_.end(stream_, kPassTangentSeed);
     count_launch();
+    const bool keep = r.keeps_all(true);
+    Segment* sg = nullptr;
+    if (!keep)
+        if (int rc = segment_workspace(&sg)) return rc;
     for (uint32_t k = 0; k < K; ++k) {
-        const float4* xk = r.iterate(k, K, true);
-        const StoredList list{r.list_entries[k], r.list_counts[k], r.list_capacity};
-        DensityLambdaJvpArgs dl{gc, list, xk, ws->x[k & 1u], ws->params_a, r.density[k], r.gsum[k], ws->lambda};
+        const float4* xk;
+        StoredList list;
+        const float* lambda_k;
+        const float* density_k;
+        const float4* gsum_k;
+        if (keep) {
+            xk = r.iterate(k, K, true);
+            list = StoredList{r.list_entries[k], r.list_counts[k], r.list_capacity};
+            lambda_k = r.lambda[k];
+            density_k = r.density[k];
+            gsum_k = r.gsum[k];
+        } else {
+            // Checkpoint recomputation: the primal iterations run again in order (pbf/pbf.cpp:198-212),
+            // one at a time in the segment workspace's first slot, the iterates in its two ping-pong
+            // buffers (iterate 0 is x*).
+            xk = k == 0 ? r.topology : sg->positions[(k - 1u) & 1u];
+            list = StoredList{sg->list_entries[0], sg->list_counts[0], kListCapacity};
+            lambda_k = sg->lambda[0];
+            density_k = sg->density[0];
+            gsum_k = sg->gsum[0];
+            ListScanArgs scan{gc, xk, list, 1};
+            if (k > 0) scan.packed = packed_;   // written by the previous primal correction
+            DensityLambdaArgs d{gc, xk, sg->lambda[0], sg->density[0], sg->gsum[0], nullptr, list};
+            if (fuses_density(shape_, scan)) {
+                if (int rc = check(launch_scan_density_lambda(stream_, scan, d, shape_), "recompute: scan + density/lambda"))
+                    return rc;
+            } else {
+                if (int rc = check(launch_list_scan(stream_, scan, shape_), "recompute: neighbour list scan")) return rc;
+                if (int rc = check(launch_density_lambda(stream_, d, shape_.block), "recompute: density/lambda")) return rc;
+            }
+        }
+        DensityLambdaJvpArgs dl{gc, list, xk, ws->x[k & 1u], ws->params_a, density_k, gsum_k, ws->lambda};
         timer_.begin(stream_, kPassDensityLambdaJvp);
         density_lambda_jvp_kernel<<<blocks, block, 0, stream_>>>(dl);
         timer_.end(stream_, kPassDensityLambdaJvp);
-        CorrectionJvpArgs ca{gc, list, xk, ws->x[k & 1u], r.lambda[k], ws->lambda, ws->params_a, ws->params_b, r.mask[k],
+        if (!keep && k + 1u < K) {   // the next primal iterate (the last one, x_K, is kept)
+            CorrectionArgs c{gc, xk, sg->lambda[0], sg->positions[k & 1u], nullptr, 0, Field3{}, r.sorted_index, MutField3{},
+                             nullptr, list};
+            c.packed = packed_;
+            if (int rc = check(launch_correction(stream_, c, shape_.block), "recompute: correction/project")) return rc;
+        }
+        CorrectionJvpArgs ca{gc, list, xk, ws->x[k & 1u], lambda_k, ws->lambda, ws->params_a, ws->params_b, r.mask[k],
                              ws->x[(k + 1u) & 1u], k + 1u == K ? 1 : 0, r.sorted_index, ws->x_state, ws->velocity, out_x};
         timer_.begin(stream_, kPassCorrectionJvp);
         correction_jvp_kernel<<<blocks, block, 0, stream_>>>(ca);
@@ -637,7 +676,7 @@ int Engine::tangent(const pbf_particle_state* state, const StepRecord& r, const 
         count_launch();
     }
     const float4* xK = r.iterate(K, K, true);
-    const StoredList post{r.list_entries[K], r.list_counts[K], r.list_capacity};
+    const StoredList post{r.list_entries[keep ? K : 0u], r.list_counts[keep ? K : 0u], r.list_capacity};
     VorticityJvpArgs va{gc, post, xK, x_dot_K, r.velocity, ws->velocity, r.vorticity, ws->vorticity};
     timer_.begin(stream_, kPassVorticityJvp);
     vorticity_jvp_kernel<<<blocks, block, 0, stream_>>>(va);

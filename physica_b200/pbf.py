@@ -222,6 +222,8 @@ def library() -> ctypes.CDLL:
         lib.pbf_batch_scene_sums.argtypes = [vp, vp, vp]
         lib.pbf_batch_set_graph_mode.argtypes = [vp, ctypes.c_int]
         lib.pbf_set_graph_mode.argtypes = [vp, ctypes.c_int]
+        lib.pbf_set_checkpoint_recompute.argtypes = [vp, ctypes.c_int]
+        lib.pbf_batch_set_checkpoint_recompute.argtypes = [vp, ctypes.c_int]
         lib.pbf_sum_compensated.argtypes = [vp, vp, ctypes.c_uint32, vp]
         lib.pbf_profile_enable.argtypes = [vp, ctypes.c_int]
         lib.pbf_batch_profile_enable.argtypes = [vp, ctypes.c_int]
@@ -567,6 +569,11 @@ class PBF:
         """Replay the forward launch sequence as a CUDA graph per buffer set."""
         check(library().pbf_set_graph_mode(self.handle, 1 if enable else 0))
 
+    def set_checkpoint_recompute(self, enable: bool = True):
+        """Step caches allocated afterwards keep every checkpoint_interval-th Jacobi iterate only;
+        vjp_step / jvp_step recompute the rest (the reference's StepCache::checkpoints)."""
+        check(library().pbf_set_checkpoint_recompute(self.handle, 1 if enable else 0))
+
     def export_frame(self, state: State, cache: "StepCache | None" = None) -> dict:
         """Frame of `state` for a viewer or a file dump: positions and velocities as (N, 3) float32,
         and, with the step cache that produced `state`, the vorticity magnitudes (N,)."""
@@ -709,6 +716,10 @@ class Batch:
 
     def set_graph_mode(self, enable: bool = True):
         check(library().pbf_batch_set_graph_mode(self.handle, 1 if enable else 0))
+
+    def set_checkpoint_recompute(self, enable: bool = True):
+        """Cache slots reserved afterwards keep every checkpoint_interval-th Jacobi iterate only."""
+        check(library().pbf_batch_set_checkpoint_recompute(self.handle, 1 if enable else 0))
 
     def set_input_checks(self, enable: bool = True):
         check(library().pbf_batch_set_input_checks(self.handle, 1 if enable else 0))
