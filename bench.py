@@ -429,29 +429,49 @@ def fixed_shape(text: str):
 
 
 def bench_grad(args, world, rank):
+    """grad-steps/s of the 64k rollout, with every Jacobi iterate kept (the default) and with the
+    reference's in-step checkpoints (checkpoint_interval 2, the iterations between recomputed)."""
     from physica_b200 import pbf, scenes, trajectory
     sc = scenes.differentiable(seed=3 + rank)
-    solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
     targets = torch.from_numpy(sc.targets).cuda()
     steps = 20
-    if args.launch_shape:
-        shape = fixed_shape(args.launch_shape)
-        solver.launch_shape = shape
-    else:
-        shape, _ = solver.autotune(state, control, params, repeats=2)
-    solver.set_graph_mode(True)
-    rollout = trajectory.Rollout(solver, control, params, steps, 10)   # buffers allocated once, outside the timing
-    trajectory.loss_and_gradients(solver, state, control, params, targets, steps, rollout=rollout)   # warm-up
-    torch.cuda.synchronize()
-    barrier(world)
-    a = torch.cuda.Event(enable_timing=True)
-    b = torch.cuda.Event(enable_timing=True)
-    a.record(solver.stream)
-    g = trajectory.loss_and_gradients(solver, state, control, params, targets, steps, rollout=rollout)
-    b.record(solver.stream)
-    torch.cuda.synchronize()
-    ms = max_over_ranks(a.elapsed_time(b), world)
+
+    def run(recompute, shape=None):
+        solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable,
+                                                              checkpoint_interval=2 if recompute else 1)
+        if shape is not None:
+            solver.launch_shape = shape
+        elif args.launch_shape:
+            solver.launch_shape = fixed_shape(args.launch_shape)
+        else:
+            solver.autotune(state, control, params, repeats=2)
+        solver.set_checkpoint_recompute(recompute)
+        solver.set_graph_mode(True)
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        rollout = trajectory.Rollout(solver, control, params, steps, 10)   # buffers allocated once, outside the timing
+        g = trajectory.loss_and_gradients(solver, state, control, params, targets, steps, rollout=rollout)   # warm-up
+        torch.cuda.synchronize()
+        held = free0 - torch.cuda.mem_get_info()[0]
+        barrier(world)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(solver.stream)
+        g = trajectory.loss_and_gradients(solver, state, control, params, targets, steps, rollout=rollout)
+        b.record(solver.stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(a.elapsed_time(b), world)
+        shape = solver.launch_shape
+        del rollout, solver
+        return ms, g, shape, held
+
+    ms, g, shape, held = run(False)
+    ms_r, g_r, _, held_r = run(True, shape)
     return {"value": round(world * steps / (ms * 1e-3), 3), "unit": "grad-steps/s",
+            "rollout_memory_bytes": held,
+            "checkpoint_recompute": {"value": round(world * steps / (ms_r * 1e-3), 3), "unit": "grad-steps/s",
+                                     "in_step_checkpoint_interval": 2, "rollout_memory_bytes": held_r,
+                                     "same_gradient": bool(torch.equal(g.initial_velocities, g_r.initial_velocities))},
             "config": {"workload": "differentiable_64k: 65,536 particles (32x64x32 lattice), v0 ~ N(0, 0.1), "
                                    "4 iterations, target-cloud loss", "rollout_steps": steps,
                        "trajectory_checkpoint_every": 10, "graphs": True,
