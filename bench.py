@@ -246,15 +246,17 @@ def bench_b200(args, world, rank):
 
     # throughput past the ejections (they start at substep 27): advance the scene to substep 97,
     # then time 20 more substeps after 3 warm-up ones, the same way
-    done = args.warmup + args.steps + 3
-    for _ in range(max(0, 97 - done)):
-        step()
-    ms_late, _ = timed(step, 20, 3, world, stream, flush)
-    ms_late = max_over_ranks(ms_late, world) / 20
-    first_late = max(done, 97) + 3
-    late = {"substeps": f"{first_late}-{first_late + 20}", "ms_per_step": round(ms_late, 4),
-            "value": round(world * n / (ms_late * 1e-3), 1), "unit": UNIT,
-            "mean_neighbors": round(float(cache.read(CacheField.NEIGHBOR_COUNTS).double().mean()), 3)}
+    late = None
+    if not args.no_late:
+        done = args.warmup + args.steps + 3
+        for _ in range(max(0, 97 - done)):
+            step()
+        ms_late, _ = timed(step, 20, 3, world, stream, flush)
+        ms_late = max_over_ranks(ms_late, world) / 20
+        first_late = max(done, 97) + 3
+        late = {"substeps": f"{first_late}-{first_late + 20}", "ms_per_step": round(ms_late, 4),
+                "value": round(world * n / (ms_late * 1e-3), 1), "unit": UNIT,
+                "mean_neighbors": round(float(cache.read(CacheField.NEIGHBOR_COUNTS).double().mean()), 3)}
     K = sc.pressure_iterations
     cells = solver.cells
     bytes_per_particle = {"list_scan": 16, "density_lambda": 16, "correction_project": 28, "vorticity": 36, "normal_confinement": 48,
@@ -1090,6 +1092,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-sph", action="store_true", help="skip the SPH family's substeps")
+    ap.add_argument("--no-late", action="store_true", help="skip the window timed after substep 100 (profiling)")
     ap.add_argument("--sph-only", default="", help="time only these SPH methods (comma list, e.g. pcisph) and print "
                                                    "their line (profiling)")
     ap.add_argument("--grad-only", action="store_true", help="time only the 64k differentiable rollout and print its "
