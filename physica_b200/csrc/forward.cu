@@ -460,9 +460,18 @@ __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLam
 // (the rest, if any, from the stored list).  The list, its order and every sum are those of the
 // two-kernel path, so the results are bit-identical.  Scenes with boundary particles use the two
 // kernels.
-constexpr uint32_t kStagedEntries = 48;   // 24 KB of shared memory per 128-thread block
+// Staged entries per lane and the blocks per SM the register budget is sized for (compile-time
+// tuning knobs; the defaults measured fastest at 1M particles).
+#ifndef PBF_FUSED_STAGED_ENTRIES
+#define PBF_FUSED_STAGED_ENTRIES 48
+#endif
+#ifndef PBF_FUSED_MIN_BLOCKS
+#define PBF_FUSED_MIN_BLOCKS 8
+#endif
+constexpr uint32_t kStagedEntries = PBF_FUSED_STAGED_ENTRIES;   // 48: 24 KB of shared memory per 128-thread block
 
-__global__ void __launch_bounds__(kBlock, 8) scan_density_lambda_kernel(const ListScanArgs a, const DensityLambdaArgs d) {
+__global__ void __launch_bounds__(kBlock, PBF_FUSED_MIN_BLOCKS) scan_density_lambda_kernel(const ListScanArgs a,
+                                                                                          const DensityLambdaArgs d) {
     __shared__ uint32_t staged[kStagedEntries][kBlock];
     const Particle p = locate(a.g);
     if (!p.active) return;
