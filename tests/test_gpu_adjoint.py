@@ -225,14 +225,14 @@ def test_rollout_reuse_and_graph_mode_give_identical_gradients():
 
 
 def test_benchmark_rollout_gradient_matches_reference_rollout():
-    """The 65,536-particle gradient benchmark (20 steps, 4 iterations, trajectory checkpoints every
-    10): the checkpointed rollout gradient equals the one chained through the reference's own
-    forward_step / vjp_step to FP64 rounding."""
+    """The 65,536-particle differentiable configuration at its full length (60 steps, 4 iterations,
+    trajectory checkpoints every 10): the checkpointed rollout gradient equals the one chained
+    through the reference's own forward_step / vjp_step to FP64 rounding."""
     from oracle import reference
     if not reference.available():
         pytest.skip("reference kernels (oracle/_ref) not built")
     sc = scenes.differentiable()
-    steps, every = 20, 10
+    steps, every = 60, 10
     n = sc.count
     targets = torch.from_numpy(sc.targets).cuda()
     solver, state, control, params = pbf.solver_for_scene(sc, mode=pbf.ExecutionMode.differentiable, checkpoint_interval=1)
@@ -269,6 +269,8 @@ def test_benchmark_rollout_gradient_matches_reference_rollout():
             refs[j].vjp_step(xs[j], vs[j], adj, prev, ctrl, pa)
             adj = prev
     torch.cuda.synchronize()
+    print("relative differences:", rel(mine.initial_positions.cpu().numpy(), adj["positions"].cpu().numpy()),
+          rel(mine.initial_velocities.cpu().numpy(), adj["velocities"].cpu().numpy()))
     assert rel(mine.initial_positions.cpu().numpy(), adj["positions"].cpu().numpy()) < 1e-7
     assert rel(mine.initial_velocities.cpu().numpy(), adj["velocities"].cpu().numpy()) < 1e-7
     assert rel(mine.controls.cpu().numpy(), ctrl.cpu().numpy()) < 1e-7
