@@ -541,13 +541,51 @@ def bench_batch(args, world, rank):
 
     ms_l, _ = timed(loop_step, steps, 3, world, solvers[0][0].stream, flush)
     ms_l = max_over_ranks(ms_l, world) / steps
-    return {"unit": UNIT, "batched": round(world * total / (ms_b * 1e-3), 1),
+    del solvers
+    buckets = bucket_shapes(scs, shape, world, flush)
+    return {"unit": UNIT, "batched": round(world * total / (ms_b * 1e-3), 1), "count_buckets": buckets,
             "per_scene_solvers": round(world * total / (ms_l * 1e-3), 1), "speedup": round(ms_l / ms_b, 3),
             "batched_ms_per_step": round(ms_b, 4), "per_scene_ms_per_step": round(ms_l, 4),
             "config": {"workload": "batched_forward_256: 256 dam-break scenes, counts log-uniform in [2048, 65536], "
                                    "4 iterations", "particles_per_gpu": total, "scenes_per_gpu": len(scs),
                        "graphs": True, "launch_shape": {"list_scan": SCAN_VARIANTS[shape.list_scan],
                                                          "scan_block": shape.scan_block_size, "block": shape.block_size}}}
+
+
+def bucket_shapes(scs, shape, world, flush):
+    """Per particle-count bucket (powers of two): the bucket's scenes as a batch of their own, timed
+    with the shape its own autotuning picks and with the whole batch's shape.  One batch runs one
+    launch per pass over all its scenes, so it runs one shape; this shows what a shape per bucket
+    would gain."""
+    from physica_b200 import pbf
+    out = {}
+    edges = [2048, 4096, 8192, 16384, 32768, 65537]
+    for lo, hi in zip(edges[:-1], edges[1:]):
+        sub = [s for s in scs if lo <= s.count < hi]
+        if not sub:
+            continue
+        b, st, ct, pr = pbf.batch_for_scenes(sub)
+        own, _ = b.autotune(st, ct, pr, repeats=2)
+        b.set_graph_mode(True)
+
+        def time_shape(sh):
+            b.launch_shape = sh
+            h = {"cur": pbf.State(st.positions.clone(), st.velocities.clone(), 0), "nxt": b.allocate_state()}
+
+            def stp():
+                b.forward_step(h["cur"], ct, pr, h["nxt"])
+                h["cur"], h["nxt"] = h["nxt"], h["cur"]
+
+            ms, _ = timed(stp, 5, 3, world, b.stream, flush)
+            return max_over_ranks(ms, world) / 5
+
+        own_ms, batch_ms = time_shape(own), time_shape(shape)
+        out[f"{lo}-{hi - 1}"] = {"scenes": len(sub), "particles": sum(s.count for s in sub),
+                                 "own_shape": [SCAN_VARIANTS[own.list_scan], own.scan_block_size, own.block_size],
+                                 "own_ms_per_step": round(own_ms, 4), "batch_shape_ms_per_step": round(batch_ms, 4),
+                                 "batch_shape_over_own": round(batch_ms / own_ms, 4)}
+        del b, st, ct, pr
+    return out
 
 
 def bench_batch_grad(args, world, rank):
