@@ -293,6 +293,11 @@ struct PBF final {
     PBF(PBF&&) = delete;
     PBF& operator=(PBF&&) = delete;
 
+    // Step caches allocated afterwards keep every checkpoint_interval-th Jacobi iterate only, as the
+    // reference's StepCache does, and vjp_step / jvp_step recompute the iterations in between
+    // (differentiable mode; off by default: every iterate kept).
+    void set_checkpoint_recompute(bool enable) { detail::check(pbf_set_checkpoint_recompute(handle_, enable ? 1 : 0)); }
+
     [[nodiscard]] State allocate_state() const {
         return {{detail::vector_field(count_, stream_), detail::vector_field(count_, stream_), 0u}};
     }
