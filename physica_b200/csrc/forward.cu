@@ -462,13 +462,15 @@ __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLam
 // kernels.
 // Staged entries per lane and the blocks per SM the register budget is sized for (compile-time
 // tuning knobs; the defaults measured fastest at 1M particles).
+// At 1M particles (steps 3-13 of the dam break, ms per launch): 9 blocks and 40 entries 0.336;
+// 8 and 32 0.341; 8 and 48 0.360; 10 and 40 (spilling) 0.400; 8 and 64 0.410; 12 and 32 0.513.
 #ifndef PBF_FUSED_STAGED_ENTRIES
-#define PBF_FUSED_STAGED_ENTRIES 48
+#define PBF_FUSED_STAGED_ENTRIES 40
 #endif
 #ifndef PBF_FUSED_MIN_BLOCKS
-#define PBF_FUSED_MIN_BLOCKS 8
+#define PBF_FUSED_MIN_BLOCKS 9
 #endif
-constexpr uint32_t kStagedEntries = PBF_FUSED_STAGED_ENTRIES;   // 48: 24 KB of shared memory per 128-thread block
+constexpr uint32_t kStagedEntries = PBF_FUSED_STAGED_ENTRIES;   // 40: 20 KB of shared memory per 128-thread block
 
 __global__ void __launch_bounds__(kBlock, PBF_FUSED_MIN_BLOCKS) scan_density_lambda_kernel(const ListScanArgs a,
                                                                                           const DensityLambdaArgs d) {

@@ -113,6 +113,28 @@ __device__ __forceinline__ void replay(Op& op, const Particle& p, const GatherCo
     }
     const uint32_t* __restrict__ entries = list.entries + list_row(p.s, list.capacity);
     if (n == 0) return;
+#ifndef PBF_REPLAY_INDEX_DEPTH
+#define PBF_REPLAY_INDEX_DEPTH 2
+#endif
+#if PBF_REPLAY_INDEX_DEPTH >= 2
+    // Pipeline: the indices of entries k+1 and k+2 and the data of entry k are in flight while
+    // entry k-1 is applied.  The indices come from the stored list, which a replay after another
+    // pass reads from DRAM; two entries of lead cover that latency.
+    uint32_t t = entries[0];
+    uint32_t tn = n > 1u ? entries[32] : 0u;
+    uint32_t tnn = n > 2u ? entries[64] : 0u;
+    auto data = op.prefetch(t);
+    for (uint32_t k = 1; k < n; ++k) {
+        const uint32_t t3 = k + 2u < n ? entries[static_cast<size_t>(k + 2u) * 32u] : 0u;
+        const auto next = op.prefetch(tn);
+        op.apply(t, data);
+        t = tn;
+        tn = tnn;
+        tnn = t3;
+        data = next;
+    }
+    op.apply(t, data);
+#else
     // Two-stage pipeline: the index of entry k+1 and the data of entry k are in flight while
     // entry k-1 is applied.
     uint32_t t = entries[0];
@@ -127,6 +149,7 @@ __device__ __forceinline__ void replay(Op& op, const Particle& p, const GatherCo
         data = next;
     }
     op.apply(t, data);
+#endif
 }
 
 }  // namespace gather_detail
