@@ -368,7 +368,7 @@ def bench_b200(args, world, rank):
     }
 
 
-def read_profile(lib, handle):
+def read_profile(lib, handle, batch=False):
     import ctypes
     from physica_b200 import pbf
 
@@ -377,8 +377,9 @@ def read_profile(lib, handle):
 
     arr = (PassTime * 32)()
     cnt = ctypes.c_uint32()
-    lib.pbf_profile_read.argtypes = [ctypes.c_void_p, ctypes.POINTER(PassTime), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
-    pbf.check(lib.pbf_profile_read(handle, arr, 32, ctypes.byref(cnt)))
+    fn = lib.pbf_batch_profile_read if batch else lib.pbf_profile_read
+    fn.argtypes = [ctypes.c_void_p, ctypes.POINTER(PassTime), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+    pbf.check(fn(handle, arr, 32, ctypes.byref(cnt)))
     return [{"name": arr[k].name.decode(), "launches": int(arr[k].launches), "ms": float(arr[k].milliseconds)}
             for k in range(cnt.value)]
 
@@ -591,6 +592,7 @@ def bucket_shapes(scs, shape, world, flush):
 def bench_batch_grad(args, world, rank):
     """32 differentiable scenes (16,384-131,072 particles, uniform), each with its own target-cloud
     loss: one checkpointed batched rollout against one rollout per scene, CUDA events on the stream."""
+    import ctypes
     import gc
     from physica_b200 import pbf, scenes, trajectory
     scs = scenes.batched_adjoint(seed=5 + rank)
@@ -616,6 +618,16 @@ def bench_batch_grad(args, world, rank):
     targets = torch.from_numpy(np.concatenate([s.targets for s in scs], axis=1)).cuda()
     barrier(world)
     ms_b = max_over_ranks(timed_rollout(batch, state, control, params, targets), world)
+    # where the batched rollout's time goes: one more rollout with per-pass CUDA events (no graphs)
+    lib = pbf.library()
+    lib.pbf_batch_profile_enable.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.pbf_batch_profile_enable(batch.handle, 1)
+    trajectory.loss_and_gradients(batch, state, control, params, targets, steps, every)
+    passes = read_profile(lib, batch.handle, batch=True)
+    lib.pbf_batch_profile_enable(batch.handle, 0)
+    total_pass_ms = sum(q["ms"] for q in passes) or 1.0
+    pass_shares = {q["name"]: {"ms": round(q["ms"], 3), "share": round(q["ms"] / total_pass_ms, 4)}
+                   for q in sorted(passes, key=lambda q: -q["ms"])}
     del batch, state, control, params, targets
     gc.collect()
     torch.cuda.synchronize()
@@ -631,6 +643,7 @@ def bench_batch_grad(args, world, rank):
     return {"unit": "grad-steps/s", "batched": round(world * steps / (ms_b * 1e-3), 3),
             "per_scene_rollouts": round(world * steps / (ms_l * 1e-3), 3), "speedup": round(ms_l / ms_b, 3),
             "particle_grad_steps_per_s": round(world * total * steps / (ms_b * 1e-3), 1),
+            "batched_passes": pass_shares,
             "config": {"workload": "batched_adjoint_32: 32 dam-break scenes, counts uniform in [16384, 131072], "
                                    "v0 ~ N(0, 0.1), 4 iterations, per-scene target-cloud loss and dL/dc_s",
                        "particles_per_gpu": total, "scenes_per_gpu": len(scs), "rollout_steps": steps,

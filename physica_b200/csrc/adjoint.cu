@@ -856,6 +856,10 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
               parameter_adjoint->vorticity_confinement};
     }
     const GatherCommon gc = gather_common(r);
+    // Passes that replay the same list run in alternating block orders, each starting on the entries
+    // the previous pass read last (still in L2).
+    GatherCommon gc_reverse = gc;
+    gc_reverse.reverse = 1;
     const AdjField3 prev_x{previous_adjoint->positions.x, previous_adjoint->positions.y, previous_adjoint->positions.z};
     const AdjField3 prev_v{previous_adjoint->velocities.x, previous_adjoint->velocities.y, previous_adjoint->velocities.z};
     const AdjField3 ctrl{control_adjoint->external_accelerations.x, control_adjoint->external_accelerations.y,
@@ -877,7 +881,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
     timer_.begin(stream_, kPassXsphVjp);
     xsph_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(xa);
     timer_.end(stream_, kPassXsphVjp);
-    NormalVjpArgs na{gc, post_list, xK, r.vorticity, ws->eta, ws->x[0], ws->vorticity};
+    NormalVjpArgs na{gc_reverse, post_list, xK, r.vorticity, ws->eta, ws->x[0], ws->vorticity};
     timer_.begin(stream_, kPassNormalVjp);
     normal_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(na);
     timer_.end(stream_, kPassNormalVjp);
@@ -920,7 +924,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
         timer_.begin(stream_, kPassCorrectionVjp);
         correction_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(ca);
         timer_.end(stream_, kPassCorrectionVjp);
-        LambdaVjpArgs la{gc, it_list, r.sorted_index, xk, density_k, gsum_k, ws->lambda, acc, ws->density, pa};
+        LambdaVjpArgs la{gc_reverse, it_list, r.sorted_index, xk, density_k, gsum_k, ws->lambda, acc, ws->density, pa};
         timer_.begin(stream_, kPassLambdaVjp);
         lambda_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(la);
         timer_.end(stream_, kPassLambdaVjp);

@@ -576,7 +576,11 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
             if (int rc = check(launch_density_lambda(stream, d, shape_.block), "density/lambda")) return rc;
             timer_.end(stream, kPassDensityLambda);
         }
-        CorrectionArgs c{gc, xk, lam, xk1, diff ? r.mask[k] : nullptr, k + 1 == K ? 1 : 0, previous, r.sorted_index,
+        // The correction replays the list the scan has just written, last particles first (their
+        // entries are the ones still in L2).
+        GatherCommon gc_reverse = gc;
+        gc_reverse.reverse = 1;
+        CorrectionArgs c{gc_reverse, xk, lam, xk1, diff ? r.mask[k] : nullptr, k + 1 == K ? 1 : 0, previous, r.sorted_index,
                          out_positions, r.velocity, list};
         c.packed = packed_;
         timer_.begin(stream, kPassCorrection);
@@ -605,7 +609,11 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
     post_scan.packed = packed_;
     if (int rc = check(launch_list_scan(stream, post_scan, shape_), "neighbour list scan")) return rc;
     timer_.end(stream, kPassListScan);
-    VorticityArgs v{gc, xK, r.velocity, r.vorticity, post};
+    // The three post-loop passes replay one list in alternating directions, each starting where the
+    // previous one ended.
+    GatherCommon gc_reverse = gc;
+    gc_reverse.reverse = 1;
+    VorticityArgs v{gc_reverse, xK, r.velocity, r.vorticity, post};
     timer_.begin(stream, kPassVorticity);
     if (int rc = check(launch_vorticity(stream, v, shape_.block), "vorticity")) return rc;
     timer_.end(stream, kPassVorticity);
@@ -613,8 +621,8 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
     timer_.begin(stream, kPassNormal);
     if (int rc = check(launch_normal(stream, nm, shape_.block), "normal/confinement")) return rc;
     timer_.end(stream, kPassNormal);
-    XsphArgs x{gc, xK, r.confined, r.sorted_index, {next_state->velocities.x, next_state->velocities.y, next_state->velocities.z},
-               post};
+    XsphArgs x{gc_reverse, xK, r.confined, r.sorted_index,
+               {next_state->velocities.x, next_state->velocities.y, next_state->velocities.z}, post};
     timer_.begin(stream, kPassXsph);
     if (int rc = check(launch_xsph(stream, x, shape_.block), "xsph")) return rc;
     timer_.end(stream, kPassXsph);

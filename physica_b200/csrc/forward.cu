@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLam
     op.denominator = pa.y;  // relaxation
     op.neighbors = 0;
     op.ratio.reset(xi.w, op.rest_density);
-    replay(op, p, a.g, a.list);
+    replay<2>(op, p, a.g, a.list);
     const float denominator = __fadd_rn(op.denominator, sq_yfirst(op.gradient_sum));
     a.lambda[p.s] = __fdiv_rn(-__fsub_rn(__fdiv_rn(op.density, op.rest_density), 1.0F), denominator);
     if (a.density) a.density[p.s] = op.density;
@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs
     op.artificial_full = pb.x != 0.0F;
     op.reference_weight = op.artificial_full ? poly6(mk(pb.z, 0.0F, 0.0F), p.k) : 1.0F;
     op.correction = mk(0.0F, 0.0F, 0.0F);
-    replay(op, p, a.g, a.list);
+    replay<2>(op, p, a.g, a.list);
     const Box& box = p.scene->box;
     const f3 candidate = add(op.x, op.correction);
     uint32_t mask = 0u;
@@ -711,7 +711,7 @@ __global__ void __launch_bounds__(kBlock) vorticity_kernel(const VorticityArgs a
     op.x = xyz(a.pos[p.s]);
     op.v = xyz(a.velocity[p.s]);
     op.vorticity = mk(0.0F, 0.0F, 0.0F);
-    replay(op, p, a.g, a.list);
+    replay<2>(op, p, a.g, a.list);
     a.vorticity[p.s] = make_float4(op.vorticity.x, op.vorticity.y, op.vorticity.z, __fsqrt_rn(sq_xfirst(op.vorticity)));
 }
 
@@ -754,7 +754,7 @@ __global__ void __launch_bounds__(kBlock) normal_kernel(const NormalArgs a) {
     op.x = xyz(a.pos[p.s]);
     op.magnitude = wi.w;
     op.gradient = mk(0.0F, 0.0F, 0.0F);
-    replay(op, p, a.g, a.list);
+    replay<2>(op, p, a.g, a.list);
     const float normalizer = __fsqrt_rn(sq_yfirst(op.gradient));
     const f3 normal = normalizer > 0.0F ? scale(op.gradient, __fdiv_rn(1.0F, normalizer)) : mk(0.0F, 0.0F, 0.0F);
     a.normal[p.s] = make_float4(normal.x, normal.y, normal.z, normalizer);
@@ -796,7 +796,7 @@ __global__ void __launch_bounds__(kBlock) xsph_kernel(const XsphArgs a) {
     op.x = xyz(a.pos[p.s]);
     op.v = xyz(a.confined[p.s]);
     op.smoothing = mk(0.0F, 0.0F, 0.0F);
-    replay(op, p, a.g, a.list);
+    replay<2>(op, p, a.g, a.list);
     const float viscosity = a.g.params_a[p.s].z;
     const f3 out = fma3(viscosity, op.smoothing, op.v);
     const uint32_t i = a.sorted_index[p.s];

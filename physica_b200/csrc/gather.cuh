@@ -58,7 +58,8 @@ __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
 __device__ __forceinline__ Particle locate(const GatherCommon& g) {
     Particle p;
-    p.s = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t block = g.reverse ? gridDim.x - 1u - blockIdx.x : blockIdx.x;
+    p.s = block * blockDim.x + threadIdx.x;
     p.active = p.s < g.count;
     p.c = p.active ? g.cell[p.s] : make_int4(0, 0, 0, 0);
     p.scene = g.scenes + p.c.w;
@@ -102,8 +103,9 @@ __device__ void walk(Op& op, const Particle& p, const GatherCommon& g) {
 }
 
 // Drain this lane's stored list in order.  Op::prefetch(t) starts the loads of entry t and
-// returns them; Op::apply(t, data) consumes them.
-template <class Op>
+// returns them; Op::apply(t, data) consumes them.  IndexLead: how many list indices ahead of the
+// applied entry are loaded (1 or 2).
+template <int IndexLead = 1, class Op>
 __device__ __forceinline__ void replay(Op& op, const Particle& p, const GatherCommon& g, const StoredList& list) {
     if (!p.active) return;
     const uint32_t n = list.counts[p.s];
@@ -113,43 +115,40 @@ __device__ __forceinline__ void replay(Op& op, const Particle& p, const GatherCo
     }
     const uint32_t* __restrict__ entries = list.entries + list_row(p.s, list.capacity);
     if (n == 0) return;
-#ifndef PBF_REPLAY_INDEX_DEPTH
-#define PBF_REPLAY_INDEX_DEPTH 2
-#endif
-#if PBF_REPLAY_INDEX_DEPTH >= 2
-    // Pipeline: the indices of entries k+1 and k+2 and the data of entry k are in flight while
-    // entry k-1 is applied.  The indices come from the stored list, which a replay after another
-    // pass reads from DRAM; two entries of lead cover that latency.
-    uint32_t t = entries[0];
-    uint32_t tn = n > 1u ? entries[32] : 0u;
-    uint32_t tnn = n > 2u ? entries[64] : 0u;
-    auto data = op.prefetch(t);
-    for (uint32_t k = 1; k < n; ++k) {
-        const uint32_t t3 = k + 2u < n ? entries[static_cast<size_t>(k + 2u) * 32u] : 0u;
-        const auto next = op.prefetch(tn);
+    if constexpr (IndexLead >= 2) {
+        // Pipeline: the indices of entries k+1 and k+2 and the data of entry k are in flight while
+        // entry k-1 is applied.  The indices come from the stored list, which a replay after another
+        // pass reads from DRAM; two entries of lead cover that latency.
+        uint32_t t = entries[0];
+        uint32_t tn = n > 1u ? entries[32] : 0u;
+        uint32_t tnn = n > 2u ? entries[64] : 0u;
+        auto data = op.prefetch(t);
+        for (uint32_t k = 1; k < n; ++k) {
+            const uint32_t t3 = k + 2u < n ? entries[static_cast<size_t>(k + 2u) * 32u] : 0u;
+            const auto next = op.prefetch(tn);
+            op.apply(t, data);
+            t = tn;
+            tn = tnn;
+            tnn = t3;
+            data = next;
+        }
         op.apply(t, data);
-        t = tn;
-        tn = tnn;
-        tnn = t3;
-        data = next;
-    }
-    op.apply(t, data);
-#else
-    // Two-stage pipeline: the index of entry k+1 and the data of entry k are in flight while
-    // entry k-1 is applied.
-    uint32_t t = entries[0];
-    uint32_t tn = n > 1u ? entries[32] : 0u;
-    auto data = op.prefetch(t);
-    for (uint32_t k = 1; k < n; ++k) {
-        const uint32_t tnn = k + 1u < n ? entries[static_cast<size_t>(k + 1u) * 32u] : 0u;
-        const auto next = op.prefetch(tn);
+    } else {
+        // Two-stage pipeline: the index of entry k+1 and the data of entry k are in flight while
+        // entry k-1 is applied.
+        uint32_t t = entries[0];
+        uint32_t tn = n > 1u ? entries[32] : 0u;
+        auto data = op.prefetch(t);
+        for (uint32_t k = 1; k < n; ++k) {
+            const uint32_t tnn = k + 1u < n ? entries[static_cast<size_t>(k + 1u) * 32u] : 0u;
+            const auto next = op.prefetch(tn);
+            op.apply(t, data);
+            t = tn;
+            tn = tnn;
+            data = next;
+        }
         op.apply(t, data);
-        t = tn;
-        tn = tnn;
-        data = next;
     }
-    op.apply(t, data);
-#endif
 }
 
 }  // namespace gather_detail

@@ -601,6 +601,10 @@ int Engine::tangent(const pbf_particle_state* state, const StepRecord& r, const 
               parameter_tangent->vorticity_confinement};
     }
     const GatherCommon gc = gather_common(r);
+    // Passes that replay the same list run in alternating block orders, each starting on the entries
+    // the previous pass read last (still in L2).
+    GatherCommon gc_reverse = gc;
+    gc_reverse.reverse = 1;
     const unsigned block = shape_.block;
     const unsigned blocks = blocks_of(n, block);
     const MutField3 out_x{next_state_tangent->positions.x, next_state_tangent->positions.y, next_state_tangent->positions.z};
@@ -662,7 +666,7 @@ int Engine::tangent(const pbf_particle_state* state, const StepRecord& r, const 
             c.packed = packed_;
             if (int rc = check(launch_correction(stream_, c, shape_.block), "recompute: correction/project")) return rc;
         }
-        CorrectionJvpArgs ca{gc, list, xk, ws->x[k & 1u], lambda_k, ws->lambda, ws->params_a, ws->params_b, r.mask[k],
+        CorrectionJvpArgs ca{gc_reverse, list, xk, ws->x[k & 1u], lambda_k, ws->lambda, ws->params_a, ws->params_b, r.mask[k],
                              ws->x[(k + 1u) & 1u], k + 1u == K ? 1 : 0, r.sorted_index, ws->x_state, ws->velocity, out_x};
         timer_.begin(stream_, kPassCorrectionJvp);
         correction_jvp_kernel<<<blocks, block, 0, stream_>>>(ca);
@@ -681,7 +685,7 @@ int Engine::tangent(const pbf_particle_state* state, const StepRecord& r, const 
     timer_.begin(stream_, kPassVorticityJvp);
     vorticity_jvp_kernel<<<blocks, block, 0, stream_>>>(va);
     timer_.end(stream_, kPassVorticityJvp);
-    NormalJvpArgs na{gc, post, xK, x_dot_K, r.vorticity, ws->vorticity, r.normal, ws->velocity, ws->params_b, ws->confined};
+    NormalJvpArgs na{gc_reverse, post, xK, x_dot_K, r.vorticity, ws->vorticity, r.normal, ws->velocity, ws->params_b, ws->confined};
     timer_.begin(stream_, kPassNormalJvp);
     normal_jvp_kernel<<<blocks, block, 0, stream_>>>(na);
     timer_.end(stream_, kPassNormalJvp);

@@ -75,6 +75,9 @@ struct GatherCommon {
     // cell-sorted boundary array and its entries (position at the step's time, volume).
     const uint32_t* boundary_offsets = nullptr;
     const float4* boundary = nullptr;
+    // Hand the blocks out last particles first.  A pass that replays the list the previous pass wrote
+    // (or read) front to back then starts on the entries still in L2.  Results do not depend on it.
+    int reverse = 0;
 };
 
 // Boundary particles (neighborhood/neighborhood.cu:63-69): keyed and sorted into the same cells
