@@ -418,7 +418,7 @@ def issue_roofline(kernel: str, launch_ms: float):
             "frac": round(achieved / peak, 4), "warp_instructions": instructions}
 
 
-SCAN_VARIANTS = ["per_lane", "cooperative", "staged", "fused_density"]   # pbf_launch_shape.list_scan 0..3
+SCAN_VARIANTS = ["per_lane", "cooperative", "staged", "fused_density", "fused_masks"]   # pbf_launch_shape.list_scan 0..4
 
 
 def fixed_shape(text: str):

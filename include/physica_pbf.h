@@ -153,7 +153,8 @@ typedef struct pbf_step_cache pbf_step_cache;  /* PBF::StepCache (pbf/pbf.ixx:54
 typedef struct pbf_batch pbf_batch;            /* many independent scenes in one launch sequence (no reference counterpart) */
 typedef struct pbf_launch_shape {
     uint32_t list_scan;         /* 0: per-lane walk, 1: warp-cooperative scan, 2: shared-memory staged walk,
-                                   3: per-lane walk with density + lambda in the same kernel */
+                                   3: per-lane walk with density + lambda in the same kernel,
+                                   4: as 3, with hit-mask neighbour lists in forward mode */
     uint32_t scan_block_size;   /* threads per block of the list scan: 32, 64, 96 or 128 */
     uint32_t block_size;        /* threads per block of the gather passes: 32, 64, 96 or 128 */
 } pbf_launch_shape;
@@ -339,8 +340,11 @@ int pbf_forward_step_preallocated(const pbf_domain_configuration* domain, const 
  *      candidates once, 2 = each lane walks its stencil in a shared-memory copy of its warp's
  *      stencil columns, 3 = as 0, and each Jacobi iteration's scan also computes density and lambda
  *      in the same kernel, replaying the list from shared memory (scenes with boundary particles run
- *      3 as 0); scan_block_size and block_size: 32, 64, 96 or 128 threads.  pbf_autotune
- *      times the sixteen list-scan shapes by their scan and density + lambda time, then the gather block sizes by the
+ *      3 as 0), 4 = as 3, and a forward-mode step stores each neighbour list as hit masks (one
+ *      slot base and 32-bit mask per stencil block with a neighbour) instead of one index per
+ *      neighbour (differentiable steps and scenes with boundary particles store index lists);
+ *      scan_block_size and block_size: 32, 64, 96 or 128 threads.  pbf_autotune
+ *      times the twenty list-scan shapes by their scan and density + lambda time, then the gather block sizes by the
  *      gather passes' time, on `repeats` forward steps from `state` (writing `scratch_state` and
  *      the cache, which then hold that step); it keeps the fastest shape, returns it in `chosen`
  *      (may be NULL) and the substep time with it in `milliseconds_per_step` (may be NULL).  It

@@ -111,7 +111,7 @@ int pbf_batch_set_launch_shape(pbf_batch* batch, const pbf_launch_shape* shape) 
     if (!batch || !shape) return PBF_ERROR_INVALID_ARGUMENT;
     const pbf::LaunchShape s{shape->list_scan, shape->scan_block_size, shape->block_size};
     if (!pbf::valid_shape(s)) {
-        pbf::set_error("launch shape: list_scan must be 0, 1, 2 or 3 and the block sizes one of 32, 64, 96, 128");
+        pbf::set_error("launch shape: list_scan must be 0 to 4 and the block sizes one of 32, 64, 96, 128");
         return PBF_ERROR_INVALID_ARGUMENT;
     }
     batch->engine.set_shape(s);

@@ -553,12 +553,14 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
     const GatherCommon gc = gather_common(r);
     const Field3 previous{state->positions.x, state->positions.y, state->positions.z};
     const MutField3 out_positions{next_state->positions.x, next_state->positions.y, next_state->positions.z};
+    // Forward-mode steps of scenes without boundary particles may store hit-mask lists (launch shape).
+    const int masks = stores_masks(shape_, diff, boundary_count_ > 0) ? 1 : 0;
     for (uint32_t k = 0; k < K; ++k) {
         const float4* xk = r.iterate(k, K, diff);
         float4* xk1 = const_cast<float4*>(r.iterate(k + 1, K, diff));
         float* lam = keep ? r.lambda[k] : (k == 0 ? r.first_lambda : r.lambda[0]);
         const uint32_t l = keep ? k : 0u;
-        const StoredList list{r.list_entries[l], r.list_counts[l], r.list_capacity};
+        const StoredList list{r.list_entries[l], r.list_counts[l], r.list_capacity, masks};
         ListScanArgs scan{gc, xk, list, 1};
         scan.packed = packed_;
         DensityLambdaArgs d{gc, xk, lam, keep ? r.density[k] : (k == 0 ? r.first_density : nullptr),
@@ -603,7 +605,7 @@ int Engine::launch_forward(cudaStream_t stream, const pbf_particle_state* state,
         if (int rc = check(cudaEventRecordWithFlags(positions_ready_, stream, flags), "positions event")) return rc;
     }
     const uint32_t lp = keep ? K : 0u;
-    const StoredList post{r.list_entries[lp], r.list_counts[lp], r.list_capacity};
+    const StoredList post{r.list_entries[lp], r.list_counts[lp], r.list_capacity, masks};
     timer_.begin(stream, kPassListScan);
     ListScanArgs post_scan{gc, xK, post};
     post_scan.packed = packed_;
@@ -728,7 +730,7 @@ int Engine::autotune(const pbf_particle_state* state, const pbf_control* control
         timer_.enable(false);
         return rc;
     };
-    const uint32_t scans[4] = {kScanPerLane, kScanCooperative, kScanStaged, kScanFusedDensity};
+    const uint32_t scans[5] = {kScanPerLane, kScanCooperative, kScanStaged, kScanFusedDensity, kScanFusedMasks};
     const uint32_t blocks[4] = {32u, 64u, 96u, 128u};
     double ms[kPassCount];
     int rc = PBF_SUCCESS;
@@ -737,7 +739,7 @@ int Engine::autotune(const pbf_particle_state* state, const pbf_control* control
     LaunchShape best = previous;
     best.block = 128u;
     double best_scan = -1.0;
-    for (int v = 0; v < 4 && !rc; ++v)
+    for (int v = 0; v < 5 && !rc; ++v)
         for (int b = 0; b < 4 && !rc; ++b) {
             shape_ = best;
             shape_.scan = scans[v];

@@ -106,24 +106,42 @@ struct PackedScan {
             mask &= mask - 1u;
         }
     }
+    // Hit mask of the 32-slot block at `base` (4-aligned) of the range [first, end).
+    __device__ __forceinline__ uint32_t block_mask(const PackedPositions p, const uint32_t base, const uint32_t first,
+                                                   const uint32_t end) const {
+        const uint32_t stop = min(end, base + 32u);
+        uint32_t mask = 0u;
+        for (uint32_t k = 0u; base + k < stop; k += 4u) {
+            const uint32_t t = base + k;
+            mask |= hits4(*reinterpret_cast<const float4*>(p.x + t), *reinterpret_cast<const float4*>(p.y + t),
+                          *reinterpret_cast<const float4*>(p.z + t))
+                    << k;
+        }
+        if (base < first) mask &= ~0u << (first - base);
+        if (end - base < 32u) mask &= (1u << (end - base)) - 1u;
+        return mask;
+    }
     __device__ __forceinline__ void run(const PackedPositions p, const uint32_t first, const uint32_t end) {
         if (first >= end) return;
+        for (uint32_t base = first & ~3u; base < end; base += 32u) append(block_mask(p, base, first, end), base);
+    }
+    // The same blocks stored as a hit-mask list: one (base, mask) pair per block with a hit, `pairs`
+    // of them so far (at most `pair_capacity` are written), `n` neighbours.
+    __device__ __forceinline__ void run_masks(const PackedPositions p, const uint32_t first, const uint32_t end,
+                                              uint2* __restrict__ row, const uint32_t pair_capacity, uint32_t& pairs) {
+        if (first >= end) return;
         for (uint32_t base = first & ~3u; base < end; base += 32u) {
-            const uint32_t stop = min(end, base + 32u);
-            uint32_t mask = 0u;
-            for (uint32_t k = 0u; base + k < stop; k += 4u) {
-                const uint32_t t = base + k;
-                mask |= hits4(*reinterpret_cast<const float4*>(p.x + t), *reinterpret_cast<const float4*>(p.y + t),
-                              *reinterpret_cast<const float4*>(p.z + t))
-                        << k;
+            const uint32_t mask = block_mask(p, base, first, end);
+            if (mask) {
+                if (pairs < pair_capacity) row[static_cast<size_t>(pairs) * 32u] = make_uint2(base, mask);
+                ++pairs;
+                n += static_cast<uint32_t>(__popc(mask));
             }
-            if (base < first) mask &= ~0u << (first - base);
-            if (end - base < 32u) mask &= (1u << (end - base)) - 1u;
-            append(mask, base);
         }
     }
 };
 
+template <bool Masks>
 __global__ void __launch_bounds__(kBlock, 12) list_walk_kernel(const ListScanArgs a) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.g.count) return;
@@ -167,6 +185,20 @@ __global__ void __launch_bounds__(kBlock, 12) list_walk_kernel(const ListScanArg
         packed.capacity = scan.capacity;
         packed.entries = scan.entries;
         packed.n = 0;
+        if constexpr (Masks) {
+            const uint32_t pair_capacity = scan.capacity / 2u;
+            uint2* row = reinterpret_cast<uint2*>(a.list.entries) + mask_row(s, pair_capacity);
+            uint32_t pairs = 0;
+#pragma unroll 1
+            for (int o = 0; o < 9; ++o) {
+                const int x = c.x + o / 3 - 1, y = c.y + o % 3 - 1;
+                if (x < 0 || x >= cx || y < 0 || y >= cy) continue;
+                packed.run_masks(a.packed, offsets[cell_index(grid, x, y, z_lo)], offsets[cell_index(grid, x, y, z_hi) + 1u],
+                                 row, pair_capacity, pairs);
+            }
+            a.list.counts[s] = pairs <= pair_capacity ? packed.n : kOverflow;
+            return;
+        }
 #pragma unroll 1
         for (int o = 0; o < 9; ++o) {
             const int x = c.x + o / 3 - 1, y = c.y + o % 3 - 1;
@@ -472,9 +504,14 @@ __global__ void __launch_bounds__(kBlock) density_lambda_kernel(const DensityLam
 #endif
 constexpr uint32_t kStagedEntries = PBF_FUSED_STAGED_ENTRIES;   // 40: 20 KB of shared memory per 128-thread block
 
+// Masks: the list is stored as a hit-mask list (one (base, mask) pair per block with a hit), the
+// first kStagedEntries / 2 pairs staged in the same shared memory.
+template <bool Masks>
 __global__ void __launch_bounds__(kBlock, PBF_FUSED_MIN_BLOCKS) scan_density_lambda_kernel(const ListScanArgs a,
                                                                                           const DensityLambdaArgs d) {
-    __shared__ uint32_t staged[kStagedEntries][kBlock];
+    __shared__ __align__(8) uint32_t staged[kStagedEntries * kBlock];
+    constexpr uint32_t kStagedPairs = kStagedEntries / 2u;
+    uint2* const staged_pairs = reinterpret_cast<uint2*>(staged);
     const Particle p = locate(a.g);
     if (!p.active) return;
     const uint32_t s = p.s, lane_slot = threadIdx.x;
@@ -484,18 +521,18 @@ __global__ void __launch_bounds__(kBlock, PBF_FUSED_MIN_BLOCKS) scan_density_lam
     const uint32_t z_hi = static_cast<uint32_t>(p.c.z + 1 < cz ? p.c.z + 1 : cz - 1);
     const float4 xi = a.pos[s];
     const uint32_t capacity = a.list.capacity;
+    const uint32_t pair_capacity = capacity / 2u;
     uint32_t* __restrict__ entries = a.list.entries + list_row(s, capacity);
+    uint2* __restrict__ pairs_row = reinterpret_cast<uint2*>(a.list.entries) + mask_row(s, pair_capacity);
     const uint32_t* __restrict__ offsets = a.g.cell_offsets;
     // 1. the per-lane packed scan (PackedScan), appending to the stored list and the stage
-    uint32_t n = 0;
+    uint32_t n = 0, pairs = 0;
     {
-        const float threshold = p.k.list_threshold;
-        const float2 nx = make_float2(-xi.x, -xi.x), ny = make_float2(-xi.y, -xi.y), nz = make_float2(-xi.z, -xi.z);
-        auto hits2 = [&](const float2 x, const float2 y, const float2 z) -> uint32_t {
-            const float2 dx = __fadd2_rn(x, nx), dy = __fadd2_rn(y, ny), dz = __fadd2_rn(z, nz);
-            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
-            return (r2.x < threshold ? 1u : 0u) | (r2.y < threshold ? 2u : 0u);
-        };
+        PackedScan scan;
+        scan.nx = make_float2(-xi.x, -xi.x);
+        scan.ny = make_float2(-xi.y, -xi.y);
+        scan.nz = make_float2(-xi.z, -xi.z);
+        scan.threshold = p.k.list_threshold;
         const PackedPositions pk = a.packed;
 #pragma unroll 1
         for (int o = 0; o < 9; ++o) {
@@ -505,29 +542,29 @@ __global__ void __launch_bounds__(kBlock, PBF_FUSED_MIN_BLOCKS) scan_density_lam
             const uint32_t end = offsets[cell_index(grid, x, y, z_hi) + 1u];
             if (first >= end) continue;
             for (uint32_t base = first & ~3u; base < end; base += 32u) {
-                const uint32_t stop = min(end, base + 32u);
-                uint32_t mask = 0u;
-                for (uint32_t k = 0u; base + k < stop; k += 4u) {
-                    const uint32_t t = base + k;
-                    const float4 qx = *reinterpret_cast<const float4*>(pk.x + t);
-                    const float4 qy = *reinterpret_cast<const float4*>(pk.y + t);
-                    const float4 qz = *reinterpret_cast<const float4*>(pk.z + t);
-                    mask |= (hits2(make_float2(qx.x, qx.y), make_float2(qy.x, qy.y), make_float2(qz.x, qz.y)) |
-                             (hits2(make_float2(qx.z, qx.w), make_float2(qy.z, qy.w), make_float2(qz.z, qz.w)) << 2))
-                            << k;
-                }
-                if (base < first) mask &= ~0u << (first - base);
-                if (end - base < 32u) mask &= (1u << (end - base)) - 1u;
-                while (mask) {
-                    const uint32_t k = static_cast<uint32_t>(__ffs(mask)) - 1u;
-                    if (n < capacity) entries[static_cast<size_t>(n) * 32u] = base + k;
-                    if (n < kStagedEntries) staged[n][lane_slot] = base + k;
-                    ++n;
-                    mask &= mask - 1u;
+                uint32_t mask = scan.block_mask(pk, base, first, end);
+                if constexpr (Masks) {
+                    if (mask) {
+                        const uint2 pair = make_uint2(base, mask);
+                        if (pairs < pair_capacity) pairs_row[static_cast<size_t>(pairs) * 32u] = pair;
+                        if (pairs < kStagedPairs) staged_pairs[pairs * kBlock + lane_slot] = pair;
+                        ++pairs;
+                        n += static_cast<uint32_t>(__popc(mask));
+                    }
+                } else {
+                    while (mask) {
+                        const uint32_t k = static_cast<uint32_t>(__ffs(mask)) - 1u;
+                        if (n < capacity) entries[static_cast<size_t>(n) * 32u] = base + k;
+                        if (n < kStagedEntries) staged[n * kBlock + lane_slot] = base + k;
+                        ++n;
+                        mask &= mask - 1u;
+                    }
                 }
             }
         }
-        a.list.counts[s] = n <= capacity ? n : kOverflow;
+        const bool overflow = Masks ? pairs > pair_capacity : n > capacity;
+        a.list.counts[s] = overflow ? kOverflow : n;
+        if (overflow) n = kOverflow;
     }
     // 2. density (density/density.cu:18-40) and lambda (pbf/pbf.cu:95-127) over the same list
     DensityLambdaOp<false> op;
@@ -543,11 +580,32 @@ __global__ void __launch_bounds__(kBlock, PBF_FUSED_MIN_BLOCKS) scan_density_lam
     op.denominator = pa.y;  // relaxation
     op.neighbors = 0;
     op.ratio.reset(xi.w, op.rest_density);
-    if (n > capacity) {
+    if (n == kOverflow) {
         walk(op, p, a.g);
     } else if (n > 0) {
+        uint2 current{}, upcoming{};
+        uint32_t next_pair = 2u;
+        auto pair_at = [&](const uint32_t j) -> uint2 {
+            return j < kStagedPairs ? staged_pairs[j * kBlock + lane_slot] : pairs_row[static_cast<size_t>(j) * 32u];
+        };
+        if constexpr (Masks) {
+            current = pair_at(0);
+            upcoming = pairs > 1u ? pair_at(1) : make_uint2(0u, 0u);
+        }
         auto entry = [&](const uint32_t k) -> uint32_t {
-            return k < kStagedEntries ? staged[k][lane_slot] : entries[static_cast<size_t>(k) * 32u];
+            if constexpr (Masks) {
+                (void)k;
+                if (current.y == 0u) {
+                    current = upcoming;
+                    upcoming = next_pair < pairs ? pair_at(next_pair) : make_uint2(0u, 0u);
+                    ++next_pair;
+                }
+                const uint32_t bit = static_cast<uint32_t>(__ffs(current.y)) - 1u;
+                current.y &= current.y - 1u;
+                return current.x + bit;
+            } else {
+                return k < kStagedEntries ? staged[k * kBlock + lane_slot] : entries[static_cast<size_t>(k) * 32u];
+            }
         };
         uint32_t t = entry(0);
         uint32_t tn = n > 1u ? entry(1) : 0u;
@@ -625,7 +683,7 @@ struct CorrectionOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-template <bool WithBoundary>
+template <bool WithBoundary, bool Masks>
 __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
@@ -647,7 +705,7 @@ __global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs
     op.artificial_full = pb.x != 0.0F;
     op.reference_weight = op.artificial_full ? poly6(mk(pb.z, 0.0F, 0.0F), p.k) : 1.0F;
     op.correction = mk(0.0F, 0.0F, 0.0F);
-    replay<2>(op, p, a.g, a.list);
+    replay_list<Masks>(op, p, a.g, a.list);
     const Box& box = p.scene->box;
     const f3 candidate = add(op.x, op.correction);
     uint32_t mask = 0u;
@@ -700,6 +758,7 @@ struct VorticityOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
+template <bool Masks>
 __global__ void __launch_bounds__(kBlock) vorticity_kernel(const VorticityArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
@@ -711,7 +770,7 @@ __global__ void __launch_bounds__(kBlock) vorticity_kernel(const VorticityArgs a
     op.x = xyz(a.pos[p.s]);
     op.v = xyz(a.velocity[p.s]);
     op.vorticity = mk(0.0F, 0.0F, 0.0F);
-    replay<2>(op, p, a.g, a.list);
+    replay_list<Masks>(op, p, a.g, a.list);
     a.vorticity[p.s] = make_float4(op.vorticity.x, op.vorticity.y, op.vorticity.z, __fsqrt_rn(sq_xfirst(op.vorticity)));
 }
 
@@ -742,6 +801,7 @@ struct NormalOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
+template <bool Masks>
 __global__ void __launch_bounds__(kBlock) normal_kernel(const NormalArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
@@ -754,7 +814,7 @@ __global__ void __launch_bounds__(kBlock) normal_kernel(const NormalArgs a) {
     op.x = xyz(a.pos[p.s]);
     op.magnitude = wi.w;
     op.gradient = mk(0.0F, 0.0F, 0.0F);
-    replay<2>(op, p, a.g, a.list);
+    replay_list<Masks>(op, p, a.g, a.list);
     const float normalizer = __fsqrt_rn(sq_yfirst(op.gradient));
     const f3 normal = normalizer > 0.0F ? scale(op.gradient, __fdiv_rn(1.0F, normalizer)) : mk(0.0F, 0.0F, 0.0F);
     a.normal[p.s] = make_float4(normal.x, normal.y, normal.z, normalizer);
@@ -785,6 +845,7 @@ struct XsphOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
+template <bool Masks>
 __global__ void __launch_bounds__(kBlock) xsph_kernel(const XsphArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
@@ -796,7 +857,7 @@ __global__ void __launch_bounds__(kBlock) xsph_kernel(const XsphArgs a) {
     op.x = xyz(a.pos[p.s]);
     op.v = xyz(a.confined[p.s]);
     op.smoothing = mk(0.0F, 0.0F, 0.0F);
-    replay<2>(op, p, a.g, a.list);
+    replay_list<Masks>(op, p, a.g, a.list);
     const float viscosity = a.g.params_a[p.s].z;
     const f3 out = fma3(viscosity, op.smoothing, op.v);
     const uint32_t i = a.sorted_index[p.s];
@@ -927,12 +988,17 @@ cudaError_t launch_constants(cudaStream_t stream, const float* radii, const uint
 bool valid_shape(const LaunchShape& shape) {
     auto ok = [](const uint32_t b) { return b >= 32u && b <= static_cast<uint32_t>(kBlock) && b % 32u == 0u; };
     return (shape.scan == kScanPerLane || shape.scan == kScanCooperative || shape.scan == kScanStaged ||
-            shape.scan == kScanFusedDensity) &&
+            shape.scan == kScanFusedDensity || shape.scan == kScanFusedMasks) &&
            ok(shape.scan_block) && ok(shape.block);
 }
 
 bool fuses_density(const LaunchShape& shape, const ListScanArgs& a) {
-    return shape.scan == kScanFusedDensity && a.packed.x && !a.g.boundary && !a.g.boundary_offsets;
+    return (shape.scan == kScanFusedDensity || shape.scan == kScanFusedMasks) && a.packed.x && !a.g.boundary &&
+           !a.g.boundary_offsets;
+}
+
+bool stores_masks(const LaunchShape& shape, const bool differentiable, const bool boundary) {
+    return shape.scan == kScanFusedMasks && !differentiable && !boundary;
 }
 
 namespace {
@@ -947,12 +1013,15 @@ cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a, const L
     // the cooperative and staged scans list fluid particles only; lists with boundary particles
     // use the per-lane walk
     const bool fluid_only = !(a.boundary && a.g.boundary_offsets);
-    if (shape.scan == kScanCooperative && fluid_only)
+    if (a.list.masks) {   // hit-mask lists: the per-lane packed walk, scenes without boundary particles
+        if (!fluid_only || !a.packed.x) return cudaErrorInvalidValue;
+        list_walk_kernel<true><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    } else if (shape.scan == kScanCooperative && fluid_only)
         list_scan_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     else if (shape.scan == kScanStaged && fluid_only)
         list_staged_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     else
-        list_walk_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+        list_walk_kernel<false><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }
@@ -961,13 +1030,17 @@ cudaError_t launch_scan_density_lambda(cudaStream_t stream, const ListScanArgs& 
                                        const LaunchShape& shape) {
     if (a.g.count == 0) return cudaSuccess;
     const unsigned block = block_of(shape.scan_block);
-    scan_density_lambda_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a, d);
+    if (a.list.masks)
+        scan_density_lambda_kernel<true><<<grid_of(a.g.count, block), block, 0, stream>>>(a, d);
+    else
+        scan_density_lambda_kernel<false><<<grid_of(a.g.count, block), block, 0, stream>>>(a, d);
     count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_density_lambda(cudaStream_t stream, const DensityLambdaArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
+    if (a.list.masks) return cudaErrorInvalidValue;   // hit-mask lists are read by the fused scan only
     const unsigned block = block_of(block_size);
     if (a.g.boundary)
         density_lambda_kernel<true><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
@@ -980,10 +1053,14 @@ cudaError_t launch_density_lambda(cudaStream_t stream, const DensityLambdaArgs& 
 cudaError_t launch_correction(cudaStream_t stream, const CorrectionArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
     const unsigned block = block_of(block_size);
-    if (a.g.boundary)
-        correction_kernel<true><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
-    else
-        correction_kernel<false><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    if (a.g.boundary) {
+        if (a.list.masks) return cudaErrorInvalidValue;
+        correction_kernel<true, false><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    } else if (a.list.masks) {
+        correction_kernel<false, true><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    } else {
+        correction_kernel<false, false><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    }
     count_launch();
     return cudaGetLastError();
 }
@@ -991,7 +1068,10 @@ cudaError_t launch_correction(cudaStream_t stream, const CorrectionArgs& a, cons
 cudaError_t launch_vorticity(cudaStream_t stream, const VorticityArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
     const unsigned block = block_of(block_size);
-    vorticity_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    if (a.list.masks)
+        vorticity_kernel<true><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    else
+        vorticity_kernel<false><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }
@@ -999,7 +1079,10 @@ cudaError_t launch_vorticity(cudaStream_t stream, const VorticityArgs& a, const 
 cudaError_t launch_normal(cudaStream_t stream, const NormalArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
     const unsigned block = block_of(block_size);
-    normal_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    if (a.list.masks)
+        normal_kernel<true><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    else
+        normal_kernel<false><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }
@@ -1007,7 +1090,10 @@ cudaError_t launch_normal(cudaStream_t stream, const NormalArgs& a, const unsign
 cudaError_t launch_xsph(cudaStream_t stream, const XsphArgs& a, const unsigned block_size) {
     if (a.g.count == 0) return cudaSuccess;
     const unsigned block = block_of(block_size);
-    xsph_kernel<<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    if (a.list.masks)
+        xsph_kernel<true><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
+    else
+        xsph_kernel<false><<<grid_of(a.g.count, block), block, 0, stream>>>(a);
     count_launch();
     return cudaGetLastError();
 }

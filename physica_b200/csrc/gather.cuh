@@ -151,5 +151,69 @@ __device__ __forceinline__ void replay(Op& op, const Particle& p, const GatherCo
     }
 }
 
+// Hit-mask lists: pair j of particle s is one 8-byte word of its warp's interleaved row.
+__device__ __forceinline__ size_t mask_row(const uint32_t s, const uint32_t capacity_pairs) {
+    return (static_cast<size_t>(s >> 5) * capacity_pairs) * 32u + (s & 31u);
+}
+
+// Yields the slots of a hit-mask list in order: the set bits of each (base, mask) pair, ascending.
+// The next pair is loaded while the current one is drained.
+struct MaskCursor {
+    const uint2* __restrict__ pairs;   // the particle's row (stride 32 pairs)
+    uint32_t capacity;
+    uint32_t next_index;
+    uint2 current, upcoming;
+    __device__ __forceinline__ void start(const uint2* row, const uint32_t capacity_pairs) {
+        pairs = row;
+        capacity = capacity_pairs;
+        current = row[0];
+        upcoming = capacity_pairs > 1u ? row[32] : make_uint2(0u, 0u);
+        next_index = 2u;
+    }
+    // The next slot; call at most as many times as the list has neighbours.
+    __device__ __forceinline__ uint32_t take() {
+        if (current.y == 0u) {
+            current = upcoming;
+            upcoming = next_index < capacity ? pairs[static_cast<size_t>(next_index) * 32u] : make_uint2(0u, 0u);
+            ++next_index;
+        }
+        const uint32_t k = static_cast<uint32_t>(__ffs(current.y)) - 1u;
+        current.y &= current.y - 1u;
+        return current.x + k;
+    }
+};
+
+// replay over a hit-mask list: the same entries in the same order as the index list.
+template <class Op>
+__device__ __forceinline__ void replay_masks(Op& op, const Particle& p, const GatherCommon& g, const StoredList& list) {
+    if (!p.active) return;
+    const uint32_t n = list.counts[p.s];
+    if (n == kOverflow) {
+        walk(op, p, g);
+        return;
+    }
+    if (n == 0) return;
+    MaskCursor cursor;
+    const uint32_t capacity = list.capacity / 2u;
+    cursor.start(reinterpret_cast<const uint2*>(list.entries) + mask_row(p.s, capacity), capacity);
+    uint32_t t = cursor.take();
+    auto data = op.prefetch(t);
+    for (uint32_t k = 1; k < n; ++k) {
+        const uint32_t tn = cursor.take();
+        const auto next = op.prefetch(tn);
+        op.apply(t, data);
+        t = tn;
+        data = next;
+    }
+    op.apply(t, data);
+}
+
+// The replay of either list format (Masks: a hit-mask list).
+template <bool Masks, class Op>
+__device__ __forceinline__ void replay_list(Op& op, const Particle& p, const GatherCommon& g, const StoredList& list) {
+    if constexpr (Masks) replay_masks(op, p, g, list);
+    else replay<2>(op, p, g, list);
+}
+
 }  // namespace gather_detail
 }  // namespace pbf

@@ -55,11 +55,18 @@ cudaError_t launch_reference_order(cudaStream_t stream, uint32_t count, const Sc
                                    const uint32_t* sorted_index, const uint32_t* keys, const uint32_t* cell_offsets,
                                    const uint32_t* reference_offsets, uint32_t* out_index, unsigned long long* out_keys);
 
-// A stored neighbour list (warp-interleaved entries + per-particle counts).
+// A stored neighbour list (warp-interleaved entries + per-particle counts).  Two formats share the
+// buffer of `capacity` 32-bit words per particle:
+// - index lists (masks = 0): one sorted slot per in-support neighbour, counts = entries;
+// - hit-mask lists (masks = 1): one (slot of bit 0, 32-bit hit mask) pair per 32-slot block of a
+//   stencil column that holds a neighbour, capacity / 2 pairs per particle, counts = neighbours.
+// Either lists the same neighbours in the same order; kOverflow marks a particle whose list did not
+// fit (it walks its stencil instead).
 struct StoredList {
     uint32_t* entries;
     uint32_t* counts;
     uint32_t capacity;
+    int masks = 0;
 };
 
 // Common inputs of every neighbour-gather pass.
@@ -169,6 +176,8 @@ enum ListScanVariant : uint32_t {
     kScanStaged = 2,        // a warp stages its column group's candidates in shared memory
     kScanFusedDensity = 3,  // per lane, and the Jacobi iterations' scans also run density + lambda
                             // in the same kernel (scenes without boundary particles)
+    kScanFusedMasks = 4,    // as 3, and forward-mode steps store hit-mask lists (scenes without
+                            // boundary particles; differentiable steps store index lists)
 };
 struct LaunchShape {
     uint32_t scan = kScanPerLane;
@@ -180,6 +189,8 @@ bool valid_shape(const LaunchShape& shape);
 cudaError_t launch_list_scan(cudaStream_t stream, const ListScanArgs& a, const LaunchShape& shape = LaunchShape{});
 // Whether `shape` runs the scan of `a` fused with density + lambda (launch_scan_density_lambda).
 bool fuses_density(const LaunchShape& shape, const ListScanArgs& a);
+// Whether a forward-mode step with `shape` stores hit-mask lists (no boundary particles).
+bool stores_masks(const LaunchShape& shape, bool differentiable, bool boundary);
 // The list scan of a Jacobi iteration and its density + lambda pass in one kernel (same list and
 // results as launch_list_scan followed by launch_density_lambda).
 cudaError_t launch_scan_density_lambda(cudaStream_t stream, const ListScanArgs& a, const DensityLambdaArgs& d,

@@ -92,7 +92,8 @@ class LaunchShapeC(ctypes.Structure):
 class LaunchShape:
     """Launch shape of the neighbour-list and gather kernels (results are identical for every shape).
     list_scan: 0 = per-lane walk, 1 = warp-cooperative scan, 2 = shared-memory staged walk,
-    3 = per-lane walk with each Jacobi iteration's density + lambda in the same kernel;
+    3 = per-lane walk with each Jacobi iteration's density + lambda in the same kernel,
+    4 = as 3 with hit-mask neighbour lists in forward mode;
     scan_block_size (list scan) and
     block_size (gather passes): 32, 64, 96 or 128."""
     list_scan: int = 0

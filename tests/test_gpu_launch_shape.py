@@ -9,7 +9,7 @@ from physica_b200 import pbf, scenes
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [pbf.LaunchShape(v, b, g) for v, b, g in itertools.product((0, 1, 2, 3), (32, 64, 96, 128), (32, 64, 96, 128))]
+SHAPES = [pbf.LaunchShape(v, b, g) for v, b, g in itertools.product((0, 1, 2, 3, 4), (32, 64, 96, 128), (32, 64, 96, 128))]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -44,7 +44,7 @@ def test_every_shape_gives_identical_substeps():
 
 def test_invalid_shapes_are_rejected():
     solver, _, _, _ = pbf.solver_for_scene(scenes.dam_break((4, 4, 4), (0, 0, 0), (1, 2, 1), 32, 2))
-    for bad in (pbf.LaunchShape(4, 128, 128), pbf.LaunchShape(0, 48, 128), pbf.LaunchShape(0, 128, 256),
+    for bad in (pbf.LaunchShape(5, 128, 128), pbf.LaunchShape(0, 48, 128), pbf.LaunchShape(0, 128, 256),
                 pbf.LaunchShape(1, 0, 64)):
         with pytest.raises(pbf.PBFError):
             solver.launch_shape = bad
@@ -66,7 +66,7 @@ def test_batch_autotune_and_shapes_give_identical_substeps():
     batch, state, control, params = pbf.batch_for_scenes(scs)
     out = []
     for shape in (pbf.LaunchShape(0, 128, 128), pbf.LaunchShape(1, 64, 96), pbf.LaunchShape(2, 128, 64),
-                  pbf.LaunchShape(3, 96, 128)):
+                  pbf.LaunchShape(3, 96, 128), pbf.LaunchShape(4, 64, 32)):
         batch.launch_shape = shape
         cur = pbf.State(state.positions.clone(), state.velocities.clone(), 0)
         nxt = batch.allocate_state()
@@ -108,3 +108,20 @@ def test_fused_density_records_the_same_iterates_for_the_adjoint():
         assert torch.equal(x, y)
     for x, y in zip(a[4], b[4]):
         assert torch.equal(x, y)
+
+
+def test_hit_mask_lists_equal_index_lists_over_a_long_run_and_when_crowded():
+    """Launch-shape variant 4 stores each neighbour list as (slot base, 32-bit hit mask) pairs: 60
+    steps of a 3,375-particle dam break, and 3 steps of a clump eight times denser than the lattice
+    (its hit-mask lists overflow and walk the stencil), equal the index-list solver bit for bit."""
+    sc = scenes.dam_break((15, 15, 15), (0, 0, 0), (1, 2, 1), 35, 4, velocity_sigma=0.2)
+    crowded = scenes.dam_break((16, 16, 16), (0, 0, 0), (1, 2, 1), 36, 3)
+    crowded.positions = (crowded.positions * 0.5 + 0.1).astype(crowded.positions.dtype)
+    for scene, steps in ((sc, 60), (crowded, 3)):
+        out = []
+        for shape in (pbf.LaunchShape(3, 128, 128), pbf.LaunchShape(4, 128, 128), pbf.LaunchShape(4, 32, 64)):
+            solver, state, control, params = pbf.solver_for_scene(scene)
+            solver.launch_shape = shape
+            out.append(_run(solver, state, control, params, steps))
+        for x, v in out[1:]:
+            assert torch.equal(x, out[0][0]) and torch.equal(v, out[0][1])

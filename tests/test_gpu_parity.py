@@ -188,6 +188,17 @@ def test_trajectory_matches_reference_after_100_steps():
     assert errs[100][2] == 0, errs   # and in fact bit for bit
 
 
+def test_hit_mask_lists_trajectory_matches_reference():
+    """The 32,768-particle dam break through hit-mask lists (launch-shape variant 4), 100 steps,
+    bit for bit against the reference."""
+    reference = reference_or_skip()
+    sc = scenes.plain_small()
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    solver.launch_shape = pbf.LaunchShape(4, 128, 64)
+    errs = _trajectory_with(solver, state, control, params, solver.allocate_step_cache(), sc, 100, reference)
+    assert all(e[2] == 0 for e in errs.values()), {k: e for k, e in errs.items() if e[2]}
+
+
 def test_batched_scene_layout_trajectory_matches_reference():
     """A truncated-lattice scene (the batched scenes' shape) over 30 steps, bit for bit."""
     reference = reference_or_skip()
