@@ -536,6 +536,7 @@ struct LambdaVjpOp {
     KernelConstants k;
     d3 pc;
     double mc;
+    double rc_pairs;   // the second neighbour loop's terms (pbf.cu:233-246), summed in this loop
     f3 self_gradient;
 
     __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
@@ -561,6 +562,7 @@ struct LambdaVjpOp {
         const d3 neighbor_gradient_adjoint = times(neighbor_gradient, 2.0 * db);
         const d3 gradient_adjoint = times(sb - neighbor_gradient_adjoint, coefficient);
         self_gradient = fma3(coefficient, gradient, self_gradient);
+        rc_pairs -= dot(neighbor_gradient_adjoint, neighbor_gradient) / rest_density;
         const float rrest = params_a[t].x;
         const float4 gj = gsum[t];
         const double rconstraint = static_cast<double>(density[t]) / rrest - 1.0;
@@ -579,32 +581,10 @@ struct LambdaVjpOp {
     }
 };
 
-// The reference's second neighbour loop of lambda_vjp_kernel (pbf.cu:233-246).
-struct LambdaVjpSecondOp {
-    const float4* __restrict__ pos;
-    f3 x;
-    float rest_density;
-    double db;
-    uint32_t self;
-    KernelConstants k;
-    double rc;
-
-    __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
-    __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
-    __device__ __forceinline__ void process(const uint32_t t) {
-        if (t == self || (t & kBoundaryBit)) return;   // fluid neighbours only (pbf.cu:233-246)
-        const float4 q = pos[t];
-        const f3 d = sub(x, xyz(q));
-        const float r2 = squared(d);
-        if (r2 == 0.0F || r2 >= k.spiky_threshold) return;
-        const f3 gradient = spiky_gradient(d, k);
-        const f3 neighbor_gradient = times(gradient, -q.w / rest_density);
-        const d3 neighbor_gradient_adjoint = times(neighbor_gradient, 2.0 * db);
-        rc -= dot(neighbor_gradient_adjoint, neighbor_gradient) / rest_density;
-    }
-};
-
-__global__ void __launch_bounds__(kBlock) lambda_vjp_kernel(const LambdaVjpArgs a) {
+#ifndef PBF_LAMBDA_VJP_MIN_BLOCKS
+#define PBF_LAMBDA_VJP_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(kBlock, PBF_LAMBDA_VJP_MIN_BLOCKS) lambda_vjp_kernel(const LambdaVjpArgs a) {
     const Particle p = locate(a.g);
     LambdaVjpOp op;
     op.pos = a.pos;
@@ -628,25 +608,21 @@ __global__ void __launch_bounds__(kBlock) lambda_vjp_kernel(const LambdaVjpArgs 
     op.sb = times(xyz(gi), 2.0 * op.db);
     op.pc = {0.0, 0.0, 0.0};
     op.mc = 0.0;
+    op.rc_pairs = 0.0;
     op.self_gradient = mk(0.0F, 0.0F, 0.0F);
     replay(op, p, a.g, a.list);
+    // The reference sums the rest-density adjoint in a second neighbour loop after the first
+    // (pbf.cu:233-246); its per-pair terms need nothing the first loop lacks, so they are summed
+    // there and added here (FP64 rounding of a different summation order).
     double rc = lb * rho / (static_cast<double>(gi.w) * pa.x * pa.x);
     rc -= dot(op.sb, op.self_gradient) / pa.x;
-    LambdaVjpSecondOp second;
-    second.pos = a.pos;
-    second.x = op.x;
-    second.rest_density = pa.x;
-    second.db = op.db;
-    second.self = p.s;
-    second.k = p.k;
-    second.rc = rc;
-    replay(second, p, a.g, a.list);
+    rc += op.rc_pairs;
     if (!p.active) return;
     const uint32_t i = a.sorted_index[p.s];
     a.x[p.s] = st3(ld3(a.x[p.s]) + op.pc);
     a.density_adjoint[p.s] = 0.0 - lb / (static_cast<double>(gi.w) * pa.x);
     add_to(a.pa.masses, i, op.mc);
-    add_to(a.pa.rest_densities, i, second.rc);
+    add_to(a.pa.rest_densities, i, rc);
     add_to(a.pa.relaxation, i, op.db);
 }
 
