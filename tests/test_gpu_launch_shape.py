@@ -125,3 +125,23 @@ def test_hit_mask_lists_equal_index_lists_over_a_long_run_and_when_crowded():
             out.append(_run(solver, state, control, params, steps))
         for x, v in out[1:]:
             assert torch.equal(x, out[0][0]) and torch.equal(v, out[0][1])
+
+
+def test_hit_mask_lists_with_no_particles_and_no_iterations():
+    """An empty scene and a scene with zero Jacobi iterations (only the post-loop list) step with
+    hit-mask lists, the latter equal to index lists bit for bit."""
+    dc = pbf.DomainConfiguration(particle_count=0, time_step=1.0 / 120.0, support_radius=0.025, particle_radius=0.005,
+                                 boundary=pbf.BoxBoundary((0, 0, 0), (1, 2, 1), (0, 0, 0), True))
+    solver = pbf.PBF(dc, pbf.Configuration(4, 2))
+    solver.launch_shape = pbf.LaunchShape(4, 128, 128)
+    state, nxt = solver.allocate_state(), solver.allocate_state()
+    solver.forward_step(state, solver.allocate_control(), solver.allocate_parameters(), nxt, solver.allocate_step_cache())
+    solver.synchronize()
+    assert nxt.step_index == 1
+    sc = scenes.dam_break((10, 10, 10), (0, 0, 0), (1, 2, 1), 37, 0, velocity_sigma=0.3)
+    out = []
+    for shape in (pbf.LaunchShape(0, 128, 128), pbf.LaunchShape(4, 128, 128)):
+        solver, state, control, params = pbf.solver_for_scene(sc)
+        solver.launch_shape = shape
+        out.append(_run(solver, state, control, params, 3))
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])

@@ -248,8 +248,9 @@ def test_forward_against_fp64_oracle():
 
 
 # ------------------------------------------------------------------------ edge cases
+@pytest.mark.parametrize("list_scan", [0, 4])
 @pytest.mark.parametrize("case", ["single", "ragged", "one_cell", "outside_grid", "two_coincident"])
-def test_edge_cases_match_oracle(case):
+def test_edge_cases_match_oracle(case, list_scan):
     from oracle import oracle
     if case == "single":
         sc = scenes.dam_break((1, 1, 1), (0, 0, 0), (1, 2, 1), 3, 3)
@@ -267,6 +268,7 @@ def test_edge_cases_match_oracle(case):
         sc = scenes.dam_break((4, 4, 4), (0, 0, 0), (1, 2, 1), 7, 3)
         sc.positions[:, 1] = sc.positions[:, 0]    # two particles at the same point (zero distance)
     solver, state, control, params = pbf.solver_for_scene(sc)
+    solver.launch_shape = pbf.LaunchShape(list_scan, 128, 128)   # index lists, hit-mask lists
     cache = solver.allocate_step_cache()
     nxt = step(solver, state, control, params, cache)
     x1, v1 = oracle.forward_step(sc, sc.positions, sc.velocities)
