@@ -30,6 +30,7 @@ struct AdjointWorkspace {
     double4* eta = nullptr;               // adjoint of the unnormalised vorticity-magnitude gradient
     double* lambda = nullptr;
     double* density = nullptr;
+    double* constraint_weight = nullptr;   // lambda adjoint x C / D^2 of each particle (the lambda VJP's db)
     float2* s_corr = nullptr;             // (W(s_corr radius), 1 when the strength is zero and the power stays finite)
 };
 
@@ -380,6 +381,12 @@ struct CorrectionVjpArgs {
     double4* x;
     double* lambda_adjoint;
     ParamAdjoint pa;
+    // For each particle the correction VJP also writes lambda_adjoint * (rho / rho0 - 1) / D^2, the
+    // factor the lambda VJP (pbf.cu:180-200) applies to the particle's own gradient terms and, for
+    // every neighbour, to that neighbour's: evaluated once per particle instead of once per pair.
+    const float* density;
+    const float4* gsum;          // (S, D)
+    double* constraint_weight;
 };
 
 struct CorrectionVjpOp {
@@ -437,7 +444,7 @@ struct CorrectionVjpOp {
         pc = pc + hessian;
         pc = pc + times(ap.gradient, scalar_adjoint);
         lc += scalar_adjoint;
-        rc -= dot(ob, times(gradient, coefficient * multiplier)) / rest_density;
+        rc += dot(ob, times(gradient, coefficient * multiplier));   // divided by -rho0_i once, at the end
         sc += scalar_adjoint * ap.d_strength;
         ec += scalar_adjoint * ap.d_exponent;
         qc += scalar_adjoint * ap.d_radius;
@@ -498,9 +505,13 @@ __global__ void __launch_bounds__(kBlock, 4) correction_vjp_kernel(const Correct
     if (!p.active) return;
     const uint32_t i = a.sorted_index[p.s];
     a.x[p.s] = st3(ld3(a.x[p.s]) + op.pc);
-    a.lambda_adjoint[p.s] = 0.0 + op.lc;
+    const double lb = 0.0 + op.lc;
+    a.lambda_adjoint[p.s] = lb;
+    const double constraint = static_cast<double>(a.density[p.s]) / pa.x - 1.0;
+    const float denominator = a.gsum[p.s].w;
+    a.constraint_weight[p.s] = lb * constraint / (static_cast<double>(denominator) * denominator);
     add_to(a.pa.masses, i, op.mc);
-    add_to(a.pa.rest_densities, i, op.rc);
+    add_to(a.pa.rest_densities, i, -op.rc / pa.x);
     add_to(a.pa.strength, i, op.sc);
     add_to(a.pa.exponent, i, op.ec);
     add_to(a.pa.radius, i, op.qc);
@@ -515,6 +526,7 @@ struct LambdaVjpArgs {
     const float* density;
     const float4* gsum;          // (S, D)
     const double* lambda_adjoint;
+    const double* constraint_weight;
     double4* x;
     double* density_adjoint;
     ParamAdjoint pa;
@@ -526,7 +538,7 @@ struct LambdaVjpOp {
     const float4* __restrict__ boundary;
     const float* __restrict__ density;
     const float4* __restrict__ gsum;
-    const double* __restrict__ lambda_adjoint;
+    const double* __restrict__ constraint_weight;
     const float4* __restrict__ params_a;
     f3 x;
     float mass, rest_density;
@@ -562,11 +574,10 @@ struct LambdaVjpOp {
         const d3 neighbor_gradient_adjoint = times(neighbor_gradient, 2.0 * db);
         const d3 gradient_adjoint = times(sb - neighbor_gradient_adjoint, coefficient);
         self_gradient = fma3(coefficient, gradient, self_gradient);
-        rc_pairs -= dot(neighbor_gradient_adjoint, neighbor_gradient) / rest_density;
+        rc_pairs += dot(neighbor_gradient_adjoint, neighbor_gradient);   // divided by -rho0_i once, at the end
         const float rrest = params_a[t].x;
         const float4 gj = gsum[t];
-        const double rconstraint = static_cast<double>(density[t]) / rrest - 1.0;
-        const double rdb = lambda_adjoint[t] * rconstraint / (static_cast<double>(gj.w) * gj.w);
+        const double rdb = constraint_weight[t];   // the neighbour's db, as its own lambda VJP forms it
         const d3 rsb = times(xyz(gj), 2.0 * rdb);
         const f3 rg = scale(gradient, -1.0F);   // spiky_gradient(-d), exactly
         const float rcoefficient = mass / rrest;
@@ -591,7 +602,7 @@ __global__ void __launch_bounds__(kBlock, PBF_LAMBDA_VJP_MIN_BLOCKS) lambda_vjp_
     op.boundary = a.g.boundary;
     op.density = a.density;
     op.gsum = a.gsum;
-    op.lambda_adjoint = a.lambda_adjoint;
+    op.constraint_weight = a.constraint_weight;
     op.params_a = a.g.params_a;
     op.self = p.s;
     op.k = p.k;
@@ -603,8 +614,7 @@ __global__ void __launch_bounds__(kBlock, PBF_LAMBDA_VJP_MIN_BLOCKS) lambda_vjp_
     op.x = xyz(xi);
     op.mass = xi.w;
     op.rest_density = pa.x;
-    const double constraint = static_cast<double>(rho) / pa.x - 1.0;
-    op.db = lb * constraint / (static_cast<double>(gi.w) * gi.w);
+    op.db = p.active ? a.constraint_weight[p.s] : 0.0;   // lb (rho / rho0 - 1) / D^2
     op.sb = times(xyz(gi), 2.0 * op.db);
     op.pc = {0.0, 0.0, 0.0};
     op.mc = 0.0;
@@ -616,7 +626,7 @@ __global__ void __launch_bounds__(kBlock, PBF_LAMBDA_VJP_MIN_BLOCKS) lambda_vjp_
     // there and added here (FP64 rounding of a different summation order).
     double rc = lb * rho / (static_cast<double>(gi.w) * pa.x * pa.x);
     rc -= dot(op.sb, op.self_gradient) / pa.x;
-    rc += op.rc_pairs;
+    rc += -op.rc_pairs / pa.x;
     if (!p.active) return;
     const uint32_t i = a.sorted_index[p.s];
     a.x[p.s] = st3(ld3(a.x[p.s]) + op.pc);
@@ -817,6 +827,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
         ws->eta = ws->arena.alloc<double4>(n, e);
         ws->lambda = ws->arena.alloc<double>(n, e);
         ws->density = ws->arena.alloc<double>(n, e);
+        ws->constraint_weight = ws->arena.alloc<double>(n, e);
         ws->s_corr = ws->arena.alloc<float2>(n, e);
         if (e != cudaSuccess) {
             delete ws;
@@ -896,11 +907,13 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
             density_k = segment_->density[j];
             gsum_k = segment_->gsum[j];
         }
-        CorrectionVjpArgs ca{gc, it_list, r.sorted_index, xk, ws->s_corr, lambda_k, ws->correction, acc, ws->lambda, pa};
+        CorrectionVjpArgs ca{gc, it_list, r.sorted_index, xk, ws->s_corr, lambda_k, ws->correction, acc, ws->lambda, pa,
+                             density_k, gsum_k, ws->constraint_weight};
         timer_.begin(stream_, kPassCorrectionVjp);
         correction_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(ca);
         timer_.end(stream_, kPassCorrectionVjp);
-        LambdaVjpArgs la{gc_reverse, it_list, r.sorted_index, xk, density_k, gsum_k, ws->lambda, acc, ws->density, pa};
+        LambdaVjpArgs la{gc_reverse, it_list, r.sorted_index, xk, density_k, gsum_k, ws->lambda, ws->constraint_weight, acc,
+                         ws->density, pa};
         timer_.begin(stream_, kPassLambdaVjp);
         lambda_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(la);
         timer_.end(stream_, kPassLambdaVjp);
