@@ -52,6 +52,33 @@ struct ParamAdjoint {
     double* vorticity;
 };
 
+// Per-pair quotients whose varying operand mostly repeats (uniform masses and rest densities): the
+// last quotient is kept and reused while that operand's bits repeat.  The operands are then the
+// same, so the correctly rounded quotient is the same.
+struct DividendCache {   // x / divisor for varying x
+    uint32_t key = 0xffffffffu;
+    float value = 0.0F;
+    __device__ __forceinline__ float operator()(const float x, const float divisor) {
+        if (__float_as_uint(x) != key) {
+            key = __float_as_uint(x);
+            value = x / divisor;
+        }
+        return value;
+    }
+};
+struct DivisorCache {    // dividend / y and 1 / y in FP64 for varying y
+    uint32_t key = 0xffffffffu;
+    float value = 0.0F;
+    double reciprocal = 0.0;
+    __device__ __forceinline__ void update(const float dividend, const float y) {
+        if (__float_as_uint(y) != key) {
+            key = __float_as_uint(y);
+            value = dividend / y;
+            reciprocal = 1.0 / static_cast<double>(y);
+        }
+    }
+};
+
 __device__ __forceinline__ void add_to(double* p, const uint32_t i, const double v) {
     if (p) p[i] += v;
 }
@@ -407,6 +434,8 @@ struct CorrectionVjpOp {
     KernelConstants k;
     d3 pc;
     double lc, mc, rc, sc, ec, qc;
+    DividendCache own_ratio;      // m_j / rho0_i
+    DivisorCache reverse_ratio;   // m_i / rho0_j
 
     __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
     __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
@@ -429,12 +458,13 @@ struct CorrectionVjpOp {
         const float2 sj = s_corr[t];
         const ArtificialPressure rap = sj.y != 0.0F ? zero_strength_pressure(weight, sj.x, pb.x, pb.y, false)
                                                     : artificial_pressure(scale(d, -1.0F), k, pb.x, pb.y, pb.z);
-        const float coefficient = q.w / rest_density;
+        const float coefficient = own_ratio(q.w, rest_density);
         const float lambda_j = lambda[t];
         const float multiplier = lambda_i + lambda_j + ap.value;
         const double scalar_adjoint = coefficient * dot(ob, gradient);
         const float rrest = params_a[t].x;
-        const float rcoefficient = mass / rrest;
+        reverse_ratio.update(mass, rrest);
+        const float rcoefficient = reverse_ratio.value;
         const float rmultiplier = lambda_j + lambda_i + rap.value;
         const d3 rob = ld3(correction[t]);
         const double rscalar = rcoefficient * dot(rob, rg);
@@ -550,6 +580,8 @@ struct LambdaVjpOp {
     double mc;
     double rc_pairs;   // the second neighbour loop's terms (pbf.cu:233-246), summed in this loop
     f3 self_gradient;
+    DividendCache own_ratio;      // m_j / rho0_i
+    DivisorCache reverse_ratio;   // m_i / rho0_j and 1 / rho0_j
 
     __device__ __forceinline__ uint32_t prefetch(const uint32_t t) const { return t; }
     __device__ __forceinline__ void apply(const uint32_t t, uint32_t) { process(t); }
@@ -569,7 +601,7 @@ struct LambdaVjpOp {
         const float r2 = squared(d);
         if (r2 == 0.0F || r2 >= k.adjoint_threshold) return;
         const f3 gradient = spiky_gradient(d, k);
-        const float coefficient = q.w / rest_density;
+        const float coefficient = own_ratio(q.w, rest_density);
         const f3 neighbor_gradient = times(gradient, -coefficient);
         const d3 neighbor_gradient_adjoint = times(neighbor_gradient, 2.0 * db);
         const d3 gradient_adjoint = times(sb - neighbor_gradient_adjoint, coefficient);
@@ -580,7 +612,8 @@ struct LambdaVjpOp {
         const double rdb = constraint_weight[t];   // the neighbour's db, as its own lambda VJP forms it
         const d3 rsb = times(xyz(gj), 2.0 * rdb);
         const f3 rg = scale(gradient, -1.0F);   // spiky_gradient(-d), exactly
-        const float rcoefficient = mass / rrest;
+        reverse_ratio.update(mass, rrest);
+        const float rcoefficient = reverse_ratio.value;
         const f3 rneighbor_gradient = times(rg, -rcoefficient);
         const d3 rneighbor_gradient_adjoint = times(rneighbor_gradient, 2.0 * rdb);
         const d3 rgradient_adjoint = times(rsb - rneighbor_gradient_adjoint, rcoefficient);
@@ -588,7 +621,7 @@ struct LambdaVjpOp {
         spiky_hessian_products(d, gradient_adjoint, rgradient_adjoint, k, hessian, reverse_hessian);
         pc = pc + hessian;
         pc = pc + times(reverse_hessian, -1.0);
-        mc += dot(rsb - rneighbor_gradient_adjoint, rg) / rrest;
+        mc += dot(rsb - rneighbor_gradient_adjoint, rg) * reverse_ratio.reciprocal;
     }
 };
 
