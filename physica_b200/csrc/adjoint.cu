@@ -191,16 +191,18 @@ struct XsphVjpOp {
         const f3 vj = xyz(confined[t]);
         const f3 difference = vj - v;
         const float weight = poly6(d, k);
+        const f3 gradient = poly6_gradient(d, k);
         vc = vc + times(ob, -viscosity * weight);
-        pc = pc + times(poly6_gradient(d, k), viscosity * dot(ob, difference));
+        pc = pc + times(gradient, viscosity * dot(ob, difference));
         cc += weight * dot(ob, difference);
-        const f3 rd = scale(d, -1.0F);
         const d3 rob = ld3(output_velocity[t]);
         const f3 rdiff = v - vj;
-        const float rweight = poly6(rd, k);
+        // W(-d) = W(d) and grad W(-d) = -grad W(d), exactly (the same squared distance; every
+        // component is a product whose sign alone flips)
+        const float rweight = weight;
         const float rviscosity = params_a[t].z;
         vc = vc + times(rob, rviscosity * rweight);
-        pc = pc + times(poly6_gradient(rd, k), -rviscosity * dot(rob, rdiff));
+        pc = pc + times(scale(gradient, -1.0F), -rviscosity * dot(rob, rdiff));
     }
 };
 
@@ -272,13 +274,14 @@ struct NormalVjpOp {
         const f3 gradient = spiky_gradient(d, k);
         const float magnitude_j = vorticity[t].w;
         const float difference = magnitude_j - magnitude;
-        pc = pc + spiky_hessian_product(d, times(eb, difference), k);
-        mc -= dot(eb, gradient);
-        const f3 rd = scale(d, -1.0F);
-        const f3 rg = spiky_gradient(rd, k);
+        const f3 rg = scale(gradient, -1.0F);   // spiky_gradient(-d), exactly
         const d3 reb = ld3(eta[t]);
         const float rdiff = magnitude - magnitude_j;
-        pc = pc + times(spiky_hessian_product(rd, times(reb, rdiff), k), -1.0);
+        d3 hessian, reverse_hessian;   // H(d) applied to both sides' adjoints; H(-d) = H(d)
+        spiky_hessian_products(d, times(eb, difference), times(reb, rdiff), k, hessian, reverse_hessian);
+        pc = pc + hessian;
+        mc -= dot(eb, gradient);
+        pc = pc + times(reverse_hessian, -1.0);
         mc += dot(reb, rg);
     }
 };
@@ -336,14 +339,15 @@ struct VorticityVjpOp {
         const f3 gradient = spiky_gradient(d, k);
         const f3 vj = xyz(velocity[t]);
         const f3 difference = vj - v;
-        vc = vc + cross(wb, gradient);
-        pc = pc + spiky_hessian_product(d, cross(wb, difference), k);
         const d3 rwb = ld3(vorticity_adjoint[t]);
-        const f3 rd = scale(d, -1.0F);
-        const f3 rg = spiky_gradient(rd, k);
+        const f3 rg = scale(gradient, -1.0F);   // spiky_gradient(-d), exactly
         const f3 rdiff = v - vj;
+        d3 hessian, reverse_hessian;   // H(d) applied to both sides' adjoints; H(-d) = H(d)
+        spiky_hessian_products(d, cross(wb, difference), cross(rwb, rdiff), k, hessian, reverse_hessian);
+        vc = vc + cross(wb, gradient);
+        pc = pc + hessian;
         vc = vc + cross(rg, rwb);
-        pc = pc + times(spiky_hessian_product(rd, cross(rwb, rdiff), k), -1.0);
+        pc = pc + times(reverse_hessian, -1.0);
     }
 };
 
