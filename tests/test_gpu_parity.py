@@ -353,7 +353,7 @@ def test_benchmark_workload_matches_reference_bit_for_bit():
     """The 1,048,576-particle benchmark dam break (8 iterations, 4,096,000 cells) for its full 200
     substeps: through the graph-replayed, autotuned solver, every substep equals the reference
     kernels' bit for bit, past substep 27, from where single particles jump by up to 220 h in one
-    iteration.  The north-star bar is 1e-4 h after 100 steps; max |dx| / h and max |dv| are printed
+    iteration.  The accuracy bar is 1e-4 h after 100 steps; max |dx| / h and max |dv| are printed
     at substeps 1, 10, 100 and 200."""
     reference = reference_or_skip()
     sc = scenes.plain_large()
