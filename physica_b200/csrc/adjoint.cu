@@ -32,6 +32,8 @@ struct AdjointWorkspace {
     double* density = nullptr;
     double* constraint_weight = nullptr;   // lambda adjoint x C / D^2 of each particle (the lambda VJP's db)
     float2* s_corr = nullptr;             // (W(s_corr radius), 1 when the strength is zero and the power stays finite)
+    float4* reverse = nullptr;            // (rho0, s_corr strength, exponent, zero-strength flag): a neighbour's
+                                          // reverse-term inputs in one load
 };
 
 void destroy_adjoint_workspace(void* workspace) { delete static_cast<AdjointWorkspace*>(workspace); }
@@ -131,7 +133,7 @@ __device__ __forceinline__ void finish(const Tail& t, const uint32_t s, const ui
 // ----------------------------------------------------------------- seed
 __global__ void seed_kernel(const GatherCommon g, const uint32_t* __restrict__ sorted_index, const ConstAdjField3 next_x,
                             const ConstAdjField3 next_v, double4* __restrict__ x, double4* __restrict__ out_v,
-                            float2* __restrict__ s_corr) {
+                            float2* __restrict__ s_corr, float4* __restrict__ reverse) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.count) return;
     const uint32_t i = sorted_index[s];
@@ -150,6 +152,7 @@ __global__ void seed_kernel(const GatherCommon g, const uint32_t* __restrict__ s
         zero_strength = largest < 1e30F;
     }
     s_corr[s] = make_float2(reference, zero_strength ? 1.0F : 0.0F);
+    reverse[s] = make_float4(g.params_a[s].x, pb.x, pb.y, zero_strength ? 1.0F : 0.0F);
 }
 
 // ------------------------------------------------------- XSPH + confinement
@@ -407,6 +410,7 @@ struct CorrectionVjpArgs {
     const uint32_t* sorted_index;
     const float4* pos;
     const float2* s_corr;
+    const float4* reverse;
     const float* lambda;
     const double4* correction;
     double4* x;
@@ -424,13 +428,12 @@ struct CorrectionVjpOp {
     static constexpr bool kBoundary = true;
     const float4* __restrict__ pos;
     const float4* __restrict__ boundary;
-    const float2* __restrict__ s_corr;
     float reference_i;
     bool zero_strength_i;
     const float* __restrict__ lambda;
     const double4* __restrict__ correction;
-    const float4* __restrict__ params_a;
     const float4* __restrict__ params_b;
+    const float4* __restrict__ reverse;
     f3 x;
     float mass, rest_density, lambda_i, strength, exponent, radius;
     d3 ob;
@@ -458,15 +461,14 @@ struct CorrectionVjpOp {
         const float weight = r2 >= k.h2 ? 0.0F : poly6_inside(r2, k);   // W(d) = W(-d)
         const ArtificialPressure ap = zero_strength_i ? zero_strength_pressure(weight, reference_i, strength, exponent, true)
                                                       : artificial_pressure(d, k, strength, exponent, radius);
-        const float4 pb = params_b[t];
-        const float2 sj = s_corr[t];
-        const ArtificialPressure rap = sj.y != 0.0F ? zero_strength_pressure(weight, sj.x, pb.x, pb.y, false)
-                                                    : artificial_pressure(scale(d, -1.0F), k, pb.x, pb.y, pb.z);
+        const float4 rv = reverse[t];   // (rho0_j, strength_j, exponent_j, zero-strength flag)
+        const ArtificialPressure rap = rv.w != 0.0F ? zero_strength_pressure(weight, 1.0F, rv.y, rv.z, false)
+                                                    : artificial_pressure(scale(d, -1.0F), k, rv.y, rv.z, params_b[t].z);
         const float coefficient = own_ratio(q.w, rest_density);
         const float lambda_j = lambda[t];
         const float multiplier = lambda_i + lambda_j + ap.value;
         const double scalar_adjoint = coefficient * dot(ob, gradient);
-        const float rrest = params_a[t].x;
+        const float rrest = rv.x;
         reverse_ratio.update(mass, rrest);
         const float rcoefficient = reverse_ratio.value;
         const float rmultiplier = lambda_j + lambda_i + rap.value;
@@ -512,14 +514,13 @@ __global__ void __launch_bounds__(kBlock, 4) correction_vjp_kernel(const Correct
     CorrectionVjpOp op;
     op.pos = a.pos;
     op.boundary = a.g.boundary;
-    op.s_corr = a.s_corr;
     const float2 si = p.active ? a.s_corr[p.s] : make_float2(1.0F, 0.0F);
     op.reference_i = si.x;
     op.zero_strength_i = si.y != 0.0F;
     op.lambda = a.lambda;
     op.correction = a.correction;
-    op.params_a = a.g.params_a;
     op.params_b = a.g.params_b;
+    op.reverse = a.reverse;
     op.self = p.s;
     op.k = p.k;
     const float4 xi = p.active ? a.pos[p.s] : make_float4(0, 0, 0, 0);
@@ -866,6 +867,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
         ws->density = ws->arena.alloc<double>(n, e);
         ws->constraint_weight = ws->arena.alloc<double>(n, e);
         ws->s_corr = ws->arena.alloc<float2>(n, e);
+        ws->reverse = ws->arena.alloc<float4>(n, e);
         if (e != cudaSuccess) {
             delete ws;
             return check(e, "adjoint workspace");
@@ -898,7 +900,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
     seed_kernel<<<grid_of(n, 256), 256, 0, stream_>>>(
         gc, r.sorted_index, {next_adjoint->positions.x, next_adjoint->positions.y, next_adjoint->positions.z},
         {next_adjoint->velocities.x, next_adjoint->velocities.y, next_adjoint->velocities.z}, ws->x[0], ws->output_velocity,
-        ws->s_corr);
+        ws->s_corr, ws->reverse);
     timer_.end(stream_, kPassSeed);
     XsphVjpArgs xa{gc, post_list, r.sorted_index, xK, r.confined, r.vorticity, r.normal, ws->output_velocity, ws->x[0], ws->velocity,
                    ws->vorticity, ws->eta, pa};
@@ -944,8 +946,8 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
             density_k = segment_->density[j];
             gsum_k = segment_->gsum[j];
         }
-        CorrectionVjpArgs ca{gc, it_list, r.sorted_index, xk, ws->s_corr, lambda_k, ws->correction, acc, ws->lambda, pa,
-                             density_k, gsum_k, ws->constraint_weight};
+        CorrectionVjpArgs ca{gc, it_list, r.sorted_index, xk, ws->s_corr, ws->reverse, lambda_k, ws->correction, acc,
+                             ws->lambda, pa, density_k, gsum_k, ws->constraint_weight};
         timer_.begin(stream_, kPassCorrectionVjp);
         correction_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(ca);
         timer_.end(stream_, kPassCorrectionVjp);
