@@ -31,6 +31,7 @@ struct AdjointWorkspace {
     double* lambda = nullptr;
     double* density = nullptr;
     double* constraint_weight = nullptr;   // lambda adjoint x C / D^2 of each particle (the lambda VJP's db)
+    float4* gradient_sum_rest = nullptr;   // (S, rho0) of each particle, the lambda VJP's per-neighbour inputs
     float2* s_corr = nullptr;             // (W(s_corr radius), 1 when the strength is zero and the power stays finite)
     float4* reverse = nullptr;            // (rho0, s_corr strength, exponent, zero-strength flag): a neighbour's
                                           // reverse-term inputs in one load
@@ -422,6 +423,7 @@ struct CorrectionVjpArgs {
     const float* density;
     const float4* gsum;          // (S, D)
     double* constraint_weight;
+    float4* gradient_sum_rest;   // (S, rho0): the lambda VJP reads a neighbour's in one load
 };
 
 struct CorrectionVjpOp {
@@ -543,8 +545,10 @@ __global__ void __launch_bounds__(kBlock, 4) correction_vjp_kernel(const Correct
     const double lb = 0.0 + op.lc;
     a.lambda_adjoint[p.s] = lb;
     const double constraint = static_cast<double>(a.density[p.s]) / pa.x - 1.0;
-    const float denominator = a.gsum[p.s].w;
+    const float4 gsum = a.gsum[p.s];
+    const float denominator = gsum.w;
     a.constraint_weight[p.s] = lb * constraint / (static_cast<double>(denominator) * denominator);
+    a.gradient_sum_rest[p.s] = make_float4(gsum.x, gsum.y, gsum.z, pa.x);
     add_to(a.pa.masses, i, op.mc);
     add_to(a.pa.rest_densities, i, -op.rc / pa.x);
     add_to(a.pa.strength, i, op.sc);
@@ -562,6 +566,7 @@ struct LambdaVjpArgs {
     const float4* gsum;          // (S, D)
     const double* lambda_adjoint;
     const double* constraint_weight;
+    const float4* gradient_sum_rest;
     double4* x;
     double* density_adjoint;
     ParamAdjoint pa;
@@ -572,9 +577,8 @@ struct LambdaVjpOp {
     const float4* __restrict__ pos;
     const float4* __restrict__ boundary;
     const float* __restrict__ density;
-    const float4* __restrict__ gsum;
+    const float4* __restrict__ gradient_sum_rest;
     const double* __restrict__ constraint_weight;
-    const float4* __restrict__ params_a;
     f3 x;
     float mass, rest_density;
     double db;
@@ -612,8 +616,8 @@ struct LambdaVjpOp {
         const d3 gradient_adjoint = times(sb - neighbor_gradient_adjoint, coefficient);
         self_gradient = fma3(coefficient, gradient, self_gradient);
         rc_pairs += dot(neighbor_gradient_adjoint, neighbor_gradient);   // divided by -rho0_i once, at the end
-        const float rrest = params_a[t].x;
-        const float4 gj = gsum[t];
+        const float4 gj = gradient_sum_rest[t];   // (S_j, rho0_j)
+        const float rrest = gj.w;
         const double rdb = constraint_weight[t];   // the neighbour's db, as its own lambda VJP forms it
         const d3 rsb = times(xyz(gj), 2.0 * rdb);
         const f3 rg = scale(gradient, -1.0F);   // spiky_gradient(-d), exactly
@@ -639,9 +643,8 @@ __global__ void __launch_bounds__(kBlock, PBF_LAMBDA_VJP_MIN_BLOCKS) lambda_vjp_
     op.pos = a.pos;
     op.boundary = a.g.boundary;
     op.density = a.density;
-    op.gsum = a.gsum;
+    op.gradient_sum_rest = a.gradient_sum_rest;
     op.constraint_weight = a.constraint_weight;
-    op.params_a = a.g.params_a;
     op.self = p.s;
     op.k = p.k;
     const float4 xi = p.active ? a.pos[p.s] : make_float4(0, 0, 0, 0);
@@ -866,6 +869,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
         ws->lambda = ws->arena.alloc<double>(n, e);
         ws->density = ws->arena.alloc<double>(n, e);
         ws->constraint_weight = ws->arena.alloc<double>(n, e);
+        ws->gradient_sum_rest = ws->arena.alloc<float4>(n, e);
         ws->s_corr = ws->arena.alloc<float2>(n, e);
         ws->reverse = ws->arena.alloc<float4>(n, e);
         if (e != cudaSuccess) {
@@ -947,12 +951,12 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
             gsum_k = segment_->gsum[j];
         }
         CorrectionVjpArgs ca{gc, it_list, r.sorted_index, xk, ws->s_corr, ws->reverse, lambda_k, ws->correction, acc,
-                             ws->lambda, pa, density_k, gsum_k, ws->constraint_weight};
+                             ws->lambda, pa, density_k, gsum_k, ws->constraint_weight, ws->gradient_sum_rest};
         timer_.begin(stream_, kPassCorrectionVjp);
         correction_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(ca);
         timer_.end(stream_, kPassCorrectionVjp);
-        LambdaVjpArgs la{gc_reverse, it_list, r.sorted_index, xk, density_k, gsum_k, ws->lambda, ws->constraint_weight, acc,
-                         ws->density, pa};
+        LambdaVjpArgs la{gc_reverse, it_list, r.sorted_index, xk, density_k, gsum_k, ws->lambda, ws->constraint_weight,
+                         ws->gradient_sum_rest, acc, ws->density, pa};
         timer_.begin(stream_, kPassLambdaVjp);
         lambda_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(la);
         timer_.end(stream_, kPassLambdaVjp);
