@@ -107,24 +107,71 @@ def test_batched_rollout_gradients_equal_per_scene_rollouts():
 
 def test_benchmark_batch_equals_per_scene_solvers():
     """The 256-scene batched benchmark (2,048-65,536 particles per scene, 4 iterations), autotuned
-    and graph-replayed as bench.py runs it: three substeps equal each scene's own solver bit for bit."""
+    and graph-replayed as bench.py runs it, for its full 100 substeps: every scene equals its own
+    solver bit for bit, and eight of them (every 32nd) equal the reference's kernels bit for bit."""
+    from oracle import reference
     scs = scenes.batched_forward()
+    steps = 100
     batch, state, control, params = pbf.batch_for_scenes(scs)
     batch.autotune(state, control, params, repeats=1)
     batch.set_graph_mode(True)
     cur, nxt = pbf.State(state.positions.clone(), state.velocities.clone(), 0), batch.allocate_state()
-    for _ in range(3):
+    for _ in range(steps):
         batch.forward_step(cur, control, params, nxt)
         cur, nxt = nxt, cur
     torch.cuda.synchronize()
     for s, sc in enumerate(scs):
         solver, st, ctl, prm = pbf.solver_for_scene(sc)
+        solver.set_graph_mode(True)
         cache = solver.allocate_step_cache()
         a, b = st, solver.allocate_state()
-        for _ in range(3):
+        for _ in range(steps):
             solver.forward_step(a, ctl, prm, b, cache)
             a, b = b, a
         sl = batch.particle_range(s)
         assert torch.equal(cur.positions[:, sl], a.positions), s
         assert torch.equal(cur.velocities[:, sl], a.velocities), s
         del solver, cache
+    if not reference.available():
+        return
+    for s in range(0, len(scs), 32):
+        ref = reference.ReferencePBF(scs[s])
+        x = torch.from_numpy(scs[s].positions).cuda().contiguous()
+        v = torch.from_numpy(scs[s].velocities).cuda().contiguous()
+        xo, vo = torch.zeros_like(x), torch.zeros_like(v)
+        for k in range(steps):
+            ref.forward_step(x, v, xo, vo, k)
+            x, xo, v, vo = xo, x, vo, v
+        torch.cuda.synchronize()
+        sl = batch.particle_range(s)
+        assert torch.equal(cur.positions[:, sl], x), s
+        assert torch.equal(cur.velocities[:, sl], v), s
+        ref.close()
+
+
+def test_batched_adjoint_benchmark_equals_per_scene_rollouts():
+    """The 32-scene batched adjoint configuration (16,384-131,072 particles per scene, 4 iterations)
+    at its full length: a 100-step rollout with trajectory checkpoints every 10 gives every scene
+    exactly the loss, dL/dv0 and dL/dc of that scene's own rollout."""
+    import gc
+    from physica_b200 import trajectory
+    scs = scenes.batched_adjoint()
+    steps, every = 100, 10
+    diff = pbf.ExecutionMode.differentiable
+    batch, state, control, params = pbf.batch_for_scenes(scs, mode=diff)
+    targets = torch.from_numpy(np.concatenate([sc.targets for sc in scs], axis=1)).cuda()
+    g = trajectory.loss_and_gradients(batch, state, control, params, targets, steps, every)
+    torch.cuda.synchronize()
+    ranges = [batch.particle_range(s) for s in range(len(scs))]
+    velocities = g.initial_velocities.clone()
+    losses, viscosity = list(g.loss), list(g.scalar["xsph_viscosity"])
+    del g, batch, state, control, params, targets
+    gc.collect()
+    for s, sc in enumerate(scs):
+        solver, st, ctl, prm = pbf.solver_for_scene(sc, mode=diff)
+        gs = trajectory.loss_and_gradients(solver, st, ctl, prm, torch.from_numpy(sc.targets).cuda(), steps, every)
+        assert losses[s] == gs.loss, s
+        assert torch.equal(velocities[:, ranges[s]], gs.initial_velocities), s
+        assert viscosity[s] == gs.scalar["xsph_viscosity"], s
+        del solver, gs
+        gc.collect()
