@@ -511,7 +511,11 @@ struct CorrectionVjpOp {
 };
 
 // Four resident blocks per SM (at most 128 registers) hide more latency than the unbounded 144.
-__global__ void __launch_bounds__(kBlock, 4) correction_vjp_kernel(const CorrectionVjpArgs a) {
+// 5 blocks per SM (96 registers, 616 bytes of spills) took the 64k rollout from 720 to 644 grad-steps/s.
+#ifndef PBF_CORRECTION_VJP_MIN_BLOCKS
+#define PBF_CORRECTION_VJP_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(kBlock, PBF_CORRECTION_VJP_MIN_BLOCKS) correction_vjp_kernel(const CorrectionVjpArgs a) {
     const Particle p = locate(a.g);
     CorrectionVjpOp op;
     op.pos = a.pos;
