@@ -67,6 +67,7 @@ int run(const char* input, const char* output) {
     const auto n = read_one<std::uint32_t>(in);
     const auto iterations = read_one<std::uint32_t>(in);
     const auto steps = read_one<std::uint32_t>(in);
+    const bool recompute = read_one<std::uint32_t>(in) != 0u;   // keep checkpoints only (interval 2)
     pp::DomainConfiguration domain{};
     domain.particle_count = n;
     domain.time_step = read_one<float>(in);
@@ -87,7 +88,9 @@ int run(const char* input, const char* output) {
     {
         pp::PBF::Configuration configuration;
         configuration.pressure_iterations = iterations;
+        configuration.checkpoint_interval = 2u;
         pp::PBF solver(domain, configuration, pp::ExecutionMode::differentiable, stream);
+        solver.set_checkpoint_recompute(recompute);
         pp::PBF::State current = solver.allocate_state(), next = solver.allocate_state();
         pp::upload(fields[0], current.particles.positions.x, stream);
         pp::upload(fields[1], current.particles.positions.y, stream);

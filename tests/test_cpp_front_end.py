@@ -41,7 +41,10 @@ def test_cpp_front_end_compiles_and_links():
 
 
 @pytest.mark.gpu
-def test_cpp_front_end_matches_python_binding(tmp_path, cuda_lib):
+@pytest.mark.parametrize("recompute", [0, 1])
+def test_cpp_front_end_matches_python_binding(tmp_path, cuda_lib, recompute):
+    """recompute 1: the C++ solver keeps every second iterate only and recomputes the rest for the
+    tangent and the adjoint; the Python solver keeps them all.  The results are the same bits."""
     import torch
     from physica_b200 import pbf, scenes
 
@@ -54,7 +57,7 @@ def test_cpp_front_end_matches_python_binding(tmp_path, cuda_lib):
     names = ("masses", "rest_densities", "viscosities", "surface_tensions", "relaxation", "artificial_pressure_strength",
              "artificial_pressure_exponent", "artificial_pressure_radius", "xsph_viscosity", "vorticity_confinement")
     with open(tmp_path / "in.bin", "wb") as f:
-        np.array([n, sc.pressure_iterations, steps], dtype=np.uint32).tofile(f)
+        np.array([n, sc.pressure_iterations, steps, recompute], dtype=np.uint32).tofile(f)
         np.array([sc.time_step, sc.support_radius, sc.particle_radius, *sc.gravity, *sc.box_min, *sc.box_max,
                   *sc.box_velocity], dtype=np.float32).tofile(f)
         np.array([1 if sc.no_slip else 0], dtype=np.uint32).tofile(f)
