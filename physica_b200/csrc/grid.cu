@@ -127,12 +127,28 @@ __global__ void scan_apply_kernel(uint32_t* __restrict__ data, const uint64_t n,
     uint32_t vals[kScanItems];
     uint32_t local = 0;
     const uint64_t first = base + static_cast<uint64_t>(threadIdx.x) * kScanItems;
+    // a whole tile of a 16-byte aligned array moves as uint4 (four loads and stores per thread
+    // instead of sixteen); the last tile and unaligned arrays take the element loop
+    const bool vector = base + kScanTile <= n && (reinterpret_cast<uintptr_t>(data) & 15u) == 0u;
+    if (vector) {
+        const uint4* const src = reinterpret_cast<const uint4*>(data + first);
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint64_t idx = first + k;
-        vals[k] = idx < n ? data[idx] : 0u;
-        local += vals[k];
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            const uint4 v = src[q];
+            vals[4 * q] = v.x;
+            vals[4 * q + 1] = v.y;
+            vals[4 * q + 2] = v.z;
+            vals[4 * q + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            const uint64_t idx = first + k;
+            vals[k] = idx < n ? data[idx] : 0u;
+        }
     }
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) local += vals[k];
     __shared__ uint32_t warp_tot[kScanThreads / 32];
     const uint32_t inc = warp_inclusive(local);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -141,6 +157,23 @@ __global__ void scan_apply_kernel(uint32_t* __restrict__ data, const uint64_t n,
     uint32_t warp_prefix = 0;
     for (int w = 0; w < warp; ++w) warp_prefix += warp_tot[w];
     uint32_t running = tile_sums[blockIdx.x] + warp_prefix + inc - local;
+    if (vector) {
+        uint4* const dst = reinterpret_cast<uint4*>(data + first);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            uint4 v;
+            v.x = running;
+            running += vals[4 * q];
+            v.y = running;
+            running += vals[4 * q + 1];
+            v.z = running;
+            running += vals[4 * q + 2];
+            v.w = running;
+            running += vals[4 * q + 3];
+            dst[q] = v;
+        }
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         const uint64_t idx = first + k;
