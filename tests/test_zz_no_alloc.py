@@ -103,6 +103,32 @@ def test_repeated_calls_allocate_no_device_memory():
     assert free_after == free_before
 
 
+def test_a_call_records_into_a_cuda_graph_under_global_capture():
+    """After the set-up call, a call records into a CUDA graph in global capture mode, where
+    cudaMalloc and every synchronising call fail the capture; the replayed graph gives the direct
+    call's bits.  This also catches an allocation freed again before the call returns."""
+    sc = scenes.plain_small(seed=24)
+    fn = _entry()
+    solver, state, control, params = pbf.solver_for_scene(sc)
+    dc = pbf.DomainConfiguration.from_scene(sc).to_c()
+    cc = pbf.ConfigurationC(sc.pressure_iterations, 1)
+    direct = solver.allocate_state()
+    _preallocated_step(fn, dc, cc, state, control, params, direct, solver.stream)
+    torch.cuda.synchronize()
+    replayed = solver.allocate_state()
+    stream = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream, capture_error_mode="global"):
+        _preallocated_step(fn, dc, cc, state, control, params, replayed, stream)
+    replayed.positions.fill_(float("nan"))
+    replayed.velocities.fill_(float("nan"))
+    graph.replay()
+    torch.cuda.synchronize()
+    assert replayed.step_index == direct.step_index
+    assert torch.equal(replayed.positions, direct.positions)
+    assert torch.equal(replayed.velocities, direct.velocities)
+
+
 def test_sizes_beyond_the_maximum_are_rejected():
     fn = _entry()
     sc = scenes.dam_break((4, 4, 4), (0, 0, 0), (1, 2, 1), 23, 2)
