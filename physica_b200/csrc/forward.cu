@@ -683,8 +683,21 @@ struct CorrectionOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
+// Resident 128-thread blocks per SM the register budget of the correction and of the post-loop
+// passes is sized for (compile-time tuning knobs; 1 leaves the register count to the compiler).
+// At 1M particles (substeps 25-28, ms per launch): the correction at 9 (56 registers instead of
+// 58, 36 resident warps instead of 32) 0.193 against 0.203, at 10 (48, spilling) 0.286; the
+// vorticity / normal / XSPH passes at 10 (48 registers) 0.192 / 0.176 / 0.188 against 0.207 /
+// 0.183 / 0.196 unbounded.
+#ifndef PBF_CORRECTION_MIN_BLOCKS
+#define PBF_CORRECTION_MIN_BLOCKS 9
+#endif
+#ifndef PBF_POST_MIN_BLOCKS
+#define PBF_POST_MIN_BLOCKS 10
+#endif
+
 template <bool WithBoundary, bool Masks>
-__global__ void __launch_bounds__(kBlock) correction_kernel(const CorrectionArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_CORRECTION_MIN_BLOCKS) correction_kernel(const CorrectionArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
     CorrectionOp<WithBoundary> op;
@@ -759,7 +772,7 @@ struct VorticityOp {
 };
 
 template <bool Masks>
-__global__ void __launch_bounds__(kBlock) vorticity_kernel(const VorticityArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_POST_MIN_BLOCKS) vorticity_kernel(const VorticityArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
     VorticityOp op;
@@ -802,7 +815,7 @@ struct NormalOp {
 };
 
 template <bool Masks>
-__global__ void __launch_bounds__(kBlock) normal_kernel(const NormalArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_POST_MIN_BLOCKS) normal_kernel(const NormalArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
     NormalOp op;
@@ -846,7 +859,7 @@ struct XsphOp {
 };
 
 template <bool Masks>
-__global__ void __launch_bounds__(kBlock) xsph_kernel(const XsphArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_POST_MIN_BLOCKS) xsph_kernel(const XsphArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
     XsphOp op;
