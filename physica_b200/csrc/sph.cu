@@ -31,6 +31,23 @@ namespace {
 using namespace gather_detail;
 using namespace detail;
 
+// Resident 128-thread blocks per SM the register budgets of the list-replay passes are sized for
+// (compile-time tuning knobs; 1 leaves the register count to the compiler).  The density passes'
+// per-entry work is a few multiply-adds, so they wait on their neighbours' loads and gain from
+// more resident warps even with a few spills.  At 1M particles (ms per substep, PCISPH / DFSPH,
+// same box): unbounded 2.60 / 4.17; density at 14 (32 registers) and pressure at 10 (48) 2.30 /
+// 3.65; density at 12 (40) 2.37 / 3.75 (with pressure at 10); density at 20 (24) 2.36 / 3.73;
+// pressure at 12 (40) 2.52 / 4.05; the non-pressure pass at 8 (64 instead of 72) no change.
+#ifndef PBF_SPH_DENSITY_MIN_BLOCKS
+#define PBF_SPH_DENSITY_MIN_BLOCKS 14
+#endif
+#ifndef PBF_SPH_NON_PRESSURE_MIN_BLOCKS
+#define PBF_SPH_NON_PRESSURE_MIN_BLOCKS 1
+#endif
+#ifndef PBF_SPH_PRESSURE_MIN_BLOCKS
+#define PBF_SPH_PRESSURE_MIN_BLOCKS 10
+#endif
+
 // ------------------------------------------------------------------ density (+ Tait EOS)
 template <bool WithBoundary>
 struct DensityOp {
@@ -58,7 +75,7 @@ struct DensityOp {
 };
 
 template <bool WithBoundary>
-__global__ void __launch_bounds__(kBlock) sph_density_kernel(const SphStep st, const uint32_t method, float* density_record,
+__global__ void __launch_bounds__(kBlock, PBF_SPH_DENSITY_MIN_BLOCKS) sph_density_kernel(const SphStep st, const uint32_t method, float* density_record,
                                                              float* pressure, float* pressure_term, const float* warm) {
     const Own o = own(st);
     if (!o.p.active) return;
@@ -293,7 +310,7 @@ struct NonPressureOp {
 };
 
 template <bool WithBoundary>
-__global__ void __launch_bounds__(kBlock) non_pressure_kernel(const SphStep st, const int mode, const MutField3 out_positions,
+__global__ void __launch_bounds__(kBlock, PBF_SPH_NON_PRESSURE_MIN_BLOCKS) non_pressure_kernel(const SphStep st, const int mode, const MutField3 out_positions,
                                                               const MutField3 out_velocities, const uint32_t displacement_slot) {
     const Own o = own(st);
     if (!o.p.active) return;
@@ -360,7 +377,7 @@ struct PredictedDensityOp {
 
 
 template <bool WithBoundary>
-__global__ void __launch_bounds__(kBlock) predicted_density_kernel(const SphStep st, const PressureUpdate update,
+__global__ void __launch_bounds__(kBlock, PBF_SPH_DENSITY_MIN_BLOCKS) predicted_density_kernel(const SphStep st, const PressureUpdate update,
                                                                    float* pressure, float* pressure_term, float* record) {
     const Own o = own(st);
     if (!o.p.active) return;
@@ -436,7 +453,7 @@ struct PressureKernelArgs {
 };
 
 template <bool WithBoundary>
-__global__ void __launch_bounds__(kBlock) pressure_kernel(const PressureKernelArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_SPH_PRESSURE_MIN_BLOCKS) pressure_kernel(const PressureKernelArgs a) {
     const SphStep& st = a.st;
     const Own o = own(st);
     if (!o.p.active) return;
