@@ -1150,6 +1150,8 @@ def main():
                                                              "line (profiling)")
     ap.add_argument("--tangent-only", action="store_true", help="time only the 1M differentiable substep + jvp_step "
                                                                 "and print its line (profiling)")
+    ap.add_argument("--batch-grad-only", action="store_true", help="time only the 32-scene batched rollout against "
+                                                                   "one rollout per scene and print its line (profiling)")
     ap.add_argument("--launch-shape", default="", help="fixed list-scan variant, its block size and optionally the "
                                                         "gather passes' block size, e.g. per_lane:128 or per_lane:128:32 "
                                                         "(gather passes at 128 unless given; default: autotuned)")
@@ -1166,6 +1168,9 @@ def main():
         sc = scenes.plain_large(seed=2 + rank)
         run = reference_tangent_ms if args.impl == "reference" else tangent_ms
         out = {"impl": args.impl, "tangent_ms_per_step": run(args, world, sc)}
+    elif args.batch_grad_only:   # the reference has no batched form
+        out = {"impl": args.impl,
+               "batched_grad_steps_per_s": None if args.impl == "reference" else bench_batch_grad(args, world, rank)}
     elif args.grad_only:
         out = {"impl": args.impl,
                "grad_steps_per_s": bench_reference_grad(world, rank) if args.impl == "reference" else bench_grad(args, world, rank)}

@@ -210,7 +210,16 @@ struct XsphVjpOp {
     }
 };
 
-__global__ void __launch_bounds__(kBlock) xsph_vjp_kernel(const XsphVjpArgs a) {
+// Resident 128-thread blocks per SM the register budgets of the post-loop reverse passes and of
+// the density VJP are sized for (compile-time tuning knobs; 1 leaves the register count to the
+// compiler).
+#ifndef PBF_POST_VJP_MIN_BLOCKS
+#define PBF_POST_VJP_MIN_BLOCKS 1
+#endif
+#ifndef PBF_DENSITY_VJP_MIN_BLOCKS
+#define PBF_DENSITY_VJP_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(kBlock, PBF_POST_VJP_MIN_BLOCKS) xsph_vjp_kernel(const XsphVjpArgs a) {
     const Particle p = locate(a.g);
     XsphVjpOp op;
     op.pos = a.pos;
@@ -290,7 +299,7 @@ struct NormalVjpOp {
     }
 };
 
-__global__ void __launch_bounds__(kBlock) normal_vjp_kernel(const NormalVjpArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_POST_VJP_MIN_BLOCKS) normal_vjp_kernel(const NormalVjpArgs a) {
     const Particle p = locate(a.g);
     NormalVjpOp op;
     op.pos = a.pos;
@@ -355,7 +364,7 @@ struct VorticityVjpOp {
     }
 };
 
-__global__ void __launch_bounds__(kBlock) vorticity_vjp_kernel(const VorticityVjpArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_POST_VJP_MIN_BLOCKS) vorticity_vjp_kernel(const VorticityVjpArgs a) {
     const Particle p = locate(a.g);
     VorticityVjpOp op;
     op.pos = a.pos;
@@ -728,7 +737,7 @@ struct DensityVjpOp {
     }
 };
 
-__global__ void __launch_bounds__(kBlock) density_vjp_kernel(const DensityVjpArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_DENSITY_VJP_MIN_BLOCKS) density_vjp_kernel(const DensityVjpArgs a) {
     const Particle p = locate(a.g);
     DensityVjpOp op;
     op.pos = a.pos;

@@ -174,7 +174,12 @@ struct DensityLambdaJvpOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-__global__ void __launch_bounds__(kBlock) density_lambda_jvp_kernel(const DensityLambdaJvpArgs a) {
+// Resident 128-thread blocks per SM the register budget of the tangent's list-replay passes is
+// sized for (a compile-time tuning knob; 1 leaves the register count to the compiler).
+#ifndef PBF_JVP_MIN_BLOCKS
+#define PBF_JVP_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(kBlock, PBF_JVP_MIN_BLOCKS) density_lambda_jvp_kernel(const DensityLambdaJvpArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
     DensityLambdaJvpOp op;
@@ -382,7 +387,7 @@ struct VorticityJvpOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-__global__ void __launch_bounds__(kBlock) vorticity_jvp_kernel(const VorticityJvpArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_JVP_MIN_BLOCKS) vorticity_jvp_kernel(const VorticityJvpArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
     VorticityJvpOp op;
@@ -448,7 +453,7 @@ struct NormalJvpOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-__global__ void __launch_bounds__(kBlock) normal_jvp_kernel(const NormalJvpArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_JVP_MIN_BLOCKS) normal_jvp_kernel(const NormalJvpArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
     NormalJvpOp op;
@@ -522,7 +527,7 @@ struct XsphJvpOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-__global__ void __launch_bounds__(kBlock) xsph_jvp_kernel(const XsphJvpArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_JVP_MIN_BLOCKS) xsph_jvp_kernel(const XsphJvpArgs a) {
     const Particle p = locate(a.g);
     if (!p.active) return;
     XsphJvpOp op;
