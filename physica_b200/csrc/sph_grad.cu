@@ -17,6 +17,22 @@
 //           predicted density + the prediction that produced it -> non-pressure -> density
 #include "sph_math.cuh"
 
+// Resident 128-thread blocks per SM the register budgets of the reverse and tangent list-replay
+// passes are sized for (compile-time tuning knobs; 1 leaves the register count to the compiler).
+// At 1M particles (ms per tangent step, PCISPH / DFSPH, same box): unbounded 8.76 / 15.13; the
+// density tangents at 12 (40 registers) and the pressure tangent at 8 (64) 7.75 / 13.24; the
+// density tangents at 10 (48) 7.88 / 13.43, at 14 (32) 8.93 / 15.40.  The density VJP at 10 (48)
+// made the gradient step 0.4 % slower.
+#ifndef PBF_SPH_DENSITY_VJP_MIN_BLOCKS
+#define PBF_SPH_DENSITY_VJP_MIN_BLOCKS 1
+#endif
+#ifndef PBF_SPH_DENSITY_JVP_MIN_BLOCKS
+#define PBF_SPH_DENSITY_JVP_MIN_BLOCKS 12
+#endif
+#ifndef PBF_SPH_PRESSURE_JVP_MIN_BLOCKS
+#define PBF_SPH_PRESSURE_JVP_MIN_BLOCKS 8
+#endif
+
 namespace pbf {
 namespace sph {
 
@@ -399,7 +415,7 @@ struct DensityVjpOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-__global__ void __launch_bounds__(kBlock) density_vjp_kernel(const DensityVjpArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_SPH_DENSITY_VJP_MIN_BLOCKS) density_vjp_kernel(const DensityVjpArgs a) {
     const SphStep& st = a.st;
     const Own o = own(st);
     if (!o.p.active) return;
@@ -907,7 +923,7 @@ struct DensityJvpOp {
 
 // The density tangent at the step's positions (+ WCSPH's equation of state, sph/wcsph.cu:102-117;
 // DFSPH: the divergence phase's warm-start pressure tangent).
-__global__ void __launch_bounds__(kBlock) density_jvp_kernel(const SphTangentStep t, const uint32_t method, const float* warm) {
+__global__ void __launch_bounds__(kBlock, PBF_SPH_DENSITY_JVP_MIN_BLOCKS) density_jvp_kernel(const SphTangentStep t, const uint32_t method, const float* warm) {
     const SphStep& st = t.st;
     const Own o = own(st);
     if (!o.p.active) return;
@@ -1257,7 +1273,7 @@ struct PredictedDensityJvpOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-__global__ void __launch_bounds__(kBlock) predicted_density_jvp_kernel(const SphTangentStep t, const PredictedJvp u) {
+__global__ void __launch_bounds__(kBlock, PBF_SPH_DENSITY_JVP_MIN_BLOCKS) predicted_density_jvp_kernel(const SphTangentStep t, const PredictedJvp u) {
     const SphStep& st = t.st;
     const Own o = own(st);
     if (!o.p.active) return;
@@ -1334,7 +1350,7 @@ struct PressureJvpOp {
     }
 };
 
-__global__ void __launch_bounds__(kBlock) pressure_jvp_kernel(const SphTangentStep t, const PressureJvp u) {
+__global__ void __launch_bounds__(kBlock, PBF_SPH_PRESSURE_JVP_MIN_BLOCKS) pressure_jvp_kernel(const SphTangentStep t, const PressureJvp u) {
     const SphStep& st = t.st;
     const Own o = own(st);
     if (!o.p.active) return;
