@@ -47,6 +47,9 @@ using namespace detail;
 #ifndef PBF_SPH_PRESSURE_MIN_BLOCKS
 #define PBF_SPH_PRESSURE_MIN_BLOCKS 10
 #endif
+#ifndef PBF_WCSPH_FORCE_MIN_BLOCKS
+#define PBF_WCSPH_FORCE_MIN_BLOCKS 4
+#endif
 
 // ------------------------------------------------------------------ density (+ Tait EOS)
 template <bool WithBoundary>
@@ -207,7 +210,7 @@ struct WcsphForceArgs {
 };
 
 template <bool WithBoundary>
-__global__ void __launch_bounds__(kBlock, 4) wcsph_force_kernel(const WcsphForceArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_WCSPH_FORCE_MIN_BLOCKS) wcsph_force_kernel(const WcsphForceArgs a) {
     const SphStep& st = a.st;
     const Own o = own(st);
     if (!o.p.active) return;
