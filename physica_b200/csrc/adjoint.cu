@@ -211,15 +211,15 @@ struct XsphVjpOp {
 };
 
 // Resident 128-thread blocks per SM the register budgets of the post-loop reverse passes and of
-// the density VJP are sized for (compile-time tuning knobs; 1 leaves the register count to the
+// the density VJP are sized for (compile-time tuning knobs; 0 leaves the register count to the
 // compiler).  Measured and not kept: the post-loop passes at 6 (80 registers) took the 32-scene
 // batched rollout from 34.6 to 35.3 grad-steps/s but the 64k rollout from 724 to 721; the density
 // VJP at 10 (48) 34.9 and 720.
 #ifndef PBF_POST_VJP_MIN_BLOCKS
-#define PBF_POST_VJP_MIN_BLOCKS 1
+#define PBF_POST_VJP_MIN_BLOCKS 0
 #endif
 #ifndef PBF_DENSITY_VJP_MIN_BLOCKS
-#define PBF_DENSITY_VJP_MIN_BLOCKS 1
+#define PBF_DENSITY_VJP_MIN_BLOCKS 0
 #endif
 __global__ void __launch_bounds__(kBlock, PBF_POST_VJP_MIN_BLOCKS) xsph_vjp_kernel(const XsphVjpArgs a) {
     const Particle p = locate(a.g);

@@ -684,7 +684,7 @@ struct CorrectionOp {
 };
 
 // Resident 128-thread blocks per SM the register budget of the correction and of the post-loop
-// passes is sized for (compile-time tuning knobs; 1 leaves the register count to the compiler).
+// passes is sized for (compile-time tuning knobs; 0 leaves the register count to the compiler).
 // At 1M particles (substeps 25-28, ms per launch): the correction at 9 (56 registers instead of
 // 58, 36 resident warps instead of 32) 0.193 against 0.203, at 10 (48, spilling) 0.286; the
 // vorticity / normal / XSPH passes at 10 (48 registers) 0.192 / 0.176 / 0.188 against 0.207 /

@@ -175,10 +175,10 @@ struct DensityLambdaJvpOp {
 };
 
 // Resident 128-thread blocks per SM the register budget of the tangent's list-replay passes is
-// sized for (a compile-time tuning knob; 1 leaves the register count to the compiler).  At 1M
+// sized for (a compile-time tuning knob; 0 leaves the register count to the compiler).  At 1M
 // particles the tangent step took 8.47 ms unbounded, 8.53 at 9 (56 registers), 9.78 at 10 (48).
 #ifndef PBF_JVP_MIN_BLOCKS
-#define PBF_JVP_MIN_BLOCKS 1
+#define PBF_JVP_MIN_BLOCKS 0
 #endif
 __global__ void __launch_bounds__(kBlock, PBF_JVP_MIN_BLOCKS) density_lambda_jvp_kernel(const DensityLambdaJvpArgs a) {
     const Particle p = locate(a.g);

@@ -32,23 +32,23 @@ using namespace gather_detail;
 using namespace detail;
 
 // Resident 128-thread blocks per SM the register budgets of the list-replay passes are sized for
-// (compile-time tuning knobs; 1 leaves the register count to the compiler).  The density passes'
+// (compile-time tuning knobs; 0 leaves the register count to the compiler).  The density passes'
 // per-entry work is a few multiply-adds, so they wait on their neighbours' loads and gain from
-// more resident warps even with a few spills.  At 1M particles (ms per substep, PCISPH / DFSPH,
-// same box): unbounded 2.60 / 4.17; density at 14 (32 registers) and pressure at 10 (48) 2.30 /
-// 3.65; density at 12 (40) 2.37 / 3.75 (with pressure at 10); density at 20 (24) 2.36 / 3.73;
-// pressure at 12 (40) 2.52 / 4.05; the non-pressure pass at 8 (64 instead of 72) no change.
+// more resident warps even with a few spills.  At 1M particles, ms per substep WCSPH / PCISPH /
+// DFSPH on one box: the compiler's registers (the force pass bounded to 4 blocks) 0.89 / 2.43 /
+// 3.85; these budgets 0.71 / 2.32 / 3.68.  Also measured, each against its neighbours in a sweep:
+// density at 12 (40 registers) or 20 (24) slower than at 14 (32); pressure at 12 (40) slower than
+// at 10 (48); the non-pressure pass at 8 (64 instead of 72) no change; the force pass at 7 (72,
+// spilling) slower than at 6 (80, 24 resident warps instead of 20 at 88).
 #ifndef PBF_SPH_DENSITY_MIN_BLOCKS
 #define PBF_SPH_DENSITY_MIN_BLOCKS 14
 #endif
 #ifndef PBF_SPH_NON_PRESSURE_MIN_BLOCKS
-#define PBF_SPH_NON_PRESSURE_MIN_BLOCKS 1
+#define PBF_SPH_NON_PRESSURE_MIN_BLOCKS 0
 #endif
 #ifndef PBF_SPH_PRESSURE_MIN_BLOCKS
 #define PBF_SPH_PRESSURE_MIN_BLOCKS 10
 #endif
-// The WCSPH force pass at 6 (80 registers, 24 resident warps instead of 20 at the compiler's 88):
-// 0.839 -> 0.690 ms per WCSPH substep at 1M; at 7 (72, spilling) 0.72.
 #ifndef PBF_WCSPH_FORCE_MIN_BLOCKS
 #define PBF_WCSPH_FORCE_MIN_BLOCKS 6
 #endif

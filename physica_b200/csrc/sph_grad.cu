@@ -18,19 +18,36 @@
 #include "sph_math.cuh"
 
 // Resident 128-thread blocks per SM the register budgets of the reverse and tangent list-replay
-// passes are sized for (compile-time tuning knobs; 1 leaves the register count to the compiler).
-// At 1M particles (ms per tangent step, PCISPH / DFSPH, same box): unbounded 8.76 / 15.13; the
-// density tangents at 12 (40 registers) and the pressure tangent at 8 (64) 7.75 / 13.24; the
-// density tangents at 10 (48) 7.88 / 13.43, at 14 (32) 8.93 / 15.40.  The density VJP at 10 (48)
-// made the gradient step 0.4 % slower.
+// passes are sized for (compile-time tuning knobs; 0 leaves the register count to the compiler).
+// At 1M particles, ms per tangent step WCSPH / PCISPH / DFSPH on one box: the compiler's registers
+// 2.35 / 8.91 / 15.36; these budgets 1.89 / 7.75 / 13.20.  Gradient steps: 3.28 / 10.74 / 17.81
+// against 3.01 / 10.63 / 17.62 (the WCSPH force VJP at 168 registers instead of 220).  Measured
+// and not kept: the pressure and non-pressure VJPs at 96 registers (spilling; PCISPH gradient
+// 10.63 -> 11.02), the density VJP at 48 (0.4 % slower), the density tangents at 14 (32; slower
+// than at 12).
 #ifndef PBF_SPH_DENSITY_VJP_MIN_BLOCKS
-#define PBF_SPH_DENSITY_VJP_MIN_BLOCKS 1
+#define PBF_SPH_DENSITY_VJP_MIN_BLOCKS 0
 #endif
 #ifndef PBF_SPH_DENSITY_JVP_MIN_BLOCKS
 #define PBF_SPH_DENSITY_JVP_MIN_BLOCKS 12
 #endif
 #ifndef PBF_SPH_PRESSURE_JVP_MIN_BLOCKS
 #define PBF_SPH_PRESSURE_JVP_MIN_BLOCKS 8
+#endif
+#ifndef PBF_WCSPH_FORCE_VJP_MIN_BLOCKS
+#define PBF_WCSPH_FORCE_VJP_MIN_BLOCKS 3
+#endif
+#ifndef PBF_WCSPH_FORCE_JVP_MIN_BLOCKS
+#define PBF_WCSPH_FORCE_JVP_MIN_BLOCKS 6
+#endif
+#ifndef PBF_SPH_PRESSURE_VJP_MIN_BLOCKS
+#define PBF_SPH_PRESSURE_VJP_MIN_BLOCKS 0
+#endif
+#ifndef PBF_SPH_NON_PRESSURE_VJP_MIN_BLOCKS
+#define PBF_SPH_NON_PRESSURE_VJP_MIN_BLOCKS 0
+#endif
+#ifndef PBF_SPH_NON_PRESSURE_JVP_MIN_BLOCKS
+#define PBF_SPH_NON_PRESSURE_JVP_MIN_BLOCKS 8
 #endif
 
 namespace pbf {
@@ -299,7 +316,7 @@ struct ForceVjpOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-__global__ void __launch_bounds__(kBlock) wcsph_force_vjp_kernel(const ForceVjpArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_WCSPH_FORCE_VJP_MIN_BLOCKS) wcsph_force_vjp_kernel(const ForceVjpArgs a) {
     const SphStep& st = a.st;
     const Own o = own(st);
     if (!o.p.active) return;
@@ -585,7 +602,7 @@ struct PressureVjpOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-__global__ void __launch_bounds__(kBlock) pressure_vjp_kernel(const PressureVjpArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_SPH_PRESSURE_VJP_MIN_BLOCKS) pressure_vjp_kernel(const PressureVjpArgs a) {
     const SphStep& st = a.st;
     const Own o = own(st);
     if (!o.p.active) return;
@@ -715,7 +732,7 @@ struct NonPressureVjpOp {
     __device__ __forceinline__ void process(const uint32_t t) { apply(t, prefetch(t)); }
 };
 
-__global__ void __launch_bounds__(kBlock) non_pressure_vjp_kernel(const NonPressureVjpArgs a) {
+__global__ void __launch_bounds__(kBlock, PBF_SPH_NON_PRESSURE_VJP_MIN_BLOCKS) non_pressure_vjp_kernel(const NonPressureVjpArgs a) {
     const SphStep& st = a.st;
     const Own o = own(st);
     if (!o.p.active) return;
@@ -1087,7 +1104,7 @@ __device__ __forceinline__ void predict_tangent(const f3 x, const f3 v, const f3
     out_v = tv;
 }
 
-__global__ void __launch_bounds__(kBlock) wcsph_force_jvp_kernel(const SphTangentStep t, const float* pressure,
+__global__ void __launch_bounds__(kBlock, PBF_WCSPH_FORCE_JVP_MIN_BLOCKS) wcsph_force_jvp_kernel(const SphTangentStep t, const float* pressure,
                                                                  const float4* total, const Field3 control_tangent,
                                                                  const MutField3 out_x, const MutField3 out_v) {
     const SphStep& st = t.st;
@@ -1200,7 +1217,7 @@ struct NonPressureJvpOp {
     }
 };
 
-__global__ void __launch_bounds__(kBlock) non_pressure_jvp_kernel(const SphTangentStep t, const Field3 control_tangent,
+__global__ void __launch_bounds__(kBlock, PBF_SPH_NON_PRESSURE_JVP_MIN_BLOCKS) non_pressure_jvp_kernel(const SphTangentStep t, const Field3 control_tangent,
                                                                   const int mode, const MutField3 out_x, const MutField3 out_v) {
     const SphStep& st = t.st;
     const Own o = own(st);
