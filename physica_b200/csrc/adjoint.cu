@@ -212,9 +212,9 @@ struct XsphVjpOp {
 
 // Resident 128-thread blocks per SM the register budgets of the post-loop reverse passes and of
 // the density VJP are sized for (compile-time tuning knobs; 0 leaves the register count to the
-// compiler).  Measured and not kept: the post-loop passes at 6 (80 registers) took the 32-scene
-// batched rollout from 34.6 to 35.3 grad-steps/s but the 64k rollout from 724 to 721; the density
-// VJP at 10 (48) 34.9 and 720.
+// compiler).  Measured (64k rollout / 32-scene batched rollout, grad-steps/s): the compiler's
+// registers 721 / 35.2; a one-block minimum 724 / 34.6; the post-loop passes at 6 (80 registers)
+// 721 / 35.3; the density VJP at 10 (48) 720 / 34.9.
 #ifndef PBF_POST_VJP_MIN_BLOCKS
 #define PBF_POST_VJP_MIN_BLOCKS 0
 #endif

@@ -176,7 +176,8 @@ struct DensityLambdaJvpOp {
 
 // Resident 128-thread blocks per SM the register budget of the tangent's list-replay passes is
 // sized for (a compile-time tuning knob; 0 leaves the register count to the compiler).  At 1M
-// particles the tangent step took 8.47 ms unbounded, 8.53 at 9 (56 registers), 9.78 at 10 (48).
+// particles the tangent step took 8.46 ms with the compiler's registers (61-72), 8.47 at a
+// one-block minimum (62-88), 8.53 at 9 (56 registers) and 9.78 at 10 (48).
 #ifndef PBF_JVP_MIN_BLOCKS
 #define PBF_JVP_MIN_BLOCKS 0
 #endif
