@@ -222,7 +222,8 @@ struct XsphVjpOp {
 #define PBF_DENSITY_VJP_MIN_BLOCKS 0
 #endif
 __global__ void __launch_bounds__(kBlock, PBF_POST_VJP_MIN_BLOCKS) xsph_vjp_kernel(const XsphVjpArgs a) {
-    const Particle p = locate(a.g);
+    uint32_t half;
+    const Particle p = locate_pair(a.g, half);
     XsphVjpOp op;
     op.pos = a.pos;
     op.confined = a.confined;
@@ -236,10 +237,13 @@ __global__ void __launch_bounds__(kBlock, PBF_POST_VJP_MIN_BLOCKS) xsph_vjp_kern
     op.ob = p.active ? ld3(a.output_velocity[p.s]) : d3{0, 0, 0};
     op.viscosity = pa.z;
     op.pc = {0.0, 0.0, 0.0};
-    op.vc = op.ob;
+    op.vc = {0.0, 0.0, 0.0};
     op.cc = 0.0;
-    replay(op, p, a.g, a.list);
-    if (!p.active) return;
+    replay_pair(op, p, a.g, a.list, half);
+    op.pc = pair_sum(op.pc);
+    op.vc = op.ob + pair_sum(op.vc);
+    op.cc = pair_sum(op.cc);
+    if (!p.active || half) return;
     const uint32_t i = a.sorted_index[p.s];
     a.x[p.s] = st3(ld3(a.x[p.s]) + op.pc);
     add_to(a.pa.xsph, i, op.cc);
@@ -302,7 +306,8 @@ struct NormalVjpOp {
 };
 
 __global__ void __launch_bounds__(kBlock, PBF_POST_VJP_MIN_BLOCKS) normal_vjp_kernel(const NormalVjpArgs a) {
-    const Particle p = locate(a.g);
+    uint32_t half;
+    const Particle p = locate_pair(a.g, half);
     NormalVjpOp op;
     op.pos = a.pos;
     op.vorticity = a.vorticity;
@@ -315,8 +320,10 @@ __global__ void __launch_bounds__(kBlock, PBF_POST_VJP_MIN_BLOCKS) normal_vjp_ke
     op.eb = p.active ? ld3(a.eta[p.s]) : d3{0, 0, 0};
     op.pc = {0.0, 0.0, 0.0};
     op.mc = 0.0;
-    replay(op, p, a.g, a.list);
-    if (!p.active) return;
+    replay_pair(op, p, a.g, a.list, half);
+    op.pc = pair_sum(op.pc);
+    op.mc = pair_sum(op.mc);
+    if (!p.active || half) return;
     a.x[p.s] = st3(ld3(a.x[p.s]) + op.pc);
     if (wi.w > 0.0F) a.vorticity_adjoint[p.s] = st3(ld3(a.vorticity_adjoint[p.s]) + times(xyz(wi), op.mc / wi.w));
 }
@@ -367,7 +374,8 @@ struct VorticityVjpOp {
 };
 
 __global__ void __launch_bounds__(kBlock, PBF_POST_VJP_MIN_BLOCKS) vorticity_vjp_kernel(const VorticityVjpArgs a) {
-    const Particle p = locate(a.g);
+    uint32_t half;
+    const Particle p = locate_pair(a.g, half);
     VorticityVjpOp op;
     op.pos = a.pos;
     op.velocity = a.velocity;
@@ -379,8 +387,10 @@ __global__ void __launch_bounds__(kBlock, PBF_POST_VJP_MIN_BLOCKS) vorticity_vjp
     op.wb = p.active ? ld3(a.vorticity_adjoint[p.s]) : d3{0, 0, 0};
     op.pc = {0.0, 0.0, 0.0};
     op.vc = {0.0, 0.0, 0.0};
-    replay(op, p, a.g, a.list);
-    if (!p.active) return;
+    replay_pair(op, p, a.g, a.list, half);
+    op.pc = pair_sum(op.pc);
+    op.vc = pair_sum(op.vc);
+    if (!p.active || half) return;
     const uint32_t i = a.sorted_index[p.s];
     d3 xb = ld3(a.x[p.s]) + op.pc;
     const d3 vr = ld3(a.velocity_adjoint[p.s]) + op.vc;
@@ -527,7 +537,8 @@ struct CorrectionVjpOp {
 #define PBF_CORRECTION_VJP_MIN_BLOCKS 4
 #endif
 __global__ void __launch_bounds__(kBlock, PBF_CORRECTION_VJP_MIN_BLOCKS) correction_vjp_kernel(const CorrectionVjpArgs a) {
-    const Particle p = locate(a.g);
+    uint32_t half;
+    const Particle p = locate_pair(a.g, half);
     CorrectionVjpOp op;
     op.pos = a.pos;
     op.boundary = a.g.boundary;
@@ -553,8 +564,15 @@ __global__ void __launch_bounds__(kBlock, PBF_CORRECTION_VJP_MIN_BLOCKS) correct
     op.ob = p.active ? ld3(a.correction[p.s]) : d3{0, 0, 0};
     op.pc = {0.0, 0.0, 0.0};
     op.lc = op.mc = op.rc = op.sc = op.ec = op.qc = 0.0;
-    replay(op, p, a.g, a.list);
-    if (!p.active) return;
+    replay_pair(op, p, a.g, a.list, half);
+    op.pc = pair_sum(op.pc);
+    op.lc = pair_sum(op.lc);
+    op.mc = pair_sum(op.mc);
+    op.rc = pair_sum(op.rc);
+    op.sc = pair_sum(op.sc);
+    op.ec = pair_sum(op.ec);
+    op.qc = pair_sum(op.qc);
+    if (!p.active || half) return;
     const uint32_t i = a.sorted_index[p.s];
     a.x[p.s] = st3(ld3(a.x[p.s]) + op.pc);
     const double lb = 0.0 + op.lc;
@@ -740,7 +758,8 @@ struct DensityVjpOp {
 };
 
 __global__ void __launch_bounds__(kBlock, PBF_DENSITY_VJP_MIN_BLOCKS) density_vjp_kernel(const DensityVjpArgs a) {
-    const Particle p = locate(a.g);
+    uint32_t half;
+    const Particle p = locate_pair(a.g, half);
     DensityVjpOp op;
     op.pos = a.pos;
     op.boundary = a.g.boundary;
@@ -754,8 +773,11 @@ __global__ void __launch_bounds__(kBlock, PBF_DENSITY_VJP_MIN_BLOCKS) density_vj
     op.pc = {0.0, 0.0, 0.0};
     op.mc = 0.0;
     op.rc = 0.0;
-    replay(op, p, a.g, a.list);
-    if (!p.active) return;
+    replay_pair(op, p, a.g, a.list, half);
+    op.pc = pair_sum(op.pc);
+    op.mc = pair_sum(op.mc);
+    op.rc = pair_sum(op.rc);
+    if (!p.active || half) return;
     const uint32_t i = a.sorted_index[p.s];
     const d3 xb = ld3(a.x[p.s]) + op.pc;
     add_to(a.pa.masses, i, op.mc);
@@ -911,6 +933,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
                          control_adjoint->external_accelerations.z};
     const float4* xK = r.iterate(K, K, true);
     const unsigned blocks = grid_of(n, kBlock);
+    const unsigned pair_blocks = grid_of(2u * n, kBlock);   // the passes with two lanes per particle
     const bool keep = r.keeps_all(true);
     // A checkpoint-recompute record keeps one list: the post-loop list.
     const StoredList post_list{r.list_entries[keep ? K : 0u], r.list_counts[keep ? K : 0u], r.list_capacity};
@@ -924,16 +947,16 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
     XsphVjpArgs xa{gc, post_list, r.sorted_index, xK, r.confined, r.vorticity, r.normal, ws->output_velocity, ws->x[0], ws->velocity,
                    ws->vorticity, ws->eta, pa};
     timer_.begin(stream_, kPassXsphVjp);
-    xsph_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(xa);
+    xsph_vjp_kernel<<<pair_blocks, kBlock, 0, stream_>>>(xa);
     timer_.end(stream_, kPassXsphVjp);
     NormalVjpArgs na{gc_reverse, post_list, xK, r.vorticity, ws->eta, ws->x[0], ws->vorticity};
     timer_.begin(stream_, kPassNormalVjp);
-    normal_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(na);
+    normal_vjp_kernel<<<pair_blocks, kBlock, 0, stream_>>>(na);
     timer_.end(stream_, kPassNormalVjp);
     Tail tail{K ? r.mask[K - 1] : nullptr, ws->x[1], ws->correction, prev_x, prev_v, ctrl};
     VorticityVjpArgs va{gc, post_list, r.sorted_index, xK, r.velocity, ws->vorticity, ws->x[0], ws->velocity, tail};
     timer_.begin(stream_, kPassVorticityVjp);
-    vorticity_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(va);
+    vorticity_vjp_kernel<<<pair_blocks, kBlock, 0, stream_>>>(va);
     timer_.end(stream_, kPassVorticityVjp);
     count_launch(4);
     // Checkpoint recomputation (pbf/pbf.cpp:232-245): before the iterations of a segment between two
@@ -968,7 +991,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
         CorrectionVjpArgs ca{gc, it_list, r.sorted_index, xk, ws->s_corr, ws->reverse, lambda_k, ws->correction, acc,
                              ws->lambda, pa, density_k, gsum_k, ws->constraint_weight, ws->gradient_sum_rest};
         timer_.begin(stream_, kPassCorrectionVjp);
-        correction_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(ca);
+        correction_vjp_kernel<<<pair_blocks, kBlock, 0, stream_>>>(ca);
         timer_.end(stream_, kPassCorrectionVjp);
         LambdaVjpArgs la{gc_reverse, it_list, r.sorted_index, xk, density_k, gsum_k, ws->lambda, ws->constraint_weight,
                          ws->gradient_sum_rest, acc, ws->density, pa};
@@ -978,7 +1001,7 @@ int Engine::reverse(const pbf_particle_state* state, const pbf_control* control,
         Tail t{k ? r.mask[k - 1] : nullptr, other, ws->correction, prev_x, prev_v, ctrl};
         DensityVjpArgs da{gc, it_list, r.sorted_index, xk, ws->density, acc, pa, t};
         timer_.begin(stream_, kPassDensityVjp);
-        density_vjp_kernel<<<blocks, kBlock, 0, stream_>>>(da);
+        density_vjp_kernel<<<pair_blocks, kBlock, 0, stream_>>>(da);
         timer_.end(stream_, kPassDensityVjp);
         count_launch(3);
     }

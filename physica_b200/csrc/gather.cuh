@@ -151,6 +151,73 @@ __device__ __forceinline__ void replay(Op& op, const Particle& p, const GatherCo
     }
 }
 
+// Two lanes per particle (the FP64 reverse passes, whose sums carry a tolerance rather than the
+// forward's bit-exact order).  Threads 2q and 2q + 1 of the grid share particle q; lane `half` (0 or
+// 1) takes the list entries half, half + 2, ... (or every other candidate of the stencil walk), and
+// pair_sum() then adds the two partial sums, giving both lanes the same total.  A particle's
+// result depends only on its own list, never on which particles share its warp.
+__device__ __forceinline__ Particle locate_pair(const GatherCommon& g, uint32_t& half) {
+    Particle p;
+    const uint32_t block = g.reverse ? gridDim.x - 1u - blockIdx.x : blockIdx.x;
+    const uint32_t thread = block * blockDim.x + threadIdx.x;
+    half = thread & 1u;
+    p.s = thread >> 1;
+    p.active = p.s < g.count;
+    p.c = p.active ? g.cell[p.s] : make_int4(0, 0, 0, 0);
+    p.scene = g.scenes + p.c.w;
+    p.k = g.constants[p.scene->constants];
+    return p;
+}
+
+// walk() with the candidates dealt alternately to the two lanes of a particle.
+template <class Op>
+struct Alternate {
+    static constexpr bool kBoundary = takes_boundary<Op>::value;
+    Op& op;
+    uint32_t turn;
+    __device__ __forceinline__ void process(const uint32_t t) {
+        if ((turn & 1u) == 0u) op.process(t);
+        ++turn;
+    }
+};
+
+template <class Op>
+__device__ void walk_pair(Op& op, const Particle& p, const GatherCommon& g, const uint32_t half) {
+    Alternate<Op> alternate{op, half};
+    walk(alternate, p, g);
+}
+
+// replay() over this lane's half of the list: entries half, half + 2, ...
+template <class Op>
+__device__ __forceinline__ void replay_pair(Op& op, const Particle& p, const GatherCommon& g, const StoredList& list,
+                                            const uint32_t half) {
+    if (!p.active) return;
+    const uint32_t n = list.counts[p.s];
+    if (n == kOverflow) {
+        walk_pair(op, p, g, half);
+        return;
+    }
+    if (half >= n) return;
+    const uint32_t* __restrict__ entries = list.entries + list_row(p.s, list.capacity);
+    uint32_t t = entries[static_cast<size_t>(half) * 32u];
+    uint32_t k = half + 2u;
+    uint32_t tn = k < n ? entries[static_cast<size_t>(k) * 32u] : 0u;
+    auto data = op.prefetch(t);
+    for (; k < n; k += 2u) {
+        const uint32_t tnn = k + 2u < n ? entries[static_cast<size_t>(k + 2u) * 32u] : 0u;
+        const auto next = op.prefetch(tn);
+        op.apply(t, data);
+        t = tn;
+        tn = tnn;
+        data = next;
+    }
+    op.apply(t, data);
+}
+
+// The sum of a value over the two lanes of a particle (every lane of the warp must call it).
+__device__ __forceinline__ double pair_sum(const double v) { return v + __shfl_xor_sync(kFull, v, 1); }
+__device__ __forceinline__ d3 pair_sum(const d3 v) { return {pair_sum(v.x), pair_sum(v.y), pair_sum(v.z)}; }
+
 // Hit-mask lists: pair j of particle s is one 8-byte word of its warp's interleaved row.
 __device__ __forceinline__ size_t mask_row(const uint32_t s, const uint32_t capacity_pairs) {
     return (static_cast<size_t>(s >> 5) * capacity_pairs) * 32u + (s & 31u);
