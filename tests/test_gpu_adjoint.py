@@ -43,15 +43,11 @@ def _scene(lattice=(10, 10, 10), seed=12):
     return scenes.dam_break(lattice, (0, 0, 0), (1, 2, 1), seed, 4, velocity_sigma=0.1)
 
 
-def test_vjp_matches_reference_vjp():
-    """The adjoint of one substep equals the reference's vjp_step to FP64 rounding."""
+def reference_vjp(sc, nxa, nva):
+    """The reference's forward_step and vjp_step (its own kernels) on the same scene and adjoints."""
     from oracle import reference
     if not reference.available():
         pytest.skip("reference kernels (oracle/_ref) not built")
-    sc = _scene()
-    rng = np.random.default_rng(5)
-    nxa, nva = rng.normal(size=(3, sc.count)), rng.normal(size=(3, sc.count))
-    mine = my_vjp(sc, nxa, nva)
     ref = reference.ReferencePBF(sc, checkpoint_interval=2, differentiable=True)
     x = torch.from_numpy(sc.positions).cuda().contiguous()
     v = torch.from_numpy(sc.velocities).cuda().contiguous()
@@ -63,10 +59,39 @@ def test_vjp_matches_reference_vjp():
     pa = {k: torch.zeros(sc.count, dtype=torch.float64, device="cuda") for k in NAMES}
     ref.vjp_step(x, v, {"positions": torch.from_numpy(nxa).cuda(), "velocities": torch.from_numpy(nva).cuda()},
                  prev, ctrl, pa)
-    theirs = {"position": prev["positions"].cpu().numpy(), "velocity": prev["velocities"].cpu().numpy(),
-              "control": ctrl.cpu().numpy(), **{k: pa[k].cpu().numpy() for k in NAMES}}
-    for k in ("position", "velocity", "control", "masses", "rest_densities", "relaxation",
-              "artificial_pressure_strength", "xsph_viscosity", "vorticity_confinement"):
+    return {"position": prev["positions"].cpu().numpy(), "velocity": prev["velocities"].cpu().numpy(),
+            "control": ctrl.cpu().numpy(), **{k: pa[k].cpu().numpy() for k in NAMES}}
+
+
+COMPARED = ("position", "velocity", "control", "masses", "rest_densities", "relaxation", "artificial_pressure_strength",
+            "xsph_viscosity", "vorticity_confinement")
+
+
+def test_vjp_matches_reference_vjp():
+    """The adjoint of one substep equals the reference's vjp_step to FP64 rounding."""
+    sc = _scene()
+    rng = np.random.default_rng(5)
+    nxa, nva = rng.normal(size=(3, sc.count)), rng.normal(size=(3, sc.count))
+    mine = my_vjp(sc, nxa, nva)
+    theirs = reference_vjp(sc, nxa, nva)
+    for k in COMPARED:
+        assert rel(mine[k], theirs[k]) < 1e-9, (k, rel(mine[k], theirs[k]))
+
+
+def test_vjp_of_overflowing_lists_matches_reference_vjp():
+    """125 particles packed into a 0.02 m cube: every particle has more neighbours than its stored
+    list holds, so each pass walks its stencil (in the reverse passes split between two lanes); the
+    adjoint still equals the reference's vjp_step to FP64 rounding."""
+    sc = scenes.dam_break((5, 5, 5), (0, 0, 0), (1, 2, 1), 68, 3, velocity_sigma=0.1)
+    rng = np.random.default_rng(13)
+    sc.positions[:] = (np.array([[0.5], [0.3], [0.5]]) + rng.uniform(0, 0.02, sc.positions.shape)).astype(np.float32)
+    p = sc.positions.T.astype(np.float64)
+    in_support = (np.sqrt(((p[:, None, :] - p[None, :, :]) ** 2).sum(-1)) < sc.support_radius).sum(1)
+    assert in_support.min() > 96   # more than a stored list holds
+    nxa, nva = rng.normal(size=(3, sc.count)), rng.normal(size=(3, sc.count))
+    mine = my_vjp(sc, nxa, nva)
+    theirs = reference_vjp(sc, nxa, nva)
+    for k in COMPARED:
         assert rel(mine[k], theirs[k]) < 1e-9, (k, rel(mine[k], theirs[k]))
 
 
